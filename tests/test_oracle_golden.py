@@ -1,0 +1,58 @@
+"""Pin the FP64 oracle against golden vectors produced by the reference's own
+code (``pymdp/algos.py::run_factorized_fpi``, ``pymdp/control.py::
+update_posterior_policies``; see ``tests/golden/make_golden.py``)."""
+
+import numpy as np
+import pytest
+
+from conftest import deps_from, load_golden, unpack
+from oracle import efe as oefe
+from oracle import fpi as ofpi
+
+FPI = ["fpi_plain", "fpi_single_factor", "fpi_rank123", "fpi_rank4", "fpi_orphan_factor",
+       "fpi_cfg2", "fpi_large"]
+EFE = ["efe_plain", "efe_mixed", "efe_bdeps", "efe_cfg3_t1", "efe_cfg3_small"]
+
+
+@pytest.mark.parametrize("name", FPI)
+def test_fpi_oracle_matches_reference(name):
+    d = load_golden(name)
+    deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    A = unpack(d, "A")
+    prior = [p.astype(np.float64) for p in unpack(d, "prior")]
+    qs_ref = unpack(d, "qs")
+    qs = ofpi.run_fpi_batch([a.astype(np.float64) for a in A], d["obs"], prior, deps, int(d["num_iter"]))
+    for f in range(len(qs)):
+        np.testing.assert_allclose(qs[f], qs_ref[f], rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", FPI)
+def test_fpi_oracle_from_ll_matches_reference(name):
+    d = load_golden(name)
+    deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    ll = unpack(d, "ll")
+    prior = unpack(d, "prior")
+    qs_ref = unpack(d, "qs")
+    for b in range(d["obs"].shape[0]):
+        if len(prior) == 1:
+            continue  # reference takes the one-pass branch before the FFI call
+        qs = ofpi.fpi_from_ll([l[b] for l in ll], [ofpi.log_stable(p[b]) for p in prior], deps,
+                              int(d["num_iter"]))
+        for f in range(len(qs)):
+            np.testing.assert_allclose(qs[f], qs_ref[f][b], rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", EFE)
+def test_efe_oracle_matches_reference(name):
+    d = load_golden(name)
+    A_deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    B_deps = deps_from(d["B_dep_flat"], d["B_dep_offsets"])
+    S, U, T = d["S"].tolist(), d["U"].tolist(), int(d["T"])
+    pol = oefe.construct_policies(S, U, T)
+    np.testing.assert_array_equal(pol, d["policies"])
+    q_pi, G = oefe.update_posterior_policies(pol, unpack(d, "qs"), unpack(d, "A"), unpack(d, "B"),
+                                             unpack(d, "C"), d["E"], A_deps, B_deps,
+                                             gamma=float(d["gamma"]))
+    np.testing.assert_allclose(G, d["G"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(q_pi, d["q_pi"], rtol=1e-10, atol=1e-300)
+    np.testing.assert_array_equal(oefe.sample_policy(pol, q_pi), d["action"])
