@@ -1,0 +1,332 @@
+"""Benchmark: agent-steps/s of the FPI + EFE agent step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one "step" = one agent step for every agent of the batch):
+the EFE benchmark model — 256 agents, num_states [32, 16, 8],
+num_controls [4, 4, 1], policy_len 3 (4096 policies), 5 modalities with
+num_obs [16, 16, 8, 8, 4] depending on all factors, A ~ Dirichlet(0.5),
+B ~ Dirichlet(0.5) per action slice, C ~ N(0, 1), E uniform, gamma 16 —
+running infer_states (fused FPI, 16 iterations, one-hot observations) ->
+infer_policies (neg-EFE of all policies + q_pi) -> sample_action
+(deterministic). Synthetic seeded inputs with those shapes/distributions.
+
+* ``value``: device time (CUDA events, max over ranks) with every input
+  resident in HBM; L2 is flushed (a 256 MiB write) between timed steps,
+  outside the per-step event pairs.
+* ``e2e``: the same step through the public ``Agent`` API with host
+  buffers: pinned observations + priors copied in, actions copied out,
+  inside the timed region.
+* ``roofline``: the dominant kernel (neg-EFE), its algorithmic FLOPs
+  2*T*P*sum_m(O_m*K_m) per agent over its measured launch time.
+* ``cpu_baseline``: the FP64 oracle on the host cores for a bounded sample.
+
+Multi-GPU: agents are independent, so each rank runs its own 256 agents
+(weak scaling, no data-path collective); the only collective is the
+max-over-ranks of the timing.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+S = [32, 16, 8]
+O = [16, 16, 8, 8, 4]
+U = [4, 4, 1]
+T = 3
+AGENTS = 256
+NUM_ITER = 16
+GAMMA = 16.0
+WORKLOAD = "agent step (FPI 16 iters + EFE all 4096 policies + action), 256 agents, S=[32,16,8], " \
+           "O=[16,16,8,8,4], U=[4,4,1], policy_len=3"
+
+
+def make_model(seed: int, agents: int):
+    rng = np.random.default_rng(seed)
+
+    def dirc(shape, alpha):
+        g = rng.gamma(alpha, size=shape) + 1e-30
+        return (g / g.sum(1, keepdims=True)).astype(np.float32)
+
+    F, M = len(S), len(O)
+    A = [dirc((agents, O[m]) + tuple(S), 0.5) for m in range(M)]
+    B = [dirc((agents, S[f], S[f], U[f]), 0.5) for f in range(F)]
+    C = [rng.normal(size=(agents, o)).astype(np.float32) for o in O]
+    D = [dirc((agents, s), 1.0) for s in S]
+    obs = rng.integers(0, np.array(O), size=(agents, M)).astype(np.int32)
+    return A, B, C, D, obs
+
+
+def efe_flops_per_agent() -> float:
+    K = int(np.prod(S))
+    P = int(np.prod(U)) ** T
+    return 2.0 * T * P * sum(o * K for o in O)
+
+
+def fpi_bytes_per_agent() -> float:
+    K = int(np.prod(S))
+    return 4.0 * len(O) * K + 8.0 * sum(S) + 4.0 * len(O)
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.rows, self._stop = index, [], threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:  # noqa: BLE001
+                return
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if "Active" in r[2 + i]
+                          and "Not" not in r[2 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline_run(agents: int, seed: int = 0):
+    """FP64 oracle agent steps on the host (bounded sample): (agent-steps/s, sample)."""
+    from oracle import efe as oefe
+    from oracle import fpi as ofpi
+
+    A, B, C, D, obs = make_model(seed, agents)
+    F, M = len(S), len(O)
+    A_deps = [list(range(F))] * M
+    B_deps = [[f] for f in range(F)]
+    pol = oefe.construct_policies(S, U, T)
+    E = np.full(len(pol), 1.0 / len(pol))
+    t0 = time.perf_counter()
+    for b in range(agents):
+        o_vec = [np.eye(O[m])[obs[b, m]] for m in range(M)]
+        qs = ofpi.run_factorized_fpi([a[b].astype(np.float64) for a in A], o_vec, [d[b] for d in D], A_deps,
+                                     NUM_ITER)
+        q_pi, _ = oefe.update_posterior_policies(pol, qs, [a[b] for a in A], [x[b] for x in B],
+                                                 [c[b] for c in C], E, A_deps, B_deps, gamma=GAMMA)
+        oefe.sample_policy(pol, q_pi)
+    dt = time.perf_counter() - t0
+    return agents / dt, dt
+
+
+def threads_used() -> int:
+    try:
+        from threadpoolctl import threadpool_info
+
+        return max([i.get("num_threads", 1) for i in threadpool_info()] or [1])
+    except Exception:  # noqa: BLE001
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    per_step = 1  # one agent's full FPI + EFE step per timed step (bounded sample)
+    for _ in range(args.warmup):
+        cpu_baseline_run(per_step, seed=1)
+    times = []
+    for i in range(args.steps):
+        _, dt = cpu_baseline_run(per_step, seed=2 + i)
+        times.append(dt)
+    total = sum(times)
+    value = args.steps * per_step / total
+    line = {
+        "impl": "reference", "metric": "agent-steps/s", "value": value, "unit": "agent-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "agents_per_step": per_step},
+        "cpu_baseline": {"value": value, "unit": "agent-steps/s", "cores": threads_used(), "kind": "port",
+                         "sample": f"{per_step} agent per step of the same model (FP64 NumPy oracle: FPI + "
+                                   f"EFE over 4096 policies + q_pi + action)"},
+        "e2e": {"value": value, "unit": "agent-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from pymdp_b200 import Agent, _lib, ffi
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    A, B, C, D, obs = make_model(1234 + rank, AGENTS)
+    agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=AGENTS, num_iter=NUM_ITER, device=dev)
+    obs_d = torch.as_tensor(obs, device=dev)
+    prior_d = [torch.as_tensor(d, device=dev) for d in D]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    efe_ev = []
+
+    def step(timed_efe=False):
+        qs = agent.infer_states(obs_d, prior_d)
+        if timed_efe:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        q_pi, G = agent.infer_policies(qs)
+        if timed_efe:
+            e1.record(stream)
+            efe_ev.append((e0, e1))
+        return agent.sample_action(q_pi)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    evs = []
+    n0 = _lib.launch_count()
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(timed_efe=True)
+            e1.record(stream)
+            evs.append((e0, e1))
+        barrier()
+    launches = _lib.launch_count() - n0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    efe_ms = sum(a.elapsed_time(b) for a, b in efe_ev) / len(efe_ev)
+    # e2e through the public API with host buffers
+    obs_h = torch.as_tensor(obs).pin_memory()
+    prior_h = [torch.as_tensor(d).pin_memory() for d in D]
+    act_h = torch.empty((AGENTS, len(S)), dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        o = obs_h.to(dev, non_blocking=True)
+        p = [x.to(dev, non_blocking=True) for x in prior_h]
+        qs = agent.infer_states(o, p)
+        q_pi, _ = agent.infer_policies(qs)
+        act_h.copy_(agent.sample_action(q_pi), non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    ev1.record(stream)
+    barrier()
+    e2e_ms = ev0.elapsed_time(ev1)
+    h2d = obs_h.numel() * 4 + sum(x.numel() * 4 for x in prior_h)
+    d2h = act_h.numel() * 4
+    t = torch.tensor([ms, e2e_ms, efe_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms, efe_ms = [float(x) for x in t.tolist()]
+    if rank != 0:
+        return
+    import json as _json
+    peaks = {}
+    try:
+        peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:  # noqa: BLE001
+        pass
+    peak_tf = peaks.get("bf16_tflops", 1590.0)
+    flops = efe_flops_per_agent() * AGENTS
+    achieved_tf = flops / (efe_ms * 1e-3) / 1e12
+    total_agents = AGENTS * world
+    value = total_agents * args.steps / (ms * 1e-3)
+    sample = 2 if args.cpu_sample is None else args.cpu_sample
+    cpu_val, cpu_dt = cpu_baseline_run(sample, seed=7) if (world == 1 and sample > 0) else (None, None)
+    line = {
+        "metric": "agent-steps/s", "value": value, "unit": "agent-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "agents_per_gpu": AGENTS, "fpi_iters": NUM_ITER, "policies": 4096,
+                   "precision": agent.precision, "l2": "flushed (256 MiB write) between timed steps",
+                   "parallelism": f"agents sharded over {world} GPU(s), no collective"},
+        "e2e": {"value": total_agents * args.steps / (e2e_ms * 1e-3), "unit": "agent-steps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": achieved_tf / peak_tf, "traffic": None,
+                     "kernel": "neg-EFE (linear rows + policy evaluation), per launch over 256 agents",
+                     "flops_per_launch": flops, "ms_per_launch": efe_ms,
+                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"},
+        "cpu_baseline": None if cpu_val is None else {
+            "value": cpu_val, "unit": "agent-steps/s", "cores": threads_used(), "kind": "port",
+            "sample": f"{sample} agents of the same model, full agent step, FP64 NumPy oracle ({cpu_dt:.1f} s)"},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

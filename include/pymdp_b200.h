@@ -1,0 +1,157 @@
+/*
+ * pymdp_b200 — C-ABI of the B200-native (sm_100a) FPI and EFE hot paths.
+ *
+ * Every entry point takes plain pointers and sizes (no framework types), runs
+ * on the caller's CUDA stream, never synchronises the stream and never copies
+ * to the host, and returns an int32 status (0 = success). On failure the
+ * thread-local message from b2_last_error() names the entry point and the
+ * offending argument, in the style of the reference's
+ * `ffi::Error(kInvalidArgument, "fpi_ffi: ...")` (pymdp/ffi/common/error_helpers.h:24-49).
+ *
+ * Device pointers must be CUDA device (or managed) memory on the current
+ * device. Unless stated otherwise, float buffers are float32, integer buffers
+ * int32, attribute arrays (shapes, offsets, dependency lists) are HOST int64
+ * arrays, exactly like the reference's XLA FFI attributes.
+ */
+#ifndef PYMDP_B200_H_
+#define PYMDP_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+  B2_OK = 0,
+  B2_ERR_INVALID_ARGUMENT = 1, /* shape / offset / dependency inconsistency   */
+  B2_ERR_UNSUPPORTED = 2,      /* valid input outside this build's limits     */
+  B2_ERR_CUDA = 3,             /* CUDA runtime error (launch, allocation ...) */
+  B2_ERR_NO_DEVICE = 4         /* no sm_100 device / kernel image unavailable */
+};
+
+/* Limits of this build. Rank cap matches the reference's
+ * kMaxFfiDependencyRank = 8 (pymdp/ffi/common/modality_dispatch.h:25). */
+#define B2_MAX_DEP_RANK 8
+#define B2_MAX_FACTORS 16
+#define B2_MAX_MODALITIES 32
+
+/* EFE flag bits: identical values to the reference ABI
+ * (pymdp/ffi/neg_efe/neg_efe_layout.h:23-42, pymdp/ffi/_efe.py FLAG_*). */
+#define B2_FLAG_USE_UTILITY 1
+#define B2_FLAG_USE_STATES_INFO_GAIN 2
+#define B2_FLAG_USE_INDUCTIVE 4
+#define B2_FLAG_USE_PARAM_INFO_GAIN 8
+#define B2_FLAG_MODEL_PARAMS_STATIC 16
+/* Precision selector, bits 8-9 of `flags` (unused by the reference ABI). */
+#define B2_PRECISION_SHIFT 8
+#define B2_PRECISION_FP32 0  /* SIMT FP32, FP32 accumulate (default)        */
+#define B2_PRECISION_TF32X3 1 /* tcgen05 kind::tf32, hi/lo split, FP32-exact */
+#define B2_PRECISION_BF16 2  /* tcgen05 kind::f16 BF16 operands, FP32 accum  */
+
+/* Message describing the last failing call on this thread ("" if none). */
+const char* b2_last_error(void);
+/* ABI version of this library (bumped on any signature change). */
+int32_t b2_abi_version(void);
+/* Capability bits; bit 2 = CUDA, mirroring pymdp_ffi_cpu_capabilities
+ * (pymdp/ffi/registration/xla_register.cc:162-164, _core.py _CAP_CUDA). */
+int32_t b2_capabilities(void);
+/* Number of kernels this library has launched in this process (all entry
+ * points, all devices). Lets callers count launches inside a timed region. */
+uint64_t b2_launch_count(void);
+
+/* ================================================================== FPI ==
+ * Drop-in for `pymdp_fpi_cuda_native` / FpiCudaDevice
+ * (pymdp/ffi/registration/xla_register.cc:151-157, pymdp/ffi/fpi/fpi.h:30-33,
+ * Python side pymdp/ffi/_fpi.py:143-270). Same buffers and attributes:
+ *
+ *   ll_flat  [batch, ll_offsets[M]]   per-modality log-likelihoods, each
+ *                                      ll_m row-major over S[A_dep[m]]
+ *   lp_flat  [batch, lp_offsets[F]]   per-factor log priors
+ *   q_out    [batch, lp_offsets[F]]   posterior marginals (softmax of log q)
+ *
+ * Attributes S[F], ll_offsets[M+1], lp_offsets[F+1], A_dep_flat[...],
+ * A_dep_offsets[M+1], num_iter. As in the reference, the batch is inferred
+ * from the element counts (`lp_count / total_S`, fpi/fpi_entry.h:55-66) and
+ * all three counts are checked. Runs exactly num_iter Jacobi iterations
+ * (the reference JAX semantics, pymdp/algos.py:121-133; no early stop). */
+int32_t b2_fpi(void* stream, const float* ll_flat, int64_t ll_count, const float* lp_flat,
+               int64_t lp_count, float* q_out, int64_t q_count, const int64_t* S, int64_t S_len,
+               const int64_t* ll_offsets, int64_t ll_offsets_len, const int64_t* lp_offsets,
+               int64_t lp_offsets_len, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+               const int64_t* A_dep_offsets, int64_t A_dep_offsets_len, int32_t num_iter);
+
+/* Fused observation form of the same update: the log-likelihood slice gather
+ * log(clip(A_m[o_m], eps)) (pymdp/maths.py:214-238 with a one-hot o_m) and
+ * the log prior log(clip(prior, eps)) (pymdp/algos.py:110) are done inside
+ * the kernel, so ll never exists in HBM.
+ *
+ *   A_flat    A_m of agent b at A_flat + b*A_agent_stride + A_offsets[m],
+ *             shape (O[m], *S[A_dep[m]]) row-major. A_agent_stride = 0
+ *             shares one A across the batch.
+ *   obs       [batch, M] int32 observation indices, 0 <= obs < O[m].
+ *             Out-of-range indices produce NaN posteriors for that agent.
+ *   prior     [batch, lp_offsets[F]] prior probabilities (not logs).
+ *   q_out     [batch, lp_offsets[F]]
+ *
+ * The reference path this replaces is Agent.infer_states ->
+ * inference.update_posterior_states -> algos.run_factorized_fpi
+ * (pymdp/agent.py:773-821, pymdp/inference.py:171-191, pymdp/algos.py:88-155). */
+int32_t b2_fpi_obs(void* stream, const float* A_flat, int64_t A_agent_stride,
+                   const int64_t* A_offsets, int64_t A_offsets_len, const int64_t* O, int64_t O_len,
+                   const int32_t* obs, const float* prior, float* q_out, int64_t batch,
+                   const int64_t* S, int64_t S_len, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                   const int64_t* A_dep_offsets, int64_t A_dep_offsets_len, int32_t num_iter);
+
+/* ================================================================== EFE ==
+ * Drop-in for `pymdp_neg_efe_cuda_dev_execute` / NegEfeCudaDev
+ * (pymdp/ffi/registration/xla_register.cc:89-96, pymdp/ffi/neg_efe/neg_efe.h:41-46,
+ * Python side pymdp/ffi/_efe.py:491-711). Same 9 inputs, 1 output and
+ * 13 int64 attribute arrays + flags:
+ *
+ *   policy_matrix int32 [P, T, F] (pm_batched = 0) or [Bn, P, T, F] (= 1)
+ *   qs_init [Bn, qs_offsets[F]], A [Bn, A_offsets[M]], B [Bn, B_offsets[F]]
+ *   (B_f flattened (S_f, *S[B_dep[f]], U_f)), C [Bn, C_offsets[M]] (C_m as
+ *   (T, O_m)), I [Bn, I_offsets[F]], pA/pB (0 elements when unused),
+ *   inductive_epsilon [1] or [Bn] (eps_batched).
+ *   neg_efe_out [Bn, P]: G = -EFE per policy (pymdp/control.py:604-690).
+ *
+ * Element counts are checked like validate_buffer_counts
+ * (neg_efe/neg_efe_layout.h:342-363). This build implements the utility and
+ * state-information-gain terms (flag bits 0 and 1); inductive (bit 2) and
+ * parameter-information-gain (bit 3) return B2_ERR_UNSUPPORTED. Bits 8-9 pick
+ * the contraction precision (B2_PRECISION_*). Out-of-range actions in
+ * policy_matrix give NaN for that policy. */
+int32_t b2_neg_efe(void* stream, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+                   const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
+                   const float* B, int64_t B_count, const float* C, int64_t C_count,
+                   const float* I, int64_t I_count, const float* pA, int64_t pA_count,
+                   const float* pB, int64_t pB_count, const float* inductive_epsilon,
+                   int64_t eps_count, float* neg_efe_out, int64_t out_count, int64_t Bn, int64_t P,
+                   int64_t T, int64_t F, int64_t M, const int64_t* S, const int64_t* O,
+                   const int64_t* U, const int64_t* qs_offsets, const int64_t* A_offsets,
+                   const int64_t* B_offsets, const int64_t* C_offsets, const int64_t* I_offsets,
+                   const int64_t* I_depths, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                   const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
+                   const int64_t* B_dep_offsets, int32_t flags);
+
+/* q_pi = softmax(gamma * neg_efe + log(clip(E, eps))) per agent — the step
+ * the reference runs in XLA right after the FFI call
+ * (pymdp/control.py:349 and :963). gamma is [Bn] (gamma_batched = 1) or a
+ * single value; E is [Bn, P] (E_batched = 1) or [P]. */
+int32_t b2_policy_posterior(void* stream, const float* neg_efe, const float* E, int32_t E_batched,
+                            const float* gamma, int32_t gamma_batched, float* q_pi, int64_t Bn,
+                            int64_t P);
+
+/* Deterministic action selection (pymdp/control.py:115-150,
+ * sampling_mode="full", action_selection="deterministic"): action[b, f] =
+ * policy_matrix[argmax_p q_pi[b, p], 0, f], the first maximum on ties.
+ * policy_matrix is [P, T, F] (shared) int32. */
+int32_t b2_select_action(void* stream, const float* q_pi, const int32_t* policy_matrix,
+                         int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYMDP_B200_H_ */

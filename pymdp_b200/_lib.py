@@ -1,0 +1,128 @@
+"""ctypes binding of ``libpymdp_b200.so`` (the C-ABI in ``include/pymdp_b200.h``).
+
+There is no fallback: if the library cannot be loaded every entry point
+raises. Mirrors the role of the reference's library loader
+(``pymdp/ffi/_core.py:41-80``), including the ``PYMDP_B200_LIB`` override
+(the reference's is ``PYMDP_FFI_LIB``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_float, c_int32, c_int64, c_uint64, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("PYMDP_B200_LIB", os.path.join(HERE, "libpymdp_b200.so"))
+
+B2_OK = 0
+B2_ERR_INVALID_ARGUMENT = 1
+B2_ERR_UNSUPPORTED = 2
+B2_ERR_CUDA = 3
+B2_ERR_NO_DEVICE = 4
+
+FLAG_USE_UTILITY = 1 << 0
+FLAG_USE_STATES_INFO_GAIN = 1 << 1
+FLAG_USE_INDUCTIVE = 1 << 2
+FLAG_USE_PARAM_INFO_GAIN = 1 << 3
+FLAG_MODEL_PARAMS_STATIC = 1 << 4
+PRECISION_SHIFT = 8
+PRECISIONS = {"fp32": 0, "tf32x3": 1, "bf16": 2}
+
+MAX_DEP_RANK = 8
+MAX_FACTORS = 16
+MAX_MODALITIES = 32
+
+
+class B2Error(RuntimeError):
+    """A failing C-ABI call; ``code`` is the B2_ERR_* status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+class UnsupportedError(B2Error, NotImplementedError):
+    pass
+
+
+class InvalidArgumentError(B2Error, ValueError):
+    pass
+
+
+_P64 = POINTER(c_int64)
+_PF = c_void_p  # device float pointers are passed as raw addresses
+_SIGS = {
+    "b2_last_error": (ctypes.c_char_p, []),
+    "b2_abi_version": (c_int32, []),
+    "b2_capabilities": (c_int32, []),
+    "b2_launch_count": (c_uint64, []),
+    "b2_fpi": (c_int32, [c_void_p, _PF, c_int64, _PF, c_int64, _PF, c_int64, _P64, c_int64, _P64, c_int64,
+                         _P64, c_int64, _P64, c_int64, _P64, c_int64, c_int32]),
+    "b2_fpi_obs": (c_int32, [c_void_p, _PF, c_int64, _P64, c_int64, _P64, c_int64, c_void_p, _PF, _PF,
+                             c_int64, _P64, c_int64, _P64, c_int64, _P64, c_int64, c_int32]),
+    "b2_neg_efe": (c_int32, [c_void_p, c_void_p, c_int64, c_int32, _PF, c_int64, _PF, c_int64, _PF, c_int64,
+                             _PF, c_int64, _PF, c_int64, _PF, c_int64, _PF, c_int64, _PF, c_int64, _PF,
+                             c_int64, c_int64, c_int64, c_int64, c_int64, c_int64, _P64, _P64, _P64, _P64,
+                             _P64, _P64, _P64, _P64, _P64, _P64, c_int64, _P64, _P64, c_int64, _P64,
+                             c_int32]),
+    "b2_policy_posterior": (c_int32, [c_void_p, _PF, _PF, c_int32, _PF, c_int32, _PF, c_int64, c_int64]),
+    "b2_select_action": (c_int32, [c_void_p, _PF, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64]),
+}
+
+_lib = None
+_load_error: Exception | None = None
+
+
+def load():
+    """Load and type the library (idempotent). Raises if unavailable."""
+    global _lib, _load_error
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"pymdp_b200 native library not found at {LIB_PATH}; "
+                           "build it with `python -m pymdp_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def is_available() -> bool:
+    """True if the native library loads (mirrors ``pymdp.ffi.is_available``)."""
+    try:
+        load()
+        return True
+    except Exception as exc:  # noqa: BLE001
+        global _load_error
+        _load_error = exc
+        return False
+
+
+def last_error() -> str:
+    return load().b2_last_error().decode()
+
+
+def check(rc: int) -> None:
+    if rc == B2_OK:
+        return
+    msg = last_error()
+    if rc == B2_ERR_INVALID_ARGUMENT:
+        raise InvalidArgumentError(rc, msg)
+    if rc == B2_ERR_UNSUPPORTED:
+        raise UnsupportedError(rc, msg)
+    raise B2Error(rc, msg)
+
+
+def i64(values) -> ctypes.Array:
+    """Host int64 attribute array (kept alive by the caller)."""
+    vals = [int(v) for v in values]
+    arr = (c_int64 * max(1, len(vals)))(*vals)
+    return arr
+
+
+def launch_count() -> int:
+    return int(load().b2_launch_count())

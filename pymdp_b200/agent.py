@@ -1,0 +1,175 @@
+"""``Agent`` — the reference's ``pymdp.agent.Agent`` surface for the FPI + EFE path.
+
+Keeps the signatures and return shapes of ``Agent.infer_states``
+(``pymdp/agent.py:675-823``), ``Agent.infer_policies`` (``:853-906``) and
+``Agent.sample_action`` (``:939-967``) for ``inference_algo="fpi"``,
+``sampling_mode="full"`` and deterministic action selection, with the
+batch-broadcasting rules of ``pymdp/agent.py:228-330`` (unbatched A/B/C/D/E
+are broadcast to ``batch_size``; defaults C = uniform 1/O, D = uniform,
+E = uniform).
+
+Model tensors are flattened ONCE into device buffers at construction (the
+reference re-flattens A/B/C on every call, ``pymdp/ffi/_efe.py:596-613``), so
+each call is a handful of kernel launches on the current stream and nothing
+else.
+"""
+
+from __future__ import annotations
+
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import ffi
+from .control import construct_policies
+
+
+def _t(x, dev) -> torch.Tensor:
+    if isinstance(x, torch.Tensor):
+        return x.to(device=dev, dtype=torch.float32)
+    return torch.as_tensor(np.asarray(x, dtype=np.float32), device=dev)
+
+
+class Agent:
+    """Batched active-inference agent whose hot paths run on sm_100a kernels."""
+
+    def __init__(self, A: Sequence, B: Sequence, C: Sequence | None = None, D: Sequence | None = None,
+                 E=None, A_dependencies: Sequence[Sequence[int]] | None = None,
+                 B_dependencies: Sequence[Sequence[int]] | None = None, num_controls=None, policy_len: int = 1,
+                 policies=None, control_fac_idx=None, gamma: float = 1.0, alpha: float = 1.0,
+                 use_utility: bool = True, use_states_info_gain: bool = True, use_param_info_gain: bool = False,
+                 use_inductive: bool = False, action_selection: str = "deterministic",
+                 sampling_mode: str = "full", inference_algo: str = "fpi", num_iter: int = 16,
+                 batch_size: int = 1, precision: str = "fp32", device="cuda"):
+        if inference_algo.lower() != "fpi":
+            raise NotImplementedError("only inference_algo='fpi' is on the accelerated path")
+        if use_param_info_gain or use_inductive:
+            raise NotImplementedError("parameter information gain / inductive terms are not built yet")
+        if action_selection != "deterministic" or sampling_mode != "full":
+            raise NotImplementedError("only deterministic action selection with sampling_mode='full'")
+        dev = torch.device(device)
+        self.device = dev
+        self.batch_size = int(batch_size)
+        self.num_iter = int(num_iter)
+        self.precision = precision
+        self.use_utility, self.use_states_info_gain = use_utility, use_states_info_gain
+        self.action_selection, self.sampling_mode = action_selection, sampling_mode
+        M, F = len(A), len(B)
+        self.num_modalities, self.num_factors = M, F
+        self.A_dependencies = [list(d) for d in (A_dependencies or [list(range(F)) for _ in range(M)])]
+        self.B_dependencies = [list(d) for d in (B_dependencies or [[f] for f in range(F)])]
+        A = [_t(a, dev) for a in A]
+        B = [_t(b, dev) for b in B]
+        # num_states from B (pymdp/agent.py:399-414: the self-dependency axis)
+        S = []
+        for f, deps in enumerate(self.B_dependencies):
+            if f not in deps:
+                raise ValueError(f"num_states cannot be inferred from B, B_dependencies if the dynamics of "
+                                 f"hidden state {f} is not conditioned on itself")
+            S.append(int(B[f].shape[-(len(deps) + 1 - deps.index(f))]))
+        self.num_states = S
+        nbat = self.batch_size
+
+        def batched(x, core_ndim, name):
+            if x.ndim == core_ndim + 1:
+                if x.shape[0] == 1 and nbat > 1:
+                    return x.expand((nbat,) + tuple(x.shape[1:]))
+                if x.shape[0] != nbat:
+                    raise ValueError(f"Batch size {nbat} does not match the first dimension of {name} with shape "
+                                     f"{tuple(x.shape)}")
+                return x
+            if x.ndim == core_ndim:
+                return x.unsqueeze(0).expand((nbat,) + tuple(x.shape))
+            raise ValueError(f"{name} has unexpected shape {tuple(x.shape)}")
+
+        # C follows A's batching (pymdp/agent.py:278-294): broadcast when A[m] was unbatched
+        A_was_batched = [a.ndim == len(self.A_dependencies[m]) + 2 for m, a in enumerate(A)]
+        A = [batched(a, len(self.A_dependencies[m]) + 1, f"A[{m}]") for m, a in enumerate(A)]
+        B = [batched(b, len(self.B_dependencies[f]) + 2, f"B[{f}]") for f, b in enumerate(B)]
+        self.num_obs = [int(a.shape[1]) for a in A]
+        self.num_controls = [int(b.shape[-1]) for b in B]
+        if control_fac_idx is None:
+            control_fac_idx = [f for f in range(F) if self.num_controls[f] > 1]
+        self.control_fac_idx = list(control_fac_idx)
+        self.policy_len = int(policy_len)
+        pol = construct_policies(S, self.num_controls, self.policy_len, self.control_fac_idx) \
+            if policies is None else np.asarray(policies, dtype=np.int32)
+        self.policies = torch.as_tensor(pol, device=dev, dtype=torch.int32).contiguous()
+        P = int(pol.shape[0])
+        if C is None:
+            C = [torch.full((nbat, o), 1.0 / o, device=dev) for o in self.num_obs]
+        else:
+            C = [_t(c, dev) for c in C]
+            C = [c if A_was_batched[m] and c.shape[0] == nbat else
+                 (c.expand((nbat,) + tuple(c.shape[1:])) if A_was_batched[m] else
+                  c.unsqueeze(0).expand((nbat,) + tuple(c.shape)))
+                 for m, c in enumerate(C)]
+        if D is None:
+            D = [torch.full((nbat, s), 1.0 / s, device=dev) for s in S]
+        else:
+            D = [batched(_t(d, dev), 1, f"D[{f}]") for f, d in enumerate(D)]
+        if E is None:
+            E = torch.full((nbat, P), 1.0 / P, device=dev)
+        else:
+            E = batched(_t(E, dev), 1, "E")
+        self.D = [d.contiguous() for d in D]
+        self.E = E.contiguous()
+        self.gamma = _t(np.broadcast_to(np.asarray(gamma, np.float32), (nbat,)).copy(), dev)
+        self.alpha = _t(np.broadcast_to(np.asarray(alpha, np.float32), (nbat,)).copy(), dev)
+        # one-time flattening into the kernels' layouts
+        self._A_flat, self._A_offsets = ffi.flatten_ragged_f32(A, 1, dev)
+        self._B_flat, _ = ffi.flatten_ragged_f32(B, 1, dev)
+        C_t = []
+        for m, c in enumerate(C):
+            if c.ndim == 2:  # (batch, O)
+                c = c.unsqueeze(1).expand(nbat, self.policy_len, self.num_obs[m])
+            C_t.append(c)
+        self._C_flat, _ = ffi.flatten_ragged_f32(C_t, 1, dev)
+        self._qs_offsets = np.cumsum([0] + S)
+        self._layout = ffi.EfeLayout(S, self.num_obs, self.num_controls, self.policy_len, self.A_dependencies,
+                                     self.B_dependencies)
+        self._I_flat = torch.zeros((nbat, int(self._layout.I_offsets[-1])), device=dev)
+        self._eps = torch.full((1,), 1e-3, device=dev)
+        self._flags = ffi.efe_flags(use_utility, use_states_info_gain, precision=precision)
+        self.A, self.B, self.C = A, B, C
+
+    # ------------------------------------------------------------------ API
+    def infer_states(self, observations, empirical_prior: Sequence[torch.Tensor]):
+        """``pymdp/agent.py:675-823`` (fpi): returns ``qs[f]`` of shape ``(batch, 1, S_f)``.
+
+        ``observations``: list of M index arrays of shape ``(batch,)`` (or a
+        ``(batch, M)`` array) — discrete observations, one-hot in the reference.
+        """
+        if not isinstance(empirical_prior, (list, tuple)):
+            raise ValueError("`empirical_prior` must be a list/tuple with one entry per hidden-state factor.")
+        if len(empirical_prior) != self.num_factors:
+            raise ValueError(f"`empirical_prior` has {len(empirical_prior)} factor(s), expected {self.num_factors}")
+        dev = self.device
+        if isinstance(observations, (list, tuple)):
+            obs = torch.stack([torch.as_tensor(o, device=dev).reshape(-1) for o in observations], dim=-1)
+        else:
+            obs = torch.as_tensor(observations, device=dev)
+        obs = obs.to(torch.int32).reshape(self.batch_size, self.num_modalities).contiguous()
+        prior_flat, _ = ffi.flatten_ragged_f32(
+            [torch.broadcast_to(_t(p, dev), (self.batch_size, self.num_states[f]))
+             for f, p in enumerate(empirical_prior)], 1, dev)
+        q = ffi.fpi_obs_flat(self._A_flat, int(self._A_offsets[-1]), self._A_offsets, self.num_obs, obs,
+                             prior_flat, self.num_states, self.A_dependencies, self.num_iter)
+        o = self._qs_offsets
+        return [q[:, o[f]:o[f + 1]].unsqueeze(1) for f in range(self.num_factors)]
+
+    def infer_policies(self, qs: Sequence[torch.Tensor]):
+        """``pymdp/agent.py:853-906``: returns ``(q_pi, neg_efe)``, each ``(batch, P)``."""
+        latest = [q[:, -1] if q.ndim == 3 else q for q in qs]
+        qs_flat, _ = ffi.flatten_ragged_f32(latest, 1, self.device)
+        P = self.policies.shape[0]
+        G = torch.empty((self.batch_size, P), device=self.device)
+        self._layout.call(None, self.policies, 0, qs_flat, self._A_flat, self._B_flat, self._C_flat,
+                          self._I_flat, None, None, self._eps, G, self.batch_size, P, self._flags)
+        q_pi = ffi.policy_posterior(G, self.E, self.gamma)
+        return q_pi, G
+
+    def sample_action(self, q_pi: torch.Tensor, rng_key=None) -> torch.Tensor:
+        """``pymdp/agent.py:939-967`` (full, deterministic): ``(batch, F)`` int32."""
+        return ffi.select_action(q_pi, self.policies)

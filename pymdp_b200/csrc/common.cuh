@@ -1,0 +1,61 @@
+// Shared host/device helpers for the pymdp_b200 sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <string>
+
+#include "../../include/pymdp_b200.h"
+
+namespace b2 {
+
+// float32 image of the reference's clip floor MINVAL = finfo(float64).eps
+// (pymdp/maths.py:15); the reference's float32 path clips at this value.
+constexpr float kMinVal = 2.220446049250313e-16f;
+
+// ----------------------------------------------------------------- errors
+int32_t fail(int32_t code, const std::string& msg);
+int32_t cuda_fail(const char* op, cudaError_t err);
+void note_launches(uint64_t n);
+
+#define B2_TRY(expr)                       \
+  do {                                     \
+    int32_t _b2_rc = (expr);               \
+    if (_b2_rc != B2_OK) return _b2_rc;    \
+  } while (0)
+
+#define B2_CUDA_TRY(op, expr)                          \
+  do {                                                 \
+    cudaError_t _b2_e = (expr);                        \
+    if (_b2_e != cudaSuccess) return ::b2::cuda_fail(op, _b2_e); \
+  } while (0)
+
+// Check the launch that just happened (configuration errors surface here).
+inline int32_t check_launch(const char* op, uint64_t n = 1) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(op, e);
+  note_launches(n);
+  return B2_OK;
+}
+
+// Opt a kernel into `bytes` of dynamic shared memory once per process/device.
+int32_t ensure_smem_attr(const void* kernel, int bytes, const char* op);
+
+// ---------------------------------------------------------------- device
+__device__ __forceinline__ float log_stable(float x) { return logf(fmaxf(x, kMinVal)); }
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+}  // namespace b2

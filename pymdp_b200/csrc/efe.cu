@@ -1,0 +1,443 @@
+// Expected free energy (neg-EFE, "G") over all policies — reference-ABI entry,
+// validation, the per-(agent, policy) SIMT FP32 kernel, and the policy
+// posterior / action-selection kernels.
+//
+// Semantics: pymdp/control.py:604-690 (compute_neg_efe_policy) vmapped over
+// policies (control.py:347), i.e. for each policy, from G = 0 and qs = qs_init:
+//   for t < T: qs_f <- factor_dot(B_f[..., u_{t,f}], qs[B_deps[f]])   (:351-389)
+//              qo_m  = factor_dot(A_m, qs[A_deps[m]])                  (:420-447)
+//              G    += sum_m [ H(qo_m) - H_A_m . x_m ]   (if states info gain, :449-481)
+//                    + sum_m qo_m . C_m[t]               (if utility, :483-509)
+// with x_m = outer product of the dependency marginals and
+// H_A_m[k] = -sum_o A_m[o,k] log(clip(A_m[o,k])).
+//
+// Both linear terms collapse into one per-(t, m) row computed once per agent
+// (the reference's own trick, neg_efe_cuda_kernels.cu:1426-1445):
+//   lin[t,m,k] = sum_o A_m[o,k] * (log(clip(A_m[o,k])) [ig] + C_m[t,o] [util])
+// so the only per-policy nonlinearity is H(qo_m).
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "efe.cuh"
+
+namespace b2 {
+
+const char* const kEfeName = "efe_ffi";
+
+namespace {
+
+int32_t bad(const std::string& msg) { return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": " + msg); }
+
+}  // namespace
+
+// Mirrors parse_call_shape / validate_attr_spans / validate_layout /
+// validate_buffer_counts (pymdp/ffi/neg_efe/neg_efe_layout.h:209-363).
+int32_t build_efe_params(EfeParams* p, int64_t P, int64_t T, int64_t F, int64_t M, const int64_t* S,
+                         const int64_t* O, const int64_t* U, const int64_t* qs_offsets,
+                         const int64_t* A_offsets, const int64_t* B_offsets, const int64_t* C_offsets,
+                         const int64_t* I_offsets, const int64_t* I_depths, const int64_t* A_dep_flat,
+                         int64_t A_dep_flat_len, const int64_t* A_dep_offsets, const int64_t* B_dep_flat,
+                         int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int32_t flags) {
+  std::memset(p, 0, sizeof(*p));
+  if (!S || !O || !U || !qs_offsets || !A_offsets || !B_offsets || !C_offsets || !I_offsets || !I_depths ||
+      !A_dep_flat || !A_dep_offsets || !B_dep_flat || !B_dep_offsets)
+    return bad("null attribute array");
+  if (F <= 0 || M <= 0 || P <= 0 || T <= 0) return bad("F/M/P/T must all be positive");
+  if (F > kEfeMaxF || M > kEfeMaxM)
+    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": F or M exceeds this build's limits");
+  if (P > 0x7fffffff / 4 || T > 64) return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": P or T too large");
+  if (qs_offsets[0] != 0 || A_offsets[0] != 0 || B_offsets[0] != 0 || C_offsets[0] != 0 || I_offsets[0] != 0 ||
+      A_dep_offsets[0] != 0 || B_dep_offsets[0] != 0)
+    return bad("offset tables must start at zero");
+  if (A_dep_flat_len != A_dep_offsets[M]) return bad("A_dep_flat size inconsistent with A_dep_offsets");
+  if (B_dep_flat_len != B_dep_offsets[F]) return bad("B_dep_flat size inconsistent with B_dep_offsets");
+  p->P = (int32_t)P;
+  p->T = (int32_t)T;
+  p->F = (int32_t)F;
+  p->M = (int32_t)M;
+  p->flags = flags;
+  uint64_t total_actions = 1;
+  for (int64_t f = 0; f < F; ++f) {
+    if (S[f] <= 0 || U[f] <= 0) return bad("S[f] and U[f] must be positive");
+    if (total_actions > 0xffffffffull / (uint64_t)U[f])
+      return bad("action encoding overflows 32 bits (prod(U[f]) > UINT32_MAX)");
+    total_actions *= (uint64_t)U[f];
+    if (qs_offsets[f + 1] < qs_offsets[f]) return bad("qs_off must be monotonic");
+    if (qs_offsets[f + 1] - qs_offsets[f] != S[f]) return bad("qs_off inconsistent with S");
+    if (B_offsets[f + 1] < B_offsets[f]) return bad("B_off must be monotonic");
+    if (B_dep_offsets[f + 1] < B_dep_offsets[f]) return bad("B_dep_off must be monotonic");
+    const int64_t r = B_dep_offsets[f + 1] - B_dep_offsets[f];
+    if (r < 1 || r > B2_MAX_DEP_RANK) return bad("B_dep rank of factor " + std::to_string(f) + " outside [1, 8]");
+    EfeFactor& fb = p->fac[f];
+    fb.rank = (int32_t)r;
+    int64_t K = 1;
+    for (int64_t i = 0; i < r; ++i) {
+      const int64_t d = B_dep_flat[B_dep_offsets[f] + i];
+      if (d < 0 || d >= F) return bad("B_dep factor index out of range");
+      fb.dep[i] = (int8_t)d;
+      K *= S[d];
+    }
+    if (B_offsets[f + 1] - B_offsets[f] != S[f] * K * U[f]) return bad("B_off inconsistent with S/U/deps");
+    fb.K = (int32_t)K;
+    fb.B_off = B_offsets[f];
+    p->S[f] = (int32_t)S[f];
+    p->U[f] = (int32_t)U[f];
+    p->qs_off[f] = (int32_t)qs_offsets[f];
+  }
+  p->qs_off[F] = (int32_t)qs_offsets[F];
+  p->S_tot = (int32_t)qs_offsets[F];
+  if (p->S_tot > kEfePlainMaxStot)
+    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": total states exceed this build's limit");
+  int64_t koff = 0;
+  for (int64_t m = 0; m < M; ++m) {
+    if (O[m] <= 0) return bad("O[m] must be positive");
+    if (A_offsets[m + 1] < A_offsets[m]) return bad("A_off must be monotonic");
+    if (C_offsets[m + 1] < C_offsets[m]) return bad("C_off must be monotonic");
+    if (C_offsets[m + 1] - C_offsets[m] != T * O[m]) return bad("C_off inconsistent with T/O");
+    if (A_dep_offsets[m + 1] < A_dep_offsets[m]) return bad("A_dep_off must be monotonic");
+    const int64_t r = A_dep_offsets[m + 1] - A_dep_offsets[m];
+    if (r < 1 || r > B2_MAX_DEP_RANK) return bad("A_dep rank of modality " + std::to_string(m) + " outside [1, 8]");
+    EfeModality& md = p->mod[m];
+    md.rank = (int32_t)r;
+    int64_t K = 1;
+    for (int64_t i = 0; i < r; ++i) {
+      const int64_t d = A_dep_flat[A_dep_offsets[m] + i];
+      if (d < 0 || d >= F) return bad("A_dep factor index out of range");
+      md.dep[i] = (int8_t)d;
+      K *= S[d];
+    }
+    if (A_offsets[m + 1] - A_offsets[m] != O[m] * K) return bad("A_off inconsistent with O/deps");
+    if (O[m] > kEfePlainMaxO)
+      return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": O[m] exceeds this build's limit");
+    if (K > (1 << 26)) return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": modality too large");
+    md.O = (int32_t)O[m];
+    md.K = (int32_t)K;
+    md.A_off = A_offsets[m];
+    md.C_off = C_offsets[m];
+    md.lin_off = koff;
+    koff += K;
+  }
+  p->K_tot = koff;
+  for (int64_t f = 0; f < F; ++f) {
+    if (I_depths[f] <= 0) return bad("I_depths[f] must be positive");
+    if (I_offsets[f + 1] < I_offsets[f]) return bad("I_off must be monotonic");
+    if (I_offsets[f + 1] - I_offsets[f] != I_depths[f] * S[f]) return bad("I_off inconsistent with depth/S");
+  }
+  p->A_stride = A_offsets[M];
+  p->B_stride = B_offsets[F];
+  p->C_stride = C_offsets[M];
+  return B2_OK;
+}
+
+// ------------------------------------------------------------------ kernels
+// lin[b, t, koff_m + k] for every agent, step and modality (one thread per k).
+__global__ void efe_linear_rows_kernel(const __grid_constant__ EfeParams p, const float* __restrict__ A,
+                                       const float* __restrict__ C, float* __restrict__ lin) {
+  const int64_t b = blockIdx.z;
+  const int t = blockIdx.y;
+  const int64_t kk = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (kk >= p.K_tot) return;
+  int m = 0;
+  while (m + 1 < p.M && p.mod[m + 1].lin_off <= kk) ++m;
+  const EfeModality& md = p.mod[m];
+  const int64_t k = kk - md.lin_off;
+  const float* Am = A + b * p.A_stride + md.A_off;
+  const float* Cm = C + b * p.C_stride + md.C_off + (int64_t)t * md.O;
+  const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
+  const bool ut = (p.flags & B2_FLAG_USE_UTILITY) != 0;
+  float acc = 0.f;
+  for (int o = 0; o < md.O; ++o) {
+    const float a = __ldg(Am + (int64_t)o * md.K + k);
+    float w = 0.f;
+    if (ig) w += log_stable(a);
+    if (ut) w += __ldg(Cm + o);
+    acc = fmaf(a, w, acc);
+  }
+  lin[(b * p.T + t) * p.K_tot + kk] = acc;
+}
+
+// One thread = one (agent, policy): the plain per-policy SIMT evaluation.
+__global__ void __launch_bounds__(128)
+    efe_plain_kernel(const __grid_constant__ EfeParams p, const int32_t* __restrict__ pm, int pm_batched,
+                     const float* __restrict__ qs_init, const float* __restrict__ A, const float* __restrict__ B,
+                     const float* __restrict__ lin, float* __restrict__ G) {
+  const int64_t b = blockIdx.y;
+  const int pol = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pol >= p.P) return;
+  float qs[2][kEfePlainMaxStot];
+  float qo[kEfePlainMaxO];
+  int cur = 0;
+  for (int i = 0; i < p.S_tot; ++i) qs[0][i] = __ldg(qs_init + b * p.S_tot + i);
+  const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (int64_t)pol * p.T * p.F;
+  const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
+  float g = 0.f;
+  bool bad_action = false;
+  for (int t = 0; t < p.T; ++t) {
+    // expected states
+    const float* qc = qs[cur];
+    float* qn = qs[cur ^ 1];
+    for (int f = 0; f < p.F; ++f) {
+      const EfeFactor& fb = p.fac[f];
+      int u = u_pol[t * p.F + f];
+      if (u < 0 || u >= p.U[f]) {
+        bad_action = true;
+        u = 0;
+      }
+      const float* Bf = B + b * p.B_stride + fb.B_off;
+      const int U = p.U[f];
+      for (int s = 0; s < p.S[f]; ++s) {
+        float acc = 0.f;
+        int dig[B2_MAX_DEP_RANK] = {0};
+        for (int k = 0; k < fb.K; ++k) {
+          float w = 1.f;
+          for (int i = 0; i < fb.rank; ++i) w *= qc[p.qs_off[fb.dep[i]] + dig[i]];
+          acc = fmaf(__ldg(Bf + ((int64_t)s * fb.K + k) * U + u), w, acc);
+          for (int i = fb.rank - 1; i >= 0; --i) {
+            if (++dig[i] < p.S[fb.dep[i]]) break;
+            dig[i] = 0;
+          }
+        }
+        qn[p.qs_off[f] + s] = acc;
+      }
+    }
+    cur ^= 1;
+    const float* q = qs[cur];
+    // expected observations, entropy and the linear row
+    for (int m = 0; m < p.M; ++m) {
+      const EfeModality& md = p.mod[m];
+      const float* Am = A + b * p.A_stride + md.A_off;
+      const float* Lm = lin + (b * p.T + t) * p.K_tot + md.lin_off;
+      for (int o = 0; o < md.O; ++o) qo[o] = 0.f;
+      float la = 0.f;
+      int dig[B2_MAX_DEP_RANK] = {0};
+      for (int k = 0; k < md.K; ++k) {
+        float w = 1.f;
+        for (int i = 0; i < md.rank; ++i) w *= q[p.qs_off[md.dep[i]] + dig[i]];
+        for (int o = 0; o < md.O; ++o) qo[o] = fmaf(__ldg(Am + (int64_t)o * md.K + k), w, qo[o]);
+        la = fmaf(__ldg(Lm + k), w, la);
+        for (int i = md.rank - 1; i >= 0; --i) {
+          if (++dig[i] < p.S[md.dep[i]]) break;
+          dig[i] = 0;
+        }
+      }
+      float h = 0.f;
+      if (ig)
+        for (int o = 0; o < md.O; ++o) h -= qo[o] * log_stable(qo[o]);
+      g += h + la;
+    }
+  }
+  G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : g;
+}
+
+// q_pi[b] = softmax(gamma_b * G[b] + log(clip(E_b))) — one CTA per agent.
+__global__ void __launch_bounds__(256)
+    policy_posterior_kernel(const float* __restrict__ G, const float* __restrict__ E, int E_batched,
+                            const float* __restrict__ gamma, int gamma_batched, float* __restrict__ q_pi, int P) {
+  __shared__ float red[32];
+  const int64_t b = blockIdx.x;
+  const float gm = gamma[gamma_batched ? b : 0];
+  const float* g = G + b * P;
+  const float* e = E + (E_batched ? b * P : 0);
+  float mx = -INFINITY;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) mx = fmaxf(mx, gm * g[i] + log_stable(e[i]));
+  mx = warp_max(mx);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
+    v = warp_max(v);
+    if (threadIdx.x == 0) red[0] = v;
+  }
+  __syncthreads();
+  mx = red[0];
+  __syncthreads();
+  float sum = 0.f;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) sum += expf(gm * g[i] + log_stable(e[i]) - mx);
+  sum = warp_sum(sum);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) red[0] = v;
+  }
+  __syncthreads();
+  sum = red[0];
+  for (int i = threadIdx.x; i < P; i += blockDim.x) q_pi[b * P + i] = expf(gm * g[i] + log_stable(e[i]) - mx) / sum;
+}
+
+// action[b, :] = policy_matrix[first argmax q_pi[b], 0, :] — one CTA per agent.
+__global__ void __launch_bounds__(256)
+    select_action_kernel(const float* __restrict__ q_pi, const int32_t* __restrict__ pm, int32_t* __restrict__ action,
+                         int P, int T, int F) {
+  __shared__ float sv[32];
+  __shared__ int si[32];
+  const int64_t b = blockIdx.x;
+  float best = -INFINITY;
+  int bi = 0x7fffffff;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    const float v = q_pi[b * P + i];
+    if (v > best || (v == best && i < bi) || (bi == 0x7fffffff && v != v)) {
+      best = v;
+      bi = i;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > best || (ov == best && oi < bi)) {
+      best = ov;
+      bi = oi;
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sv[threadIdx.x >> 5] = best;
+    si[threadIdx.x >> 5] = bi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (sv[w] > best || (sv[w] == best && si[w] < bi)) {
+        best = sv[w];
+        bi = si[w];
+      }
+    if (bi == 0x7fffffff) bi = 0;
+    si[0] = bi;
+  }
+  __syncthreads();
+  bi = si[0];
+  for (int f = threadIdx.x; f < F; f += blockDim.x) action[b * F + f] = pm[(int64_t)bi * T * F + f];
+}
+
+int32_t launch_linear_rows(const EfeParams& p, int64_t Bn, const float* A, const float* C, float* lin,
+                           cudaStream_t stream) {
+  dim3 grid((unsigned)((p.K_tot + 127) / 128), (unsigned)p.T, (unsigned)Bn);
+  efe_linear_rows_kernel<<<grid, 128, 0, stream>>>(p, A, C, lin);
+  return check_launch("efe_ffi linear rows");
+}
+
+int32_t launch_efe_plain(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
+                         const float* A, const float* B, const float* lin, float* G, cudaStream_t stream) {
+  dim3 grid((unsigned)((p.P + 127) / 128), (unsigned)Bn);
+  efe_plain_kernel<<<grid, 128, 0, stream>>>(p, pm, pm_batched, qs, A, B, lin, G);
+  return check_launch("efe_ffi plain");
+}
+
+// Workspace from the device's stream-ordered pool; freed stream-ordered.
+int32_t ws_alloc(void** ptr, size_t bytes, cudaStream_t stream, const char* op) {
+  static std::mutex mu;
+  static std::set<int> tuned;
+  int dev = 0;
+  B2_CUDA_TRY(op, cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!tuned.count(dev)) {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~0ull;  // keep freed blocks cached in this process
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      tuned.insert(dev);
+    }
+  }
+  B2_CUDA_TRY(op, cudaMallocAsync(ptr, bytes, stream));
+  return B2_OK;
+}
+
+}  // namespace b2
+
+using namespace b2;
+
+extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+                              const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
+                              const float* B, int64_t B_count, const float* C, int64_t C_count, const float* I,
+                              int64_t I_count, const float* pA, int64_t pA_count, const float* pB,
+                              int64_t pB_count, const float* inductive_epsilon, int64_t eps_count,
+                              float* neg_efe_out, int64_t out_count, int64_t Bn, int64_t P, int64_t T, int64_t F,
+                              int64_t M, const int64_t* S, const int64_t* O, const int64_t* U,
+                              const int64_t* qs_offsets, const int64_t* A_offsets, const int64_t* B_offsets,
+                              const int64_t* C_offsets, const int64_t* I_offsets, const int64_t* I_depths,
+                              const int64_t* A_dep_flat, int64_t A_dep_flat_len, const int64_t* A_dep_offsets,
+                              const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets,
+                              int32_t flags) {
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (Bn < 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": negative Bn");
+  EfeParams p;
+  B2_TRY(build_efe_params(&p, P, T, F, M, S, O, U, qs_offsets, A_offsets, B_offsets, C_offsets, I_offsets,
+                          I_depths, A_dep_flat, A_dep_flat_len, A_dep_offsets, B_dep_flat, B_dep_flat_len,
+                          B_dep_offsets, flags));
+  const int64_t I_stride = I_offsets[F];
+  struct Chk {
+    const char* name;
+    int64_t actual, expected;
+  } chks[] = {
+      {"policy_matrix", pm_count, (pm_batched ? Bn : 1) * P * T * F},
+      {"qs_init", qs_count, Bn * (int64_t)p.S_tot},
+      {"A", A_count, Bn * p.A_stride},
+      {"B", B_count, Bn * p.B_stride},
+      {"C", C_count, Bn * p.C_stride},
+      {"I", I_count, Bn * I_stride},
+      {"out", out_count, Bn * P},
+  };
+  for (const Chk& c : chks)
+    if (c.actual != c.expected)
+      return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": " + c.name + " element_count = " +
+                                               std::to_string(c.actual) + ", expected " + std::to_string(c.expected));
+  if (eps_count != 1 && eps_count != Bn)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": inductive_epsilon must have 1 or Bn elements");
+  if (flags & B2_FLAG_USE_PARAM_INFO_GAIN) {
+    if (pA_count == 0 && pB_count == 0)
+      return fail(B2_ERR_INVALID_ARGUMENT,
+                  std::string(kEfeName) + ": use_param_info_gain=true requires at least one of pA, pB");
+    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": parameter information gain is not built yet");
+  }
+  if (flags & B2_FLAG_USE_INDUCTIVE)
+    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": inductive planning term is not built yet");
+  const int prec = (flags >> B2_PRECISION_SHIFT) & 3;
+  if (prec != B2_PRECISION_FP32)
+    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": requested precision is not built yet");
+  if (Bn == 0) return B2_OK;
+  if (!policy_matrix || !qs_init || !A || !B || !C || !neg_efe_out)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": null buffer");
+  if (Bn > 65535) return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": Bn > 65535");
+  (void)I;
+  (void)pA;
+  (void)pB;
+  (void)inductive_epsilon;
+  float* lin = nullptr;
+  const size_t bytes = (size_t)Bn * p.T * p.K_tot * sizeof(float);
+  B2_TRY(ws_alloc((void**)&lin, bytes, stream, kEfeName));
+  int32_t rc = launch_linear_rows(p, Bn, A, C, lin, stream);
+  if (rc == B2_OK) rc = launch_efe_plain(p, Bn, policy_matrix, pm_batched, qs_init, A, B, lin, neg_efe_out, stream);
+  cudaError_t fe = cudaFreeAsync(lin, stream);
+  if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
+  return rc;
+}
+
+extern "C" int32_t b2_policy_posterior(void* stream, const float* neg_efe, const float* E, int32_t E_batched,
+                                       const float* gamma, int32_t gamma_batched, float* q_pi, int64_t Bn,
+                                       int64_t P) {
+  if (Bn < 0 || P <= 0 || P > 0x7fffffff)
+    return fail(B2_ERR_INVALID_ARGUMENT, "policy_posterior: invalid Bn or P");
+  if (Bn == 0) return B2_OK;
+  if (!neg_efe || !E || !gamma || !q_pi) return fail(B2_ERR_INVALID_ARGUMENT, "policy_posterior: null buffer");
+  if (Bn > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, "policy_posterior: Bn too large");
+  policy_posterior_kernel<<<(unsigned)Bn, 256, 0, (cudaStream_t)stream>>>(neg_efe, E, E_batched, gamma,
+                                                                           gamma_batched, q_pi, (int)P);
+  return check_launch("policy_posterior");
+}
+
+extern "C" int32_t b2_select_action(void* stream, const float* q_pi, const int32_t* policy_matrix,
+                                    int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F) {
+  if (Bn < 0 || P <= 0 || T <= 0 || F <= 0 || P > 0x7fffffff)
+    return fail(B2_ERR_INVALID_ARGUMENT, "select_action: invalid sizes");
+  if (Bn == 0) return B2_OK;
+  if (!q_pi || !policy_matrix || !action) return fail(B2_ERR_INVALID_ARGUMENT, "select_action: null buffer");
+  select_action_kernel<<<(unsigned)Bn, 256, 0, (cudaStream_t)stream>>>(q_pi, policy_matrix, action, (int)P,
+                                                                        (int)T, (int)F);
+  return check_launch("select_action");
+}

@@ -1,0 +1,56 @@
+// Kernel-parameter layout shared by the EFE kernels.
+#pragma once
+
+#include <cstring>
+
+#include "common.cuh"
+
+namespace b2 {
+
+constexpr int kEfeMaxF = B2_MAX_FACTORS;
+constexpr int kEfeMaxM = B2_MAX_MODALITIES;
+constexpr int kEfePlainMaxStot = 256;  // per-policy state vector kept per thread
+constexpr int kEfePlainMaxO = 128;
+
+struct EfeFactor {
+  int64_t B_off;  // offset of B_f inside one agent's flat B
+  int32_t K;      // prod of parent state counts
+  int32_t rank;
+  int8_t dep[B2_MAX_DEP_RANK];
+};
+
+struct EfeModality {
+  int64_t A_off;    // offset of A_m inside one agent's flat A
+  int64_t C_off;    // offset of C_m (T, O_m) inside one agent's flat C
+  int64_t lin_off;  // offset of modality m inside one (agent, t) linear row
+  int32_t O, K, rank;
+  int8_t dep[B2_MAX_DEP_RANK];
+};
+
+struct EfeParams {
+  int32_t P, T, F, M, S_tot, flags;
+  int64_t K_tot;  // sum_m K_m
+  int64_t A_stride, B_stride, C_stride;
+  int32_t S[kEfeMaxF];
+  int32_t U[kEfeMaxF];
+  int32_t qs_off[kEfeMaxF + 1];
+  EfeFactor fac[kEfeMaxF];
+  EfeModality mod[kEfeMaxM];
+};
+
+extern const char* const kEfeName;
+
+int32_t build_efe_params(EfeParams* p, int64_t P, int64_t T, int64_t F, int64_t M, const int64_t* S,
+                         const int64_t* O, const int64_t* U, const int64_t* qs_offsets, const int64_t* A_offsets,
+                         const int64_t* B_offsets, const int64_t* C_offsets, const int64_t* I_offsets,
+                         const int64_t* I_depths, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                         const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
+                         const int64_t* B_dep_offsets, int32_t flags);
+
+int32_t launch_linear_rows(const EfeParams& p, int64_t Bn, const float* A, const float* C, float* lin,
+                           cudaStream_t stream);
+int32_t launch_efe_plain(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
+                         const float* A, const float* B, const float* lin, float* G, cudaStream_t stream);
+int32_t ws_alloc(void** ptr, size_t bytes, cudaStream_t stream, const char* op);
+
+}  // namespace b2

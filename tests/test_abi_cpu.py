@@ -1,0 +1,144 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol
+declared in include/pymdp_b200.h, and its host-side validation rejects the
+inputs the reference's validators reject (pymdp/ffi/fpi/fpi_entry.h:24-82,
+pymdp/ffi/neg_efe/neg_efe_layout.h:269-363) before touching the device."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from pymdp_b200 import _lib
+
+HEADER = os.path.join(ROOT, "include", "pymdp_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(b2_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    syms = declared_symbols()
+    assert len(syms) >= 9
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert lib.b2_abi_version() >= 1
+    assert lib.b2_capabilities() & (1 << 2)
+    assert _lib.launch_count() >= 0
+
+
+def _fpi(S, ll_offsets, lp_offsets, dep_flat, dep_offs, num_iter, ll_count, lp_count, q_count):
+    lib = _lib.load()
+    i64 = _lib.i64
+    return lib.b2_fpi(None, 1, ll_count, 1, lp_count, 1, q_count, i64(S), len(S), i64(ll_offsets),
+                      len(ll_offsets), i64(lp_offsets), len(lp_offsets), i64(dep_flat), len(dep_flat),
+                      i64(dep_offs), len(dep_offs), num_iter)
+
+
+GOOD = dict(S=[3, 2], ll_offsets=[0, 6, 12], lp_offsets=[0, 3, 5], dep_flat=[0, 1, 0, 1], dep_offs=[0, 2, 4],
+            num_iter=16, ll_count=12, lp_count=5, q_count=5)
+
+
+@pytest.mark.parametrize("change,msg", [
+    (dict(num_iter=0), "num_iter = 0, must be positive"),
+    (dict(S=[3, 0]), "S[1] must be positive"),
+    (dict(dep_flat=[0, 0, 0, 1]), "duplicate factor"),
+    (dict(dep_flat=[0, 2, 0, 1]), "out of range"),
+    (dict(lp_offsets=[0, 3]), "lp_offsets size = 2, expected 3"),
+    (dict(ll_offsets=[0, 6, 11], ll_count=11), "ll_offsets inconsistent"),
+    (dict(lp_count=7), "not divisible by total_S"),
+    (dict(ll_count=13), "ll_flat element_count = 13, expected 12"),
+    (dict(q_count=10), "q_out element_count = 10, expected 5"),
+    (dict(dep_flat=list(range(9)) + [0, 1], dep_offs=[0, 9, 11], S=[2] * 9,
+          lp_offsets=list(range(0, 20, 2)), lp_count=18, q_count=18), "rank 9 outside [1, 8]"),
+])
+def test_fpi_validation_errors(change, msg):
+    args = dict(GOOD)
+    args.update(change)
+    rc = _fpi(**args)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT, (rc, _lib.last_error())
+    assert msg in _lib.last_error()
+    assert _lib.last_error().startswith("fpi_ffi:")
+
+
+def test_fpi_limits_are_reported_as_unsupported():
+    F = 17
+    rc = _fpi(S=[2] * F, ll_offsets=[0, 2], lp_offsets=list(range(0, 2 * F + 1, 2)), dep_flat=[0],
+              dep_offs=[0, 1], num_iter=1, ll_count=2, lp_count=2 * F, q_count=2 * F)
+    assert rc == _lib.B2_ERR_UNSUPPORTED
+    assert "limits" in _lib.last_error()
+
+
+def _efe_layout_args(S=(3, 2), O=(3, 5), U=(3, 1), T=1, A_deps=((0, 1), (0, 1)), B_deps=((0,), (1,))):
+    from pymdp_b200.ffi import EfeLayout
+    return EfeLayout(S, O, U, T, A_deps, B_deps)
+
+
+def _efe_call(lay, Bn=0, P=3, flags=3, counts=None):
+    lib = _lib.load()
+    c = lay._c
+    cnt = dict(pm=P * lay.T * lay.F, qs=Bn * lay.qs_offsets[-1], A=Bn * lay.A_offsets[-1],
+               B=Bn * lay.B_offsets[-1], C=Bn * lay.C_offsets[-1], I=Bn * lay.I_offsets[-1], pA=0, pB=0, eps=1,
+               out=Bn * P)
+    cnt.update(counts or {})
+    return lib.b2_neg_efe(None, 1, cnt["pm"], 0, 1, cnt["qs"], 1, cnt["A"], 1, cnt["B"], 1, cnt["C"], 1, cnt["I"],
+                          1, cnt["pA"], 1, cnt["pB"], 1, cnt["eps"], 1, cnt["out"], Bn, P, lay.T, lay.F, lay.M,
+                          c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9], len(lay.A_dep_flat), c[10],
+                          c[11], len(lay.B_dep_flat), c[12], flags)
+
+
+def test_efe_valid_empty_batch_is_a_noop():
+    assert _efe_call(_efe_layout_args(), Bn=0) == _lib.B2_OK
+
+
+@pytest.mark.parametrize("counts,msg", [
+    (dict(A=5), "A element_count = 5, expected 0"),
+    (dict(pm=4), "policy_matrix element_count = 4, expected 6"),
+    (dict(eps=3), "inductive_epsilon must have 1 or Bn elements"),
+])
+def test_efe_count_errors(counts, msg):
+    rc = _efe_call(_efe_layout_args(), Bn=0, P=3, counts=counts)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT
+    assert msg in _lib.last_error() and _lib.last_error().startswith("efe_ffi:")
+
+
+def test_efe_layout_errors():
+    lay = _efe_layout_args()
+    lay.B_offsets[2] += 1
+    lay._c[5] = _lib.i64(lay.B_offsets)
+    assert _efe_call(lay) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "B_off inconsistent" in _lib.last_error()
+    lay = _efe_layout_args()
+    lay.A_dep_flat[3] = 3
+    lay._c[9] = _lib.i64(lay.A_dep_flat)
+    assert _efe_call(lay) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "out of range" in _lib.last_error()
+
+
+def test_efe_unbuilt_terms_are_unsupported():
+    lay = _efe_layout_args()
+    assert _efe_call(lay, flags=3 | 4) == _lib.B2_ERR_UNSUPPORTED
+    assert "inductive" in _lib.last_error()
+    assert _efe_call(lay, flags=3 | 8, counts=dict(pA=1)) == _lib.B2_ERR_UNSUPPORTED
+    assert _efe_call(lay, flags=3 | 8) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "requires at least one of pA, pB" in _lib.last_error()
+
+
+def test_construct_policies_matches_oracle_order():
+    from oracle.efe import construct_policies as ref
+    from pymdp_b200.control import construct_policies
+    for S, U, T in [([3, 2], [3, 1], 1), ([32, 16, 8], [4, 4, 1], 3), ([4, 3, 2], [3, 2, 1], 2)]:
+        np.testing.assert_array_equal(construct_policies(S, U, T), ref(S, U, T))
+
+
+def test_package_imports_without_gpu():
+    import pymdp_b200
+    from pymdp_b200 import Agent, ffi  # noqa: F401
+    assert callable(ffi.fpi_ffi) and callable(ffi.neg_efe_all_policies_ffi)
+    assert pymdp_b200.Agent is Agent
+    assert ffi.is_available()

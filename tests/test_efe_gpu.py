@@ -1,0 +1,97 @@
+"""EFE parity on the GPU: neg-EFE (G), q_pi and the selected action from the
+sm_100a kernels (through the C-ABI) against golden vectors made by the
+reference's own code (pymdp/control.py) and against the FP64 oracle.
+
+Tolerance (FP32 path vs FP64 reference): G rtol 1e-5 / atol 1e-5; q_pi rtol
+2e-4 / atol 1e-6 (gamma = 16 multiplies G's absolute error inside the
+softmax); selected actions identical."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import deps_from, load_golden, unpack
+from oracle import efe as oefe
+
+pytestmark = pytest.mark.gpu
+
+G_RTOL, G_ATOL = 1e-5, 1e-5
+Q_RTOL, Q_ATOL = 2e-4, 1e-6
+EFE = ["efe_plain", "efe_mixed", "efe_bdeps", "efe_cfg3_t1", "efe_cfg3_small"]
+
+
+def cuda(x, dtype=torch.float32):
+    return torch.as_tensor(np.asarray(x), device="cuda").to(dtype)
+
+
+def run_golden(d, precision="fp32"):
+    from pymdp_b200 import ffi
+    A_deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    B_deps = deps_from(d["B_dep_flat"], d["B_dep_offsets"])
+    qs = [cuda(q) for q in unpack(d, "qs")]
+    I = [torch.zeros((1, q.shape[0]), device="cuda") for q in qs]
+    G = ffi.neg_efe_all_policies_ffi(d["policies"], qs, [cuda(a) for a in unpack(d, "A")],
+                                     [cuda(b) for b in unpack(d, "B")], [cuda(c) for c in unpack(d, "C")], I,
+                                     A_deps, B_deps, use_inductive=False, precision=precision)
+    q_pi = ffi.policy_posterior(G, cuda(d["E"]), float(d["gamma"]))
+    act = ffi.select_action(q_pi, d["policies"])
+    return G.cpu().numpy(), q_pi.cpu().numpy(), act.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", EFE)
+def test_neg_efe_matches_reference(name):
+    d = load_golden(name)
+    G, q_pi, act = run_golden(d)
+    np.testing.assert_allclose(G, d["G"], rtol=G_RTOL, atol=G_ATOL)
+    np.testing.assert_allclose(q_pi, d["q_pi"], rtol=Q_RTOL, atol=Q_ATOL)
+    np.testing.assert_array_equal(act, d["action"])
+
+
+def random_efe(rng, S, O, U, T, A_deps, B_deps, batch, C2d=False):
+    def dirc(shape, alpha=0.5):
+        g = rng.gamma(alpha, size=shape) + 1e-30
+        return (g / g.sum(1, keepdims=True)).astype(np.float32)
+    A = [dirc((batch, O[m]) + tuple(S[d] for d in A_deps[m])) for m in range(len(O))]
+    B = [dirc((batch, S[f]) + tuple(S[d] for d in B_deps[f]) + (U[f],)) for f in range(len(S))]
+    C = [rng.normal(size=(batch, T, o) if C2d else (batch, o)).astype(np.float32) for o in O]
+    qs = [dirc((batch, s), 1.0) for s in S]
+    return A, B, C, qs
+
+
+@pytest.mark.parametrize("case", [
+    dict(S=[3, 4, 2], O=[4, 5, 3], U=[2, 3, 2], T=2, A_deps=[[0, 2], [1, 2, 0], [1]], B_deps=[[0], [1, 0], [2, 1]]),
+    dict(S=[5, 3], O=[7], U=[3, 2], T=3, A_deps=[[1, 0]], B_deps=[[0], [1]], C2d=True),
+    dict(S=[2, 2, 2, 2], O=[3, 3], U=[2, 1, 2, 1], T=2, A_deps=[[0, 1, 2, 3], [3, 1]],
+         B_deps=[[0], [1], [2, 3], [3]]),
+    dict(S=[6], O=[4, 2], U=[5], T=1, A_deps=[[0], [0]], B_deps=[[0]]),
+])
+@pytest.mark.parametrize("flags", [(True, True), (True, False), (False, True), (False, False)])
+def test_neg_efe_random_models_match_oracle(case, flags):
+    from pymdp_b200 import ffi
+    rng = np.random.default_rng(len(case["S"]) * 7 + case["T"])
+    batch = 3
+    A, B, C, qs = random_efe(rng, case["S"], case["O"], case["U"], case["T"], case["A_deps"], case["B_deps"],
+                             batch, case.get("C2d", False))
+    pol = oefe.construct_policies(case["S"], case["U"], case["T"])
+    I = [torch.zeros((batch, 1, s), device="cuda") for s in case["S"]]
+    G = ffi.neg_efe_all_policies_ffi(pol, [cuda(q) for q in qs], [cuda(a) for a in A], [cuda(b) for b in B],
+                                     [cuda(c) for c in C], I, case["A_deps"], case["B_deps"], use_utility=flags[0],
+                                     use_states_info_gain=flags[1], use_inductive=False).cpu().numpy()
+    for b in range(batch):
+        ref = oefe.neg_efe_all_policies(pol, [q[b] for q in qs], [a[b] for a in A], [x[b] for x in B],
+                                        [c[b] for c in C], case["A_deps"], case["B_deps"], use_utility=flags[0],
+                                        use_states_info_gain=flags[1])
+        np.testing.assert_allclose(G[b], ref, rtol=G_RTOL, atol=G_ATOL)
+
+
+def test_invalid_action_gives_nan_for_that_policy():
+    from pymdp_b200 import ffi
+    rng = np.random.default_rng(0)
+    S, O, U = [3, 2], [3], [2, 1]
+    A, B, C, qs = random_efe(rng, S, O, U, 1, [[0, 1]], [[0], [1]], 1)
+    pol = oefe.construct_policies(S, U, 1)
+    pol[1, 0, 0] = 7
+    G = ffi.neg_efe_all_policies_ffi(pol, [cuda(q) for q in qs], [cuda(a) for a in A], [cuda(b) for b in B],
+                                     [cuda(c) for c in C], [torch.zeros((1, 1, s), device="cuda") for s in S],
+                                     [[0, 1]], [[0], [1]], use_inductive=False).cpu().numpy()
+    assert np.isnan(G[0, 1]) and np.isfinite(G[0, 0])
