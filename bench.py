@@ -189,7 +189,8 @@ def run_b200(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     A, B, C, D, obs = make_model(1234 + rank, AGENTS)
-    agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=AGENTS, num_iter=NUM_ITER, device=dev)
+    agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=AGENTS, num_iter=NUM_ITER, device=dev,
+                  precision=args.precision)
     obs_d = torch.as_tensor(obs, device=dev)
     prior_d = [torch.as_tensor(d, device=dev) for d in D]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -303,6 +304,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
+    ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
+                    help="EFE contraction: fp32 (SIMT), tf32x3 or bf16 (tcgen05 tensor cores)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -46,9 +46,13 @@ enum {
 #define B2_FLAG_MODEL_PARAMS_STATIC 16
 /* Precision selector, bits 8-9 of `flags` (unused by the reference ABI). */
 #define B2_PRECISION_SHIFT 8
-#define B2_PRECISION_FP32 0  /* SIMT FP32, FP32 accumulate (default)        */
-#define B2_PRECISION_TF32X3 1 /* tcgen05 kind::tf32, hi/lo split, FP32-exact */
-#define B2_PRECISION_BF16 2  /* tcgen05 kind::f16 BF16 operands, FP32 accum  */
+#define B2_PRECISION_FP32 0   /* SIMT FP32, FP32 accumulate (default)         */
+#define B2_PRECISION_TF32X3 1 /* tcgen05 kind::tf32, 3-pass hi/lo split        */
+#define B2_PRECISION_BF16 2   /* tcgen05 kind::f16 BF16 operands, FP32 accum   */
+/* The two tensor-core selectors fall back to the SIMT FP32 kernel when the
+ * model exceeds their limits (more than 8 distinct dependency tuples, more
+ * than 256 - T observation rows per tuple, or a working set above 227 KB
+ * of shared memory). */
 
 /* Message describing the last failing call on this thread ("" if none). */
 const char* b2_last_error(void);
@@ -60,6 +64,11 @@ int32_t b2_capabilities(void);
 /* Number of kernels this library has launched in this process (all entry
  * points, all devices). Lets callers count launches inside a timed region. */
 uint64_t b2_launch_count(void);
+/* Reads and clears the device error word that a kernel sets when one of its
+ * bounded waits runs out (it then stops, frees its tensor memory and exits
+ * instead of hanging). Synchronises the current device: diagnostics only.
+ * Returns 0 (no error), 1 (a wait ran out) or -1 (the read failed). */
+int32_t b2_device_error(void);
 
 /* ================================================================== FPI ==
  * Drop-in for `pymdp_fpi_cuda_native` / FpiCudaDevice

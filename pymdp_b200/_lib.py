@@ -57,6 +57,7 @@ _SIGS = {
     "b2_abi_version": (c_int32, []),
     "b2_capabilities": (c_int32, []),
     "b2_launch_count": (c_uint64, []),
+    "b2_device_error": (c_int32, []),
     "b2_fpi": (c_int32, [c_void_p, _PF, c_int64, _PF, c_int64, _PF, c_int64, _P64, c_int64, _P64, c_int64,
                          _P64, c_int64, _P64, c_int64, _P64, c_int64, c_int32]),
     "b2_fpi_obs": (c_int32, [c_void_p, _PF, c_int64, _P64, c_int64, _P64, c_int64, c_void_p, _PF, _PF,

@@ -398,8 +398,8 @@ extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64
   if (flags & B2_FLAG_USE_INDUCTIVE)
     return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": inductive planning term is not built yet");
   const int prec = (flags >> B2_PRECISION_SHIFT) & 3;
-  if (prec != B2_PRECISION_FP32)
-    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": requested precision is not built yet");
+  if (prec > B2_PRECISION_BF16)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": unknown precision selector");
   if (Bn == 0) return B2_OK;
   if (!policy_matrix || !qs_init || !A || !B || !C || !neg_efe_out)
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": null buffer");
@@ -408,6 +408,12 @@ extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64
   (void)pA;
   (void)pB;
   (void)inductive_epsilon;
+  if (prec != B2_PRECISION_FP32) {
+    // tensor-core path; models outside its limits take the SIMT FP32 path
+    bool used = false;
+    B2_TRY(launch_efe_tc(p, prec, Bn, policy_matrix, pm_batched, qs_init, A, B, C, neg_efe_out, stream, &used));
+    if (used) return B2_OK;
+  }
   float* lin = nullptr;
   const size_t bytes = (size_t)Bn * p.T * p.K_tot * sizeof(float);
   B2_TRY(ws_alloc((void**)&lin, bytes, stream, kEfeName));

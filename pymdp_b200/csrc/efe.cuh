@@ -52,5 +52,9 @@ int32_t launch_linear_rows(const EfeParams& p, int64_t Bn, const float* A, const
 int32_t launch_efe_plain(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
                          const float* A, const float* B, const float* lin, float* G, cudaStream_t stream);
 int32_t ws_alloc(void** ptr, size_t bytes, cudaStream_t stream, const char* op);
+// Tensor-core path (efe_tc.cu); *used = false when the model is outside its
+// limits and nothing was launched.
+int32_t launch_efe_tc(const EfeParams& p, int prec, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
+                      const float* A, const float* B, const float* C, float* G, cudaStream_t stream, bool* used);
 
 }  // namespace b2

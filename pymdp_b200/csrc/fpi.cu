@@ -11,24 +11,28 @@
 // stop at max|d log q| < 1e-5, fpi/fpi_cpu_core.h:245-248; its JAX path,
 // which defines the results, does not).
 //
-// Design (one warp = one agent, several agents per CTA):
+// Design (a team of 32, 128 or 256 threads per agent, by work size):
 //  * Load phase: each modality's log-likelihood block is read once from HBM
 //    with coalesced loads and written into shared memory in a padded layout
 //    whose non-innermost strides are odd, so a sweep along ANY axis by the
 //    lanes of a warp is bank-conflict free. In the fused observation form the
 //    loaded values are the observed slice A_m[o_m] (K contiguous floats) and
 //    log(clip(., eps)) is applied on the fly — ll never exists in HBM.
-//  * Precision: FP32 inputs and outputs; on-chip values are FP64. The
-//    products of two FP32 numbers are exact in FP64, so the marginal dot
-//    products and the per-factor sums carry FP64 accumulation error only
-//    (FP32 accumulation misses the 1e-5-relative posterior target vs the FP64
-//    reference on ill-conditioned Dirichlet(0.5) models; FP64 accumulation
-//    stays near 1e-6). B200 runs DFMA at half the FP32 FMA rate.
+//  * Precision: FP32 inputs and outputs; the ll blocks, marginals and log q
+//    live in FP64 on chip. The products of two FP32 numbers are exact in
+//    FP64, so the marginal dot products and the per-factor sums carry FP64
+//    accumulation error only (FP32 accumulation misses the 1e-5-relative
+//    posterior target vs the FP64 reference on ill-conditioned Dirichlet(0.5)
+//    models; FP64 accumulation stays near 1e-6). log/exp stay FP32.
+//  * Modalities with identical dependency tuples are merged at plan time
+//    (their ll blocks are summed once at load), removing duplicate
+//    contractions; the marginals are linear in ll so this is exact algebra.
 //  * Iterations run entirely on-chip: phase A = warp-shuffle softmax per
-//    factor, phase B = one output state per lane group (group size = 32/S_f
-//    rounded down to a power of two), each group summing the contributions of
-//    every (modality, axis) pair that touches the factor, then a butterfly
-//    reduction inside the group. No atomics: results are deterministic.
+//    factor, phase B = one output state per lane group (group size =
+//    team/S_f rounded down to a power of two, at most 32), each group summing
+//    the contributions of every (group, axis) pair that touches the factor,
+//    then a butterfly reduction inside the group. No atomics: results are
+//    deterministic.
 //  * Final softmax is written straight to the caller's output.
 #include <cstring>
 #include <mutex>
@@ -43,27 +47,46 @@ namespace {
 constexpr int kMaxRank = B2_MAX_DEP_RANK;
 constexpr int kMaxF = B2_MAX_FACTORS;
 constexpr int kMaxM = B2_MAX_MODALITIES;
+constexpr int kMaxContrib = 128;
 constexpr int kMaxSmemPerCta = 227 * 1024;
 
-struct FpiModality {
+// One caller modality (a source of a merged group).
+struct FpiSource {
+  int64_t src_off;  // ll form: ll_offsets[m]; fused form: A_offsets[m]
+  int32_t O;        // observation count (fused form)
+  int32_t K;        // elements of one observed slice (prod of dependency sizes)
+};
+
+// Modalities with an identical dependency tuple are merged into one group:
+// their log-likelihoods are summed once at load time, which is exact algebra
+// (every marginal is linear in ll) and removes their duplicate contractions.
+struct FpiGroup {
   int32_t sm_off;  // double offset of the padded ll block inside the agent's smem
   int32_t K;       // prod_i S[dep[i]]
-  int32_t rank;
-  int32_t O;        // observation count (fused form only)
-  int64_t src_off;  // ll form: ll_offsets[m]; fused form: A_offsets[m]
+  int8_t rank, src_begin, src_end, pad;
   int8_t dep[kMaxRank];
-  int32_t sst[kMaxRank];  // padded shared-memory stride of each axis
+  int16_t sst[kMaxRank];  // padded shared-memory stride of each axis (odd except innermost)
+};
+
+// One (factor, group axis) contraction with its addressing precomputed.
+struct FpiContrib {
+  int16_t sm_off, base_st;  // group block, stride of the output axis
+  int16_t d0, st0, q0;      // first other axis: size, smem stride, offset of its q
+  int16_t d1, st1, q1;      // second other axis (rank 3)
+  int8_t rank, ax, g, pad;
 };
 
 struct FpiParams {
-  int32_t F, M, num_iter, S_tot;
+  int32_t F, M, G, num_iter, S_tot;
   int32_t agent_words;  // shared-memory doubles per agent
   int32_t ll_sm_total;  // doubles of padded ll blocks
   int32_t S[kMaxF];
   int32_t lp_off[kMaxF + 1];
-  int32_t contrib_off[kMaxF + 1];
-  int16_t contrib[kMaxM * kMaxRank];  // m * 8 + axis, grouped by factor
-  FpiModality mod[kMaxM];
+  int32_t con_off[kMaxF + 1];
+  int8_t src_order[kMaxM];  // modalities sorted by group
+  FpiSource src[kMaxM];
+  FpiGroup grp[kMaxM];
+  FpiContrib con[kMaxContrib];
 };
 
 struct FpiIO {
@@ -75,71 +98,38 @@ struct FpiIO {
   int64_t batch;
 };
 
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
 __device__ __forceinline__ double warp_max_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
-// Softmax of n values of `in` into `out` by one warp (FP64 on-chip).
+// softmax(logq) of n values by one warp; FP32 exponentials on the
+// max-shifted FP64 logits.
 template <typename OutT>
-__device__ __forceinline__ void softmax_warp(const double* in, OutT* out, int n, int lane) {
+__device__ __forceinline__ void softmax_warp(const double* __restrict__ logq, OutT* __restrict__ out, int n,
+                                             int lane) {
   double mx = -INFINITY;
-  for (int i = lane; i < n; i += 32) mx = fmax(mx, in[i]);
+  for (int i = lane; i < n; i += 32) mx = fmax(mx, logq[i]);
   mx = warp_max_d(mx);
-  double sum = 0.0;
-  for (int i = lane; i < n; i += 32) sum += exp(in[i] - mx);
-  sum = warp_sum_d(sum);
-  for (int i = lane; i < n; i += 32) out[i] = (OutT)(exp(in[i] - mx) / sum);
+  float sum = 0.f;
+  for (int i = lane; i < n; i += 32) sum += expf((float)(logq[i] - mx));
+  sum = warp_sum(sum);
+  for (int i = lane; i < n; i += 32) out[i] = (OutT)(expf((float)(logq[i] - mx)) / sum);
 }
 
-// Contribution of modality `md` to output state `s` of its axis `ax`, summed
-// over the flattened "other" indices t = j, j+G, ... of this lane.
-__device__ __forceinline__ double contract(const FpiModality& md, const FpiParams& p,
-                                           const double* __restrict__ ll, const double* __restrict__ q,
-                                           int ax, int s, int j, int G) {
-  const double* L = ll + md.sm_off + s * md.sst[ax];
-  if (md.rank == 1) return j == 0 ? L[0] : 0.0;
-  if (md.rank == 2) {
-    const int o = 1 - ax;
-    const int d = p.S[md.dep[o]];
-    const int st = md.sst[o];
-    const double* qo = q + p.lp_off[md.dep[o]];
-    double acc = 0.0;
-    for (int t = j; t < d; t += G) acc = fma(L[t * st], qo[t], acc);
-    return acc;
-  }
-  if (md.rank == 3) {
-    const int a0 = ax == 0 ? 1 : 0;
-    const int a1 = ax == 2 ? 1 : 2;
-    const int d0 = p.S[md.dep[a0]], d1 = p.S[md.dep[a1]];
-    const int st0 = md.sst[a0], st1 = md.sst[a1];
-    const double* q0 = q + p.lp_off[md.dep[a0]];
-    const double* q1 = q + p.lp_off[md.dep[a1]];
-    const int total = d0 * d1;
-    int i0 = j / d1, i1 = j - (j / d1) * d1;
-    double acc = 0.0;
-    for (int t = j; t < total; t += G) {
-      acc = fma(L[i0 * st0 + i1 * st1], q0[i0] * q1[i1], acc);
-      i1 += G;
-      while (i1 >= d1) { i1 -= d1; ++i0; }
-    }
-    return acc;
-  }
-  // rank 4..8: mixed-radix counter over the other axes (innermost last).
+// rank >= 4: mixed-radix counter over the other axes (innermost last).
+__device__ __noinline__ double contract_generic(const FpiGroup& gr, const FpiParams& p,
+                                                const double* __restrict__ ll, const double* __restrict__ q,
+                                                int ax, int s, int j, int G) {
+  const double* L = ll + gr.sm_off + s * gr.sst[ax];
   int dd[kMaxRank - 1], st[kMaxRank - 1], qoff[kMaxRank - 1], dig[kMaxRank - 1];
   int n = 0, total = 1;
-  for (int x = 0; x < md.rank; ++x) {
+  for (int x = 0; x < gr.rank; ++x) {
     if (x == ax) continue;
-    dd[n] = p.S[md.dep[x]];
-    st[n] = md.sst[x];
-    qoff[n] = p.lp_off[md.dep[x]];
+    dd[n] = p.S[gr.dep[x]];
+    st[n] = gr.sst[x];
+    qoff[n] = p.lp_off[gr.dep[x]];
     total *= dd[n];
     ++n;
   }
@@ -166,85 +156,152 @@ __device__ __forceinline__ double contract(const FpiModality& md, const FpiParam
   return acc;
 }
 
-template <int APC, bool FUSED>
-__global__ void __launch_bounds__(32 * APC)
-    fpi_warp_kernel(const __grid_constant__ FpiParams p, const FpiIO io) {
+// Contribution of one (factor, group axis) pair to output state `s`, summed
+// over this lane's share (t = j, j+G, ...) of the other indices. FP64 FMA
+// chains, four independent accumulators for ILP.
+template <bool GENERIC>
+__device__ __forceinline__ double contract(const FpiContrib& c, const FpiParams& p, const double* __restrict__ ll,
+                                           const double* __restrict__ q, int s, int j, int G) {
+  const double* L = ll + c.sm_off + s * c.base_st;
+  if (c.rank == 1) return j == 0 ? L[0] : 0.0;
+  if (c.rank == 2) {
+    const double* qa = q + c.q0;
+    const int d = c.d0, st = c.st0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int t = j;
+    for (; t + 3 * G < d; t += 4 * G) {
+      a0 = fma(L[t * st], qa[t], a0);
+      a1 = fma(L[(t + G) * st], qa[t + G], a1);
+      a2 = fma(L[(t + 2 * G) * st], qa[t + 2 * G], a2);
+      a3 = fma(L[(t + 3 * G) * st], qa[t + 3 * G], a3);
+    }
+    for (; t < d; t += G) a0 = fma(L[t * st], qa[t], a0);
+    return (a0 + a1) + (a2 + a3);
+  }
+  if (c.rank == 3) {
+    const double* qa = q + c.q0;
+    const double* qb = q + c.q1;
+    const int d1 = c.d1, st0 = c.st0, st1 = c.st1;
+    const int total = c.d0 * d1;
+    int i0 = j / d1, i1 = j - i0 * d1;
+    double a0 = 0.0, a1 = 0.0;
+    int t = j;
+    for (; t + G < total; t += 2 * G) {
+      a0 = fma(L[i0 * st0 + i1 * st1], qa[i0] * qb[i1], a0);
+      i1 += G;
+      while (i1 >= d1) { i1 -= d1; ++i0; }
+      a1 = fma(L[i0 * st0 + i1 * st1], qa[i0] * qb[i1], a1);
+      i1 += G;
+      while (i1 >= d1) { i1 -= d1; ++i0; }
+    }
+    if (t < total) a0 = fma(L[i0 * st0 + i1 * st1], qa[i0] * qb[i1], a0);
+    return a0 + a1;
+  }
+  if (GENERIC) return contract_generic(p.grp[c.g], p, ll, q, c.ax, s, j, G);
+  return 0.0;
+}
+
+template <int TEAM>
+__device__ __forceinline__ void team_sync() {
+  if (TEAM == 32) __syncwarp(); else __syncthreads();
+}
+
+// TEAM threads per agent: TEAM = 32 runs APC agents (one per warp) per CTA;
+// TEAM > 32 runs one agent per CTA of TEAM threads. GENERIC adds the
+// rank >= 4 contraction path (kept out of the rank <= 3 instantiations so
+// their hot loop has no call and no local memory).
+template <int TEAM, int APC, bool FUSED, bool GENERIC>
+__global__ void __launch_bounds__(TEAM * APC)
+    fpi_kernel(const __grid_constant__ FpiParams p, const FpiIO io) {
   extern __shared__ double smem_d[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t b = (int64_t)blockIdx.x * APC + warp;
-  if (b >= io.batch) return;  // whole warp leaves; only warp-level syncs below
-  double* ll = smem_d + warp * p.agent_words;
+  const int slot = threadIdx.x / TEAM;
+  const int t = threadIdx.x % TEAM;
+  const int lane = threadIdx.x & 31;
+  const int wid = t >> 5;
+  const int64_t b = (int64_t)blockIdx.x * APC + slot;
+  if (b >= io.batch) return;  // TEAM > 32: APC == 1, uniform over the CTA
+  double* ll = smem_d + slot * p.agent_words;
   double* lp = ll + p.ll_sm_total;
   double* logq = lp + p.S_tot;
   double* q = logq + p.S_tot;
 
-  // ---- load phase: ll blocks (fused: observed log-A slices) and log prior
+  // ---- load phase: merged ll blocks (fused: observed log-A slices) + log prior
+  // Each source's row start (agent offset + observed slice) is resolved once
+  // into shared memory before the element loop.
+  int64_t* rowoff = reinterpret_cast<int64_t*>(q + p.S_tot);
   bool bad_obs = false;
-  for (int m = 0; m < p.M; ++m) {
-    const FpiModality& md = p.mod[m];
-    const float* src = io.src + b * io.src_stride + md.src_off;
+  if (FUSED) {
+    for (int m = 0; m < p.M; ++m) {
+      const int o = io.obs[b * p.M + m];
+      bad_obs |= (o < 0 || o >= p.src[m].O);
+    }
+  }
+  for (int m = t; m < p.M; m += TEAM) {
+    int64_t r = b * io.src_stride + p.src[m].src_off;
     if (FUSED) {
       int o = io.obs[b * p.M + m];
-      if (o < 0 || o >= md.O) {
-        bad_obs = true;
-        o = 0;
-      }
-      src += (int64_t)o * md.K;
+      o = (o < 0 || o >= p.src[m].O) ? 0 : o;
+      r += (int64_t)o * p.src[m].K;
     }
-    for (int k = lane; k < md.K; k += 32) {
-      double v = (double)__ldg(src + k);
-      if (FUSED) v = log(fmax(v, (double)kMinVal));
+    rowoff[m] = r;
+  }
+  team_sync<TEAM>();
+  for (int g = 0; g < p.G; ++g) {
+    const FpiGroup& gr = p.grp[g];
+    for (int k = t; k < gr.K; k += TEAM) {
+      double v = 0.0;
+      for (int si = gr.src_begin; si < gr.src_end; ++si) {
+        const float a = __ldg(io.src + rowoff[p.src_order[si]] + k);
+        v += FUSED ? (double)logf(fmaxf(a, kMinVal)) : (double)a;
+      }
       int rem = k, addr = 0;
-      for (int x = md.rank - 1; x > 0; --x) {
-        const int d = p.S[md.dep[x]];
+      for (int x = gr.rank - 1; x > 0; --x) {
+        const int d = p.S[gr.dep[x]];
         const int qd = rem / d;
-        addr += (rem - qd * d) * md.sst[x];
+        addr += (rem - qd * d) * gr.sst[x];
         rem = qd;
       }
-      addr += rem * md.sst[0];
-      ll[md.sm_off + addr] = v;
+      addr += rem * gr.sst[0];
+      ll[gr.sm_off + addr] = v;
     }
   }
-  for (int i = lane; i < p.S_tot; i += 32) {
-    const double v = (double)__ldg(io.prior + b * p.S_tot + i);
-    lp[i] = FUSED ? log(fmax(v, (double)kMinVal)) : v;
+  for (int i = t; i < p.S_tot; i += TEAM) {
+    const float v = __ldg(io.prior + b * p.S_tot + i);
+    lp[i] = FUSED ? (double)logf(fmaxf(v, kMinVal)) : (double)v;
     logq[i] = 0.0;
   }
-  __syncwarp();
+  team_sync<TEAM>();
 
   // ---- fixed-point iterations (Jacobi: every factor uses the previous q)
   for (int it = 0; it < p.num_iter; ++it) {
-    for (int f = 0; f < p.F; ++f) softmax_warp(logq + p.lp_off[f], q + p.lp_off[f], p.S[f], lane);
-    __syncwarp();
+    for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp(logq + p.lp_off[f], q + p.lp_off[f], p.S[f], lane);
+    team_sync<TEAM>();
     for (int f = 0; f < p.F; ++f) {
       const int Sf = p.S[f];
-      const int per = Sf >= 32 ? 1 : 32 / Sf;
-      const int G = 1 << (31 - __clz(per));  // lanes per output, power of two
-      const int groups = 32 / G;
-      const int c0 = p.contrib_off[f], c1 = p.contrib_off[f + 1];
+      int per = TEAM / Sf;
+      per = per < 1 ? 1 : (per > 32 ? 32 : per);
+      const int G = 1 << (31 - __clz(per));  // lanes per output, power of two <= 32
+      const int groups = TEAM / G;
+      const int c0 = p.con_off[f], c1 = p.con_off[f + 1];
       for (int s0 = 0; s0 < Sf; s0 += groups) {
-        const int s = s0 + lane / G;
-        const int j = lane & (G - 1);
+        const int s = s0 + t / G;
+        const int j = t & (G - 1);
         double acc = 0.0;
-        if (s < Sf) {
-          for (int c = c0; c < c1; ++c) {
-            const int m = p.contrib[c] >> 3, ax = p.contrib[c] & 7;
-            acc += contract(p.mod[m], p, ll, q, ax, s, j, G);
-          }
-        }
+        if (s < Sf)
+          for (int c = c0; c < c1; ++c) acc += contract<GENERIC>(p.con[c], p, ll, q, s, j, G);
         for (int o = G >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (s < Sf && j == 0) logq[p.lp_off[f] + s] = acc + lp[p.lp_off[f] + s];
       }
     }
-    __syncwarp();
+    team_sync<TEAM>();
   }
 
   // ---- posterior marginals
   float* out = io.q_out + b * p.S_tot;
-  for (int f = 0; f < p.F; ++f) softmax_warp(logq + p.lp_off[f], out + p.lp_off[f], p.S[f], lane);
+  for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp(logq + p.lp_off[f], out + p.lp_off[f], p.S[f], lane);
   if (FUSED && bad_obs) {
-    __syncwarp();
-    for (int i = lane; i < p.S_tot; i += 32) out[i] = __int_as_float(0x7fc00000);
+    team_sync<TEAM>();
+    for (int i = t; i < p.S_tot; i += TEAM) out[i] = __int_as_float(0x7fc00000);
   }
 }
 
@@ -257,10 +314,11 @@ std::string idx(const char* name, int64_t i) { return std::string(name) + "[" + 
 // validate_fpi_attrs / build_modality_dispatch / check_distinct_modality_factor
 // (pymdp/ffi/fpi/fpi_entry.h:24-82, fpi/fpi_precompute.h:56-112) and in
 // addition checks that offsets are the prefix sums the layout implies.
-int32_t build_params(FpiParams* p, const int64_t* S, int64_t F, const int64_t* lp_offsets,
-                     int64_t lp_offsets_len, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
-                     const int64_t* A_dep_offsets, int64_t A_dep_offsets_len, int32_t num_iter,
-                     const char* op) {
+// Fills everything except p->src[m] (set by the entry point).
+int32_t build_params(FpiParams* p, std::vector<int64_t>* Kmod, const int64_t* S, int64_t F,
+                     const int64_t* lp_offsets, int64_t lp_offsets_len, const int64_t* A_dep_flat,
+                     int64_t A_dep_flat_len, const int64_t* A_dep_offsets, int64_t A_dep_offsets_len,
+                     int32_t num_iter, const char* op) {
   std::memset(p, 0, sizeof(*p));
   const int64_t M = A_dep_offsets_len - 1;
   if (F <= 0 || M <= 0)
@@ -288,7 +346,7 @@ int32_t build_params(FpiParams* p, const int64_t* S, int64_t F, const int64_t* l
     p->S[f] = (int32_t)S[f];
     p->lp_off[f] = (int32_t)off;
     off += S[f];
-    if (off > 32767) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": total_S exceeds 32767");
+    if (off > 16384) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": total_S exceeds 16384");
   }
   if (lp_offsets && lp_offsets[F] != off)
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": lp_offsets must be the prefix sums of S");
@@ -296,8 +354,10 @@ int32_t build_params(FpiParams* p, const int64_t* S, int64_t F, const int64_t* l
   p->S_tot = (int32_t)off;
   if (A_dep_offsets[0] != 0)
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_dep_offsets must start at zero");
-  std::vector<std::vector<int>> contrib(F);
-  int64_t sm = 0;
+  // validate modalities and group identical dependency tuples
+  std::vector<std::vector<int64_t>> tuples;
+  std::vector<int> group_of(M);
+  Kmod->assign(M, 1);
   for (int64_t m = 0; m < M; ++m) {
     if (A_dep_offsets[m + 1] < A_dep_offsets[m])
       return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_dep_offsets must be monotonic");
@@ -308,43 +368,97 @@ int32_t build_params(FpiParams* p, const int64_t* S, int64_t F, const int64_t* l
                                                std::to_string(kMaxRank) + "]");
     if (A_dep_offsets[m + 1] > A_dep_flat_len)
       return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_dep_flat shorter than A_dep_offsets");
-    FpiModality& md = p->mod[m];
-    md.rank = (int32_t)rank;
+    std::vector<int64_t> tup;
     int64_t K = 1;
     for (int64_t i = 0; i < rank; ++i) {
       const int64_t d = A_dep_flat[A_dep_offsets[m] + i];
       if (d < 0 || d >= F)
         return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": modality " + std::to_string(m) +
                                                  " A_dep factor " + std::to_string(d) + " out of range");
-      for (int64_t i2 = 0; i2 < i; ++i2)
-        if (md.dep[i2] == d)
+      for (int64_t d2 : tup)
+        if (d2 == d)
           return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": modality " + std::to_string(m) +
                                                    " has duplicate factor in A_dependencies");
-      md.dep[i] = (int8_t)d;
+      tup.push_back(d);
       K *= S[d];
-      contrib[d].push_back((int)(m * 8 + i));
+      if (K > (1 << 24)) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": modality too large");
     }
-    if (K > (1 << 24)) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": modality too large");
-    md.K = (int32_t)K;
-    // padded strides: innermost 1, every other stride odd
-    int64_t st = 1;
-    for (int64_t x = rank - 1; x >= 0; --x) {
-      md.sst[x] = (int32_t)st;
-      st = st * S[md.dep[x]];
+    (*Kmod)[m] = K;
+    p->src[m].K = (int32_t)K;
+    int g = -1;
+    for (size_t i = 0; i < tuples.size(); ++i)
+      if (tuples[i] == tup) g = (int)i;
+    if (g < 0) {
+      g = (int)tuples.size();
+      tuples.push_back(tup);
+    }
+    group_of[m] = g;
+  }
+  p->G = (int32_t)tuples.size();
+  int n_src = 0;
+  int64_t sm = 0;
+  std::vector<std::vector<FpiContrib>> con(F);
+  for (int g = 0; g < p->G; ++g) {
+    FpiGroup& gr = p->grp[g];
+    const std::vector<int64_t>& tup = tuples[g];
+    const int rank = (int)tup.size();
+    gr.rank = (int8_t)rank;
+    gr.src_begin = (int8_t)n_src;
+    for (int64_t m = 0; m < M; ++m)
+      if (group_of[m] == g) p->src_order[n_src++] = (int8_t)m;
+    gr.src_end = (int8_t)n_src;
+    int64_t K = 1;
+    for (int i = 0; i < rank; ++i) {
+      gr.dep[i] = (int8_t)tup[i];
+      K *= S[tup[i]];
+    }
+    gr.K = (int32_t)K;
+    int64_t st = 1;  // padded strides: innermost 1, every other stride odd
+    for (int x = rank - 1; x >= 0; --x) {
+      if (st > 32767) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": modality too large for shared memory");
+      gr.sst[x] = (int16_t)st;
+      st = st * S[tup[x]];
       if (x > 0 && (st % 2) == 0) st += 1;
     }
-    const int64_t footprint = (int64_t)md.sst[0] * S[md.dep[0]];
-    md.sm_off = (int32_t)sm;
+    const int64_t footprint = (int64_t)gr.sst[0] * S[tup[0]];
+    gr.sm_off = (int32_t)sm;
     sm += (footprint + 1) / 2 * 2;  // 16-byte aligned blocks
+    if (sm > 32767) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": log-likelihood blocks exceed shared memory");
+    for (int ax = 0; ax < rank; ++ax) {
+      FpiContrib c;
+      std::memset(&c, 0, sizeof(c));
+      c.sm_off = (int16_t)gr.sm_off;
+      c.base_st = gr.sst[ax];
+      c.rank = (int8_t)rank;
+      c.ax = (int8_t)ax;
+      c.g = (int8_t)g;
+      int n_other = 0;
+      for (int x = 0; x < rank && rank <= 3; ++x) {
+        if (x == ax) continue;
+        const int16_t d = (int16_t)S[tup[x]], stx = gr.sst[x], qx = (int16_t)p->lp_off[tup[x]];
+        if (n_other == 0) {
+          c.d0 = d; c.st0 = stx; c.q0 = qx;
+        } else {
+          c.d1 = d; c.st1 = stx; c.q1 = qx;
+        }
+        ++n_other;
+      }
+      con[tup[ax]].push_back(c);
+    }
   }
   int n = 0;
   for (int64_t f = 0; f < F; ++f) {
-    p->contrib_off[f] = n;
-    for (int c : contrib[f]) p->contrib[n++] = (int16_t)c;
+    p->con_off[f] = n;
+    for (const FpiContrib& c : con[f]) {
+      if (n >= kMaxContrib)
+        return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": more than " + std::to_string(kMaxContrib) +
+                                            " (factor, modality) contractions");
+      p->con[n++] = c;
+    }
   }
-  p->contrib_off[F] = n;
+  p->con_off[F] = n;
   p->ll_sm_total = (int32_t)sm;
-  const int64_t agent = sm + 3 * off;
+  const int64_t agent = sm + 3 * off + M;  // ll | lp | logq | q | per-source row offsets
   p->agent_words = (int32_t)((agent + 1) / 2 * 2);
   if ((int64_t)p->agent_words * 8 > kMaxSmemPerCta)
     return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": per-agent working set of " +
@@ -353,30 +467,45 @@ int32_t build_params(FpiParams* p, const int64_t* S, int64_t F, const int64_t* l
   return B2_OK;
 }
 
+// Multiply-adds per agent per iteration: sum over groups of rank * K.
+int64_t work_per_iter(const FpiParams& p) {
+  int64_t w = 0;
+  for (int g = 0; g < p.G; ++g) w += (int64_t)p.grp[g].rank * p.grp[g].K;
+  return w;
+}
+
+template <int TEAM, int APC, bool FUSED>
+int32_t launch_one(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const char* op) {
+  const int bytes = APC * p.agent_words * 8;
+  const int64_t grid = (io.batch + APC - 1) / APC;
+  if (grid > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
+  bool generic = false;
+  for (int g = 0; g < p.G; ++g) generic |= p.grp[g].rank > 3;
+  const void* k = generic ? (const void*)fpi_kernel<TEAM, APC, FUSED, true>
+                          : (const void*)fpi_kernel<TEAM, APC, FUSED, false>;
+  B2_TRY(ensure_smem_attr(k, bytes, op));
+  if (generic)
+    fpi_kernel<TEAM, APC, FUSED, true><<<(unsigned)grid, TEAM * APC, bytes, stream>>>(p, io);
+  else
+    fpi_kernel<TEAM, APC, FUSED, false><<<(unsigned)grid, TEAM * APC, bytes, stream>>>(p, io);
+  return check_launch(op);
+}
+
 template <bool FUSED>
 int32_t launch(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const char* op) {
   if (io.batch <= 0) return B2_OK;
+  const int64_t work = work_per_iter(p);
   const int bytes_agent = p.agent_words * 8;
+  if (work >= 8192) return launch_one<256, 1, FUSED>(p, io, stream, op);
+  if (work >= 4096 || bytes_agent > 48 * 1024) return launch_one<128, 1, FUSED>(p, io, stream, op);
   int apc = 8;
   while (apc > 1 && (apc * bytes_agent > 64 * 1024 || apc / 2 >= io.batch)) apc >>= 1;
-  const int bytes = apc * bytes_agent;
-  const int64_t grid = (io.batch + apc - 1) / apc;
-  if (grid > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
-  const void* k = nullptr;
   switch (apc) {
-    case 8: k = (const void*)fpi_warp_kernel<8, FUSED>; break;
-    case 4: k = (const void*)fpi_warp_kernel<4, FUSED>; break;
-    case 2: k = (const void*)fpi_warp_kernel<2, FUSED>; break;
-    default: k = (const void*)fpi_warp_kernel<1, FUSED>; break;
+    case 8: return launch_one<32, 8, FUSED>(p, io, stream, op);
+    case 4: return launch_one<32, 4, FUSED>(p, io, stream, op);
+    case 2: return launch_one<32, 2, FUSED>(p, io, stream, op);
+    default: return launch_one<32, 1, FUSED>(p, io, stream, op);
   }
-  B2_TRY(ensure_smem_attr(k, bytes, op));
-  switch (apc) {
-    case 8: fpi_warp_kernel<8, FUSED><<<(unsigned)grid, 256, bytes, stream>>>(p, io); break;
-    case 4: fpi_warp_kernel<4, FUSED><<<(unsigned)grid, 128, bytes, stream>>>(p, io); break;
-    case 2: fpi_warp_kernel<2, FUSED><<<(unsigned)grid, 64, bytes, stream>>>(p, io); break;
-    default: fpi_warp_kernel<1, FUSED><<<(unsigned)grid, 32, bytes, stream>>>(p, io); break;
-  }
-  return check_launch(op);
 }
 
 }  // namespace
@@ -398,16 +527,17 @@ extern "C" int32_t b2_fpi(void* stream, const float* ll_flat, int64_t ll_count, 
                                              std::to_string(ll_offsets_len) + ", expected " +
                                              std::to_string(M + 1));
   FpiParams p;
-  B2_TRY(build_params(&p, S, S_len, lp_offsets, lp_offsets_len, A_dep_flat, A_dep_flat_len, A_dep_offsets,
+  std::vector<int64_t> K;
+  B2_TRY(build_params(&p, &K, S, S_len, lp_offsets, lp_offsets_len, A_dep_flat, A_dep_flat_len, A_dep_offsets,
                       A_dep_offsets_len, num_iter, op));
   if (ll_offsets[0] != 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": ll_offsets must start at zero");
   for (int64_t m = 0; m < M; ++m) {
     if (ll_offsets[m + 1] < ll_offsets[m])
       return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": ll_offsets must be monotonic");
-    if (ll_offsets[m + 1] - ll_offsets[m] != p.mod[m].K)
+    if (ll_offsets[m + 1] - ll_offsets[m] != K[m])
       return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": ll_offsets inconsistent with S/A_dep for modality " +
                                                std::to_string(m));
-    p.mod[m].src_off = ll_offsets[m];
+    p.src[m].src_off = ll_offsets[m];
   }
   const int64_t total_S = p.S_tot, total_ll = ll_offsets[M];
   if (lp_count <= 0 || lp_count % total_S != 0)
@@ -440,16 +570,17 @@ extern "C" int32_t b2_fpi_obs(void* stream, const float* A_flat, int64_t A_agent
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": O / A_offsets sizes inconsistent with M = " +
                                              std::to_string(M));
   FpiParams p;
-  B2_TRY(build_params(&p, S, S_len, nullptr, 0, A_dep_flat, A_dep_flat_len, A_dep_offsets, A_dep_offsets_len,
+  std::vector<int64_t> K;
+  B2_TRY(build_params(&p, &K, S, S_len, nullptr, 0, A_dep_flat, A_dep_flat_len, A_dep_offsets, A_dep_offsets_len,
                       num_iter, op));
   if (A_offsets[0] != 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_offsets must start at zero");
   for (int64_t m = 0; m < M; ++m) {
     if (O[m] <= 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": " + idx("O", m) + " must be positive");
-    if (A_offsets[m + 1] - A_offsets[m] != O[m] * p.mod[m].K)
+    if (A_offsets[m + 1] - A_offsets[m] != O[m] * K[m])
       return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_offsets inconsistent with O/deps for modality " +
                                                std::to_string(m));
-    p.mod[m].src_off = A_offsets[m];
-    p.mod[m].O = (int32_t)O[m];
+    p.src[m].src_off = A_offsets[m];
+    p.src[m].O = (int32_t)O[m];
   }
   if (batch < 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": negative batch");
   if (A_agent_stride != 0 && A_agent_stride < A_offsets[M])

@@ -95,3 +95,56 @@ def test_invalid_action_gives_nan_for_that_policy():
                                      [cuda(c) for c in C], [torch.zeros((1, 1, s), device="cuda") for s in S],
                                      [[0, 1]], [[0], [1]], use_inductive=False).cpu().numpy()
     assert np.isnan(G[0, 1]) and np.isfinite(G[0, 0])
+
+
+# ---------------------------------------------------------- tensor-core paths
+# TF32x3 (tcgen05 kind::tf32, hi/lo split) is held to the FP32 tolerance; BF16
+# (kind::f16) to the BF16 tier: G within 1e-3 relative of its scale.
+TC_TOL = {"tf32x3": (G_RTOL, G_ATOL), "bf16": (0.0, 1e-3)}
+
+
+def _g_close(G, ref, precision):
+    rtol, atol = TC_TOL[precision]
+    if precision == "bf16":
+        scale = np.maximum(np.abs(ref).max(), 1.0)
+        np.testing.assert_allclose(G, ref, rtol=0, atol=atol * scale * 4)
+    else:
+        np.testing.assert_allclose(G, ref, rtol=rtol, atol=atol)
+
+
+@pytest.mark.parametrize("precision", ["tf32x3", "bf16"])
+@pytest.mark.parametrize("name", EFE)
+def test_tensor_core_neg_efe_matches_reference(name, precision):
+    from pymdp_b200 import _lib
+    d = load_golden(name)
+    G, q_pi, act = run_golden(d, precision)
+    assert _lib.load().b2_device_error() == 0
+    _g_close(G, d["G"], precision)
+    if precision == "tf32x3":
+        np.testing.assert_allclose(q_pi, d["q_pi"], rtol=Q_RTOL, atol=Q_ATOL)
+        np.testing.assert_array_equal(act, d["action"])
+
+
+@pytest.mark.parametrize("precision", ["tf32x3", "bf16"])
+@pytest.mark.parametrize("case", [
+    dict(S=[3, 4, 2], O=[4, 5, 3], U=[2, 3, 2], T=2, A_deps=[[0, 2], [1, 2, 0], [1]], B_deps=[[0], [1, 0], [2, 1]]),
+    dict(S=[5, 3], O=[7], U=[3, 2], T=3, A_deps=[[1, 0]], B_deps=[[0], [1]], C2d=True),
+    dict(S=[9, 7, 5], O=[11, 3, 6], U=[4, 3, 1], T=2, A_deps=[[0, 1, 2], [0, 1, 2], [2, 0]], B_deps=[[0], [1], [2]]),
+    dict(S=[32, 16, 8], O=[16, 16, 8, 8, 4], U=[4, 4, 1], T=2, A_deps=[[0, 1, 2]] * 5, B_deps=[[0], [1], [2]]),
+])
+def test_tensor_core_random_models_match_oracle(case, precision):
+    from pymdp_b200 import _lib, ffi
+    rng = np.random.default_rng(len(case["S"]) * 11 + case["T"])
+    batch = 2
+    A, B, C, qs = random_efe(rng, case["S"], case["O"], case["U"], case["T"], case["A_deps"], case["B_deps"],
+                             batch, case.get("C2d", False))
+    pol = oefe.construct_policies(case["S"], case["U"], case["T"])
+    I = [torch.zeros((batch, 1, s), device="cuda") for s in case["S"]]
+    G = ffi.neg_efe_all_policies_ffi(pol, [cuda(q) for q in qs], [cuda(a) for a in A], [cuda(b) for b in B],
+                                     [cuda(c) for c in C], I, case["A_deps"], case["B_deps"], use_inductive=False,
+                                     precision=precision).cpu().numpy()
+    assert _lib.load().b2_device_error() == 0
+    for b in range(batch):
+        ref = oefe.neg_efe_all_policies(pol, [q[b] for q in qs], [a[b] for a in A], [x[b] for x in B],
+                                        [c[b] for c in C], case["A_deps"], case["B_deps"])
+        _g_close(G[b], ref, precision)
