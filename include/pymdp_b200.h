@@ -50,9 +50,9 @@ enum {
 #define B2_PRECISION_TF32X3 1 /* tcgen05 kind::tf32, 3-pass hi/lo split        */
 #define B2_PRECISION_BF16 2   /* tcgen05 kind::f16 BF16 operands, FP32 accum   */
 /* The two tensor-core selectors fall back to the SIMT FP32 kernel when the
- * model exceeds their limits (more than 8 distinct dependency tuples, more
- * than 256 - T observation rows per tuple, or a working set above 227 KB
- * of shared memory). */
+ * model exceeds their limits (more than 8 distinct dependency tuples, a
+ * dependency tuple of rank above 4, more than 256 - T observation rows per
+ * tuple, or a working set above 227 KB of shared memory). */
 
 /* Message describing the last failing call on this thread ("" if none). */
 const char* b2_last_error(void);

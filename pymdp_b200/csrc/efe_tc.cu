@@ -52,17 +52,16 @@ __device__ int g_b2_device_error = 0;
 namespace {
 
 constexpr int kTcMaxGroups = 8;
-constexpr int kTcThreads = 256;
 constexpr int kTcTile = 128;
-constexpr int kTcStages = 3;
 constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kTcMaxOuter = 3;  // tensor-core path: dependency rank <= 4
 
 struct TcGroup {
   int64_t pack_off;  // per-agent byte offset of this group's W image
   int32_t K;         // prod of the dependency sizes
   int32_t outer;     // K / dim[rank-1]
   int32_t Kpad;      // padded K (innermost size rounded to a power of two, then to the chunk)
-  int32_t nch;       // Kpad / chunk
+  int32_t nch;       // Kpad / chunk (a multiple of the chunks per stage)
   int32_t N, n_obs;  // rows: [0, n_obs) observations, then one linear row per step, then zeros
   int32_t rank, m_begin, m_end;
   int32_t lg;           // log2 of the padded innermost size
@@ -76,7 +75,10 @@ struct TcGroup {
 struct TcParams {
   int32_t G, Nmax;
   int32_t nacc;       // TMEM accumulators the K chunks rotate over (summed in FP64)
-  int32_t tmem_cols;  // allocated TMEM columns (power of two >= nacc * Nmax)
+  int32_t b_words;    // floats of B staged in shared memory per CTA (0 = read B from global)
+  int32_t a_col;      // first TMEM column of the A (X) stages; accumulators start at column 0
+  int32_t tmem_cols;  // allocated TMEM columns
+  int32_t pre_cap;    // outer indices the shared prefix table holds (>= every group's outer)
   int64_t pack_stride;  // bytes of W images per agent
   int8_t mod_order[B2_MAX_MODALITIES];
   TcGroup grp[kTcMaxGroups];
@@ -84,17 +86,24 @@ struct TcParams {
 
 template <int PREC>
 struct TcTraits;
+// kChunk: K elements per 128-byte row (one chunk); kCps: chunks per pipeline
+// stage (the MMA issuer handles kCps * 4 K-steps per handshake); kNst:
+// pipeline stages.
 template <>
 struct TcTraits<B2_PRECISION_BF16> {
-  static constexpr int kChunk = 64;  // K elements per 128-byte row
+  static constexpr int kChunk = 64;
   static constexpr int kPlanes = 1;
   static constexpr int kEsz = 2;
+  static constexpr int kCps = 2;
+  static constexpr int kNst = 4;
 };
 template <>
 struct TcTraits<B2_PRECISION_TF32X3> {
   static constexpr int kChunk = 32;
   static constexpr int kPlanes = 2;  // hi, lo
   static constexpr int kEsz = 4;
+  static constexpr int kCps = 1;
+  static constexpr int kNst = 3;
 };
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) {
@@ -202,335 +211,425 @@ __global__ void efe_tc_pack_kernel(const __grid_constant__ EfeParams p, const __
   }
 }
 
-// ------------------------------------------------------ X generation
-// This thread's H values of X[policy, k0 .. k0+H): the Kronecker product of
-// the policy's factor marginals in the group's K order. q is laid out
-// [state][128 policies]. DLP = padded innermost size when DLP <= H (then the
-// H values are H/DLP runs of pre * ql[0..DLP) with ql held in registers);
-// DLP = 0 selects the general path (padded innermost size > H).
-template <int H, int DLP>
-__device__ __forceinline__ void gen_x(const TcGroup& gr, const EfeParams& p, const float* __restrict__ q, int pl,
-                                      int k0, const float (&ql)[DLP > 0 ? DLP : 1], float (&out)[H]) {
-  const int r = gr.rank;
-  const int lg = gr.lg;
-  int ko = k0 >> lg;  // outer index of the first element
-  // outer digits dig[0 .. r-2] of ko (row-major over dim[0 .. r-2])
-  int dig[B2_MAX_DEP_RANK - 1];
-  {
-    int rem = ko;
-#pragma unroll
-    for (int j = B2_MAX_DEP_RANK - 2; j >= 0; --j) {
-      dig[j] = 0;
-      if (j < r - 1) {
-        const int d = gr.dim[j];
-        const int qd = rem / d;
-        dig[j] = rem - qd * d;
-        rem = qd;
-      }
-    }
+// Bounded mbarrier wait that also gives up as soon as another role of the
+// CTA has flagged an abort (so one timeout cannot cascade into long waits).
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 255 && *abort_flag) return false;
   }
-  // prefix product over dig[0 .. r-3] and the last outer factor's q base
-  auto prefix2 = [&]() {
-    float v = 1.f;
-#pragma unroll
-    for (int j = 0; j < B2_MAX_DEP_RANK - 2; ++j)
-      if (j < r - 2) v *= q[(p.qs_off[gr.dep[j]] + dig[j]) * kTcTile + pl];
-    return v;
-  };
-  float P2 = prefix2();
-  const float* q_r2 = r >= 2 ? q + p.qs_off[gr.dep[r - 2]] * kTcTile + pl : nullptr;
-  if (DLP > 0) {
-    constexpr int kRuns = DLP > 0 ? H / DLP : 1;
-#pragma unroll
-    for (int run = 0; run < kRuns; ++run) {
-      float pre = 0.f;
-      if (ko + run < gr.outer) pre = r >= 2 ? P2 * q_r2[dig[r - 2] * kTcTile] : 1.f;
-#pragma unroll
-      for (int i = 0; i < (DLP > 0 ? DLP : 1); ++i) out[run * (DLP > 0 ? DLP : 1) + i] = pre * ql[i];
-      if (run + 1 < kRuns && r >= 2) {
-        // advance the outer index by one (carry through the outer digits)
-        if (++dig[r - 2] >= gr.dim[r - 2]) {
-          dig[r - 2] = 0;
-          bool carry = true;
-#pragma unroll
-          for (int j = B2_MAX_DEP_RANK - 3; j >= 0; --j) {
-            if (carry && j < r - 2) {
-              if (++dig[j] < gr.dim[j]) carry = false;
-              else dig[j] = 0;
-            }
-          }
-          P2 = prefix2();
-        }
-      }
-    }
-  } else {
-    const int off = k0 & ((1 << lg) - 1);
-    const int dl = gr.dim[r - 1];
-    float pre = 0.f;
-    if (ko < gr.outer) pre = r >= 2 ? P2 * q_r2[dig[r - 2] * kTcTile] : 1.f;
-    const float* qlp = q + p.qs_off[gr.dep[r - 1]] * kTcTile + pl;
-#pragma unroll
-    for (int i = 0; i < H; ++i) out[i] = (off + i < dl) ? pre * qlp[(off + i) * kTcTile] : 0.f;
-  }
+  *abort_flag = 1;
+  return false;
+}
+
+// One lane polls, the warp follows: keeps 512 producer threads from
+// flooding the barrier unit that the MMA issuer also needs.
+__device__ __forceinline__ void warp_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int lane) {
+  if (lane == 0) wait_or_abort(bar, parity, abort_flag);
+  __syncwarp();
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
 }
 
 struct TcSmem {
-  uint8_t* Xs;
   uint8_t* Ws;
-  uint64_t* done;  // per stage: MMAs reading the stage finished
-  uint64_t* full;  // per stage: W bulk copy landed
+  float* pre;          // [pre_cap][128]: prefix product over the outer factors per policy
+  uint64_t* x_full;    // per stage: the producer warps wrote X into tensor memory AND the W
+                       // bulk copy landed (16 producer arrivals + the loader's expect_tx)
+  uint64_t* done;      // per stage: the MMAs reading the stage finished (tcgen05.commit)
+  uint64_t* acc_full;  // all MMAs of a (step, group) GEMM finished
+  uint64_t* acc_free;  // the epilogue has read the accumulators
   volatile int* abort_flag;
-  int xs_bytes, ws_bytes;
+  int ws_bytes;
 };
 
-// All chunks of one (step, group) GEMM: produce X, bulk-copy W, issue UMMAs.
-template <int PREC, int DLP>
-__device__ __forceinline__ void run_group(const TcGroup& gr, const TcParams& tp, const EfeParams& p,
-                                          const float* __restrict__ q, const uint8_t* __restrict__ wimg,
-                                          const TcSmem& sm, uint32_t tmem, int tid, int pl, int half, bool active,
-                                          uint32_t& it) {
+// ------------------------------------------------------ X generation
+// X[p, k] for the group's K order (innermost factor last, its size padded to
+// DLP = 2^lg) is pre[p][k >> lg] * q_inner[p][k & (DLP-1)], where pre is the
+// product of the outer factors' marginals. Producers first write this
+// policy's pre values into shared memory (once per step and group); a chunk
+// is then one shared-memory read and Q multiplies per thread.
+//   MODE 0: DLP <= Q: Q/DLP runs of pre * q_inner[0..DLP), q_inner in registers
+//   MODE 1: Q < DLP <= chunk: one run segment at a fixed offset, in registers
+//   MODE 2: DLP > chunk: one run segment at a varying offset, read per chunk
+template <int PREC, int MODE, int DLP>
+__device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams& tp, const EfeParams& p,
+                                              const float* __restrict__ q, const TcSmem& sm, uint32_t tmem, int warp,
+                                              int pl, int qt, int lane, bool active, uint32_t& it) {
   using Tr = TcTraits<PREC>;
-  constexpr int H = Tr::kChunk / 2;
-  constexpr int kQl = DLP > 0 ? DLP : 1;
+  constexpr int CH = Tr::kChunk;
+  constexpr int Q = CH / 4;
+  constexpr int CPS = Tr::kCps;
+  constexpr int NST = Tr::kNst;
+  constexpr int kPl = Tr::kPlanes;
+  constexpr int kQl = MODE == 0 ? DLP : (MODE == 1 ? Q : 1);
+  const int lg = gr.lg;
+  const int dl = gr.dim[gr.rank - 1];
+  const int outer = gr.outer;
+  const float* qin = q + p.qs_off[gr.dep[gr.rank - 1]] * kTcTile + pl;
+  const float* pre = sm.pre + pl;
   float ql[kQl];
-  if (DLP > 0) {
-    const float* qlp = q + p.qs_off[gr.dep[gr.rank - 1]] * kTcTile + pl;
-    const int dl = gr.dim[gr.rank - 1];
+  if (MODE == 0) {
 #pragma unroll
-    for (int i = 0; i < kQl; ++i) ql[i] = (i < dl && active) ? qlp[i * kTcTile] : 0.f;
+    for (int i = 0; i < kQl; ++i) ql[i] = (i < dl && active) ? qin[i * kTcTile] : 0.f;
+  } else if (MODE == 1) {
+    const int off = (qt * Q) & ((1 << lg) - 1);
+#pragma unroll
+    for (int i = 0; i < kQl; ++i) ql[i] = (off + i < dl && active) ? qin[(off + i) * kTcTile] : 0.f;
   }
-  for (int c = 0; c < gr.nch; ++c, ++it) {
-    const int st = it % kTcStages;
-    const uint32_t use = it / kTcStages;
-    if (use > 0 && !tc::mbar_wait_bounded(&sm.done[st], (use - 1) & 1, kWaitLimit)) *sm.abort_flag = 1;
-    uint8_t* xs = sm.Xs + st * sm.xs_bytes;
-    uint8_t* ws = sm.Ws + st * sm.ws_bytes;
-    if (tid == 0) {  // W chunk: one bulk copy of the pre-swizzled image
-      mbar_expect_tx(&sm.full[st], (uint32_t)gr.chunk_bytes);
-      bulk_g2s(tc::smem_u32(ws), wimg + (int64_t)c * gr.chunk_bytes, (uint32_t)gr.chunk_bytes, &sm.full[st]);
+  const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  const int nst = gr.nch / CPS;
+  for (int c = 0; c < nst; ++c, ++it) {
+    const int st = it % NST;
+    const uint32_t use = it / NST;
+    if (use > 0) {
+      warp_wait(&sm.done[st], (use - 1) & 1, sm.abort_flag, lane);
+      tc::fence_after_sync();
     }
-    float v[H];
-    gen_x<H, DLP>(gr, p, q, pl, c * Tr::kChunk + half * H, ql, v);
-    if (!active)
+    const uint32_t ta_st = lane_base + (uint32_t)(tp.a_col + st * 32 * kPl * CPS + qt * 8);
 #pragma unroll
-      for (int i = 0; i < H; ++i) v[i] = 0.f;
-    const uint32_t xa = tc::smem_u32(xs);
-    if (PREC == B2_PRECISION_BF16) {
+    for (int h = 0; h < CPS; ++h) {
+      const int k0 = (c * CPS + h) * CH + qt * Q;
+      const int ko = k0 >> lg;
+      float v[Q];
+      if (MODE == 0) {
+        constexpr int kRuns = Q / kQl;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        tc::sts128(xa + tc::sw128_offset(pl, half * 4 + j), bf16x2_bits(v[j * 8 + 0], v[j * 8 + 1]),
-                   bf16x2_bits(v[j * 8 + 2], v[j * 8 + 3]), bf16x2_bits(v[j * 8 + 4], v[j * 8 + 5]),
-                   bf16x2_bits(v[j * 8 + 6], v[j * 8 + 7]));
-    } else {
+        for (int run = 0; run < kRuns; ++run) {
+          const float pr = (ko + run < outer) ? pre[(ko + run) * kTcTile] : 0.f;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        float hi[4], lo[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          hi[e] = tf32_round(v[j * 4 + e]);
-          lo[e] = tf32_round(v[j * 4 + e] - hi[e]);
+          for (int i = 0; i < kQl; ++i) v[run * kQl + i] = pr * ql[i];
         }
-        const uint32_t off = tc::sw128_offset(pl, half * 4 + j);
-        tc::sts128(xa + off, __float_as_uint(hi[0]), __float_as_uint(hi[1]), __float_as_uint(hi[2]),
-                   __float_as_uint(hi[3]));
-        tc::sts128(xa + kTcTile * 128 + off, __float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
-                   __float_as_uint(lo[3]));
-      }
-    }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    if (*sm.abort_flag) return;
-    if (tid == 0) {
-      if (!tc::mbar_wait_bounded(&sm.full[st], use & 1, kWaitLimit)) {
-        *sm.abort_flag = 1;
+      } else if (MODE == 1) {
+        const float pr = ko < outer ? pre[ko * kTcTile] : 0.f;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) v[i] = pr * ql[i];
       } else {
-        tc::fence_after_sync();
-        const uint32_t a0 = tc::smem_u32(xs), b0 = tc::smem_u32(ws);
-        // chunk c accumulates into accumulator c % nacc: shorter FP32
-        // accumulation chains inside the tensor core
-        const uint32_t dt = tmem + (uint32_t)((c % tp.nacc) * gr.N);
+        const int off = k0 & ((1 << lg) - 1);
+        const float pr = (ko < outer && active) ? pre[ko * kTcTile] : 0.f;
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-          const uint32_t acc = (c >= tp.nacc || kk > 0) ? 1u : 0u;
-          if (PREC == B2_PRECISION_BF16) {
-            tc::mma_bf16(dt, tc::desc_kmajor_sw128(a0 + kk * 32), tc::desc_kmajor_sw128(b0 + kk * 32), gr.idesc, acc);
-          } else {
-            const uint32_t alo = a0 + kTcTile * 128, blo = b0 + gr.N * 128;
-            tc::mma_tf32(dt, tc::desc_kmajor_sw128(a0 + kk * 32), tc::desc_kmajor_sw128(b0 + kk * 32), gr.idesc, acc);
-            tc::mma_tf32(dt, tc::desc_kmajor_sw128(a0 + kk * 32), tc::desc_kmajor_sw128(blo + kk * 32), gr.idesc, 1u);
-            tc::mma_tf32(dt, tc::desc_kmajor_sw128(alo + kk * 32), tc::desc_kmajor_sw128(b0 + kk * 32), gr.idesc, 1u);
-          }
-        }
-        tc::mma_commit(&sm.done[st]);
+        for (int i = 0; i < Q; ++i) v[i] = (off + i < dl) ? pr * qin[(off + i) * kTcTile] : 0.f;
       }
+      // this warp's 32 policy rows (TMEM lanes) x 8 columns of the A stage
+      const uint32_t ta = ta_st + (uint32_t)(h * 32 * kPl);
+      if (PREC == B2_PRECISION_BF16) {
+        uint32_t r[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) r[e] = bf16x2_bits(v[2 * e], v[2 * e + 1]);
+        tc::tmem_st8(ta, r);
+      } else {
+        uint32_t hi[8], lo[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const float hv = tf32_round(v[e]);
+          hi[e] = __float_as_uint(hv);
+          lo[e] = __float_as_uint(tf32_round(v[e] - hv));
+        }
+        tc::tmem_st8(ta, hi);
+        tc::tmem_st8(ta + 32, lo);
+      }
+    }
+    tc::tmem_wait_st();
+    tc::fence_before_sync();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.x_full[st]);
+  }
+}
+
+template <int PREC>
+__device__ __forceinline__ void produce_dispatch(const TcGroup& gr, const TcParams& tp, const EfeParams& p,
+                                                 const float* __restrict__ q, const TcSmem& sm, uint32_t tmem, int warp,
+                                                 int pl, int qt, int lane, bool active, uint32_t& it) {
+  constexpr int CH = TcTraits<PREC>::kChunk;
+  constexpr int Q = CH / 4;
+  const int dlp = 1 << gr.lg;
+  if (dlp > CH) {
+    produce_group<PREC, 2, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
+  } else if (dlp > Q) {
+    produce_group<PREC, 1, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
+  } else {
+    switch (gr.lg) {
+      case 0: produce_group<PREC, 0, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
+      case 1: produce_group<PREC, 0, 2>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
+      case 2: produce_group<PREC, 0, 4>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
+      case 3: produce_group<PREC, 0, (Q >= 8 ? 8 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
+      default: produce_group<PREC, 0, (Q >= 16 ? 16 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
     }
   }
 }
 
 // ------------------------------------------------------------ main kernel
+// Warp roles: 0-15 producers (four threads per policy row: state rollout,
+// prefix table, X generation into tensor memory, epilogue), 16 = W loader
+// (bulk copies, up to kNst stages ahead), 17 = MMA issuer (kCps * 4 K-steps
+// back to back per stage). The chunk loop has no CTA-wide barrier: stages
+// are handed over through the x_full / w_full / done mbarriers.
+constexpr int kProducers = 512;
+constexpr int kThreadsAll = kProducers + 64;
+
+__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, %0;" ::"r"(kProducers) : "memory"); }
+
 template <int PREC>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kThreadsAll, 1)
     efe_tc_kernel(const __grid_constant__ EfeParams p, const __grid_constant__ TcParams tp,
                   const int32_t* __restrict__ pm, int pm_batched, const float* __restrict__ qs_init,
                   const float* __restrict__ B, const uint8_t* __restrict__ pack, float* __restrict__ G) {
   using Tr = TcTraits<PREC>;
   constexpr int kPl = Tr::kPlanes;
+  constexpr int CPS = Tr::kCps;
+  constexpr int NST = Tr::kNst;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   TcSmem sm;
-  sm.xs_bytes = kPl * kTcTile * 128;
-  sm.ws_bytes = kPl * tp.Nmax * 128;
-  sm.Xs = base;
-  sm.Ws = sm.Xs + kTcStages * sm.xs_bytes;
-  float* qsm = reinterpret_cast<float*>(sm.Ws + kTcStages * sm.ws_bytes);
-  sm.done = reinterpret_cast<uint64_t*>(qsm + 2 * p.S_tot * kTcTile);
-  sm.full = sm.done + kTcStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm.full + kTcStages);
+  sm.ws_bytes = CPS * kPl * tp.Nmax * 128;
+  sm.Ws = base;
+  double* red = reinterpret_cast<double*>(sm.Ws + NST * sm.ws_bytes);  // [4][128] partial G
+  float* qsm = reinterpret_cast<float*>(red + 4 * kTcTile);
+  float* bsm = qsm + 2 * p.S_tot * kTcTile;  // this agent's B (when tp.b_words > 0)
+  sm.pre = bsm + tp.b_words;                 // [pre_cap][128]
+  sm.x_full = reinterpret_cast<uint64_t*>(sm.pre + tp.pre_cap * kTcTile);
+  sm.done = sm.x_full + NST;
+  sm.acc_full = sm.done + NST;
+  sm.acc_free = sm.acc_full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm.acc_free + 1);
   sm.abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int pl = tid & (kTcTile - 1);
-  const int half = tid >> 7;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t b = blockIdx.y;
-  const int pol = blockIdx.x * kTcTile + pl;
-  const bool active = pol < p.P;
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, (uint32_t)tp.tmem_cols);
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) {
+    for (int s = 0; s < NST; ++s) {
+      tc::mbar_init(&sm.x_full[s], kProducers / 32 + 1);
       tc::mbar_init(&sm.done[s], 1);
-      tc::mbar_init(&sm.full[s], 1);
     }
+    tc::mbar_init(sm.acc_full, 1);
+    tc::mbar_init(sm.acc_free, kProducers / 32);
     tc::fence_mbar_init();
     *sm.abort_flag = 0;
   }
-  for (int i = tid; i < p.S_tot * kTcTile; i += kTcThreads) qsm[i] = __ldg(qs_init + b * p.S_tot + i / kTcTile);
+  for (int i = tid; i < p.S_tot * kTcTile; i += blockDim.x) qsm[i] = __ldg(qs_init + b * p.S_tot + i / kTcTile);
+  for (int i = tid; i < tp.b_words && i < p.B_stride; i += blockDim.x) bsm[i] = __ldg(B + b * p.B_stride + i);
+  const float* Bag = tp.b_words > 0 ? bsm : B + b * p.B_stride;
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
 
-  const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
-  double g_acc = 0.0;
-  bool bad_action = false;
-  int cur = 0;
-  uint32_t it = 0;
-  bool aborted = false;
-  for (int t = 0; t < p.T && !aborted; ++t) {
-    // ---- expected states (pymdp/control.py:351-389): policy pl, states s = half, half + 2, ...
-    {
-      const float* qc = qsm + cur * p.S_tot * kTcTile;
-      float* qn = qsm + (cur ^ 1) * p.S_tot * kTcTile;
-      const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) +
-                             (int64_t)(active ? pol : 0) * p.T * p.F + t * p.F;
-      for (int f = 0; f < p.F; ++f) {
-        const EfeFactor& fb = p.fac[f];
-        int u = u_pol[f];
-        if (u < 0 || u >= p.U[f]) {
-          bad_action = true;
-          u = 0;
+  if (warp == kProducers / 32) {
+    // ---------------- W loader: one bulk copy per stage, NST stages ahead
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (int t = 0; t < p.T; ++t)
+        for (int g = 0; g < tp.G; ++g) {
+          const TcGroup& gr = tp.grp[g];
+          const uint8_t* wimg = pack + b * tp.pack_stride + gr.pack_off;
+          const uint32_t bytes = (uint32_t)(CPS * gr.chunk_bytes);
+          const int nst = gr.nch / CPS;
+          for (int c = 0; c < nst; ++c, ++it) {
+            const int st = it % NST;
+            const uint32_t use = it / NST;
+            if (use > 0 && !wait_or_abort(&sm.done[st], (use - 1) & 1, sm.abort_flag)) continue;
+            if (*sm.abort_flag) continue;  // waiters give up through the abort flag
+            mbar_expect_tx(&sm.x_full[st], bytes);
+            bulk_g2s(tc::smem_u32(sm.Ws + st * sm.ws_bytes), wimg + (int64_t)c * bytes, bytes, &sm.x_full[st]);
+          }
         }
-        const float* Bf = B + b * p.B_stride + fb.B_off;
-        const int U = p.U[f];
-        for (int s = half; s < p.S[f]; s += 2) {
-          float acc = 0.f;
-          const float* Bs = Bf + (int64_t)s * fb.K * U + u;
-          if (fb.rank == 1) {
-            const float* qv = qc + p.qs_off[fb.dep[0]] * kTcTile + pl;
-            for (int k = 0; k < fb.K; ++k) acc = fmaf(__ldg(Bs + (int64_t)k * U), qv[k * kTcTile], acc);
-          } else {
-            int dig[B2_MAX_DEP_RANK];
+    }
+  } else if (warp == kProducers / 32 + 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      // per-stage operand addresses: arithmetic in the stage index (no arrays)
+      const uint64_t wdesc0 = tc::desc_kmajor_sw128(tc::smem_u32(sm.Ws));
+      const uint32_t wstep16 = (uint32_t)sm.ws_bytes >> 4;
+      const uint32_t acol0 = tmem + (uint32_t)tp.a_col;
+      uint32_t it = 0, j = 0;
+      for (int t = 0; t < p.T; ++t)
+        for (int g = 0; g < tp.G; ++g, ++j) {
+          const TcGroup& gr = tp.grp[g];
+          const uint32_t idesc = gr.idesc;
+          const uint32_t chunk16 = (uint32_t)gr.chunk_bytes >> 4;  // descriptor units per chunk tile
+          const uint32_t lo16 = (uint32_t)(gr.N * 128) >> 4;       // descriptor units to the lo plane
+          const int nst = gr.nch / CPS;
+          if (j > 0) wait_or_abort(sm.acc_free, (j - 1) & 1, sm.abort_flag);
+          int acc_slot = 0;
+          for (int c = 0; c < nst; ++c, ++it) {
+            const int st = it % NST;
+            const uint32_t use = it / NST;
+            const bool okx = wait_or_abort(&sm.x_full[st], use & 1, sm.abort_flag);
+            if (okx && !*sm.abort_flag) {
+              tc::fence_after_sync();
+              // stage c accumulates into accumulator c % nacc: shorter FP32
+              // accumulation chains inside the tensor core
+              const uint32_t dt = tmem + (uint32_t)(acc_slot * gr.N);
+              const uint32_t first = c < tp.nacc ? 0u : 1u;
+              const uint64_t wd = wdesc0 + (uint64_t)(st * wstep16);
+              const uint32_t a0 = acol0 + (uint32_t)(st * 32 * kPl * CPS);
 #pragma unroll
-            for (int i = 0; i < B2_MAX_DEP_RANK; ++i) dig[i] = 0;
-            for (int k = 0; k < fb.K; ++k) {
-              float w = 1.f;
+              for (int h = 0; h < CPS; ++h)
 #pragma unroll
-              for (int i = 0; i < B2_MAX_DEP_RANK; ++i)
-                if (i < fb.rank) w *= qc[(p.qs_off[fb.dep[i]] + dig[i]) * kTcTile + pl];
-              acc = fmaf(__ldg(Bs + (int64_t)k * U), w, acc);
-              bool carry = true;
+                for (int kk = 0; kk < 4; ++kk) {
+                  const uint32_t acc = (h | kk) ? 1u : first;
+                  const uint64_t bd = wd + (uint64_t)(h * chunk16 + kk * 2);
+                  const uint32_t at = a0 + (uint32_t)(h * 32 * kPl + kk * 8);
+                  if (PREC == B2_PRECISION_BF16) {
+                    tc::mma_bf16_ts(dt, at, bd, idesc, acc);
+                  } else {
+                    tc::mma_tf32_ts(dt, at, bd, idesc, acc);
+                    tc::mma_tf32_ts(dt, at, bd + lo16, idesc, 1u);
+                    tc::mma_tf32_ts(dt, at + 32, bd, idesc, 1u);
+                  }
+                }
+            }
+            // always arm the barriers so every waiter makes progress
+            tc::mma_commit(&sm.done[st]);
+            if (++acc_slot == tp.nacc) acc_slot = 0;
+          }
+          tc::mma_commit(sm.acc_full);
+        }
+    }
+  } else {
+    // ---------------- producers (warps 0-15): policy pl, quarter qt
+    const int pl = tid & (kTcTile - 1);
+    const int qt = tid >> 7;
+    const int pol = blockIdx.x * kTcTile + pl;
+    const bool active = pol < p.P;
+    const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
+    double g_acc = 0.0;
+    bool bad_action = false;
+    int cur = 0;
+    uint32_t it = 0, j = 0;
+    for (int t = 0; t < p.T; ++t) {
+      // expected states (pymdp/control.py:351-389): policy pl, states s = qt, qt + 4, ...
+      {
+        const float* qc = qsm + cur * p.S_tot * kTcTile;
+        float* qn = qsm + (cur ^ 1) * p.S_tot * kTcTile;
+        const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) +
+                               (int64_t)(active ? pol : 0) * p.T * p.F + t * p.F;
+        for (int f = 0; f < p.F; ++f) {
+          const EfeFactor& fb = p.fac[f];
+          int u = u_pol[f];
+          if (u < 0 || u >= p.U[f]) {
+            bad_action = true;
+            u = 0;
+          }
+          const float* Bf = Bag + fb.B_off;
+          const int U = p.U[f];
+          const int K = fb.K;
+          for (int s = qt; s < p.S[f]; s += 4) {
+            float acc = 0.f;
+            const float* Bs = Bf + s * K * U + u;
+            if (fb.rank == 1) {
+              const float* qv = qc + p.qs_off[fb.dep[0]] * kTcTile + pl;
+              float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+              int k = 0;
+              for (; k + 3 < K; k += 4) {
+                a0 = fmaf(Bs[0], qv[0], a0);
+                a1 = fmaf(Bs[U], qv[kTcTile], a1);
+                a2 = fmaf(Bs[2 * U], qv[2 * kTcTile], a2);
+                a3 = fmaf(Bs[3 * U], qv[3 * kTcTile], a3);
+                Bs += 4 * U;
+                qv += 4 * kTcTile;
+              }
+              for (; k < K; ++k, Bs += U, qv += kTcTile) a0 = fmaf(Bs[0], qv[0], a0);
+              acc = (a0 + a1) + (a2 + a3);
+            } else {
+              int dig[B2_MAX_DEP_RANK];
 #pragma unroll
-              for (int i = B2_MAX_DEP_RANK - 1; i >= 0; --i) {
-                if (carry && i < fb.rank) {
-                  if (++dig[i] < p.S[fb.dep[i]]) carry = false;
-                  else dig[i] = 0;
+              for (int i = 0; i < B2_MAX_DEP_RANK; ++i) dig[i] = 0;
+              for (int k = 0; k < K; ++k) {
+                float w = 1.f;
+#pragma unroll
+                for (int i = 0; i < B2_MAX_DEP_RANK; ++i)
+                  if (i < fb.rank) w *= qc[(p.qs_off[fb.dep[i]] + dig[i]) * kTcTile + pl];
+                acc = fmaf(Bs[k * U], w, acc);
+                bool carry = true;
+#pragma unroll
+                for (int i = B2_MAX_DEP_RANK - 1; i >= 0; --i) {
+                  if (carry && i < fb.rank) {
+                    if (++dig[i] < p.S[fb.dep[i]]) carry = false;
+                    else dig[i] = 0;
+                  }
                 }
               }
             }
+            qn[(p.qs_off[f] + s) * kTcTile + pl] = acc;
           }
-          qn[(p.qs_off[f] + s) * kTcTile + pl] = acc;
         }
       }
-    }
-    __syncthreads();
-    cur ^= 1;
-    const float* q = qsm + cur * p.S_tot * kTcTile;
-
-    for (int g = 0; g < tp.G && !aborted; ++g) {
-      const TcGroup& gr = tp.grp[g];
-      const uint8_t* wimg = pack + b * tp.pack_stride + gr.pack_off;
-      constexpr int H = Tr::kChunk / 2;
-      const int dlp = 1 << gr.lg;
-      if (dlp > H) {
-        run_group<PREC, 0>(gr, tp, p, q, wimg, sm, tmem, tid, pl, half, active, it);
-      } else {
-        switch (gr.lg) {
-          case 0: run_group<PREC, 1>(gr, tp, p, q, wimg, sm, tmem, tid, pl, half, active, it); break;
-          case 1: run_group<PREC, 2>(gr, tp, p, q, wimg, sm, tmem, tid, pl, half, active, it); break;
-          case 2: run_group<PREC, 4>(gr, tp, p, q, wimg, sm, tmem, tid, pl, half, active, it); break;
-          case 3: run_group<PREC, 8>(gr, tp, p, q, wimg, sm, tmem, tid, pl, half, active, it); break;
-          case 4: run_group<PREC, (H >= 16 ? 16 : 0)>(gr, tp, p, q, wimg, sm, tmem, tid, pl, half, active, it); break;
-          default: run_group<PREC, (H >= 32 ? 32 : 0)>(gr, tp, p, q, wimg, sm, tmem, tid, pl, half, active, it); break;
-        }
-      }
-      __syncthreads();
-      if (*sm.abort_flag) {
-        aborted = true;
-        break;
-      }
-      // ---- epilogue for (t, g): wait for the last chunk's MMAs
-      {
-        const uint32_t last = it - 1;
-        if (!tc::mbar_wait_bounded(&sm.done[last % kTcStages], (last / kTcStages) & 1, kWaitLimit))
-          *sm.abort_flag = 1;
-      }
-      tc::fence_after_sync();
-      if (warp < 4) {
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-        double h = 0.0, lin = 0.0;
-        const int nacc = gr.nch < tp.nacc ? gr.nch : tp.nacc;
-        for (int n0 = 0; n0 < gr.N; n0 += 16) {
-          double sum[16];
+      producers_sync();
+      cur ^= 1;
+      const float* q = qsm + cur * p.S_tot * kTcTile;
+      for (int g = 0; g < tp.G; ++g, ++j) {
+        const TcGroup& gr = tp.grp[g];
+        // prefix table: pre[ko][pl] = prod_{outer factors} q (digits of ko)
+        {
+          const int n = gr.rank - 1;
+          for (int ko = qt; ko < gr.outer; ko += 4) {
+            float v = 1.f;
+            int rem = ko;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) sum[j] = 0.0;
-          for (int a = 0; a < nacc; ++a) {
-            uint32_t r[16];
-            tc::tmem_ld16(taddr + (uint32_t)(a * gr.N + n0), r);
-            tc::tmem_wait_ld();
-#pragma unroll
-            for (int j = 0; j < 16; ++j) sum[j] += (double)__uint_as_float(r[j]);
+            for (int x = kTcMaxOuter - 1; x >= 0; --x)
+              if (x < n) {
+                const int d = gr.dim[x];
+                const int qd = rem / d;
+                v *= q[(p.qs_off[gr.dep[x]] + (rem - qd * d)) * kTcTile + pl];
+                rem = qd;
+              }
+            sm.pre[ko * kTcTile + pl] = active ? v : 0.f;
           }
+        }
+        producers_sync();
+        produce_dispatch<PREC>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
+        // epilogue: warp w reads TMEM lane quarter (w & 3) = its 32 policies,
+        // 16-column blocks qt*16, qt*16 + 64, ... of every accumulator
+        warp_wait(sm.acc_full, j & 1, sm.abort_flag, lane);
+        tc::fence_after_sync();
+        {
+          const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+          const int nacc = gr.nch / CPS < tp.nacc ? gr.nch / CPS : tp.nacc;
+          double h = 0.0, lin = 0.0;
+          for (int n0 = qt * 16; n0 < gr.N; n0 += 64) {
+            double sum[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int n = n0 + j;
-            if (n < gr.n_obs) {
-              if (ig) h -= sum[j] * (double)logf(fmaxf((float)sum[j], kMinVal));
-            } else if (n == gr.n_obs + t) {
-              lin = sum[j];
+            for (int k = 0; k < 16; ++k) sum[k] = 0.0;
+            for (int a = 0; a < nacc; ++a) {
+              uint32_t r[16];
+              tc::tmem_ld16(taddr + (uint32_t)(a * gr.N + n0), r);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+              const int n = n0 + k;
+              if (n < gr.n_obs) {
+                if (ig) h -= sum[k] * (double)logf(fmaxf((float)sum[k], kMinVal));
+              } else if (n == gr.n_obs + t) {
+                lin = sum[k];
+              }
             }
           }
+          g_acc += h + lin;
         }
-        g_acc += h + lin;
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(sm.acc_free);
+        producers_sync();  // every producer is done with this group's prefix table
       }
-      tc::fence_before_sync();
-      __syncthreads();
-      if (*sm.abort_flag) aborted = true;
+    }
+    red[qt * kTcTile + pl] = g_acc;
+    producers_sync();
+    if (qt == 0 && active && !*sm.abort_flag) {
+      const double gsum = ((red[pl] + red[kTcTile + pl]) + red[2 * kTcTile + pl]) + red[3 * kTcTile + pl];
+      G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : (float)gsum;
     }
   }
-  if (aborted && tid == 0) atomicExch(&g_b2_device_error, 1);
-  if (tid < kTcTile && active && !aborted) G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : (float)g_acc;
   tc::fence_before_sync();
   __syncthreads();
+  if (*sm.abort_flag && tid == 0) atomicExch(&g_b2_device_error, 1);
   if (warp == 0) tc::tmem_dealloc(tmem, (uint32_t)tp.tmem_cols);
 }
 
@@ -538,11 +637,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
 // Plan the tensor-core path; returns B2_ERR_UNSUPPORTED when the model falls
 // outside its limits (the caller then uses the SIMT kernel).
-int32_t tc_plan(const EfeParams& p, int prec, TcParams* tp, int* smem_bytes) {
+template <int PREC>
+int32_t tc_plan_t(const EfeParams& p, TcParams* tp, int* smem_bytes) {
+  using Tr = TcTraits<PREC>;
   std::memset(tp, 0, sizeof(*tp));
-  const int chunk = prec == B2_PRECISION_BF16 ? 64 : 32;
-  const int H = chunk / 2;
-  const int planes = prec == B2_PRECISION_BF16 ? 1 : 2;
+  const int chunk = Tr::kChunk;
+  const int planes = Tr::kPlanes;
+  const int cps = Tr::kCps;
+  const int nst = Tr::kNst;
   std::vector<std::vector<int>> groups;
   std::vector<std::vector<int>> tuples;
   for (int m = 0; m < p.M; ++m) {
@@ -561,18 +663,21 @@ int32_t tc_plan(const EfeParams& p, int prec, TcParams* tp, int* smem_bytes) {
   tp->G = (int32_t)groups.size();
   int n_order = 0;
   int64_t off = 0;
-  int Nmax = 16;
+  int Nmax = 16, outer_max = 1;
   for (int g = 0; g < tp->G; ++g) {
     TcGroup& gr = tp->grp[g];
     const std::vector<int>& tup = tuples[g];
     const int r = (int)tup.size();
+    if (r > kTcMaxOuter + 1) return B2_ERR_UNSUPPORTED;
     gr.rank = r;
-    // innermost factor: the largest padded size that still fits a half chunk
+    // innermost factor: the largest padded size that fits one chunk (its
+    // marginal then stays in registers), else the largest overall; either way
+    // the shared prefix table (K / innermost entries) is as small as possible
     int best = r - 1, best_p = -1;
     for (int a = 0; a < r; ++a) {
       int pw = 1;
       while (pw < p.S[tup[a]]) pw <<= 1;
-      const int score = pw <= H ? pw : 0;
+      const int score = pw <= chunk ? 4 * pw : pw / 1024;
       if (score > best_p) {
         best_p = score;
         best = a;
@@ -597,8 +702,10 @@ int32_t tc_plan(const EfeParams& p, int prec, TcParams* tp, int* smem_bytes) {
     if (K > (1 << 24)) return B2_ERR_UNSUPPORTED;
     gr.K = (int32_t)K;
     gr.outer = (int32_t)(K / p.S[tup[best]]);
+    outer_max = gr.outer > outer_max ? gr.outer : outer_max;
     const int64_t Kp = (int64_t)gr.outer << lg;
-    gr.Kpad = (int32_t)((Kp + chunk - 1) / chunk * chunk);
+    const int64_t step = (int64_t)chunk * cps;
+    gr.Kpad = (int32_t)((Kp + step - 1) / step * step);
     gr.nch = gr.Kpad / chunk;
     gr.m_begin = n_order;
     int n_obs = 0;
@@ -611,66 +718,69 @@ int32_t tc_plan(const EfeParams& p, int prec, TcParams* tp, int* smem_bytes) {
     gr.N = (n_obs + p.T + 15) / 16 * 16;
     if (gr.N > 256) return B2_ERR_UNSUPPORTED;
     Nmax = gr.N > Nmax ? gr.N : Nmax;
-    gr.idesc = tc::idesc_f32acc(prec == B2_PRECISION_BF16 ? 1u : 2u, 128u, (uint32_t)gr.N);
+    gr.idesc = tc::idesc_f32acc(PREC == B2_PRECISION_BF16 ? 1u : 2u, 128u, (uint32_t)gr.N);
     gr.chunk_bytes = planes * gr.N * 128;
     gr.pack_off = off;
     off += (int64_t)gr.nch * gr.chunk_bytes;
   }
   tp->Nmax = Nmax;
-  int nacc = 512 / Nmax;
+  const int a_cols = nst * 32 * planes * cps;  // A stages: 128 lanes x 128 bytes per plane per chunk
+  int nacc = (512 - a_cols) / Nmax;
   nacc = nacc > 8 ? 8 : nacc;
+  if (nacc < 1) return B2_ERR_UNSUPPORTED;
   tp->nacc = nacc;
-  int cols = 32;
-  while (cols < nacc * Nmax) cols <<= 1;
-  tp->tmem_cols = cols;
+  tp->a_col = (nacc * Nmax + 31) / 32 * 32;
+  if (tp->a_col + a_cols > 512) return B2_ERR_UNSUPPORTED;
+  tp->tmem_cols = 512;
+  tp->pre_cap = (outer_max + 1) / 2 * 2;
   tp->pack_stride = (off + 1023) / 1024 * 1024;
-  const int xs_bytes = planes * kTcTile * 128;
-  const int w_bytes = planes * Nmax * 128;
-  const int64_t smem = 1024 + (int64_t)kTcStages * (xs_bytes + w_bytes) + 2LL * p.S_tot * kTcTile * 4 +
-                       2 * kTcStages * 8 + 16;
+  const int w_bytes = cps * planes * Nmax * 128;
+  int64_t smem = 1024 + (int64_t)nst * w_bytes + 4LL * kTcTile * 8 + 2LL * p.S_tot * kTcTile * 4 +
+                 (int64_t)tp->pre_cap * kTcTile * 4 + (2 * nst + 2) * 8 + 16;
   if (smem > 227 * 1024) return B2_ERR_UNSUPPORTED;
+  const int64_t b_words = (p.B_stride + 1) / 2 * 2;  // keep the barriers 8-byte aligned
+  if (smem + b_words * 4 <= 227 * 1024) {
+    tp->b_words = (int32_t)b_words;
+    smem += b_words * 4;
+  }
   *smem_bytes = (int)smem;
   return B2_OK;
+}
+
+template <int PREC>
+int32_t launch_tc_t(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
+                    const float* A, const float* B, const float* C, float* G, cudaStream_t stream, bool* used) {
+  TcParams tp;
+  int smem = 0;
+  if (tc_plan_t<PREC>(p, &tp, &smem) != B2_OK) return B2_OK;
+  const size_t bytes = (size_t)Bn * (size_t)tp.pack_stride;
+  uint8_t* pack = nullptr;
+  B2_TRY(ws_alloc((void**)&pack, bytes, stream, kEfeName));
+  int Kmax = 0;
+  for (int g = 0; g < tp.G; ++g) Kmax = tp.grp[g].Kpad > Kmax ? tp.grp[g].Kpad : Kmax;
+  dim3 pgrid((unsigned)((Kmax + 127) / 128), (unsigned)(tp.G * 256), (unsigned)Bn);
+  dim3 grid((unsigned)((p.P + kTcTile - 1) / kTcTile), (unsigned)Bn);
+  efe_tc_pack_kernel<PREC><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
+  int32_t rc = check_launch("efe_ffi tc pack");
+  if (rc == B2_OK) rc = ensure_smem_attr((const void*)efe_tc_kernel<PREC>, smem, kEfeName);
+  if (rc == B2_OK) {
+    efe_tc_kernel<PREC><<<grid, kThreadsAll, smem, stream>>>(p, tp, pm, pm_batched, qs, B, pack, G);
+    rc = check_launch("efe_ffi tc");
+  }
+  cudaError_t fe = cudaFreeAsync(pack, stream);
+  if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
+  *used = rc == B2_OK;
+  return rc;
 }
 
 int32_t launch_efe_tc(const EfeParams& p, int prec, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
                       const float* A, const float* B, const float* C, float* G, cudaStream_t stream,
                       bool* used) {
   *used = false;
-  TcParams tp;
-  int smem = 0;
-  if (tc_plan(p, prec, &tp, &smem) != B2_OK) return B2_OK;
   if (Bn > 65535) return B2_OK;
-  const size_t bytes = (size_t)Bn * (size_t)tp.pack_stride;
-  uint8_t* pack = nullptr;
-  B2_TRY(ws_alloc((void**)&pack, bytes, stream, kEfeName));
-  int32_t rc = B2_OK;
-  int Kmax = 0;
-  for (int g = 0; g < tp.G; ++g) Kmax = tp.grp[g].Kpad > Kmax ? tp.grp[g].Kpad : Kmax;
-  dim3 pgrid((unsigned)((Kmax + 127) / 128), (unsigned)(tp.G * 256), (unsigned)Bn);
-  dim3 grid((unsigned)((p.P + kTcTile - 1) / kTcTile), (unsigned)Bn);
-  if (prec == B2_PRECISION_BF16) {
-    efe_tc_pack_kernel<B2_PRECISION_BF16><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
-    rc = check_launch("efe_ffi tc pack");
-    if (rc == B2_OK) rc = ensure_smem_attr((const void*)efe_tc_kernel<B2_PRECISION_BF16>, smem, kEfeName);
-    if (rc == B2_OK) {
-      efe_tc_kernel<B2_PRECISION_BF16><<<grid, kTcThreads, smem, stream>>>(p, tp, pm, pm_batched, qs, B, pack, G);
-      rc = check_launch("efe_ffi tc");
-    }
-  } else {
-    efe_tc_pack_kernel<B2_PRECISION_TF32X3><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
-    rc = check_launch("efe_ffi tc pack");
-    if (rc == B2_OK) rc = ensure_smem_attr((const void*)efe_tc_kernel<B2_PRECISION_TF32X3>, smem, kEfeName);
-    if (rc == B2_OK) {
-      efe_tc_kernel<B2_PRECISION_TF32X3><<<grid, kTcThreads, smem, stream>>>(p, tp, pm, pm_batched, qs, B, pack,
-                                                                               G);
-      rc = check_launch("efe_ffi tc");
-    }
-  }
-  cudaError_t fe = cudaFreeAsync(pack, stream);
-  if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
-  *used = rc == B2_OK;
-  return rc;
+  if (prec == B2_PRECISION_BF16)
+    return launch_tc_t<B2_PRECISION_BF16>(p, Bn, pm, pm_batched, qs, A, B, C, G, stream, used);
+  return launch_tc_t<B2_PRECISION_TF32X3>(p, Bn, pm, pm_batched, qs, A, B, C, G, stream, used);
 }
 
 }  // namespace b2
