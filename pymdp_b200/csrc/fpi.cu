@@ -23,7 +23,10 @@
 //    FP64, so the marginal dot products and the per-factor sums carry FP64
 //    accumulation error only (FP32 accumulation misses the 1e-5-relative
 //    posterior target vs the FP64 reference on ill-conditioned Dirichlet(0.5)
-//    models; FP64 accumulation stays near 1e-6). log/exp stay FP32.
+//    models). The log of each gathered A entry and prior and the softmax
+//    are FP64 as well: on models with many coupled factors the Jacobi sweeps
+//    amplify per-iteration rounding, and FP32 logf/expf alone move some
+//    posteriors by up to ~2e-5 relative after 16 iterations.
 //  * Modalities with identical dependency tuples are merged at plan time
 //    (their ll blocks are summed once at load), removing duplicate
 //    contractions; the marginals are linear in ll so this is exact algebra.
@@ -104,18 +107,24 @@ __device__ __forceinline__ double warp_max_d(double v) {
   return v;
 }
 
-// softmax(logq) of n values by one warp; FP32 exponentials on the
-// max-shifted FP64 logits.
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// softmax(logq) of n values by one warp, in FP64 throughout.
 template <typename OutT>
 __device__ __forceinline__ void softmax_warp(const double* __restrict__ logq, OutT* __restrict__ out, int n,
                                              int lane) {
   double mx = -INFINITY;
   for (int i = lane; i < n; i += 32) mx = fmax(mx, logq[i]);
   mx = warp_max_d(mx);
-  float sum = 0.f;
-  for (int i = lane; i < n; i += 32) sum += expf((float)(logq[i] - mx));
-  sum = warp_sum(sum);
-  for (int i = lane; i < n; i += 32) out[i] = (OutT)(expf((float)(logq[i] - mx)) / sum);
+  double sum = 0.0;
+  for (int i = lane; i < n; i += 32) sum += exp(logq[i] - mx);
+  sum = warp_sum_d(sum);
+  const double inv = 1.0 / sum;
+  for (int i = lane; i < n; i += 32) out[i] = (OutT)(exp(logq[i] - mx) * inv);
 }
 
 // rank >= 4: mixed-radix counter over the other axes (innermost last).
@@ -252,7 +261,7 @@ __global__ void __launch_bounds__(TEAM * APC)
       double v = 0.0;
       for (int si = gr.src_begin; si < gr.src_end; ++si) {
         const float a = __ldg(io.src + rowoff[p.src_order[si]] + k);
-        v += FUSED ? (double)logf(fmaxf(a, kMinVal)) : (double)a;
+        v += FUSED ? log((double)fmaxf(a, kMinVal)) : (double)a;
       }
       int rem = k, addr = 0;
       for (int x = gr.rank - 1; x > 0; --x) {
@@ -267,7 +276,7 @@ __global__ void __launch_bounds__(TEAM * APC)
   }
   for (int i = t; i < p.S_tot; i += TEAM) {
     const float v = __ldg(io.prior + b * p.S_tot + i);
-    lp[i] = FUSED ? (double)logf(fmaxf(v, kMinVal)) : (double)v;
+    lp[i] = FUSED ? log((double)fmaxf(v, kMinVal)) : (double)v;
     logq[i] = 0.0;
   }
   team_sync<TEAM>();
