@@ -145,6 +145,36 @@ int32_t b2_neg_efe(void* stream, const int32_t* policy_matrix, int64_t pm_count,
                    const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
                    const int64_t* B_dep_offsets, int32_t flags);
 
+/* Size of the fixed device scratch behind b2_neg_efe_noalloc (16 MiB). */
+#define B2_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* No counterpart in the reference: an addition of this library for callers
+ * that must not allocate device memory during a call (a host that owns the
+ * whole GPU through its own arena, a real-time loop that keeps allocator
+ * latency out of its step, a runtime that forbids allocation inside its
+ * handlers). Same arguments, validation and results as b2_neg_efe at
+ * B2_PRECISION_FP32 (the SIMT kernel), but its workspace of
+ * Bn * T * sum_m K_m floats lives in one fixed device array of
+ * B2_NOALLOC_SCRATCH_BYTES, held by every device that loads the library until
+ * exit, and it calls no allocating routine. Calls whose workspace would
+ * exceed that size, and tensor-core precision selectors, return
+ * B2_ERR_UNSUPPORTED. All calls on a device share the array: calls that
+ * overlap on the GPU race and give wrong results, so order them (one
+ * stream). The first call on each device looks up the array's address with
+ * that device current; make it before any stream capture begins. */
+int32_t b2_neg_efe_noalloc(void* stream, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+                           const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
+                           const float* B, int64_t B_count, const float* C, int64_t C_count,
+                           const float* I, int64_t I_count, const float* pA, int64_t pA_count,
+                           const float* pB, int64_t pB_count, const float* inductive_epsilon,
+                           int64_t eps_count, float* neg_efe_out, int64_t out_count, int64_t Bn, int64_t P,
+                           int64_t T, int64_t F, int64_t M, const int64_t* S, const int64_t* O,
+                           const int64_t* U, const int64_t* qs_offsets, const int64_t* A_offsets,
+                           const int64_t* B_offsets, const int64_t* C_offsets, const int64_t* I_offsets,
+                           const int64_t* I_depths, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                           const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
+                           const int64_t* B_dep_offsets, int32_t flags);
+
 /* q_pi = softmax(gamma * neg_efe + log(clip(E, eps))) per agent — the step
  * the reference runs in XLA right after the FFI call
  * (pymdp/control.py:349 and :963). gamma is [Bn] (gamma_batched = 1) or a

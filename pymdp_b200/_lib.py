@@ -32,6 +32,7 @@ PRECISIONS = {"fp32": 0, "tf32x3": 1, "bf16": 2}
 MAX_DEP_RANK = 8
 MAX_FACTORS = 16
 MAX_MODALITIES = 32
+NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 class B2Error(RuntimeError):
@@ -67,6 +68,11 @@ _SIGS = {
                              c_int64, c_int64, c_int64, c_int64, c_int64, c_int64, _P64, _P64, _P64, _P64,
                              _P64, _P64, _P64, _P64, _P64, _P64, c_int64, _P64, _P64, c_int64, _P64,
                              c_int32]),
+    "b2_neg_efe_noalloc": (c_int32, [c_void_p, c_void_p, c_int64, c_int32, _PF, c_int64, _PF, c_int64, _PF,
+                                     c_int64, _PF, c_int64, _PF, c_int64, _PF, c_int64, _PF, c_int64, _PF,
+                                     c_int64, _PF, c_int64, c_int64, c_int64, c_int64, c_int64, c_int64, _P64,
+                                     _P64, _P64, _P64, _P64, _P64, _P64, _P64, _P64, _P64, c_int64, _P64, _P64,
+                                     c_int64, _P64, c_int32]),
     "b2_policy_posterior": (c_int32, [c_void_p, _PF, _PF, c_int32, _PF, c_int32, _PF, c_int64, c_int64]),
     "b2_select_action": (c_int32, [c_void_p, _PF, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64]),
 }
