@@ -19,7 +19,9 @@ infer_policies (neg-EFE of all policies + q_pi) -> sample_action
   inside the timed region.
 * ``roofline``: the dominant kernel (neg-EFE), its algorithmic FLOPs
   2*T*P*sum_m(O_m*K_m) per agent over its measured launch time.
-* ``cpu_baseline``: the FP64 oracle on the host cores for a bounded sample.
+* ``cpu_baseline``: the FP64 oracle on all host cores (one spawned worker
+  process per core) for a bounded sample of the same agents; the same sample
+  gives ``error_vs_fp64``, the GPU outputs' max error against FP64.
 
 Multi-GPU: agents are independent, so each rank runs its own 256 agents
 (weak scaling, no data-path collective); the only collective is the
@@ -49,8 +51,11 @@ T = 3
 AGENTS = 256
 NUM_ITER = 16
 GAMMA = 16.0
-WORKLOAD = "agent step (FPI 16 iters + EFE all 4096 policies + action), 256 agents, S=[32,16,8], " \
-           "O=[16,16,8,8,4], U=[4,4,1], policy_len=3"
+
+
+def workload(agents: int) -> str:
+    return (f"agent step (FPI 16 iters + EFE all 4096 policies + action), {agents} agents, S=[32,16,8], "
+            "O=[16,16,8,8,4], U=[4,4,1], policy_len=3")
 
 
 def make_model(seed: int, agents: int):
@@ -73,6 +78,11 @@ def efe_flops_per_agent() -> float:
     K = int(np.prod(S))
     P = int(np.prod(U)) ** T
     return 2.0 * T * P * sum(o * K for o in O)
+
+
+# DRAM bytes per agent of the neg-EFE tensor-core kernel, from an ncu capture of 160 agents (the W image is read
+# once per agent, so traffic scales with agents); None where no capture exists yet.
+EFE_TRAFFIC_PER_AGENT = {"tf32x3": 347.2e6 / 160}
 
 
 def fpi_bytes_per_agent() -> float:
@@ -122,48 +132,88 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_baseline_run(agents: int, seed: int = 0):
-    """FP64 oracle agent steps on the host (bounded sample): (agent-steps/s, sample)."""
+def _oracle_agent_step(args):
+    """One agent's full step with the FP64 oracle: (qs, G, q_pi, action)."""
     from oracle import efe as oefe
     from oracle import fpi as ofpi
 
-    A, B, C, D, obs = make_model(seed, agents)
+    A_b, B_b, C_b, D_b, obs_b = args
     F, M = len(S), len(O)
     A_deps = [list(range(F))] * M
     B_deps = [[f] for f in range(F)]
     pol = oefe.construct_policies(S, U, T)
     E = np.full(len(pol), 1.0 / len(pol))
-    t0 = time.perf_counter()
-    for b in range(agents):
-        o_vec = [np.eye(O[m])[obs[b, m]] for m in range(M)]
-        qs = ofpi.run_factorized_fpi([a[b].astype(np.float64) for a in A], o_vec, [d[b] for d in D], A_deps,
-                                     NUM_ITER)
-        q_pi, _ = oefe.update_posterior_policies(pol, qs, [a[b] for a in A], [x[b] for x in B],
-                                                 [c[b] for c in C], E, A_deps, B_deps, gamma=GAMMA)
-        oefe.sample_policy(pol, q_pi)
-    dt = time.perf_counter() - t0
-    return agents / dt, dt
+    o_vec = [np.eye(O[m])[obs_b[m]] for m in range(M)]
+    qs = ofpi.run_factorized_fpi([a.astype(np.float64) for a in A_b], o_vec, D_b, A_deps, NUM_ITER)
+    q_pi, G = oefe.update_posterior_policies(pol, qs, A_b, B_b, C_b, E, A_deps, B_deps, gamma=GAMMA)
+    return qs, G, q_pi, oefe.sample_policy(pol, q_pi)
 
 
-def threads_used() -> int:
+def _worker_init():
+    # one BLAS thread per worker process: the pool supplies the parallelism
     try:
-        from threadpoolctl import threadpool_info
+        from threadpoolctl import threadpool_limits
 
-        return max([i.get("num_threads", 1) for i in threadpool_info()] or [1])
+        threadpool_limits(1)
     except Exception:  # noqa: BLE001
-        return os.cpu_count() or 1
+        pass
+
+
+def cpu_workers() -> int:
+    """Host worker processes for the oracle: every core, bounded by memory
+    (an agent step of this model holds about 0.6 GB)."""
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+
+        n = min(n, max(1, int(psutil.virtual_memory().available / 0.75e9)))
+    except Exception:  # noqa: BLE001
+        pass
+    return max(1, n)
+
+
+class OraclePool:
+    """Spawned process pool running oracle agent steps on all host cores."""
+
+    def __init__(self, workers: int):
+        import multiprocessing as mp
+
+        self.workers = workers
+        self.pool = mp.get_context("spawn").Pool(workers, initializer=_worker_init)
+
+    def run(self, model, idx):
+        A, B, C, D, obs = model
+        tasks = [([a[b] for a in A], [x[b] for x in B], [c[b] for c in C], [d[b] for d in D], obs[b]) for b in idx]
+        t0 = time.perf_counter()
+        out = self.pool.map(_oracle_agent_step, tasks, chunksize=1)
+        return out, time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def _max_rel(got, ref, floor):
+    got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
+    return float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), floor)))
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    per_step = 1  # one agent's full FPI + EFE step per timed step (bounded sample)
-    for _ in range(args.warmup):
-        cpu_baseline_run(per_step, seed=1)
-    times = []
-    for i in range(args.steps):
-        _, dt = cpu_baseline_run(per_step, seed=2 + i)
-        times.append(dt)
+    workers = cpu_workers()
+    n_agents = args.agents
+    model = make_model(1234, n_agents)
+    pool = OraclePool(workers)
+    try:
+        per_step = min(workers, n_agents)  # one agent per worker per step (bounded sample)
+        pool.run(model, range(per_step))
+        for _ in range(max(0, args.warmup - 1)):
+            pool.run(model, range(per_step))
+        times = [pool.run(model, [(i * per_step + k) % n_agents for k in range(per_step)])[1]
+                 for i in range(args.steps)]
+    finally:
+        pool.close()
     total = sum(times)
     value = args.steps * per_step / total
     line = {
@@ -171,10 +221,10 @@ def run_reference(args, rank, world):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "agents_per_step": per_step},
-        "cpu_baseline": {"value": value, "unit": "agent-steps/s", "cores": threads_used(), "kind": "port",
-                         "sample": f"{per_step} agent per step of the same model (FP64 NumPy oracle: FPI + "
-                                   f"EFE over 4096 policies + q_pi + action)"},
+        "config": {"workload": workload(n_agents), "agents_per_step": per_step},
+        "cpu_baseline": {"value": value, "unit": "agent-steps/s", "cores": workers, "kind": "port",
+                         "sample": f"{per_step} agents per step of the same model, one per worker process "
+                                   f"(FP64 NumPy oracle: FPI + EFE over 4096 policies + q_pi + action)"},
         "e2e": {"value": value, "unit": "agent-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -186,10 +236,15 @@ def run_b200(args, rank, world, local_rank):
 
     from pymdp_b200 import Agent, _lib, ffi
 
+    sample = 0 if world > 1 else (cpu_workers() if args.cpu_sample is None else args.cpu_sample)
+    n_agents = args.agents
+    sample = min(sample, n_agents)
+    pool = OraclePool(min(sample, cpu_workers())) if sample > 0 else None  # spawned before any GPU work
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    A, B, C, D, obs = make_model(1234 + rank, AGENTS)
-    agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=AGENTS, num_iter=NUM_ITER, device=dev,
+    model = make_model(1234 + rank, n_agents)
+    A, B, C, D, obs = model
+    agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=n_agents, num_iter=NUM_ITER, device=dev,
                   precision=args.precision)
     obs_d = torch.as_tensor(obs, device=dev)
     prior_d = [torch.as_tensor(d, device=dev) for d in D]
@@ -216,6 +271,13 @@ def run_b200(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     barrier()
+    # outputs of one step, checked against the FP64 oracle on the CPU sample
+    qs_chk = agent.infer_states(obs_d, prior_d)
+    q_pi_chk, G_chk = agent.infer_policies(qs_chk)
+    act_chk = agent.sample_action(q_pi_chk)
+    chk = ([q[:, -1].cpu().numpy() for q in qs_chk], G_chk.cpu().numpy(), q_pi_chk.cpu().numpy(),
+           act_chk.cpu().numpy())
+    barrier()
     evs = []
     n0 = _lib.launch_count()
     with ClockSampler(local_rank) as clocks:
@@ -234,7 +296,7 @@ def run_b200(args, rank, world, local_rank):
     # e2e through the public API with host buffers
     obs_h = torch.as_tensor(obs).pin_memory()
     prior_h = [torch.as_tensor(d).pin_memory() for d in D]
-    act_h = torch.empty((AGENTS, len(S)), dtype=torch.int32).pin_memory()
+    act_h = torch.empty((n_agents, len(S)), dtype=torch.int32).pin_memory()
 
     def e2e_step():
         o = obs_h.to(dev, non_blocking=True)
@@ -268,30 +330,47 @@ def run_b200(args, rank, world, local_rank):
     except Exception:  # noqa: BLE001
         pass
     peak_tf = peaks.get("bf16_tflops", 1590.0)
-    flops = efe_flops_per_agent() * AGENTS
+    flops = efe_flops_per_agent() * n_agents
     achieved_tf = flops / (efe_ms * 1e-3) / 1e12
-    total_agents = AGENTS * world
+    total_agents = n_agents * world
     value = total_agents * args.steps / (ms * 1e-3)
-    sample = 2 if args.cpu_sample is None else args.cpu_sample
-    cpu_val, cpu_dt = cpu_baseline_run(sample, seed=7) if (world == 1 and sample > 0) else (None, None)
+    cpu_val = cpu_dt = err = None
+    if pool is not None:
+        try:
+            ref, cpu_dt = pool.run(model, range(sample))
+        finally:
+            pool.close()
+        cpu_val = sample / cpu_dt
+        qs_g, G_g, q_pi_g, act_g = chk
+        err = {
+            "agents": sample,
+            "qs_max_rel": max(_max_rel(qs_g[f][b], ref[b][0][f], 1e-6) for b in range(sample) for f in range(len(S))),
+            "G_max_rel": max(_max_rel(G_g[b], ref[b][1], 1e-6) for b in range(sample)),
+            "q_pi_max_abs": max(float(np.max(np.abs(q_pi_g[b] - ref[b][2]))) for b in range(sample)),
+            "actions_equal": int(sum(bool(np.array_equal(act_g[b], ref[b][3])) for b in range(sample))),
+        }
     line = {
         "metric": "agent-steps/s", "value": value, "unit": "agent-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "agents_per_gpu": AGENTS, "fpi_iters": NUM_ITER, "policies": 4096,
+        "config": {"workload": workload(n_agents), "agents_per_gpu": n_agents, "fpi_iters": NUM_ITER, "policies": 4096,
                    "precision": agent.precision, "l2": "flushed (256 MiB write) between timed steps",
                    "parallelism": f"agents sharded over {world} GPU(s), no collective"},
         "e2e": {"value": total_agents * args.steps / (e2e_ms * 1e-3), "unit": "agent-steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
-                     "frac": achieved_tf / peak_tf, "traffic": None,
-                     "kernel": "neg-EFE (linear rows + policy evaluation), per launch over 256 agents",
+                     "frac": achieved_tf / peak_tf,
+                     "traffic": (EFE_TRAFFIC_PER_AGENT[agent.precision] * n_agents
+                                 if agent.precision in EFE_TRAFFIC_PER_AGENT else None),
+                     "kernel": f"neg-EFE launch over {n_agents} agents (W pack + policy evaluation + q_pi)",
                      "flops_per_launch": flops, "ms_per_launch": efe_ms,
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"},
         "cpu_baseline": None if cpu_val is None else {
-            "value": cpu_val, "unit": "agent-steps/s", "cores": threads_used(), "kind": "port",
-            "sample": f"{sample} agents of the same model, full agent step, FP64 NumPy oracle ({cpu_dt:.1f} s)"},
+            "value": cpu_val, "unit": "agent-steps/s", "cores": min(sample, cpu_workers()), "kind": "port",
+            "sample": f"agents 0..{sample - 1} of the timed model, full agent step, FP64 NumPy oracle, one worker "
+                      f"process per core ({cpu_dt:.1f} s wall)"},
+        "error_vs_fp64": err,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -303,6 +382,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
                     help="EFE contraction: fp32 (SIMT), tf32x3 or bf16 (tcgen05 tensor cores)")

@@ -53,24 +53,13 @@ def stable_xlogx(x):
 _LET = "abcdefghijklmnopqrstuvwxyz"
 
 
-def _contract_keep0(T, vecs):
-    """``factor_dot(T, vecs, keep_dims=(0,))`` batched over a policy axis.
-
-    ``T``: ``(D0, D1, ..., Dr)`` shared. ``vecs[j]``: ``(P, D_{j+1})``.
-    Returns ``(P, D0)``.
-    """
-    r = len(vecs)
-    sub_T = _LET[: r + 1]
-    subs = [sub_T] + ["z" + sub_T[j + 1] for j in range(r)]
-    return np.einsum(",".join(subs) + "->z" + sub_T[0], T, *vecs, optimize=True)
-
-
-def _contract_all(T, vecs):
-    """``factor_dot(T, vecs)`` (no kept dims) batched over a policy axis."""
-    r = len(vecs)
-    sub_T = _LET[:r]
-    subs = [sub_T] + ["z" + sub_T[j] for j in range(r)]
-    return np.einsum(",".join(subs) + "->z", T, *vecs, optimize=True)
+def _joint(qs, deps):
+    """Outer product of the dependency marginals per policy: ``(P, prod S)``,
+    row-major over ``deps`` (the flattening of ``A_m``'s state axes)."""
+    x = qs[deps[0]]
+    for d in deps[1:]:
+        x = (x[:, :, None] * qs[d][:, None, :]).reshape(x.shape[0], -1)
+    return np.ascontiguousarray(x)
 
 
 def expected_state(qs, B, u_t, B_deps):
@@ -103,12 +92,17 @@ def neg_efe_all_policies(policies, qs_init, A, B, C, A_deps, B_deps,
     G = np.zeros(P)
     for t in range(T):
         qs = expected_state(qs, B, policies[:, t, :], B_deps)
+        joint = {}  # dependency tuple -> (P, K) matrix of x = outer product of the marginals
         for m, (A_m, deps) in enumerate(zip(A, A_deps)):
-            qd = [qs[d] for d in deps]
-            qo = _contract_keep0(A_m, qd)                           # (P, O_m)
+            key = tuple(deps)
+            if key not in joint:
+                joint[key] = _joint(qs, deps)
+            x = joint[key]
+            # factor_dot(A_m, qs[deps], keep_dims=(0,)) == A_m (O, K) . x (K,) per policy
+            qo = x @ A_m.reshape(A_m.shape[0], -1).T                  # (P, O_m)
             if use_states_info_gain:
                 H_qo = -stable_xlogx(qo).sum(-1)
-                G += H_qo - _contract_all(H_A[m], qd)
+                G += H_qo - x @ H_A[m].reshape(-1)
             if use_utility:
                 C_m = np.asarray(C[m], np.float64)
                 c = C_m[t] if C_m.ndim > 1 else C_m
