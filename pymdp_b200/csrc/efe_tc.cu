@@ -17,23 +17,28 @@
 //
 // Mapping: one CTA = (agent, tile of 128 policies); M = 128 policies (TMEM
 // lanes), N = rows of the group, K = joint states in 128-byte chunks.
-//  * 256 threads generate the A operand (X, K-major, 128-byte swizzle) into
-//    shared memory; each policy row is written by two threads (half a chunk
-//    each). K is ordered with one factor innermost, padded to a power of two,
-//    so a half chunk is a few runs of prefix * q_inner[0..DLP) with q_inner
-//    in registers.
+//  * 16 producer warps (four threads per policy) roll the policy's factor
+//    marginals forward through B (staged in shared memory, transposed so a
+//    thread's block of next states is one broadcast vector load per parent
+//    state), build a per-policy table of the outer factors' products, and
+//    write X straight into tensor memory (tcgen05.st): the MMA's A operand,
+//    a ring of stages of kCps chunks.
 //  * W is packed once per call into ready-made shared-memory images (one per
-//    128-byte K chunk, already swizzled) and each chunk arrives with ONE
-//    cp.async.bulk (no multicast) on a transaction-count mbarrier.
-//  * Stages are triple-buffered: a "full" mbarrier per stage (W landed) and
-//    a "done" mbarrier per stage, armed by tcgen05.commit (MMAs reading the
-//    stage finished).
-//  * Thread 0 issues the UMMAs (kind::f16 BF16 operands, or kind::tf32 with
-//    the 3xTF32 hi/lo split for FP32-level accuracy), accumulating in TMEM.
-//  * Epilogue: warps 0-3 read their 32 TMEM lanes (= policies) with
-//    tcgen05.ld, form the entropy of the obs rows and add the step's linear
-//    row, accumulating G in FP64 registers.
-// Every mbarrier wait is bounded; on timeout the CTA records an error in
+//    128-byte K chunk, already swizzled). One loader thread moves several
+//    chunks per cp.async.bulk (no multicast) into a separate ring of large
+//    shared-memory slots: a bulk copy costs about the same few hundred cycles
+//    whether it moves 8 KB or 32 KB, so W arrives in big pieces.
+//  * One thread issues the UMMAs (kind::f16 BF16 operands, or kind::tf32 with
+//    the 3xTF32 hi/lo split for FP32-level accuracy, A from tensor memory and
+//    B from shared memory), accumulating in TMEM; consecutive stages rotate
+//    over `nacc` accumulators that the epilogue sums in FP64, which keeps the
+//    tensor core's FP32 accumulation chains short.
+//  * Epilogue: producer warp w reads TMEM lane quarter w % 4 (its 32
+//    policies) with tcgen05.ld, forms the entropy of the obs rows and adds the
+//    step's linear row, accumulating G in FP64 registers.
+// Hand-offs are mbarriers: x_full (X written), done (MMAs of an A stage
+// finished), w_full / w_free (W slot landed / consumed), acc_full / acc_free.
+// Every wait is bounded; on timeout the CTA records an error in
 // g_b2_device_error, stops issuing work, frees its TMEM and exits.
 #include <cuda_bf16.h>
 
@@ -54,14 +59,17 @@ namespace {
 constexpr int kTcMaxGroups = 8;
 constexpr int kTcTile = 128;
 constexpr uint32_t kWaitLimit = 1u << 22;
-constexpr int kTcMaxOuter = 3;  // tensor-core path: dependency rank <= 4
+constexpr int kTcMaxOuter = 3;       // tensor-core path: dependency rank <= 4
+constexpr int kTcMaxAStages = 8;     // A (X) stages in tensor memory
+constexpr int kTcWSlots = 2;         // W slots in shared memory
+constexpr int kTcWSlotTarget = 32768;  // preferred bytes per W bulk copy
 
 struct TcGroup {
   int64_t pack_off;  // per-agent byte offset of this group's W image
   int32_t K;         // prod of the dependency sizes
   int32_t outer;     // K / dim[rank-1]
-  int32_t Kpad;      // padded K (innermost size rounded to a power of two, then to the chunk)
-  int32_t nch;       // Kpad / chunk (a multiple of the chunks per stage)
+  int32_t Kpad;      // padded K (innermost size rounded to a power of two, then to the stage)
+  int32_t nch;       // Kpad / chunk (a multiple of the chunks per A stage)
   int32_t N, n_obs;  // rows: [0, n_obs) observations, then one linear row per step, then zeros
   int32_t rank, m_begin, m_end;
   int32_t lg;           // log2 of the padded innermost size
@@ -74,28 +82,32 @@ struct TcGroup {
 
 struct TcParams {
   int32_t G, Nmax;
-  int32_t nacc;       // TMEM accumulators the K chunks rotate over (summed in FP64)
+  int32_t nst;        // A stages in tensor memory (each kCps chunks)
+  int32_t wch;        // chunks per W slot (a multiple of kCps)
+  int32_t ws_bytes;   // bytes per W slot
+  int32_t nacc;       // TMEM accumulators the A stages rotate over (summed in FP64)
   int32_t b_words;    // floats of B staged in shared memory per CTA (0 = read B from global)
   int32_t a_col;      // first TMEM column of the A (X) stages; accumulators start at column 0
   int32_t tmem_cols;  // allocated TMEM columns
   int32_t pre_cap;    // outer indices the shared prefix table holds (>= every group's outer)
   int64_t pack_stride;  // bytes of W images per agent
+  int32_t b_off[kEfeMaxF];  // staged B of factor f: float offset in shared memory
+  int8_t b_tr[kEfeMaxF];    // 1: staged transposed as [k][u][s] (rank-1 parents, S % 4 == 0)
   int8_t mod_order[B2_MAX_MODALITIES];
   TcGroup grp[kTcMaxGroups];
 };
 
 template <int PREC>
 struct TcTraits;
-// kChunk: K elements per 128-byte row (one chunk); kCps: chunks per pipeline
-// stage (the MMA issuer handles kCps * 4 K-steps per handshake); kNst:
-// pipeline stages.
+// kChunk: K elements per 128-byte row (one chunk); kCps: chunks per A stage
+// (the MMA issuer handles kCps * 4 K-steps per stage hand-off).
 template <>
 struct TcTraits<B2_PRECISION_BF16> {
   static constexpr int kChunk = 64;
   static constexpr int kPlanes = 1;
   static constexpr int kEsz = 2;
-  static constexpr int kCps = 2;
-  static constexpr int kNst = 4;
+  static constexpr int kCps = 4;
+  static constexpr int kMaxNst = 3;
 };
 template <>
 struct TcTraits<B2_PRECISION_TF32X3> {
@@ -103,7 +115,7 @@ struct TcTraits<B2_PRECISION_TF32X3> {
   static constexpr int kPlanes = 2;  // hi, lo
   static constexpr int kEsz = 4;
   static constexpr int kCps = 1;
-  static constexpr int kNst = 3;
+  static constexpr int kMaxNst = 3;
 };
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) {
@@ -137,26 +149,29 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 // ---------------------------------------------------------- W packing
 // Writes, per agent and group, the W operand as ready-to-copy shared-memory
 // images: chunk c is planes x N rows x 128 bytes in the 128-byte-swizzled
-// K-major layout, so the main kernel moves a whole chunk with one bulk copy.
+// K-major layout, so the main kernel moves chunks with plain bulk copies.
 // K is ordered with the group's chosen innermost factor last, its size padded
-// to a power of two (padding columns are zero).
+// to a power of two (padding columns are zero). One thread = one packed
+// column kp of one group: it gathers the column's observation rows once,
+// takes their logs once, and forms all T linear rows from them.
 template <int PREC>
 __global__ void efe_tc_pack_kernel(const __grid_constant__ EfeParams p, const __grid_constant__ TcParams tp,
                                    const float* __restrict__ A, const float* __restrict__ C, uint8_t* __restrict__ pack) {
   using Tr = TcTraits<PREC>;
   const int64_t b = blockIdx.z;
-  const int g = blockIdx.y >> 8, n = blockIdx.y & 255;
+  const int g = blockIdx.y;
   if (g >= tp.G) return;
   const TcGroup& gr = tp.grp[g];
-  if (n >= gr.N) return;
   const int kp = blockIdx.x * blockDim.x + threadIdx.x;
   if (kp >= gr.Kpad) return;
   const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
   const bool ut = (p.flags & B2_FLAG_USE_UTILITY) != 0;
-  float v = 0.f;
+  const int N = gr.N, n_obs = gr.n_obs, T = p.T;
   const int inner = kp & ((1 << gr.lg) - 1);
   int outer = kp >> gr.lg;
-  if (inner < gr.dim[gr.rank - 1] && outer < gr.outer && n < gr.n_obs + p.T) {
+  const bool valid = inner < gr.dim[gr.rank - 1] && outer < gr.outer;
+  int64_t k = 0;
+  if (valid) {
     // original row-major index over the modalities' own axis order
     const EfeModality& m0 = p.mod[tp.mod_order[gr.m_begin]];
     int64_t stride[B2_MAX_DEP_RANK];
@@ -165,50 +180,53 @@ __global__ void efe_tc_pack_kernel(const __grid_constant__ EfeParams p, const __
       stride[a] = st;
       st *= p.S[m0.dep[a]];
     }
-    int64_t k = (int64_t)inner * stride[gr.axis[gr.rank - 1]];
+    k = (int64_t)inner * stride[gr.axis[gr.rank - 1]];
     for (int j = gr.rank - 2; j >= 0; --j) {
       const int d = gr.dim[j];
       const int qd = outer / d;
       k += (int64_t)(outer - qd * d) * stride[gr.axis[j]];
       outer = qd;
     }
-    if (n < gr.n_obs) {
-      int row = n;
-      for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
-        const EfeModality& md = p.mod[tp.mod_order[mi]];
-        if (row < md.O) {
-          v = __ldg(A + b * p.A_stride + md.A_off + (int64_t)row * md.K + k);
-          break;
-        }
-        row -= md.O;
-      }
-    } else {
-      const int t = n - gr.n_obs;
-      for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
-        const EfeModality& md = p.mod[tp.mod_order[mi]];
-        const float* Am = A + b * p.A_stride + md.A_off;
-        const float* Cm = C + b * p.C_stride + md.C_off + (int64_t)t * md.O;
-        for (int o = 0; o < md.O; ++o) {
-          const float a = __ldg(Am + (int64_t)o * md.K + k);
-          float w = 0.f;
-          if (ig) w += log_stable(a);
-          if (ut) w += __ldg(Cm + o);
-          v = fmaf(a, w, v);
-        }
-      }
-    }
   }
   const int c = kp / Tr::kChunk;
   const int byte = (kp % Tr::kChunk) * Tr::kEsz;
   uint8_t* img = pack + b * tp.pack_stride + gr.pack_off + (int64_t)c * gr.chunk_bytes;
-  const uint32_t off = tc::sw128_offset((uint32_t)n, (uint32_t)(byte >> 4)) + (byte & 15);
-  if (PREC == B2_PRECISION_BF16) {
-    *reinterpret_cast<uint16_t*>(img + off) = bf16_bits(v);
-  } else {
-    const float hi = tf32_round(v);
-    *reinterpret_cast<float*>(img + off) = hi;
-    *reinterpret_cast<float*>(img + (int64_t)gr.N * 128 + off) = tf32_round(v - hi);
+  auto put = [&](int n, float v) {
+    const uint32_t off = tc::sw128_offset((uint32_t)n, (uint32_t)(byte >> 4)) + (byte & 15);
+    if (PREC == B2_PRECISION_BF16) {
+      *reinterpret_cast<uint16_t*>(img + off) = bf16_bits(v);
+    } else {
+      const float hi = tf32_round(v);
+      *reinterpret_cast<float*>(img + off) = hi;
+      *reinterpret_cast<float*>(img + (int64_t)N * 128 + off) = tf32_round(v - hi);
+    }
+  };
+  // observation rows, and the information-gain part of the linear rows
+  float hl = 0.f;
+  int n = 0;
+  for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
+    const EfeModality& md = p.mod[tp.mod_order[mi]];
+    const float* Am = A + b * p.A_stride + md.A_off + k;
+    for (int o = 0; o < md.O; ++o, ++n) {
+      const float a = valid ? __ldg(Am + (int64_t)o * md.K) : 0.f;
+      if (ig) hl = fmaf(a, log_stable(a), hl);
+      put(n, a);
+    }
   }
+  // one linear row per step: the utility part re-reads the column (cached)
+  for (int t = 0; t < T; ++t) {
+    float v = hl;
+    if (ut && valid) {
+      for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
+        const EfeModality& md = p.mod[tp.mod_order[mi]];
+        const float* Am = A + b * p.A_stride + md.A_off + k;
+        const float* Cm = C + b * p.C_stride + md.C_off + (int64_t)t * md.O;
+        for (int o = 0; o < md.O; ++o) v = fmaf(__ldg(Am + (int64_t)o * md.K), __ldg(Cm + o), v);
+      }
+    }
+    put(n_obs + t, valid ? v : 0.f);
+  }
+  for (int r = n_obs + T; r < N; ++r) put(r, 0.f);
 }
 
 // Bounded mbarrier wait that also gives up as soon as another role of the
@@ -233,16 +251,30 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
 }
 
+// Position in a ring of `n` slots: slot index and the parity of its use count.
+struct Ring {
+  int slot = 0;
+  uint32_t phase = 0;  // parity of the current use of `slot`
+  bool wrapped = false;  // every slot has been used at least once
+  __device__ __forceinline__ void next(int n) {
+    if (++slot == n) {
+      slot = 0;
+      phase ^= 1u;
+      wrapped = true;
+    }
+  }
+};
+
 struct TcSmem {
-  uint8_t* Ws;
+  uint8_t* Ws;         // W slots
   float* pre;          // [pre_cap][128]: prefix product over the outer factors per policy
-  uint64_t* x_full;    // per stage: the producer warps wrote X into tensor memory AND the W
-                       // bulk copy landed (16 producer arrivals + the loader's expect_tx)
-  uint64_t* done;      // per stage: the MMAs reading the stage finished (tcgen05.commit)
+  uint64_t* x_full;    // per A stage: the 16 producer warps wrote X into tensor memory
+  uint64_t* done;      // per A stage: the MMAs reading the stage finished (tcgen05.commit)
+  uint64_t* w_full;    // per W slot: the bulk copy landed (transaction count)
+  uint64_t* w_free;    // per W slot: the MMAs reading the slot finished (tcgen05.commit)
   uint64_t* acc_full;  // all MMAs of a (step, group) GEMM finished
   uint64_t* acc_free;  // the epilogue has read the accumulators
   volatile int* abort_flag;
-  int ws_bytes;
 };
 
 // ------------------------------------------------------ X generation
@@ -254,20 +286,28 @@ struct TcSmem {
 //   MODE 0: DLP <= Q: Q/DLP runs of pre * q_inner[0..DLP), q_inner in registers
 //   MODE 1: Q < DLP <= chunk: one run segment at a fixed offset, in registers
 //   MODE 2: DLP > chunk: one run segment at a varying offset, read per chunk
+// Every parameter used inside the stage loop is copied to a register first:
+// the tcgen05 / mbarrier asm statements clobber memory, so a value read from
+// the kernel parameters (or any memory) inside the loop would be reloaded
+// after each of them.
 template <int PREC, int MODE, int DLP>
 __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams& tp, const EfeParams& p,
-                                              const float* __restrict__ q, const TcSmem& sm, uint32_t tmem, int warp,
-                                              int pl, int qt, int lane, bool active, uint32_t& it) {
+                                              const float* __restrict__ q, const TcSmem sm, uint32_t tmem, int warp,
+                                              int pl, int qt, int lane, bool active, Ring& ring) {
   using Tr = TcTraits<PREC>;
   constexpr int CH = Tr::kChunk;
   constexpr int Q = CH / 4;
   constexpr int CPS = Tr::kCps;
-  constexpr int NST = Tr::kNst;
   constexpr int kPl = Tr::kPlanes;
   constexpr int kQl = MODE == 0 ? DLP : (MODE == 1 ? Q : 1);
   const int lg = gr.lg;
   const int dl = gr.dim[gr.rank - 1];
   const int outer = gr.outer;
+  const int nst = tp.nst;
+  const int a_col = tp.a_col;
+  uint64_t* const done = sm.done;
+  uint64_t* const x_full = sm.x_full;
+  volatile int* const abort_flag = sm.abort_flag;
   const float* qin = q + p.qs_off[gr.dep[gr.rank - 1]] * kTcTile + pl;
   const float* pre = sm.pre + pl;
   float ql[kQl];
@@ -280,15 +320,14 @@ __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams&
     for (int i = 0; i < kQl; ++i) ql[i] = (off + i < dl && active) ? qin[(off + i) * kTcTile] : 0.f;
   }
   const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const int nst = gr.nch / CPS;
-  for (int c = 0; c < nst; ++c, ++it) {
-    const int st = it % NST;
-    const uint32_t use = it / NST;
-    if (use > 0) {
-      warp_wait(&sm.done[st], (use - 1) & 1, sm.abort_flag, lane);
+  const int nstages = gr.nch / CPS;
+  for (int c = 0; c < nstages; ++c) {
+    const int st = ring.slot;
+    if (ring.wrapped) {
+      warp_wait(&done[st], ring.phase ^ 1u, abort_flag, lane);
       tc::fence_after_sync();
     }
-    const uint32_t ta_st = lane_base + (uint32_t)(tp.a_col + st * 32 * kPl * CPS + qt * 8);
+    const uint32_t ta_st = lane_base + (uint32_t)(a_col + st * 32 * kPl * CPS + qt * 8);
 #pragma unroll
     for (int h = 0; h < CPS; ++h) {
       const int k0 = (c * CPS + h) * CH + qt * Q;
@@ -334,28 +373,140 @@ __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams&
     tc::tmem_wait_st();
     tc::fence_before_sync();
     __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.x_full[st]);
+    if (lane == 0) mbar_arrive(&x_full[st]);
+    ring.next(nst);
   }
 }
 
 template <int PREC>
 __device__ __forceinline__ void produce_dispatch(const TcGroup& gr, const TcParams& tp, const EfeParams& p,
-                                                 const float* __restrict__ q, const TcSmem& sm, uint32_t tmem, int warp,
-                                                 int pl, int qt, int lane, bool active, uint32_t& it) {
+                                                 const float* __restrict__ q, const TcSmem sm, uint32_t tmem, int warp,
+                                                 int pl, int qt, int lane, bool active, Ring& ring) {
   constexpr int CH = TcTraits<PREC>::kChunk;
   constexpr int Q = CH / 4;
   const int dlp = 1 << gr.lg;
   if (dlp > CH) {
-    produce_group<PREC, 2, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
+    produce_group<PREC, 2, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
   } else if (dlp > Q) {
-    produce_group<PREC, 1, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
+    produce_group<PREC, 1, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
   } else {
     switch (gr.lg) {
-      case 0: produce_group<PREC, 0, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
-      case 1: produce_group<PREC, 0, 2>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
-      case 2: produce_group<PREC, 0, 4>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
-      case 3: produce_group<PREC, 0, (Q >= 8 ? 8 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it); break;
-      default: produce_group<PREC, 0, (Q >= 16 ? 16 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
+      case 0: produce_group<PREC, 0, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
+      case 1: produce_group<PREC, 0, 2>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
+      case 2: produce_group<PREC, 0, 4>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
+      case 3: produce_group<PREC, 0, (Q >= 8 ? 8 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
+      default: produce_group<PREC, 0, (Q >= 16 ? 16 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
+    }
+  }
+}
+
+// Expected states of one policy for one step (pymdp/control.py:351-389):
+// thread quarter qt computes next states of every factor. Factors staged
+// transposed ([k][u][s], rank-1 parents, S % 4 == 0) are done in blocks of
+// four next states: per parent state one broadcast 16-byte load of B and one
+// load of the parent marginal. Other factors use the generic strided loop.
+__device__ __forceinline__ void rollout_step(const EfeParams& p, const TcParams& tp, const float* __restrict__ Bag,
+                                             bool b_staged, const int32_t* __restrict__ u_pol, const float* qc,
+                                             float* qn, int pl, int qt, bool& bad_action) {
+  for (int f = 0; f < p.F; ++f) {
+    const EfeFactor& fb = p.fac[f];
+    const int U = p.U[f];
+    const int S = p.S[f];
+    const int K = fb.K;
+    int u = u_pol[f];
+    if (u < 0 || u >= U) {
+      bad_action = true;
+      u = 0;
+    }
+    float* qnf = qn + p.qs_off[f] * kTcTile + pl;
+    if (b_staged && tp.b_tr[f]) {
+      const float* qv = qc + p.qs_off[fb.dep[0]] * kTcTile + pl;
+      const float* Bt = Bag + tp.b_off[f] + u * S;
+      const int row = U * S;
+      for (int blk = qt * 4; blk < S; blk += 16) {
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        const float* bp = Bt + blk;
+#pragma unroll 4
+        for (int k = 0; k < K; ++k) {
+          const float qk = qv[k * kTcTile];
+          const float4 w = *reinterpret_cast<const float4*>(bp + k * row);
+          a0 = fmaf(w.x, qk, a0);
+          a1 = fmaf(w.y, qk, a1);
+          a2 = fmaf(w.z, qk, a2);
+          a3 = fmaf(w.w, qk, a3);
+        }
+        qnf[(blk + 0) * kTcTile] = a0;
+        qnf[(blk + 1) * kTcTile] = a1;
+        qnf[(blk + 2) * kTcTile] = a2;
+        qnf[(blk + 3) * kTcTile] = a3;
+      }
+      continue;
+    }
+    const float* Bf = Bag + (b_staged ? (int64_t)tp.b_off[f] : fb.B_off);
+    for (int s = qt; s < S; s += 4) {
+      float acc = 0.f;
+      const float* Bs = Bf + (int64_t)s * K * U + u;
+      if (fb.rank == 1) {
+        const float* qv = qc + p.qs_off[fb.dep[0]] * kTcTile + pl;
+        for (int k = 0; k < K; ++k) acc = fmaf(Bs[k * U], qv[k * kTcTile], acc);
+      } else {
+        int dig[B2_MAX_DEP_RANK];
+#pragma unroll
+        for (int i = 0; i < B2_MAX_DEP_RANK; ++i) dig[i] = 0;
+        for (int k = 0; k < K; ++k) {
+          float w = 1.f;
+#pragma unroll
+          for (int i = 0; i < B2_MAX_DEP_RANK; ++i)
+            if (i < fb.rank) w *= qc[(p.qs_off[fb.dep[i]] + dig[i]) * kTcTile + pl];
+          acc = fmaf(Bs[k * U], w, acc);
+          bool carry = true;
+#pragma unroll
+          for (int i = B2_MAX_DEP_RANK - 1; i >= 0; --i) {
+            if (carry && i < fb.rank) {
+              if (++dig[i] < p.S[fb.dep[i]]) carry = false;
+              else dig[i] = 0;
+            }
+          }
+        }
+      }
+      qnf[s * kTcTile] = acc;
+    }
+  }
+}
+
+// pre[ko][pl] = prod over the group's outer factors of q[digit(ko)], for the
+// contiguous quarter qt of the ko range; digits advance by one per entry.
+__device__ __forceinline__ void build_prefix(const TcGroup& gr, const EfeParams& p, const float* q, float* pre,
+                                             int pl, int qt, bool active) {
+  const int n = gr.rank - 1;
+  const int outer = gr.outer;
+  const int per = (outer + 3) >> 2;
+  const int ko0 = qt * per;
+  const int ko1 = ko0 + per < outer ? ko0 + per : outer;
+  if (ko0 >= ko1) return;
+  int d[kTcMaxOuter], o[kTcMaxOuter], dig[kTcMaxOuter];
+#pragma unroll
+  for (int x = 0; x < kTcMaxOuter; ++x) {
+    d[x] = x < n ? gr.dim[x] : 1;
+    o[x] = x < n ? p.qs_off[gr.dep[x]] * kTcTile + pl : 0;
+  }
+  int rem = ko0;
+#pragma unroll
+  for (int x = kTcMaxOuter - 1; x >= 0; --x) {
+    const int qd = rem / d[x];
+    dig[x] = rem - qd * d[x];
+    rem = qd;
+  }
+  for (int ko = ko0; ko < ko1; ++ko) {
+    float v = 1.f;
+#pragma unroll
+    for (int x = 0; x < kTcMaxOuter; ++x)
+      if (x < n) v *= q[o[x] + dig[x] * kTcTile];
+    pre[ko * kTcTile + pl] = active ? v : 0.f;
+#pragma unroll
+    for (int x = kTcMaxOuter - 1; x >= 0; --x) {
+      if (++dig[x] < d[x]) break;
+      dig[x] = 0;
     }
   }
 }
@@ -363,9 +514,8 @@ __device__ __forceinline__ void produce_dispatch(const TcGroup& gr, const TcPara
 // ------------------------------------------------------------ main kernel
 // Warp roles: 0-15 producers (four threads per policy row: state rollout,
 // prefix table, X generation into tensor memory, epilogue), 16 = W loader
-// (bulk copies, up to kNst stages ahead), 17 = MMA issuer (kCps * 4 K-steps
-// back to back per stage). The chunk loop has no CTA-wide barrier: stages
-// are handed over through the x_full / w_full / done mbarriers.
+// (large bulk copies into the W slots), 17 = MMA issuer (kCps * 4 K-steps
+// back to back per A stage). The chunk loop has no CTA-wide barrier.
 constexpr int kProducers = 512;
 constexpr int kThreadsAll = kProducers + 64;
 
@@ -379,19 +529,20 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
   using Tr = TcTraits<PREC>;
   constexpr int kPl = Tr::kPlanes;
   constexpr int CPS = Tr::kCps;
-  constexpr int NST = Tr::kNst;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int nst = tp.nst;
   TcSmem sm;
-  sm.ws_bytes = CPS * kPl * tp.Nmax * 128;
   sm.Ws = base;
-  double* red = reinterpret_cast<double*>(sm.Ws + NST * sm.ws_bytes);  // [4][128] partial G
+  double* red = reinterpret_cast<double*>(sm.Ws + kTcWSlots * tp.ws_bytes);  // [4][128] partial G
   float* qsm = reinterpret_cast<float*>(red + 4 * kTcTile);
   float* bsm = qsm + 2 * p.S_tot * kTcTile;  // this agent's B (when tp.b_words > 0)
   sm.pre = bsm + tp.b_words;                 // [pre_cap][128]
   sm.x_full = reinterpret_cast<uint64_t*>(sm.pre + tp.pre_cap * kTcTile);
-  sm.done = sm.x_full + NST;
-  sm.acc_full = sm.done + NST;
+  sm.done = sm.x_full + kTcMaxAStages;
+  sm.w_full = sm.done + kTcMaxAStages;
+  sm.w_free = sm.w_full + kTcWSlots;
+  sm.acc_full = sm.w_free + kTcWSlots;
   sm.acc_free = sm.acc_full + 1;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm.acc_free + 1);
   sm.abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -401,9 +552,13 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, (uint32_t)tp.tmem_cols);
   if (tid == 0) {
-    for (int s = 0; s < NST; ++s) {
-      tc::mbar_init(&sm.x_full[s], kProducers / 32 + 1);
+    for (int s = 0; s < nst; ++s) {
+      tc::mbar_init(&sm.x_full[s], kProducers / 32);
       tc::mbar_init(&sm.done[s], 1);
+    }
+    for (int s = 0; s < kTcWSlots; ++s) {
+      tc::mbar_init(&sm.w_full[s], 1);
+      tc::mbar_init(&sm.w_free[s], 1);
     }
     tc::mbar_init(sm.acc_full, 1);
     tc::mbar_init(sm.acc_free, kProducers / 32);
@@ -411,7 +566,29 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     *sm.abort_flag = 0;
   }
   for (int i = tid; i < p.S_tot * kTcTile; i += blockDim.x) qsm[i] = __ldg(qs_init + b * p.S_tot + i / kTcTile);
-  for (int i = tid; i < tp.b_words && i < p.B_stride; i += blockDim.x) bsm[i] = __ldg(B + b * p.B_stride + i);
+  if (tp.b_words > 0) {
+    // stage B: transposed [k][u][s] where the rollout reads it that way
+    for (int f = 0; f < p.F; ++f) {
+      const EfeFactor& fb = p.fac[f];
+      const int S = p.S[f], K = fb.K, U = p.U[f];
+      const int n = S * K * U;
+      const float* src = B + b * p.B_stride + fb.B_off;
+      float* dst = bsm + tp.b_off[f];
+      const bool tr = tp.b_tr[f] != 0;
+      for (int i = tid; i < n; i += blockDim.x) {
+        const float v = __ldg(src + i);
+        if (tr) {
+          const int s = i / (K * U);
+          const int r = i - s * (K * U);
+          const int k = r / U;
+          const int u = r - k * U;
+          dst[(k * U + u) * S + s] = v;
+        } else {
+          dst[i] = v;
+        }
+      }
+    }
+  }
   const float* Bag = tp.b_words > 0 ? bsm : B + b * p.B_stride;
   tc::fence_before_sync();
   __syncthreads();
@@ -419,53 +596,71 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == kProducers / 32) {
-    // ---------------- W loader: one bulk copy per stage, NST stages ahead
+    // ---------------- W loader: large bulk copies into the W slots
     if (lane == 0) {
-      uint32_t it = 0;
-      for (int t = 0; t < p.T; ++t)
-        for (int g = 0; g < tp.G; ++g) {
-          const TcGroup& gr = tp.grp[g];
-          const uint8_t* wimg = pack + b * tp.pack_stride + gr.pack_off;
-          const uint32_t bytes = (uint32_t)(CPS * gr.chunk_bytes);
-          const int nst = gr.nch / CPS;
-          for (int c = 0; c < nst; ++c, ++it) {
-            const int st = it % NST;
-            const uint32_t use = it / NST;
-            if (use > 0 && !wait_or_abort(&sm.done[st], (use - 1) & 1, sm.abort_flag)) continue;
-            if (*sm.abort_flag) continue;  // waiters give up through the abort flag
-            mbar_expect_tx(&sm.x_full[st], bytes);
-            bulk_g2s(tc::smem_u32(sm.Ws + st * sm.ws_bytes), wimg + (int64_t)c * bytes, bytes, &sm.x_full[st]);
+      const int T = p.T, G = tp.G, wch = tp.wch, ws_bytes = tp.ws_bytes;
+      uint64_t* const w_full = sm.w_full;
+      uint64_t* const w_free = sm.w_free;
+      volatile int* const abort_flag = sm.abort_flag;
+      const uint32_t ws0 = tc::smem_u32(sm.Ws);
+      const uint8_t* const pack_b = pack + b * tp.pack_stride;
+      Ring wr;
+      for (int t = 0; t < T; ++t)
+        for (int g = 0; g < G; ++g) {
+          const int nch = tp.grp[g].nch, chunk_bytes = tp.grp[g].chunk_bytes;
+          const uint8_t* wimg = pack_b + tp.grp[g].pack_off;
+          for (int c0 = 0; c0 < nch; c0 += wch) {
+            const int cnt = nch - c0 < wch ? nch - c0 : wch;
+            const uint32_t bytes = (uint32_t)(cnt * chunk_bytes);
+            const int s = wr.slot;
+            const bool ok = !wr.wrapped || wait_or_abort(&w_free[s], wr.phase ^ 1u, abort_flag);
+            if (ok && !*abort_flag) {  // otherwise waiters give up through the abort flag
+              mbar_expect_tx(&w_full[s], bytes);
+              bulk_g2s(ws0 + (uint32_t)(s * ws_bytes), wimg + (int64_t)c0 * chunk_bytes, bytes, &w_full[s]);
+            }
+            wr.next(kTcWSlots);
           }
         }
     }
   } else if (warp == kProducers / 32 + 1) {
     // ---------------- MMA issuer
     if (lane == 0) {
-      // per-stage operand addresses: arithmetic in the stage index (no arrays)
       const uint64_t wdesc0 = tc::desc_kmajor_sw128(tc::smem_u32(sm.Ws));
-      const uint32_t wstep16 = (uint32_t)sm.ws_bytes >> 4;
       const uint32_t acol0 = tmem + (uint32_t)tp.a_col;
-      uint32_t it = 0, j = 0;
-      for (int t = 0; t < p.T; ++t)
-        for (int g = 0; g < tp.G; ++g, ++j) {
-          const TcGroup& gr = tp.grp[g];
-          const uint32_t idesc = gr.idesc;
-          const uint32_t chunk16 = (uint32_t)gr.chunk_bytes >> 4;  // descriptor units per chunk tile
-          const uint32_t lo16 = (uint32_t)(gr.N * 128) >> 4;       // descriptor units to the lo plane
-          const int nst = gr.nch / CPS;
-          if (j > 0) wait_or_abort(sm.acc_free, (j - 1) & 1, sm.abort_flag);
+      const int T = p.T, G = tp.G, wch = tp.wch, nacc = tp.nacc;
+      const uint32_t ws16 = (uint32_t)tp.ws_bytes >> 4;
+      uint64_t* const x_full = sm.x_full;
+      uint64_t* const done = sm.done;
+      uint64_t* const w_full = sm.w_full;
+      uint64_t* const w_free = sm.w_free;
+      uint64_t* const acc_full = sm.acc_full;
+      uint64_t* const acc_free = sm.acc_free;
+      volatile int* const abort_flag = sm.abort_flag;
+      Ring ar, wr;
+      uint32_t j = 0;
+      for (int t = 0; t < T; ++t)
+        for (int g = 0; g < G; ++g, ++j) {
+          const uint32_t idesc = tp.grp[g].idesc;
+          const int N = tp.grp[g].N, nch = tp.grp[g].nch;
+          const uint32_t chunk16 = (uint32_t)tp.grp[g].chunk_bytes >> 4;  // descriptor units per chunk tile
+          const uint32_t lo16 = (uint32_t)(N * 128) >> 4;                 // descriptor units to the lo plane
+          const int nstages = nch / CPS;
+          if (j > 0) wait_or_abort(acc_free, (j - 1) & 1, abort_flag);
           int acc_slot = 0;
-          for (int c = 0; c < nst; ++c, ++it) {
-            const int st = it % NST;
-            const uint32_t use = it / NST;
-            const bool okx = wait_or_abort(&sm.x_full[st], use & 1, sm.abort_flag);
-            if (okx && !*sm.abort_flag) {
+          bool w_ok = true;
+          int wk = 0;  // position of the current A stage's first chunk in its W slot
+          for (int c = 0; c < nstages; ++c) {
+            const int kc = c * CPS;  // first chunk of this A stage (group-relative)
+            if (wk == 0) w_ok = wait_or_abort(&w_full[wr.slot], wr.phase, abort_flag);
+            const int st = ar.slot;
+            const bool okx = wait_or_abort(&x_full[st], ar.phase, abort_flag);
+            if (okx && w_ok && !*abort_flag) {
               tc::fence_after_sync();
               // stage c accumulates into accumulator c % nacc: shorter FP32
               // accumulation chains inside the tensor core
-              const uint32_t dt = tmem + (uint32_t)(acc_slot * gr.N);
-              const uint32_t first = c < tp.nacc ? 0u : 1u;
-              const uint64_t wd = wdesc0 + (uint64_t)(st * wstep16);
+              const uint32_t dt = tmem + (uint32_t)(acc_slot * N);
+              const uint32_t first = c < nacc ? 0u : 1u;
+              const uint64_t wd = wdesc0 + (uint64_t)((uint32_t)wr.slot * ws16 + (uint32_t)wk * chunk16);
               const uint32_t a0 = acol0 + (uint32_t)(st * 32 * kPl * CPS);
 #pragma unroll
               for (int h = 0; h < CPS; ++h)
@@ -484,10 +679,17 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
                 }
             }
             // always arm the barriers so every waiter makes progress
-            tc::mma_commit(&sm.done[st]);
-            if (++acc_slot == tp.nacc) acc_slot = 0;
+            tc::mma_commit(&done[st]);
+            ar.next(nst);
+            wk += CPS;
+            if (wk == wch || kc + CPS == nch) {
+              tc::mma_commit(&w_free[wr.slot]);
+              wr.next(kTcWSlots);
+              wk = 0;
+            }
+            if (++acc_slot == nacc) acc_slot = 0;
           }
-          tc::mma_commit(sm.acc_full);
+          tc::mma_commit(acc_full);
         }
     }
   } else {
@@ -500,114 +702,55 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     double g_acc = 0.0;
     bool bad_action = false;
     int cur = 0;
-    uint32_t it = 0, j = 0;
+    Ring ring;
+    uint32_t j = 0;
+    const int32_t* u_base = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (int64_t)(active ? pol : 0) * p.T * p.F;
     for (int t = 0; t < p.T; ++t) {
-      // expected states (pymdp/control.py:351-389): policy pl, states s = qt, qt + 4, ...
-      {
-        const float* qc = qsm + cur * p.S_tot * kTcTile;
-        float* qn = qsm + (cur ^ 1) * p.S_tot * kTcTile;
-        const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) +
-                               (int64_t)(active ? pol : 0) * p.T * p.F + t * p.F;
-        for (int f = 0; f < p.F; ++f) {
-          const EfeFactor& fb = p.fac[f];
-          int u = u_pol[f];
-          if (u < 0 || u >= p.U[f]) {
-            bad_action = true;
-            u = 0;
-          }
-          const float* Bf = Bag + fb.B_off;
-          const int U = p.U[f];
-          const int K = fb.K;
-          for (int s = qt; s < p.S[f]; s += 4) {
-            float acc = 0.f;
-            const float* Bs = Bf + s * K * U + u;
-            if (fb.rank == 1) {
-              const float* qv = qc + p.qs_off[fb.dep[0]] * kTcTile + pl;
-              float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-              int k = 0;
-              for (; k + 3 < K; k += 4) {
-                a0 = fmaf(Bs[0], qv[0], a0);
-                a1 = fmaf(Bs[U], qv[kTcTile], a1);
-                a2 = fmaf(Bs[2 * U], qv[2 * kTcTile], a2);
-                a3 = fmaf(Bs[3 * U], qv[3 * kTcTile], a3);
-                Bs += 4 * U;
-                qv += 4 * kTcTile;
-              }
-              for (; k < K; ++k, Bs += U, qv += kTcTile) a0 = fmaf(Bs[0], qv[0], a0);
-              acc = (a0 + a1) + (a2 + a3);
-            } else {
-              int dig[B2_MAX_DEP_RANK];
-#pragma unroll
-              for (int i = 0; i < B2_MAX_DEP_RANK; ++i) dig[i] = 0;
-              for (int k = 0; k < K; ++k) {
-                float w = 1.f;
-#pragma unroll
-                for (int i = 0; i < B2_MAX_DEP_RANK; ++i)
-                  if (i < fb.rank) w *= qc[(p.qs_off[fb.dep[i]] + dig[i]) * kTcTile + pl];
-                acc = fmaf(Bs[k * U], w, acc);
-                bool carry = true;
-#pragma unroll
-                for (int i = B2_MAX_DEP_RANK - 1; i >= 0; --i) {
-                  if (carry && i < fb.rank) {
-                    if (++dig[i] < p.S[fb.dep[i]]) carry = false;
-                    else dig[i] = 0;
-                  }
-                }
-              }
-            }
-            qn[(p.qs_off[f] + s) * kTcTile + pl] = acc;
-          }
-        }
-      }
+      rollout_step(p, tp, Bag, tp.b_words > 0, u_base + t * p.F, qsm + cur * p.S_tot * kTcTile,
+                   qsm + (cur ^ 1) * p.S_tot * kTcTile, pl, qt, bad_action);
       producers_sync();
       cur ^= 1;
       const float* q = qsm + cur * p.S_tot * kTcTile;
       for (int g = 0; g < tp.G; ++g, ++j) {
         const TcGroup& gr = tp.grp[g];
-        // prefix table: pre[ko][pl] = prod_{outer factors} q (digits of ko)
-        {
-          const int n = gr.rank - 1;
-          for (int ko = qt; ko < gr.outer; ko += 4) {
-            float v = 1.f;
-            int rem = ko;
-#pragma unroll
-            for (int x = kTcMaxOuter - 1; x >= 0; --x)
-              if (x < n) {
-                const int d = gr.dim[x];
-                const int qd = rem / d;
-                v *= q[(p.qs_off[gr.dep[x]] + (rem - qd * d)) * kTcTile + pl];
-                rem = qd;
-              }
-            sm.pre[ko * kTcTile + pl] = active ? v : 0.f;
-          }
-        }
+        build_prefix(gr, p, q, sm.pre, pl, qt, active);
         producers_sync();
-        produce_dispatch<PREC>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, it);
+        produce_dispatch<PREC>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
         // epilogue: warp w reads TMEM lane quarter (w & 3) = its 32 policies,
         // 16-column blocks qt*16, qt*16 + 64, ... of every accumulator
+        const int N = gr.N, n_obs = gr.n_obs;
+        const int nacc = gr.nch / CPS < tp.nacc ? gr.nch / CPS : tp.nacc;
         warp_wait(sm.acc_full, j & 1, sm.abort_flag, lane);
         tc::fence_after_sync();
         {
           const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-          const int nacc = gr.nch / CPS < tp.nacc ? gr.nch / CPS : tp.nacc;
           double h = 0.0, lin = 0.0;
-          for (int n0 = qt * 16; n0 < gr.N; n0 += 64) {
+          for (int n0 = qt * 16; n0 < N; n0 += 64) {
             double sum[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) sum[k] = 0.0;
-            for (int a = 0; a < nacc; ++a) {
-              uint32_t r[16];
-              tc::tmem_ld16(taddr + (uint32_t)(a * gr.N + n0), r);
+            int a = 0;
+            for (; a + 1 < nacc; a += 2) {
+              uint32_t r0[16], r1[16];
+              tc::tmem_ld16(taddr + (uint32_t)(a * N + n0), r0);
+              tc::tmem_ld16(taddr + (uint32_t)((a + 1) * N + n0), r1);
               tc::tmem_wait_ld();
 #pragma unroll
-              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r[k]);
+              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r0[k]) + (double)__uint_as_float(r1[k]);
+            }
+            if (a < nacc) {
+              uint32_t r0[16];
+              tc::tmem_ld16(taddr + (uint32_t)(a * N + n0), r0);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r0[k]);
             }
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
               const int n = n0 + k;
-              if (n < gr.n_obs) {
+              if (n < n_obs) {
                 if (ig) h -= sum[k] * (double)logf(fmaxf((float)sum[k], kMinVal));
-              } else if (n == gr.n_obs + t) {
+              } else if (n == n_obs + t) {
                 lin = sum[k];
               }
             }
@@ -644,7 +787,6 @@ int32_t tc_plan_t(const EfeParams& p, TcParams* tp, int* smem_bytes) {
   const int chunk = Tr::kChunk;
   const int planes = Tr::kPlanes;
   const int cps = Tr::kCps;
-  const int nst = Tr::kNst;
   std::vector<std::vector<int>> groups;
   std::vector<std::vector<int>> tuples;
   for (int m = 0; m < p.M; ++m) {
@@ -724,24 +866,46 @@ int32_t tc_plan_t(const EfeParams& p, TcParams* tp, int* smem_bytes) {
     off += (int64_t)gr.nch * gr.chunk_bytes;
   }
   tp->Nmax = Nmax;
-  const int a_cols = nst * 32 * planes * cps;  // A stages: 128 lanes x 128 bytes per plane per chunk
-  int nacc = (512 - a_cols) / Nmax;
+  // A stages in tensor memory: as many as leave room for at least 2
+  // accumulators (BF16) / 5 (3xTF32, whose FP32 accumulation chains must stay
+  // short), within the trait's maximum.
+  const int stage_cols = 32 * planes * cps;  // 128 lanes x 128 bytes per plane per chunk
+  const int want_acc = PREC == B2_PRECISION_BF16 ? 2 : 5;
+  int nst = Tr::kMaxNst;
+  while (nst > 2 && 512 - nst * stage_cols < want_acc * Nmax) --nst;
+  int nacc = (512 - nst * stage_cols) / Nmax;
   nacc = nacc > 8 ? 8 : nacc;
   if (nacc < 1) return B2_ERR_UNSUPPORTED;
+  tp->nst = nst;
   tp->nacc = nacc;
   tp->a_col = (nacc * Nmax + 31) / 32 * 32;
-  if (tp->a_col + a_cols > 512) return B2_ERR_UNSUPPORTED;
+  if (tp->a_col + nst * stage_cols > 512) return B2_ERR_UNSUPPORTED;
   tp->tmem_cols = 512;
+  // W slots: whole A stages, about kTcWSlotTarget bytes per bulk copy
+  const int chunk_max = planes * Nmax * 128;
+  int wch = kTcWSlotTarget / chunk_max / cps * cps;
+  if (wch < cps) wch = cps;
+  tp->wch = wch;
+  tp->ws_bytes = wch * chunk_max;
   tp->pre_cap = (outer_max + 1) / 2 * 2;
   tp->pack_stride = (off + 1023) / 1024 * 1024;
-  const int w_bytes = cps * planes * Nmax * 128;
-  int64_t smem = 1024 + (int64_t)nst * w_bytes + 4LL * kTcTile * 8 + 2LL * p.S_tot * kTcTile * 4 +
-                 (int64_t)tp->pre_cap * kTcTile * 4 + (2 * nst + 2) * 8 + 16;
+  int64_t smem = 1024 + (int64_t)kTcWSlots * tp->ws_bytes + 4LL * kTcTile * 8 + 2LL * p.S_tot * kTcTile * 4 +
+                 (int64_t)tp->pre_cap * kTcTile * 4 + (2 * kTcMaxAStages + 2 * kTcWSlots + 2) * 8 + 16;
   if (smem > 227 * 1024) return B2_ERR_UNSUPPORTED;
-  const int64_t b_words = (p.B_stride + 1) / 2 * 2;  // keep the barriers 8-byte aligned
-  if (smem + b_words * 4 <= 227 * 1024) {
+  // B staged per factor at 16-byte aligned offsets (transposed where the
+  // rollout's vector path applies)
+  int64_t b_words = 0;
+  for (int f = 0; f < p.F; ++f) {
+    tp->b_off[f] = (int32_t)b_words;
+    tp->b_tr[f] = (p.fac[f].rank == 1 && p.S[f] % 4 == 0) ? 1 : 0;
+    b_words += ((int64_t)p.S[f] * p.fac[f].K * p.U[f] + 3) / 4 * 4;
+  }
+  if (smem + b_words * 4 <= 227 * 1024 && b_words < (1 << 30)) {
     tp->b_words = (int32_t)b_words;
     smem += b_words * 4;
+  } else {
+    tp->b_words = 0;
+    std::memset(tp->b_tr, 0, sizeof(tp->b_tr));
   }
   *smem_bytes = (int)smem;
   return B2_OK;
@@ -758,7 +922,7 @@ int32_t launch_tc_t(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_ba
   B2_TRY(ws_alloc((void**)&pack, bytes, stream, kEfeName));
   int Kmax = 0;
   for (int g = 0; g < tp.G; ++g) Kmax = tp.grp[g].Kpad > Kmax ? tp.grp[g].Kpad : Kmax;
-  dim3 pgrid((unsigned)((Kmax + 127) / 128), (unsigned)(tp.G * 256), (unsigned)Bn);
+  dim3 pgrid((unsigned)((Kmax + 127) / 128), (unsigned)tp.G, (unsigned)Bn);
   dim3 grid((unsigned)((p.P + kTcTile - 1) / kTcTile), (unsigned)Bn);
   efe_tc_pack_kernel<PREC><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
   int32_t rc = check_launch("efe_ffi tc pack");
