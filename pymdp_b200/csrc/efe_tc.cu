@@ -265,6 +265,139 @@ struct Ring {
   }
 };
 
+// One A stage of MMAs (kCps chunks x 4 K-steps; 3xTF32: three MMAs per
+// K-step) in a single asm block that first starts non-blocking tests of the
+// next stage's barriers: their latency overlaps the MMA issue, and the loop
+// only blocks when a test found the next stage not ready yet. Operands:
+// dt = accumulator, a0 = A stage in tensor memory, wd = descriptor of the
+// stage's first W chunk, chunk16 / lo16 = descriptor steps to the next chunk
+// / the lo plane, first = accumulate flag of the stage's first MMA.
+__device__ __forceinline__ void issue_stage_bf16(uint32_t dt, uint32_t a0, uint64_t wd, uint32_t chunk16,
+                                                 uint32_t idesc, uint32_t first, uint32_t nx, uint32_t nxp,
+                                                 uint32_t nw, uint32_t nwp, uint32_t& rx, uint32_t& rw) {
+  asm volatile(
+      "{\n\t"
+      ".reg .pred px, pw, pa, pt;\n\t"
+      ".reg .b32 at, atl;\n\t"
+      ".reg .b64 bh, bd, bdl, c16, cl;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 px, [%2], %3;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 pw, [%4], %5;\n\t"
+      "setp.ne.b32 pa, %6, 0;\n\t"
+      "setp.eq.b32 pt, 0, 0;\n\t"
+      "cvt.u64.u32 c16, %10;\n\t"
+      "mov.b64 bh, %9;\n\t"
+      "add.u32 at, %8, 0;\n\t"
+      "add.u64 bd, bh, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pa;\n\t"
+      "add.u32 at, %8, 8;\n\t"
+      "add.u64 bd, bh, 2;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 16;\n\t"
+      "add.u64 bd, bh, 4;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 24;\n\t"
+      "add.u64 bd, bh, 6;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bh, bh, c16;\n\t"
+      "add.u32 at, %8, 32;\n\t"
+      "add.u64 bd, bh, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 40;\n\t"
+      "add.u64 bd, bh, 2;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 48;\n\t"
+      "add.u64 bd, bh, 4;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 56;\n\t"
+      "add.u64 bd, bh, 6;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bh, bh, c16;\n\t"
+      "add.u32 at, %8, 64;\n\t"
+      "add.u64 bd, bh, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 72;\n\t"
+      "add.u64 bd, bh, 2;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 80;\n\t"
+      "add.u64 bd, bh, 4;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 88;\n\t"
+      "add.u64 bd, bh, 6;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bh, bh, c16;\n\t"
+      "add.u32 at, %8, 96;\n\t"
+      "add.u64 bd, bh, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 104;\n\t"
+      "add.u64 bd, bh, 2;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 112;\n\t"
+      "add.u64 bd, bh, 4;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 120;\n\t"
+      "add.u64 bd, bh, 6;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "selp.u32 %0, 1, 0, px;\n\t"
+      "selp.u32 %1, 1, 0, pw;\n\t"
+      "}"
+      : "=r"(rx), "=r"(rw)
+      : "r"(nx), "r"(nxp), "r"(nw), "r"(nwp), "r"(first), "r"(dt), "r"(a0), "l"(wd), "r"(chunk16), "r"(idesc)
+      : "memory");
+}
+
+__device__ __forceinline__ void issue_stage_tf32x3(uint32_t dt, uint32_t a0, uint64_t wd, uint32_t chunk16,
+                                                   uint32_t idesc, uint32_t first, uint32_t nx, uint32_t nxp,
+                                                   uint32_t nw, uint32_t nwp, uint32_t lo16, uint32_t& rx,
+                                                   uint32_t& rw) {
+  asm volatile(
+      "{\n\t"
+      ".reg .pred px, pw, pa, pt;\n\t"
+      ".reg .b32 at, atl;\n\t"
+      ".reg .b64 bh, bd, bdl, c16, cl;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 px, [%2], %3;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 pw, [%4], %5;\n\t"
+      "setp.ne.b32 pa, %6, 0;\n\t"
+      "setp.eq.b32 pt, 0, 0;\n\t"
+      "cvt.u64.u32 c16, %10;\n\t"
+      "cvt.u64.u32 cl, %12;\n\t"
+      "mov.b64 bh, %9;\n\t"
+      "add.u32 at, %8, 0;\n\t"
+      "add.u64 bd, bh, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pa;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 8;\n\t"
+      "add.u64 bd, bh, 2;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 16;\n\t"
+      "add.u64 bd, bh, 4;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "add.u32 at, %8, 24;\n\t"
+      "add.u64 bd, bh, 6;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "selp.u32 %0, 1, 0, px;\n\t"
+      "selp.u32 %1, 1, 0, pw;\n\t"
+      "}"
+      : "=r"(rx), "=r"(rw)
+      : "r"(nx), "r"(nxp), "r"(nw), "r"(nwp), "r"(first), "r"(dt), "r"(a0), "l"(wd), "r"(chunk16), "r"(idesc),
+        "r"(lo16)
+      : "memory");
+}
+
 struct TcSmem {
   uint8_t* Ws;         // W slots
   float* pre;          // [pre_cap][128]: prefix product over the outer factors per policy
@@ -636,8 +769,13 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
       uint64_t* const acc_full = sm.acc_full;
       uint64_t* const acc_free = sm.acc_free;
       volatile int* const abort_flag = sm.abort_flag;
+      static_assert(PREC != B2_PRECISION_BF16 || CPS == 4, "issue_stage_bf16 covers 4 chunks");
+      static_assert(PREC != B2_PRECISION_TF32X3 || CPS == 1, "issue_stage_tf32x3 covers 1 chunk");
       Ring ar, wr;
       uint32_t j = 0;
+      // results of the look-ahead barrier tests made while issuing the
+      // previous stage (false: wait here)
+      uint32_t x_ready = 0, w_ready = 0;
       for (int t = 0; t < T; ++t)
         for (int g = 0; g < G; ++g, ++j) {
           const uint32_t idesc = tp.grp[g].idesc;
@@ -651,9 +789,17 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
           int wk = 0;  // position of the current A stage's first chunk in its W slot
           for (int c = 0; c < nstages; ++c) {
             const int kc = c * CPS;  // first chunk of this A stage (group-relative)
-            if (wk == 0) w_ok = wait_or_abort(&w_full[wr.slot], wr.phase, abort_flag);
+            if (wk == 0) w_ok = w_ready ? true : wait_or_abort(&w_full[wr.slot], wr.phase, abort_flag);
             const int st = ar.slot;
-            const bool okx = wait_or_abort(&x_full[st], ar.phase, abort_flag);
+            const bool okx = x_ready ? true : wait_or_abort(&x_full[st], ar.phase, abort_flag);
+            // where the next stage's X and (if it opens a W slot) W arrive
+            const bool w_last = wk + CPS == wch || kc + CPS == nch;  // this stage ends its W slot
+            Ring nar = ar, nwr = wr;
+            nar.next(nst);
+            if (w_last) nwr.next(kTcWSlots);
+            const uint32_t nx = tc::smem_u32(&x_full[nar.slot]);
+            const uint32_t nw = w_last ? tc::smem_u32(&w_full[nwr.slot]) : nx;
+            uint32_t rx = 0, rw = 0;
             if (okx && w_ok && !*abort_flag) {
               tc::fence_after_sync();
               // stage c accumulates into accumulator c % nacc: shorter FP32
@@ -662,29 +808,20 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
               const uint32_t first = c < nacc ? 0u : 1u;
               const uint64_t wd = wdesc0 + (uint64_t)((uint32_t)wr.slot * ws16 + (uint32_t)wk * chunk16);
               const uint32_t a0 = acol0 + (uint32_t)(st * 32 * kPl * CPS);
-#pragma unroll
-              for (int h = 0; h < CPS; ++h)
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                  const uint32_t acc = (h | kk) ? 1u : first;
-                  const uint64_t bd = wd + (uint64_t)(h * chunk16 + kk * 2);
-                  const uint32_t at = a0 + (uint32_t)(h * 32 * kPl + kk * 8);
-                  if (PREC == B2_PRECISION_BF16) {
-                    tc::mma_bf16_ts(dt, at, bd, idesc, acc);
-                  } else {
-                    tc::mma_tf32_ts(dt, at, bd, idesc, acc);
-                    tc::mma_tf32_ts(dt, at, bd + lo16, idesc, 1u);
-                    tc::mma_tf32_ts(dt, at + 32, bd, idesc, 1u);
-                  }
-                }
+              if (PREC == B2_PRECISION_BF16)
+                issue_stage_bf16(dt, a0, wd, chunk16, idesc, first, nx, nar.phase, nw, nwr.phase, rx, rw);
+              else
+                issue_stage_tf32x3(dt, a0, wd, chunk16, idesc, first, nx, nar.phase, nw, nwr.phase, lo16, rx, rw);
             }
+            x_ready = rx;
+            w_ready = w_last ? rw : 1u;
             // always arm the barriers so every waiter makes progress
             tc::mma_commit(&done[st]);
-            ar.next(nst);
+            ar = nar;
             wk += CPS;
-            if (wk == wch || kc + CPS == nch) {
+            if (w_last) {
               tc::mma_commit(&w_free[wr.slot]);
-              wr.next(kTcWSlots);
+              wr = nwr;
               wk = 0;
             }
             if (++acc_slot == nacc) acc_slot = 0;
