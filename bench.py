@@ -74,6 +74,65 @@ def make_model(seed: int, agents: int):
     return A, B, C, D, obs
 
 
+# FPI-only benchmark model: 4096 agents, 4 factors x 16 states, 6 modalities x
+# 32 observations, each A_m on 2 randomly chosen factors (K = 256), A columns
+# ~ Dirichlet(0.5), D ~ Dirichlet(1), random observations, 16 iterations.
+FPI_AGENTS, FPI_S, FPI_O, FPI_ITERS = 4096, [16] * 4, [32] * 6, 16
+
+
+def fpi_bytes_per_agent_cfg(S, O, deps) -> float:
+    """Algorithmic HBM bytes of one fused FPI agent: the observed A slices, the
+    prior in, the posterior out and the observation indices."""
+    K = [int(np.prod([S[d] for d in dp])) for dp in deps]
+    return 4.0 * sum(K) + 8.0 * sum(S) + 4.0 * len(O)
+
+
+def run_fpi_config(dev, steps: int, warmup: int, flush):
+    """FPI alone on the 4096-agent model: device time per launch (L2 flushed
+    before each), agent-steps/s and algorithmic HBM GB/s."""
+    import torch
+
+    from pymdp_b200 import ffi
+
+    rng = np.random.default_rng(2)
+    deps = [sorted(rng.choice(len(FPI_S), 2, replace=False).tolist()) for _ in FPI_O]
+    gen = torch.Generator(device=dev).manual_seed(2)
+
+    def dirichlet(shape, alpha):
+        g = torch._standard_gamma(torch.full(shape, alpha, device=dev), generator=gen) + 1e-30
+        return g / g.sum(1, keepdim=True)
+
+    A = [dirichlet((FPI_AGENTS, o) + tuple(FPI_S[d] for d in dp), 0.5) for o, dp in zip(FPI_O, deps)]
+    A_flat, A_off = ffi.flatten_ragged_f32(A, 1, dev)
+    del A
+    prior = torch.cat([dirichlet((FPI_AGENTS, s), 1.0) for s in FPI_S], dim=1).contiguous()
+    obs = torch.stack([torch.randint(0, o, (FPI_AGENTS,), device=dev, generator=gen) for o in FPI_O],
+                      dim=1).to(torch.int32).contiguous()
+    out = torch.empty_like(prior)
+
+    def launch():
+        ffi.fpi_obs_flat(A_flat, int(A_off[-1]), A_off, FPI_O, obs, prior, FPI_S, deps, FPI_ITERS, out=out)
+
+    for _ in range(warmup):
+        launch()
+    torch.cuda.synchronize(dev)
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launch()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    nbytes = fpi_bytes_per_agent_cfg(FPI_S, FPI_O, deps) * FPI_AGENTS
+    return {"workload": f"FPI only, {FPI_AGENTS} agents, S={FPI_S}, O={FPI_O}, A_m on 2 random factors (K=256), "
+                        f"{FPI_ITERS} iterations, L2 flushed before each launch",
+            "agent_steps_per_s": FPI_AGENTS / (ms * 1e-3), "ms_per_launch": ms,
+            "bytes_per_launch": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
+
+
 def efe_flops_per_agent() -> float:
     K = int(np.prod(S))
     P = int(np.prod(U)) ** T
@@ -250,6 +309,7 @@ def run_b200(args, rank, world, local_rank):
     prior_d = [torch.as_tensor(d, device=dev) for d in D]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    fpi_res = run_fpi_config(dev, args.steps, args.warmup, flush)
     efe_ev = []
 
     def step(timed_efe=False):
@@ -330,6 +390,7 @@ def run_b200(args, rank, world, local_rank):
     except Exception:  # noqa: BLE001
         pass
     peak_tf = peaks.get("bf16_tflops", 1590.0)
+    peak_gbs = peaks.get("hbm_gbs", 6650.0)
     flops = efe_flops_per_agent() * n_agents
     achieved_tf = flops / (efe_ms * 1e-3) / 1e12
     total_agents = n_agents * world
@@ -371,6 +432,8 @@ def run_b200(args, rank, world, local_rank):
             "sample": f"agents 0..{sample - 1} of the timed model, full agent step, FP64 NumPy oracle, one worker "
                       f"process per core ({cpu_dt:.1f} s wall)"},
         "error_vs_fp64": err,
+        "fpi": dict(fpi_res, roofline={"bound": "hbm", "achieved": fpi_res["gbs"], "peak": peak_gbs, "unit": "GB/s",
+                                       "frac": fpi_res["gbs"] / peak_gbs}),
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -382,6 +445,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="step", choices=["step", "fpi"],
+                    help="step: the agent step (default); fpi: only the 4096-agent FPI model (for profiling)")
     ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
@@ -392,6 +457,14 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "fpi":
+        import torch
+
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        print(json.dumps(run_fpi_config(dev, args.steps, args.warmup, flush)), flush=True)
         return
     if world > 1:
         import datetime

@@ -483,6 +483,296 @@ int64_t work_per_iter(const FpiParams& p) {
   return w;
 }
 
+
+// ------------------------------------------------------ rank <= 2 fast path
+// Models whose modalities all depend on at most two factors of at most 16
+// states each (the 4096-agent FPI benchmark: 4 x 16 states, 6 modalities on
+// 2 factors each) run one warp per agent with every contraction a 16 x 16
+// matrix-vector product:
+//  * each rank-2 group's summed log-likelihood is one zero-padded 16 x 16
+//    FP64 block in shared memory (row stride 18 doubles: conflict-free
+//    16-byte row loads and 8-byte column loads);
+//  * rank-1 groups are constant in the iteration and are folded into the
+//    log prior at load time;
+//  * lane (r, h) = (lane & 15, lane >> 4) multiplies row r (or column r, for
+//    the group's second factor) segment [8h, 8h + 8) with the other factor's
+//    q and one shuffle finishes the row; the products are sorted by output
+//    factor, so each factor's new log q is accumulated in registers and
+//    written once per iteration;
+//  * the softmax handles two factors per step (one per half-warp).
+// FP64 throughout, like the generic kernel.
+constexpr int kR2MaxS = 16;
+constexpr int kR2Stride = 18;                    // doubles per padded block row
+constexpr int kR2Block = kR2MaxS * kR2Stride;    // doubles per block
+constexpr int kR2MaxMv = 2 * kMaxM;
+
+constexpr int kR2MaxWarps = 4;
+
+struct FpiR2 {
+  int32_t n_mv;         // matrix-vector products per iteration
+  int32_t warps;        // warps per agent (one agent per CTA)
+  int32_t vec4;         // 1: every observed row is 16-byte aligned, K % 4 == 0, <= 2 sources per group
+  int16_t f_begin[kR2MaxWarps + 1];   // warp w owns output factors [f_begin[w], f_begin[w+1])
+  int16_t mv_begin[kR2MaxWarps + 1];  // ... and their products [mv_begin[w], mv_begin[w+1])
+  int32_t blk_words;    // doubles of one agent's blocks
+  int32_t agent_words;  // blocks | lp' | log q | q | per-source row offsets
+  int16_t g_blk[kMaxM]; // block offset of rank-2 group g (-1: rank 1)
+  int16_t mv_blk[kR2MaxMv];
+  int8_t mv_in[kR2MaxMv], mv_out[kR2MaxMv], mv_tr[kR2MaxMv];
+};
+
+// Builds the fast-path plan; false when the model is outside it.
+bool build_r2(const FpiParams& p, FpiR2* r) {
+  std::memset(r, 0, sizeof(*r));
+  for (int f = 0; f < p.F; ++f)
+    if (p.S[f] > kR2MaxS) return false;
+  int nb = 0;
+  std::vector<std::vector<int>> by_out(p.F);  // mv indices grouped by output factor
+  struct Mv { int blk, in, out, tr; };
+  std::vector<Mv> mvs;
+  for (int g = 0; g < p.G; ++g) {
+    const FpiGroup& gr = p.grp[g];
+    if (gr.rank > 2) return false;
+    if (gr.rank == 1) {
+      r->g_blk[g] = -1;
+      continue;
+    }
+    r->g_blk[g] = (int16_t)(nb * kR2Block);
+    // block = ll[i0][i1] over (dep[0], dep[1]); row products feed dep[0]
+    mvs.push_back({nb * kR2Block, gr.dep[1], gr.dep[0], 0});
+    mvs.push_back({nb * kR2Block, gr.dep[0], gr.dep[1], 1});
+    ++nb;
+  }
+  if ((int)mvs.size() > kR2MaxMv) return false;
+  int n = 0;
+  for (int f = 0; f < p.F; ++f)
+    for (const Mv& m : mvs)
+      if (m.out == f) {
+        r->mv_blk[n] = (int16_t)m.blk;
+        r->mv_in[n] = (int8_t)m.in;
+        r->mv_out[n] = (int8_t)m.out;
+        r->mv_tr[n] = (int8_t)m.tr;
+        ++n;
+      }
+  r->n_mv = n;
+  // warps per agent: about four products per warp, then split the output
+  // factors into contiguous ranges with balanced product counts
+  int W = (n + 3) / 4;
+  W = W < 1 ? 1 : (W > kR2MaxWarps ? kR2MaxWarps : W);
+  W = W > p.F ? p.F : W;
+  std::vector<int> per_f(p.F, 0);
+  for (int i = 0; i < n; ++i) per_f[r->mv_out[i]]++;
+  r->warps = W;
+  int f = 0, mv = 0;
+  for (int w = 0; w < W; ++w) {
+    r->f_begin[w] = (int16_t)f;
+    r->mv_begin[w] = (int16_t)mv;
+    const int target = (n * (w + 1) + W - 1) / W;
+    const int f_left = p.F - f, w_left = W - w;
+    // take factors while below the target, leaving at least one per later warp
+    while (f < p.F && (f_left - (f - r->f_begin[w])) > w_left - 1 &&
+           (f == r->f_begin[w] || mv + per_f[f] <= target || w == W - 1)) {
+      mv += per_f[f];
+      ++f;
+    }
+  }
+  r->f_begin[W] = (int16_t)p.F;
+  r->mv_begin[W] = (int16_t)n;
+  r->blk_words = nb * kR2Block;
+  const int64_t words = (int64_t)r->blk_words + 4LL * p.F * kR2MaxS + p.M;
+  if (words * 8 > 48 * 1024 || words > 32767) return false;
+  r->agent_words = (int32_t)((words + 1) / 2 * 2);
+  return true;
+}
+
+template <bool FUSED>
+__global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_constant__ FpiParams p,
+                                                                  const __grid_constant__ FpiR2 r,
+                                                                  const FpiIO io) {
+  extern __shared__ double smem_d[];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nthr = blockDim.x;
+  const int64_t b = blockIdx.x;
+  if (b >= io.batch) return;  // uniform over the CTA (one agent per CTA)
+  const int F = p.F;
+  double* blk = smem_d;
+  double* lpp = blk + r.blk_words;  // log prior + rank-1 log-likelihoods, [F][16]
+  double* logq = lpp + F * kR2MaxS;
+  double* qbuf = logq + F * kR2MaxS;  // two q buffers, [2][F][16]
+  int64_t* rowoff = reinterpret_cast<int64_t*>(qbuf + 2 * F * kR2MaxS);
+
+  // ---- load phase
+  bool bad_obs = false;
+  if (FUSED) {
+    for (int m = 0; m < p.M; ++m) {
+      const int o = io.obs[b * p.M + m];
+      bad_obs |= (o < 0 || o >= p.src[m].O);
+    }
+  }
+  for (int m = tid; m < p.M; m += nthr) {
+    int64_t ro = b * io.src_stride + p.src[m].src_off;
+    if (FUSED) {
+      int o = io.obs[b * p.M + m];
+      o = (o < 0 || o >= p.src[m].O) ? 0 : o;
+      ro += (int64_t)o * p.src[m].K;
+    }
+    rowoff[m] = ro;
+  }
+  for (int i = tid; i < r.blk_words; i += nthr) blk[i] = 0.0;
+  for (int i = tid; i < F * kR2MaxS; i += nthr) {
+    const int f = i >> 4, s = i & 15;
+    double v = 0.0;
+    if (s < p.S[f]) {
+      const float x = __ldg(io.prior + b * p.S_tot + p.lp_off[f] + s);
+      v = FUSED ? log((double)fmaxf(x, kMinVal)) : (double)x;
+    }
+    lpp[i] = v;
+    logq[i] = 0.0;  // log q starts at 0 (pymdp/algos.py:121-133)
+  }
+  __syncthreads();
+  // Group blocks are disjoint and rank-1 groups fold into distinct factors, so
+  // no barrier is needed between groups.
+  auto store = [&](int g, int k, double v) {
+    const FpiGroup& gr = p.grp[g];
+    const int bo = r.g_blk[g];
+    if (bo < 0) {
+      lpp[gr.dep[0] * kR2MaxS + k] += v;  // one thread per state: no race
+    } else {
+      const int S1 = p.S[gr.dep[1]];
+      const int i0 = k / S1, i1 = k - i0 * S1;
+      blk[bo + i0 * kR2Stride + i1] = v;
+    }
+  };
+  if (r.vec4) {
+    // items (group, 4 consecutive elements): up to four items per thread per
+    // batch, all their 16-byte loads issued before any log
+    int g = 0, k4 = tid;
+    while (g < p.G && 4 * k4 >= p.grp[g].K) {
+      ++g;
+      k4 = tid;
+    }
+    while (g < p.G) {
+      float4 va[4][2];
+      int gi[4], ki[4];
+      int n = 0;
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        if (g < p.G) {
+          const FpiGroup& gr = p.grp[g];
+          gi[x] = g;
+          ki[x] = k4;
+          va[x][0] = __ldg(reinterpret_cast<const float4*>(io.src + rowoff[p.src_order[gr.src_begin]]) + k4);
+          va[x][1] = gr.src_end - gr.src_begin > 1
+                         ? __ldg(reinterpret_cast<const float4*>(io.src + rowoff[p.src_order[gr.src_begin + 1]]) + k4)
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
+          n = x + 1;
+          k4 += nthr;
+          while (g < p.G && 4 * k4 >= p.grp[g].K) {
+            ++g;
+            k4 = tid;
+          }
+        }
+      }
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        if (x < n) {
+          const bool two = p.grp[gi[x]].src_end - p.grp[gi[x]].src_begin > 1;
+          const float a0[4] = {va[x][0].x, va[x][0].y, va[x][0].z, va[x][0].w};
+          const float a1[4] = {va[x][1].x, va[x][1].y, va[x][1].z, va[x][1].w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            double v = FUSED ? log((double)fmaxf(a0[e], kMinVal)) : (double)a0[e];
+            if (two) v += FUSED ? log((double)fmaxf(a1[e], kMinVal)) : (double)a1[e];
+            store(gi[x], 4 * ki[x] + e, v);
+          }
+        }
+      }
+    }
+  } else {
+    for (int g = 0; g < p.G; ++g) {
+      const FpiGroup& gr = p.grp[g];
+      for (int k = tid; k < gr.K; k += nthr) {
+        double v = 0.0;
+        for (int si = gr.src_begin; si < gr.src_end; ++si) {
+          const float a = __ldg(io.src + rowoff[p.src_order[si]] + k);
+          v += FUSED ? log((double)fmaxf(a, kMinVal)) : (double)a;
+        }
+        store(g, k, v);
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- fixed-point iterations (Jacobi: every factor uses the previous q).
+  // Warp wid owns output factors [f0w, f1w): their softmax and their log q.
+  // q is double-buffered, so one CTA barrier per iteration separates the
+  // softmax writes from the other warps' product reads.
+  const int rr = lane & 15, h = lane >> 4;
+  const int f0w = r.f_begin[wid], f1w = r.f_begin[wid + 1];
+  const int m0w = r.mv_begin[wid], m1w = r.mv_begin[wid + 1];
+  for (int it = 0; it <= p.num_iter; ++it) {
+    double* q = qbuf + (it & 1) * F * kR2MaxS;
+    // q = softmax(log q) for this warp's factors, two per step; after the
+    // last iteration the same step writes the posterior
+    for (int fa = f0w; fa < f1w; fa += 2) {
+      const int f = fa + h;
+      const bool fok = f < f1w;
+      const bool valid = fok && rr < p.S[fok ? f : fa];
+      const double x = valid ? logq[f * kR2MaxS + rr] : -INFINITY;
+      double mx = x;
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      const double e = valid ? exp(x - mx) : 0.0;
+      double sum = e;
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (it == p.num_iter) {
+        if (valid) io.q_out[b * p.S_tot + p.lp_off[f] + rr] = (float)(e / sum);
+      } else if (fok) {
+        q[f * kR2MaxS + rr] = e / sum;
+      }
+    }
+    if (it == p.num_iter) break;
+    __syncthreads();
+    // new log q of this warp's factors: log prior + sum of its products
+    double acc = 0.0;
+    int i = m0w;
+    for (int f = f0w; f < f1w; ++f) {
+      for (; i < m1w && r.mv_out[i] == f; ++i) {
+        const double* M = blk + r.mv_blk[i];
+        const double* qv = q + r.mv_in[i] * kR2MaxS + 8 * h;
+        double a0 = 0.0, a1 = 0.0;
+        if (r.mv_tr[i]) {
+          const double* col = M + (8 * h) * kR2Stride + rr;
+#pragma unroll
+          for (int k = 0; k < 8; k += 2) {
+            a0 = fma(col[k * kR2Stride], qv[k], a0);
+            a1 = fma(col[(k + 1) * kR2Stride], qv[k + 1], a1);
+          }
+        } else {
+          const double2* row = reinterpret_cast<const double2*>(M + rr * kR2Stride + 8 * h);
+          const double2* q2 = reinterpret_cast<const double2*>(qv);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const double2 m2 = row[k], v2 = q2[k];
+            a0 = fma(m2.x, v2.x, a0);
+            a1 = fma(m2.y, v2.y, a1);
+          }
+        }
+        acc += a0 + a1;
+      }
+      acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+      if (h == 0 && rr < p.S[f]) logq[f * kR2MaxS + rr] = lpp[f * kR2MaxS + rr] + acc;
+      acc = 0.0;
+    }
+    __syncwarp();
+  }
+  if (FUSED && bad_obs) {
+    __syncthreads();
+    for (int k = tid; k < p.S_tot; k += nthr) io.q_out[b * p.S_tot + k] = __int_as_float(0x7fc00000);
+  }
+}
+
 template <int TEAM, int APC, bool FUSED>
 int32_t launch_one(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const char* op) {
   const int bytes = APC * p.agent_words * 8;
@@ -503,6 +793,18 @@ int32_t launch_one(const FpiParams& p, const FpiIO& io, cudaStream_t stream, con
 template <bool FUSED>
 int32_t launch(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const char* op) {
   if (io.batch <= 0) return B2_OK;
+  FpiR2 r2;
+  if (build_r2(p, &r2)) {
+    bool v4 = (reinterpret_cast<uintptr_t>(io.src) % 16 == 0) && io.src_stride % 4 == 0;
+    for (int m = 0; m < p.M; ++m) v4 = v4 && p.src[m].src_off % 4 == 0 && p.src[m].K % 4 == 0;
+    for (int g = 0; g < p.G; ++g) v4 = v4 && p.grp[g].src_end - p.grp[g].src_begin <= 2;
+    r2.vec4 = v4 ? 1 : 0;
+    if (io.batch > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
+    const int bytes = r2.agent_words * 8;
+    B2_TRY(ensure_smem_attr((const void*)fpi_r2_kernel<FUSED>, bytes, op));
+    fpi_r2_kernel<FUSED><<<(unsigned)io.batch, 32 * r2.warps, bytes, stream>>>(p, r2, io);
+    return check_launch(op);
+  }
   const int64_t work = work_per_iter(p);
   const int bytes_agent = p.agent_words * 8;
   if (work >= 8192) return launch_one<256, 1, FUSED>(p, io, stream, op);
