@@ -127,11 +127,15 @@ int32_t b2_fpi_obs(void* stream, const float* A_flat, int64_t A_agent_stride,
  *   neg_efe_out [Bn, P]: G = -EFE per policy (pymdp/control.py:604-690).
  *
  * Element counts are checked like validate_buffer_counts
- * (neg_efe/neg_efe_layout.h:342-363). This build implements the utility and
- * state-information-gain terms (flag bits 0 and 1); inductive (bit 2) and
- * parameter-information-gain (bit 3) return B2_ERR_UNSUPPORTED. Bits 8-9 pick
- * the contraction precision (B2_PRECISION_*). Out-of-range actions in
- * policy_matrix give NaN for that policy. */
+ * (neg_efe/neg_efe_layout.h:342-363). All four terms are implemented:
+ * utility and state information gain (flag bits 0 and 1) on every precision
+ * path; the inductive value (bit 2, pymdp/control.py:1021-1061) and parameter
+ * information gain (bit 3, pymdp/control.py:511-602 with the exact Dirichlet
+ * weight of pymdp/maths.py:783-808; pA and pB each 0 elements or
+ * Bn * A_offsets[M] / Bn * B_offsets[F]) on the SIMT FP32 kernel whatever
+ * precision bits 8-9 request. Bits 8-9 pick the contraction precision
+ * (B2_PRECISION_*) of the other calls. Out-of-range actions in policy_matrix
+ * give NaN for that policy. */
 int32_t b2_neg_efe(void* stream, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
                    const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
                    const float* B, int64_t B_count, const float* C, int64_t C_count,

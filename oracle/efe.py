@@ -12,6 +12,12 @@ Follows the pure-JAX branch of ``pymdp/control.py``:
   (``q_pi = softmax(gamma * G + log_stable(E))``)
 * ``sample_policy``             ``control.py:115-150`` (deterministic: argmax,
   first maximum)
+* parameter information gain  ``control.py:511-602`` (``calc_negative_pA_info_gain``,
+  ``calc_negative_pB_info_gain``) with the exact Dirichlet weight
+  ``spm_wnorm`` / ``_exact_wnorm`` (``maths.py:783-841``)
+* inductive value             ``control.py:1021-1061`` (``calc_inductive_value_t``,
+  anchored to ``qs_init``, ``control.py:775-777``) inside
+  ``compute_neg_efe_policy_inductive`` (``control.py:692-793``)
 
 with ``stable_xlogx(x) = xlogy(x, clip(x, MINVAL))`` (``maths.py:17-45``).
 All policies are evaluated at once (vectorised over the policy axis); the
@@ -78,20 +84,69 @@ def expected_state(qs, B, u_t, B_deps):
     return out
 
 
-def neg_efe_all_policies(policies, qs_init, A, B, C, A_deps, B_deps,
-                         use_utility=True, use_states_info_gain=True):
-    """``compute_neg_efe_policy`` (``control.py:604-690``) for every policy.
+def exact_wnorm(a):
+    """``maths.py:783-808`` (``_exact_wnorm``, the default of ``spm_wnorm``):
+    ``-(log S - log a + 1/a - 1/S + digamma(a) - digamma(S))`` with ``a``
+    clipped at MINVAL and ``S`` its clipped sum over axis 0."""
+    from scipy.special import digamma
 
-    Returns ``G`` of shape ``(P,)`` (``neg_efe``; larger is better).
+    a = np.clip(np.asarray(a, np.float64), MINVAL, None)
+    s = np.clip(a.sum(axis=0), MINVAL, None)
+    w = np.log(s) - np.log(a) + 1.0 / a - 1.0 / s + digamma(a) - digamma(s)
+    return -w
+
+
+def inductive_weights(qs_init, I, epsilon):
+    """``calc_inductive_value_t`` (``control.py:1021-1061``) is linear in the
+    predicted marginals: per factor ``path_available * (1 - I[m, :]) * log_eps``
+    with ``idx = argmax qs_init[f]`` and ``m = max(argmax I[:, idx] - 1, 0)``
+    (first maxima). Returns the weight vector of each factor."""
+    log_eps = float(log_stable(np.float64(epsilon)))
+    out = []
+    for q, I_f in zip(qs_init, I):
+        I_f = np.asarray(I_f, np.float64)
+        idx = int(np.argmax(np.asarray(q)))
+        m = max(int(np.argmax(I_f[:, idx])) - 1, 0)
+        path = float(np.clip(I_f[:, idx].sum(0), 0, 1))
+        out.append(path * (1.0 - I_f[m, :]) * log_eps)
+    return out
+
+
+def neg_efe_all_policies(policies, qs_init, A, B, C, A_deps, B_deps,
+                         use_utility=True, use_states_info_gain=True, pA=None, pB=None,
+                         use_param_info_gain=False, I=None, use_inductive=False, inductive_epsilon=1e-3):
+    """``compute_neg_efe_policy`` (``control.py:604-690``) / its inductive
+    variant (``control.py:692-793``) for every policy.
+
+    Returns ``G`` of shape ``(P,)`` (``neg_efe``; larger is better). Per step:
+    ``G += info_gain + utility - neg_param_info_gain + inductive_value``.
     """
     policies = np.asarray(policies)
     P, T, F = policies.shape
     qs = [np.broadcast_to(np.asarray(q, np.float64), (P, len(q))) for q in qs_init]
     A = [np.asarray(a, np.float64) for a in A]
     H_A = [-stable_xlogx(a).sum(0) for a in A]
+    wA = ([exact_wnorm(pa) * (np.asarray(pa) > 0) for pa in pA]
+          if (use_param_info_gain and pA is not None) else None)
+    # pB weights per action slice: spm_wnorm(pB[..., u]) * (pB[..., u] > 0), stacked back on the last axis
+    wB = None
+    if use_param_info_gain and pB is not None:
+        wB = []
+        for pb in pB:
+            pb = np.asarray(pb, np.float64)
+            wB.append(np.stack([exact_wnorm(pb[..., u]) * (pb[..., u] > 0) for u in range(pb.shape[-1])], -1))
+    wI = inductive_weights(qs_init, I, inductive_epsilon) if use_inductive else None
     G = np.zeros(P)
     for t in range(T):
+        qs_prev = qs
         qs = expected_state(qs, B, policies[:, t, :], B_deps)
+        if wB is not None:
+            fd = expected_state(qs_prev, wB, policies[:, t, :], B_deps)  # factor_dot(wB[..., u], qs_prev)
+            for f in range(F):
+                G -= (qs[f] * fd[f]).sum(-1)
+        if wI is not None:
+            for f in range(F):
+                G += qs[f] @ wI[f]
         joint = {}  # dependency tuple -> (P, K) matrix of x = outer product of the marginals
         for m, (A_m, deps) in enumerate(zip(A, A_deps)):
             key = tuple(deps)
@@ -107,14 +162,20 @@ def neg_efe_all_policies(policies, qs_init, A, B, C, A_deps, B_deps,
                 C_m = np.asarray(C[m], np.float64)
                 c = C_m[t] if C_m.ndim > 1 else C_m
                 G += qo @ c
+            if wA is not None:
+                fd = x @ wA[m].reshape(wA[m].shape[0], -1).T           # factor_dot(wA_m, qs[deps])
+                G -= (qo * fd).sum(-1)
     return G
 
 
 def update_posterior_policies(policies, qs_init, A, B, C, E, A_deps, B_deps, gamma=16.0,
-                              use_utility=True, use_states_info_gain=True):
-    """``control.py:198-349``: returns ``(q_pi, G)``."""
+                              use_utility=True, use_states_info_gain=True, pA=None, pB=None,
+                              use_param_info_gain=False, I=None, use_inductive=False, inductive_epsilon=1e-3):
+    """``control.py:198-349`` / ``:795-963``: returns ``(q_pi, G)``."""
     G = neg_efe_all_policies(policies, qs_init, A, B, C, A_deps, B_deps,
-                             use_utility=use_utility, use_states_info_gain=use_states_info_gain)
+                             use_utility=use_utility, use_states_info_gain=use_states_info_gain, pA=pA, pB=pB,
+                             use_param_info_gain=use_param_info_gain, I=I, use_inductive=use_inductive,
+                             inductive_epsilon=inductive_epsilon)
     return softmax(gamma * G + log_stable(E)), G
 
 

@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import ffi
-from .control import construct_policies
+from .control import construct_policies, generate_I_matrix
 
 
 def _t(x, dev) -> torch.Tensor:
@@ -41,11 +41,15 @@ class Agent:
                  use_utility: bool = True, use_states_info_gain: bool = True, use_param_info_gain: bool = False,
                  use_inductive: bool = False, action_selection: str = "deterministic",
                  sampling_mode: str = "full", inference_algo: str = "fpi", num_iter: int = 16,
-                 batch_size: int = 1, precision: str = "fp32", device="cuda"):
+                 batch_size: int = 1, precision: str = "fp32", device="cuda", pA: Sequence | None = None,
+                 pB: Sequence | None = None, H: Sequence | None = None, I: Sequence | None = None,
+                 inductive_depth: int = 1, inductive_threshold: float = 0.1, inductive_epsilon=1e-3):
         if inference_algo.lower() != "fpi":
             raise NotImplementedError("only inference_algo='fpi' is on the accelerated path")
-        if use_param_info_gain or use_inductive:
-            raise NotImplementedError("parameter information gain / inductive terms are not built yet")
+        if use_param_info_gain and pA is None and pB is None:
+            raise ValueError("use_param_info_gain=True requires at least one of pA or pB.")
+        if use_inductive and inductive_depth < 1:
+            raise ValueError("`inductive_depth` must be >= 1")
         if action_selection != "deterministic" or sampling_mode != "full":
             raise NotImplementedError("only deterministic action selection with sampling_mode='full'")
         dev = torch.device(device)
@@ -127,11 +131,30 @@ class Agent:
             C_t.append(c)
         self._C_flat, _ = ffi.flatten_ragged_f32(C_t, 1, dev)
         self._qs_offsets = np.cumsum([0] + S)
+        # inductive matrices (pymdp/agent.py:368-380): from H via generate_I_matrix, or given
+        if use_inductive and H is not None:
+            H_b = [np.broadcast_to(np.asarray(_t(h, "cpu")), (nbat, S[f])) for f, h in enumerate(H)]
+            per_agent = [generate_I_matrix([H_b[f][b_] for f in range(F)], [B[f][b_].cpu().numpy() for f in range(F)],
+                                           float(inductive_threshold), int(inductive_depth)) for b_ in range(nbat)]
+            I = [torch.as_tensor(np.stack([per_agent[b_][f] for b_ in range(nbat)]), device=dev) for f in range(F)]
+        elif use_inductive and I is not None:
+            I = [batched(_t(i, dev), 2, f"I[{f}]") for f, i in enumerate(I)]
+        else:
+            I = [torch.zeros((nbat, 1, s), device=dev) for s in S]
+        self.I = I
         self._layout = ffi.EfeLayout(S, self.num_obs, self.num_controls, self.policy_len, self.A_dependencies,
-                                     self.B_dependencies)
-        self._I_flat = torch.zeros((nbat, int(self._layout.I_offsets[-1])), device=dev)
-        self._eps = torch.full((1,), 1e-3, device=dev)
-        self._flags = ffi.efe_flags(use_utility, use_states_info_gain, precision=precision)
+                                     self.B_dependencies, [int(i.shape[1]) for i in I])
+        self._I_flat, _ = ffi.flatten_ragged_f32(I, 1, dev)
+        self._eps = _t(np.broadcast_to(np.asarray(inductive_epsilon, np.float32), (nbat,)).copy(), dev)
+        self.pA = [batched(_t(x, dev), len(self.A_dependencies[m]) + 1, f"pA[{m}]") for m, x in enumerate(pA)] \
+            if pA is not None else None
+        self.pB = [batched(_t(x, dev), len(self.B_dependencies[f]) + 2, f"pB[{f}]") for f, x in enumerate(pB)] \
+            if pB is not None else None
+        self._pA_flat = ffi.flatten_ragged_f32(self.pA, 1, dev)[0] if (use_param_info_gain and self.pA) else None
+        self._pB_flat = ffi.flatten_ragged_f32(self.pB, 1, dev)[0] if (use_param_info_gain and self.pB) else None
+        self._flags = ffi.efe_flags(use_utility, use_states_info_gain, use_param_info_gain, use_inductive,
+                                    precision=precision)
+        self.use_param_info_gain, self.use_inductive = use_param_info_gain, use_inductive
         self.A, self.B, self.C = A, B, C
 
     # ------------------------------------------------------------------ API
@@ -166,7 +189,7 @@ class Agent:
         P = self.policies.shape[0]
         G = torch.empty((self.batch_size, P), device=self.device)
         self._layout.call(None, self.policies, 0, qs_flat, self._A_flat, self._B_flat, self._C_flat,
-                          self._I_flat, None, None, self._eps, G, self.batch_size, P, self._flags)
+                          self._I_flat, self._pA_flat, self._pB_flat, self._eps, G, self.batch_size, P, self._flags)
         q_pi = ffi.policy_posterior(G, self.E, self.gamma)
         return q_pi, G
 

@@ -27,3 +27,29 @@ def construct_policies(num_states: Sequence[int], num_controls: Sequence[int] | 
     x = list(num_controls) * policy_len
     pols = list(itertools.product(*[range(int(i)) for i in x]))
     return np.asarray(pols, dtype=np.int32).reshape(len(pols), policy_len, F)
+
+
+def generate_I_matrix(H: Sequence, B: Sequence, threshold: float, depth: int) -> list:
+    """Backward reachability matrices of the inductive term
+    (``pymdp/control.py:965-1019``), host-side set-up for one agent.
+
+    ``H[f]``: ``(S_f,)`` goal indicator; ``B[f]``: ``(S_f, S_f, U_f)``
+    (factor-local dynamics). Row ``i`` of ``I[f]`` marks the states that can
+    still reach the goal set after ``i`` backward steps, through transitions
+    whose probability exceeds ``threshold`` under some action.
+    """
+    if depth < 1:
+        raise ValueError("`depth` must be >= 1")
+    out = []
+    for h, b in zip(H, B):
+        b = np.asarray(b, np.float64)
+        h = np.asarray(h, np.float64)
+        if b.ndim != 3 or b.shape[0] != b.shape[1]:
+            raise ValueError("generate_I_matrix needs factor-local B of shape (S, S, U)")
+        reach = ((b > threshold).sum(axis=-1) > 0).astype(np.float64)  # [next, prev]
+        pred = reach.T
+        rows = [h]
+        for _ in range(depth - 1):
+            rows.append((pred @ rows[-1] > 0).astype(np.float64))
+        out.append(np.stack(rows, axis=0).astype(np.float32))
+    return out

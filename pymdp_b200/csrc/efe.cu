@@ -125,7 +125,12 @@ int32_t build_efe_params(EfeParams* p, int64_t P, int64_t T, int64_t F, int64_t 
     if (I_depths[f] <= 0) return bad("I_depths[f] must be positive");
     if (I_offsets[f + 1] < I_offsets[f]) return bad("I_off must be monotonic");
     if (I_offsets[f + 1] - I_offsets[f] != I_depths[f] * S[f]) return bad("I_off inconsistent with depth/S");
+    if (I_offsets[f + 1] > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": I too large");
+    p->I_off[f] = (int32_t)I_offsets[f];
+    p->I_depth[f] = (int32_t)I_depths[f];
   }
+  p->I_off[F] = (int32_t)I_offsets[F];
+  p->I_stride = I_offsets[F];
   p->A_stride = A_offsets[M];
   p->B_stride = B_offsets[F];
   p->C_stride = C_offsets[M];
@@ -160,15 +165,22 @@ __global__ void efe_linear_rows_kernel(const __grid_constant__ EfeParams p, cons
 }
 
 // One thread = one (agent, policy): the plain per-policy SIMT evaluation.
+// Optional terms (null pointers when unused): wA / wB = parameter
+// information-gain weights (laid out like A / B, see efe_wnorm_kernel), wI =
+// inductive weights per factor state (efe_inductive_kernel). Per step:
+// G += info_gain + utility - (pA term + pB term) + inductive value
+// (pymdp/control.py:772-787).
 __global__ void __launch_bounds__(128)
     efe_plain_kernel(const __grid_constant__ EfeParams p, const int32_t* __restrict__ pm, int pm_batched,
                      const float* __restrict__ qs_init, const float* __restrict__ A, const float* __restrict__ B,
-                     const float* __restrict__ lin, float* __restrict__ G) {
+                     const float* __restrict__ lin, float* __restrict__ G, const float* __restrict__ wA,
+                     const float* __restrict__ wB, const float* __restrict__ wI) {
   const int64_t b = blockIdx.y;
   const int pol = blockIdx.x * blockDim.x + threadIdx.x;
   if (pol >= p.P) return;
   float qs[2][kEfePlainMaxStot];
   float qo[kEfePlainMaxO];
+  float fd[kEfePlainMaxO];  // pA term: factor_dot(wA_m, qs) per observation
   int cur = 0;
   for (int i = 0; i < p.S_tot; ++i) qs[0][i] = __ldg(qs_init + b * p.S_tot + i);
   const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (int64_t)pol * p.T * p.F;
@@ -187,36 +199,47 @@ __global__ void __launch_bounds__(128)
         u = 0;
       }
       const float* Bf = B + b * p.B_stride + fb.B_off;
+      const float* wBf = wB ? wB + b * p.B_stride + fb.B_off : nullptr;
       const int U = p.U[f];
       for (int s = 0; s < p.S[f]; ++s) {
-        float acc = 0.f;
+        float acc = 0.f, accw = 0.f;
         int dig[B2_MAX_DEP_RANK] = {0};
         for (int k = 0; k < fb.K; ++k) {
           float w = 1.f;
           for (int i = 0; i < fb.rank; ++i) w *= qc[p.qs_off[fb.dep[i]] + dig[i]];
-          acc = fmaf(__ldg(Bf + ((int64_t)s * fb.K + k) * U + u), w, acc);
+          const int64_t e = ((int64_t)s * fb.K + k) * U + u;
+          acc = fmaf(__ldg(Bf + e), w, acc);
+          if (wBf) accw = fmaf(__ldg(wBf + e), w, accw);
           for (int i = fb.rank - 1; i >= 0; --i) {
             if (++dig[i] < p.S[fb.dep[i]]) break;
             dig[i] = 0;
           }
         }
         qn[p.qs_off[f] + s] = acc;
+        // pB term: qs_next_f[s] * factor_dot(wB_f[..., u], qs_prev[B_deps])[s] (control.py:555-602)
+        if (wBf) g -= acc * accw;
       }
     }
     cur ^= 1;
     const float* q = qs[cur];
+    // inductive value: linear in the predicted marginals (control.py:1021-1061)
+    if (wI)
+      for (int i = 0; i < p.S_tot; ++i) g = fmaf(__ldg(wI + b * p.S_tot + i), q[i], g);
     // expected observations, entropy and the linear row
     for (int m = 0; m < p.M; ++m) {
       const EfeModality& md = p.mod[m];
       const float* Am = A + b * p.A_stride + md.A_off;
       const float* Lm = lin + (b * p.T + t) * p.K_tot + md.lin_off;
-      for (int o = 0; o < md.O; ++o) qo[o] = 0.f;
+      const float* wAm = wA ? wA + b * p.A_stride + md.A_off : nullptr;
+      for (int o = 0; o < md.O; ++o) qo[o] = fd[o] = 0.f;
       float la = 0.f;
       int dig[B2_MAX_DEP_RANK] = {0};
       for (int k = 0; k < md.K; ++k) {
         float w = 1.f;
         for (int i = 0; i < md.rank; ++i) w *= q[p.qs_off[md.dep[i]] + dig[i]];
         for (int o = 0; o < md.O; ++o) qo[o] = fmaf(__ldg(Am + (int64_t)o * md.K + k), w, qo[o]);
+        if (wAm)
+          for (int o = 0; o < md.O; ++o) fd[o] = fmaf(__ldg(wAm + (int64_t)o * md.K + k), w, fd[o]);
         la = fmaf(__ldg(Lm + k), w, la);
         for (int i = md.rank - 1; i >= 0; --i) {
           if (++dig[i] < p.S[md.dep[i]]) break;
@@ -226,10 +249,109 @@ __global__ void __launch_bounds__(128)
       float h = 0.f;
       if (ig)
         for (int o = 0; o < md.O; ++o) h -= qo[o] * log_stable(qo[o]);
+      // pA term: qo_m . factor_dot(wA_m, qs) (control.py:511-553)
+      if (wAm)
+        for (int o = 0; o < md.O; ++o) h -= qo[o] * fd[o];
       g += h + la;
     }
   }
   G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : g;
+}
+
+// digamma(x) for x > 0 in FP64: the recurrence psi(x) = psi(x + 1) - 1/x up
+// to x >= 10, then the asymptotic series psi(x) ~ ln x - 1/(2x) -
+// sum_k B_2k / (2k x^2k) through B_14 (truncation below 1e-16 relative).
+__device__ double digamma_fp64(double x) {
+  double acc = 0.0;
+  while (x < 10.0) {
+    acc -= 1.0 / x;
+    x += 1.0;
+  }
+  const double r = 1.0 / x, r2 = r * r;
+  // B2/2 = 1/12, B4/4 = -1/120, B6/6 = 1/252, B8/8 = -1/240, B10/10 = 1/132,
+  // B12/12 = -691/32760, B14/14 = 1/12
+  const double series =
+      r2 * (1.0 / 12 - r2 * (1.0 / 120 - r2 * (1.0 / 252 - r2 * (1.0 / 240 - r2 * (1.0 / 132 -
+                                                                                   r2 * (691.0 / 32760 - r2 / 12))))));
+  return acc + log(x) - 0.5 * r - series;
+}
+
+// Parameter information-gain weights (pymdp/control.py:543-544, :594):
+// w = spm_wnorm(p) * (p > 0) with the exact Dirichlet form of
+// pymdp/maths.py:783-808, -(log S - log a + 1/a - 1/S + digamma(a) -
+// digamma(S)), a = clip(p, eps), S = clip(sum over axis 0 of a, eps).
+// One thread per column: pA columns (modality m, joint state k) sum over the
+// observations; pB columns (factor f, parent state k, action u) over the
+// next states. Output laid out like pA / pB.
+__global__ void efe_wnorm_kernel(const __grid_constant__ EfeParams p, const float* __restrict__ src, int is_B,
+                                 float* __restrict__ w) {
+  const int64_t b = blockIdx.y;
+  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t base, stride;
+  int rows;
+  if (!is_B) {
+    if (col >= p.K_tot) return;
+    int m = 0;
+    while (m + 1 < p.M && p.mod[m + 1].lin_off <= col) ++m;
+    const EfeModality& md = p.mod[m];
+    base = b * p.A_stride + md.A_off + (col - md.lin_off);
+    stride = md.K;
+    rows = md.O;
+  } else {
+    int64_t c = col;
+    int f = 0;
+    for (; f < p.F; ++f) {
+      const int64_t n = (int64_t)p.fac[f].K * p.U[f];
+      if (c < n) break;
+      c -= n;
+    }
+    if (f >= p.F) return;
+    base = b * p.B_stride + p.fac[f].B_off + c;  // (k, u) column of (S_f, K_f, U_f)
+    stride = (int64_t)p.fac[f].K * p.U[f];
+    rows = p.S[f];
+  }
+  const double eps = 2.220446049250313e-16;
+  double s = 0.0;
+  for (int r = 0; r < rows; ++r) s += fmax((double)__ldg(src + base + r * stride), eps);
+  s = fmax(s, eps);
+  const double ls = log(s), ps = digamma_fp64(s), is = 1.0 / s;
+  for (int r = 0; r < rows; ++r) {
+    const float raw = __ldg(src + base + r * stride);
+    const double a = fmax((double)raw, eps);
+    const double wv = ls - log(a) + 1.0 / a - is + digamma_fp64(a) - ps;
+    w[base + r * stride] = raw > 0.f ? (float)(-wv) : 0.f;
+  }
+}
+
+// Inductive weights (pymdp/control.py:1021-1061, anchored to qs_init as in
+// :775-777): per factor, idx = first argmax of qs_init_f, m = max(first argmax
+// of I_f[:, idx] - 1, 0), path = clip(sum_i I_f[i, idx], 0, 1) and
+// w_f[s] = path * (1 - I_f[m, s]) * log(clip(eps)). One thread per (agent, factor).
+__global__ void efe_inductive_kernel(const __grid_constant__ EfeParams p, const float* __restrict__ qs_init,
+                                     const float* __restrict__ I, const float* __restrict__ eps, int eps_batched,
+                                     float* __restrict__ wI, int64_t Bn) {
+  const int64_t idx_all = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx_all >= Bn * p.F) return;
+  const int64_t b = idx_all / p.F;
+  const int f = (int)(idx_all - b * p.F);
+  const int S = p.S[f], D = p.I_depth[f];
+  const float* q = qs_init + b * p.S_tot + p.qs_off[f];
+  int idx = 0;
+  for (int s = 1; s < S; ++s)
+    if (q[s] > q[idx]) idx = s;
+  const float* If = I + b * p.I_stride + p.I_off[f];
+  int am = 0;
+  double colsum = 0.0;
+  for (int i = 0; i < D; ++i) {
+    const float v = If[(int64_t)i * S + idx];
+    if (v > If[(int64_t)am * S + idx]) am = i;
+    colsum += v;
+  }
+  const int m = am - 1 > 0 ? am - 1 : 0;
+  const double path = fmin(fmax(colsum, 0.0), 1.0);
+  const double log_eps = log(fmax((double)eps[eps_batched ? b : 0], 2.220446049250313e-16));
+  for (int s = 0; s < S; ++s)
+    wI[b * p.S_tot + p.qs_off[f] + s] = (float)(path * (1.0 - (double)If[(int64_t)m * S + s]) * log_eps);
 }
 
 // q_pi[b] = softmax(gamma_b * G[b] + log(clip(E_b))) — one CTA per agent.
@@ -321,9 +443,10 @@ int32_t launch_linear_rows(const EfeParams& p, int64_t Bn, const float* A, const
 }
 
 int32_t launch_efe_plain(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
-                         const float* A, const float* B, const float* lin, float* G, cudaStream_t stream) {
+                         const float* A, const float* B, const float* lin, float* G, cudaStream_t stream,
+                         const float* wA, const float* wB, const float* wI) {
   dim3 grid((unsigned)((p.P + 127) / 128), (unsigned)Bn);
-  efe_plain_kernel<<<grid, 128, 0, stream>>>(p, pm, pm_batched, qs, A, B, lin, G);
+  efe_plain_kernel<<<grid, 128, 0, stream>>>(p, pm, pm_batched, qs, A, B, lin, G, wA, wB, wI);
   return check_launch("efe_ffi plain");
 }
 
@@ -389,14 +512,21 @@ extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64
                                                std::to_string(c.actual) + ", expected " + std::to_string(c.expected));
   if (eps_count != 1 && eps_count != Bn)
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": inductive_epsilon must have 1 or Bn elements");
-  if (flags & B2_FLAG_USE_PARAM_INFO_GAIN) {
+  const bool use_pig = (flags & B2_FLAG_USE_PARAM_INFO_GAIN) != 0;
+  const bool use_ind = (flags & B2_FLAG_USE_INDUCTIVE) != 0;
+  if (use_pig) {
     if (pA_count == 0 && pB_count == 0)
       return fail(B2_ERR_INVALID_ARGUMENT,
                   std::string(kEfeName) + ": use_param_info_gain=true requires at least one of pA, pB");
-    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": parameter information gain is not built yet");
+    if (pA_count != 0 && pA_count != Bn * p.A_stride)
+      return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": pA element_count = " +
+                                               std::to_string(pA_count) + ", expected 0 or " +
+                                               std::to_string(Bn * p.A_stride));
+    if (pB_count != 0 && pB_count != Bn * p.B_stride)
+      return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": pB element_count = " +
+                                               std::to_string(pB_count) + ", expected 0 or " +
+                                               std::to_string(Bn * p.B_stride));
   }
-  if (flags & B2_FLAG_USE_INDUCTIVE)
-    return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": inductive planning term is not built yet");
   const int prec = (flags >> B2_PRECISION_SHIFT) & 3;
   if (prec > B2_PRECISION_BF16)
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": unknown precision selector");
@@ -404,10 +534,45 @@ extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64
   if (!policy_matrix || !qs_init || !A || !B || !C || !neg_efe_out)
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": null buffer");
   if (Bn > 65535) return fail(B2_ERR_UNSUPPORTED, std::string(kEfeName) + ": Bn > 65535");
-  (void)I;
-  (void)pA;
-  (void)pB;
-  (void)inductive_epsilon;
+  if ((use_pig && ((pA_count && !pA) || (pB_count && !pB))) || (use_ind && (!I || !inductive_epsilon)))
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": null buffer");
+  if (use_pig || use_ind) {
+    // the flag-gated terms run on the SIMT FP32 kernel (any precision selector)
+    const size_t lin_bytes = (size_t)Bn * p.T * p.K_tot * sizeof(float);
+    const size_t wa_bytes = (use_pig && pA_count) ? (size_t)Bn * p.A_stride * sizeof(float) : 0;
+    const size_t wb_bytes = (use_pig && pB_count) ? (size_t)Bn * p.B_stride * sizeof(float) : 0;
+    const size_t wi_bytes = use_ind ? (size_t)Bn * p.S_tot * sizeof(float) : 0;
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    uint8_t* ws = nullptr;
+    B2_TRY(ws_alloc((void**)&ws, up(lin_bytes) + up(wa_bytes) + up(wb_bytes) + up(wi_bytes), stream, kEfeName));
+    float* lin = reinterpret_cast<float*>(ws);
+    float* wA = wa_bytes ? reinterpret_cast<float*>(ws + up(lin_bytes)) : nullptr;
+    float* wB = wb_bytes ? reinterpret_cast<float*>(ws + up(lin_bytes) + up(wa_bytes)) : nullptr;
+    float* wI = wi_bytes ? reinterpret_cast<float*>(ws + up(lin_bytes) + up(wa_bytes) + up(wb_bytes)) : nullptr;
+    int32_t rc = B2_OK;
+    if (wA) {
+      efe_wnorm_kernel<<<dim3((unsigned)((p.K_tot + 127) / 128), (unsigned)Bn), 128, 0, stream>>>(p, pA, 0, wA);
+      rc = check_launch("efe_ffi pA weights");
+    }
+    if (rc == B2_OK && wB) {
+      int64_t cols = 0;
+      for (int f = 0; f < p.F; ++f) cols += (int64_t)p.fac[f].K * p.U[f];
+      efe_wnorm_kernel<<<dim3((unsigned)((cols + 127) / 128), (unsigned)Bn), 128, 0, stream>>>(p, pB, 1, wB);
+      rc = check_launch("efe_ffi pB weights");
+    }
+    if (rc == B2_OK && wI) {
+      const int64_t n = Bn * p.F;
+      efe_inductive_kernel<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(p, qs_init, I, inductive_epsilon,
+                                                                           eps_count == Bn && Bn > 1, wI, Bn);
+      rc = check_launch("efe_ffi inductive weights");
+    }
+    if (rc == B2_OK) rc = launch_linear_rows(p, Bn, A, C, lin, stream);
+    if (rc == B2_OK)
+      rc = launch_efe_plain(p, Bn, policy_matrix, pm_batched, qs_init, A, B, lin, neg_efe_out, stream, wA, wB, wI);
+    cudaError_t fe = cudaFreeAsync(ws, stream);
+    if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
+    return rc;
+  }
   if (prec != B2_PRECISION_FP32) {
     // tensor-core path; models outside its limits take the SIMT FP32 path
     bool used = false;

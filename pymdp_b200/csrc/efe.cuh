@@ -34,6 +34,9 @@ struct EfeParams {
   int32_t S[kEfeMaxF];
   int32_t U[kEfeMaxF];
   int32_t qs_off[kEfeMaxF + 1];
+  int32_t I_off[kEfeMaxF + 1];  // inductive matrix I_f (depth_f, S_f) inside one agent's flat I
+  int32_t I_depth[kEfeMaxF];
+  int64_t I_stride;
   EfeFactor fac[kEfeMaxF];
   EfeModality mod[kEfeMaxM];
 };
@@ -50,7 +53,8 @@ int32_t build_efe_params(EfeParams* p, int64_t P, int64_t T, int64_t F, int64_t 
 int32_t launch_linear_rows(const EfeParams& p, int64_t Bn, const float* A, const float* C, float* lin,
                            cudaStream_t stream);
 int32_t launch_efe_plain(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
-                         const float* A, const float* B, const float* lin, float* G, cudaStream_t stream);
+                         const float* A, const float* B, const float* lin, float* G, cudaStream_t stream,
+                         const float* wA = nullptr, const float* wB = nullptr, const float* wI = nullptr);
 int32_t ws_alloc(void** ptr, size_t bytes, cudaStream_t stream, const char* op);
 // Tensor-core path (efe_tc.cu); *used = false when the model is outside its
 // limits and nothing was launched.

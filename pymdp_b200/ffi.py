@@ -218,11 +218,11 @@ def can_handle(A_dependencies, B_dependencies, use_param_info_gain: bool, *, num
     """``pymdp/ffi/_efe.py:296-358``: the EFE kernel can run this problem.
 
     ``ffi_beneficial`` is accepted for signature parity (the reference's
-    Orin roofline router); this build always prefers the GPU path. This build
-    does not implement the parameter-information-gain or inductive terms yet,
-    so those requests return False (callers fall back to their own path).
+    Orin roofline router); this build always prefers the GPU path. The
+    parameter-information-gain and inductive terms are computed by the FP32
+    SIMT kernel whatever precision is requested.
     """
-    if not is_available() or use_param_info_gain or use_inductive:
+    if not is_available():
         return False
     if num_modalities is not None and len(A_dependencies) != num_modalities:
         return False
@@ -353,11 +353,22 @@ def neg_efe_all_policies_ffi(policy_matrix, qs_init, A, B, C, I, A_dependencies,
     C_flat, _ = flatten_ragged_f32(C_t, nb, dev)
     I_flat, _ = flatten_ragged_f32(I, nb, dev)
     _require_cuda(A_flat, "A")
+    pA_flat = pB_flat = None
+    if use_param_info_gain and pA:
+        for m, (pa, a) in enumerate(zip(pA, A)):
+            if tuple(np.shape(pa)) != tuple(np.shape(a)):
+                raise ValueError(f"pA[{m}] shape {tuple(np.shape(pa))} does not match A[{m}] {tuple(np.shape(a))}")
+        pA_flat, _ = flatten_ragged_f32(pA, nb, dev)
+    if use_param_info_gain and pB:
+        for f, (pb, bb) in enumerate(zip(pB, B)):
+            if tuple(np.shape(pb)) != tuple(np.shape(bb)):
+                raise ValueError(f"pB[{f}] shape {tuple(np.shape(pb))} does not match B[{f}] {tuple(np.shape(bb))}")
+        pB_flat, _ = flatten_ragged_f32(pB, nb, dev)
     eps = _dev_f32(torch.as_tensor(inductive_epsilon, dtype=torch.float32), dev).reshape(-1).contiguous()
     out = torch.empty(lead + (P,), dtype=torch.float32, device=dev)
     flags = efe_flags(use_utility, use_states_info_gain, use_param_info_gain, use_inductive,
                       ffi_cache_params_static, precision)
-    lay.call(None, pm, 0, qs_flat, A_flat, B_flat, C_flat, I_flat, None, None, eps, out, Bn, P, flags)
+    lay.call(None, pm, 0, qs_flat, A_flat, B_flat, C_flat, I_flat, pA_flat, pB_flat, eps, out, Bn, P, flags)
     return out
 
 

@@ -191,6 +191,78 @@ def make_efe_case(ref, name, cfg):
     return data
 
 
+# EFE with the flag-gated terms: parameter information gain (pA / pB) and the
+# inductive value (I from the reference's own generate_I_matrix)
+EFE_EXTRA_CASES = {
+    "efe_pig": dict(S=[3, 4, 2], O=[4, 5, 3], U=[2, 3, 2], T=2, A_deps=[[0, 2], [1], [1, 2, 0]],
+                    B_deps=[[0], [1, 0], [2]], pA=True, pB=True, ind=False, seed=21),
+    "efe_pigA": dict(S=[4, 3], O=[6, 2], U=[3, 2], T=2, A_deps=[[0, 1], [1]], B_deps=[[0], [1]],
+                     pA=True, pB=False, ind=False, seed=22),
+    "efe_ind": dict(S=[5, 4, 3], O=[4, 3], U=[3, 2, 1], T=3, A_deps=[[0, 1], [2, 1]], B_deps=[[0], [1], [2]],
+                    pA=False, pB=False, ind=True, seed=23),
+    "efe_all": dict(S=[4, 3, 2], O=[3, 4], U=[2, 3, 2], T=2, A_deps=[[0, 1], [2, 0]], B_deps=[[0], [1], [2]],
+                    pA=True, pB=True, ind=True, seed=24),
+}
+
+
+def dirichlet_counts(rng, shape):
+    """Positive concentration-like counts with about a tenth set to zero (the
+    (pA > 0) mask of the reference's weight)."""
+    a = rng.gamma(2.0, size=shape) * 3.0
+    a[rng.random(size=shape) < 0.1] = 0.0
+    return f32(a)
+
+
+def make_efe_extra_case(ref, name, cfg):
+    rng = np.random.default_rng(cfg["seed"])
+    S, O, U, T = cfg["S"], cfg["O"], cfg["U"], cfg["T"]
+    F, M = len(S), len(O)
+    A_deps, B_deps = cfg["A_deps"], cfg["B_deps"]
+    A = [dirichlet_cols(rng, (O[m],) + tuple(S[d] for d in A_deps[m]), 0.5) for m in range(M)]
+    B = [dirichlet_cols(rng, (S[f],) + tuple(S[d] for d in B_deps[f]) + (U[f],), 0.5) for f in range(F)]
+    C = [f32(rng.normal(size=O[m])) for m in range(M)]
+    qs = [dirichlet_cols(rng, (s,), 1.0) for s in S]
+    policies = np.asarray(ref.control.construct_policies(S, U, T)).astype(np.int32)
+    P = policies.shape[0]
+    E = dirichlet_cols(rng, (P,), 1.0)
+    pA = [dirichlet_counts(rng, a.shape) for a in A] if cfg["pA"] else None
+    pB = [dirichlet_counts(rng, b.shape) for b in B] if cfg["pB"] else None
+    use_pig = cfg["pA"] or cfg["pB"]
+    eps = 1e-3
+    if cfg["ind"]:
+        H = [f32(np.eye(s)[rng.integers(s)]) for s in S]
+        I = [np.asarray(i, np.float64) for i in ref.control.generate_I_matrix(H, B, 0.1, 3)]
+    else:
+        H = [f32(np.zeros(s)) for s in S]
+        I = [f32(np.zeros((1, s))) for s in S]
+    gamma = 16.0
+    q_pi, G = ref.control.update_posterior_policies_inductive(
+        policies, qs, A, B, C, E, pA, pB, A_deps, B_deps, I, gamma=gamma, inductive_epsilon=eps,
+        use_param_info_gain=use_pig, use_inductive=cfg["ind"])
+    action = np.asarray(ref.control.sample_policy(policies, q_pi))
+    adf, ado = deps_arrays(A_deps)
+    bdf, bdo = deps_arrays(B_deps)
+    data = dict(S=np.array(S, np.int64), O=np.array(O, np.int64), U=np.array(U, np.int64),
+                T=np.int64(T), A_dep_flat=adf, A_dep_offsets=ado, B_dep_flat=bdf, B_dep_offsets=bdo,
+                policies=policies, E=E.astype(np.float32), gamma=np.float64(gamma), eps=np.float64(eps),
+                use_param_info_gain=np.int64(use_pig), use_inductive=np.int64(cfg["ind"]),
+                has_pA=np.int64(cfg["pA"]), has_pB=np.int64(cfg["pB"]),
+                I_depths=np.array([i.shape[0] for i in I], np.int64),
+                q_pi=np.asarray(q_pi, np.float64), G=np.asarray(G, np.float64), action=action.astype(np.int32),
+                C_ndim=np.array([np.ndim(c) for c in C], np.int64))
+    data.update(pack("A", [a.astype(np.float32) for a in A]))
+    data.update(pack("B", [b.astype(np.float32) for b in B]))
+    data.update(pack("C", [c.astype(np.float32) for c in C]))
+    data.update(pack("qs", [q.astype(np.float32) for q in qs]))
+    data.update(pack("I", [i.astype(np.float32) for i in I]))
+    data.update(pack("H", H))
+    if pA is not None:
+        data.update(pack("pA", pA))
+    if pB is not None:
+        data.update(pack("pB", pB))
+    return data
+
+
 def main(ref_root):
     sys.path.insert(0, HERE)
     import refshim
@@ -201,6 +273,9 @@ def main(ref_root):
         print("wrote", name)
     for name, cfg in EFE_CASES.items():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_efe_case(ref, name, cfg))
+        print("wrote", name)
+    for name, cfg in EFE_EXTRA_CASES.items():
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_efe_extra_case(ref, name, cfg))
         print("wrote", name)
 
 

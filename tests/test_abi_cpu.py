@@ -120,13 +120,17 @@ def test_efe_layout_errors():
     assert "out of range" in _lib.last_error()
 
 
-def test_efe_unbuilt_terms_are_unsupported():
+def test_efe_flag_gated_terms_validation():
+    """Inductive (bit 2) and parameter information gain (bit 3): the count
+    checks of neg_efe_layout.h, before any device work (empty batch)."""
     lay = _efe_layout_args()
-    assert _efe_call(lay, flags=3 | 4) == _lib.B2_ERR_UNSUPPORTED
-    assert "inductive" in _lib.last_error()
-    assert _efe_call(lay, flags=3 | 8, counts=dict(pA=1)) == _lib.B2_ERR_UNSUPPORTED
+    assert _efe_call(lay, flags=3 | 4) == _lib.B2_OK
     assert _efe_call(lay, flags=3 | 8) == _lib.B2_ERR_INVALID_ARGUMENT
     assert "requires at least one of pA, pB" in _lib.last_error()
+    assert _efe_call(lay, flags=3 | 8, counts=dict(pA=1)) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "pA element_count = 1, expected 0" in _lib.last_error()
+    assert _efe_call(lay, flags=3 | 8, counts=dict(pB=2)) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "pB element_count = 2, expected 0" in _lib.last_error()
 
 
 def test_construct_policies_matches_oracle_order():
@@ -142,3 +146,16 @@ def test_package_imports_without_gpu():
     assert callable(ffi.fpi_ffi) and callable(ffi.neg_efe_all_policies_ffi)
     assert pymdp_b200.Agent is Agent
     assert ffi.is_available()
+
+
+def test_generate_I_matrix_matches_reference_fixture():
+    """pymdp_b200.control.generate_I_matrix against the I the reference's
+    generate_I_matrix (pymdp/control.py:965-1019) produced for the stored
+    goal vectors H (threshold 0.1, depth 3)."""
+    from conftest import load_golden, unpack
+    from pymdp_b200.control import generate_I_matrix
+    for name in ("efe_ind", "efe_all"):
+        d = load_golden(name)
+        I = generate_I_matrix(unpack(d, "H"), unpack(d, "B"), 0.1, 3)
+        for got, want in zip(I, unpack(d, "I")):
+            np.testing.assert_array_equal(got, want)

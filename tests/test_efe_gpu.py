@@ -148,3 +148,101 @@ def test_tensor_core_random_models_match_oracle(case, precision):
         ref = oefe.neg_efe_all_policies(pol, [q[b] for q in qs], [a[b] for a in A], [x[b] for x in B],
                                         [c[b] for c in C], case["A_deps"], case["B_deps"])
         _g_close(G[b], ref, precision)
+
+
+# ------------------------------------------- flag-gated terms (bits 2 and 3)
+# Parameter information gain (pA / pB, exact Dirichlet weight with digamma)
+# and the inductive value, against golden vectors from the reference's
+# update_posterior_policies_inductive (pymdp/control.py:795-963) and against
+# the FP64 oracle on random models. These terms run on the FP32 SIMT kernel
+# for every precision selector, so the FP32 tolerance applies to all three.
+EFE_EXTRA = ["efe_pig", "efe_pigA", "efe_ind", "efe_all"]
+
+
+def run_golden_extra(d, precision):
+    from pymdp_b200 import ffi
+    A_deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    B_deps = deps_from(d["B_dep_flat"], d["B_dep_offsets"])
+    qs = [cuda(q) for q in unpack(d, "qs")]
+    pA = [cuda(a) for a in unpack(d, "pA")] if int(d["has_pA"]) else None
+    pB = [cuda(b) for b in unpack(d, "pB")] if int(d["has_pB"]) else None
+    G = ffi.neg_efe_all_policies_ffi(d["policies"], qs, [cuda(a) for a in unpack(d, "A")],
+                                     [cuda(b) for b in unpack(d, "B")], [cuda(c) for c in unpack(d, "C")],
+                                     [cuda(i) for i in unpack(d, "I")], A_deps, B_deps, pA=pA, pB=pB,
+                                     use_param_info_gain=bool(int(d["use_param_info_gain"])),
+                                     use_inductive=bool(int(d["use_inductive"])),
+                                     inductive_epsilon=float(d["eps"]), precision=precision)
+    q_pi = ffi.policy_posterior(G, cuda(d["E"]), float(d["gamma"]))
+    act = ffi.select_action(q_pi, d["policies"])
+    return G.cpu().numpy(), q_pi.cpu().numpy(), act.cpu().numpy()
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3", "bf16"])
+@pytest.mark.parametrize("name", EFE_EXTRA)
+def test_flag_gated_terms_match_reference(name, precision):
+    d = load_golden(name)
+    G, q_pi, act = run_golden_extra(d, precision)
+    np.testing.assert_allclose(G, d["G"], rtol=G_RTOL, atol=G_ATOL)
+    np.testing.assert_allclose(q_pi, d["q_pi"], rtol=Q_RTOL, atol=Q_ATOL)
+    np.testing.assert_array_equal(act, d["action"])
+
+
+@pytest.mark.parametrize("terms", ["pA", "pB", "pApB", "ind", "all"])
+def test_flag_gated_terms_random_models_match_oracle(terms):
+    from pymdp_b200 import ffi
+    S, O, U, T = [4, 3, 2], [5, 3], [3, 2, 2], 2
+    A_deps, B_deps = [[0, 2], [1, 0]], [[0], [1, 0], [2]]
+    rng = np.random.default_rng(len(terms) + 31)
+    batch = 3
+    A, B, C, qs = random_efe(rng, S, O, U, T, A_deps, B_deps, batch)
+    counts = lambda shape: (rng.gamma(1.5, size=shape) * 2 * (rng.random(size=shape) > 0.1)).astype(np.float32)
+    pA = [counts(a.shape) for a in A] if "pA" in terms or terms == "all" else None
+    pB = [counts(b.shape) for b in B] if "pB" in terms or terms == "all" else None
+    use_ind = terms in ("ind", "all")
+    I = [(rng.random(size=(batch, 3, s)) > 0.5).astype(np.float32) for s in S]
+    eps = np.array([1e-3, 1e-2, 0.2], np.float32)
+    pol = oefe.construct_policies(S, U, T)
+    G = ffi.neg_efe_all_policies_ffi(pol, [cuda(q) for q in qs], [cuda(a) for a in A], [cuda(b) for b in B],
+                                     [cuda(c) for c in C], [cuda(i) for i in I], A_deps, B_deps,
+                                     pA=[cuda(x) for x in pA] if pA else None,
+                                     pB=[cuda(x) for x in pB] if pB else None,
+                                     use_param_info_gain=pA is not None or pB is not None, use_inductive=use_ind,
+                                     inductive_epsilon=cuda(eps)).cpu().numpy()
+    for b in range(batch):
+        ref = oefe.neg_efe_all_policies(pol, [q[b] for q in qs], [a[b] for a in A], [x[b] for x in B],
+                                        [c[b] for c in C], A_deps, B_deps,
+                                        pA=[x[b] for x in pA] if pA else None,
+                                        pB=[x[b] for x in pB] if pB else None,
+                                        use_param_info_gain=pA is not None or pB is not None,
+                                        I=[i[b] for i in I], use_inductive=use_ind,
+                                        inductive_epsilon=float(eps[b]))
+        np.testing.assert_allclose(G[b], ref, rtol=G_RTOL, atol=G_ATOL * max(1.0, np.abs(ref).max()))
+
+
+def test_agent_with_param_info_gain_and_inductive_matches_oracle():
+    """The Agent facade with pA, pB and goal vectors H (I built by
+    generate_I_matrix, pymdp/agent.py:368-380) against the FP64 oracle."""
+    from pymdp_b200 import Agent
+    from pymdp_b200.control import generate_I_matrix
+    S, O, U, T = [4, 3], [5, 3], [3, 2], 2
+    A_deps, B_deps = [[0, 1], [1]], [[0], [1]]
+    rng = np.random.default_rng(77)
+    batch = 2
+    A, B, C, qs = random_efe(rng, S, O, U, T, A_deps, B_deps, batch)
+    pA = [(rng.gamma(2.0, size=a.shape) * 2).astype(np.float32) for a in A]
+    pB = [(rng.gamma(2.0, size=b.shape) * 2).astype(np.float32) for b in B]
+    H = [np.eye(s, dtype=np.float32)[s - 1] for s in S]
+    agent = Agent(A, B, C=C, A_dependencies=A_deps, B_dependencies=B_deps, policy_len=T, gamma=16.0,
+                  batch_size=batch, pA=pA, pB=pB, H=H, inductive_depth=3, inductive_threshold=0.1,
+                  inductive_epsilon=1e-3, use_param_info_gain=True, use_inductive=True)
+    q_pi, G = agent.infer_policies([cuda(q) for q in qs])
+    pol = oefe.construct_policies(S, U, T)
+    for b in range(batch):
+        I = generate_I_matrix(H, [x[b] for x in B], 0.1, 3)
+        E = np.full(len(pol), 1.0 / len(pol))
+        q_ref, G_ref = oefe.update_posterior_policies(
+            pol, [q[b] for q in qs], [a[b] for a in A], [x[b] for x in B], [c[b] for c in C], E, A_deps, B_deps,
+            gamma=16.0, pA=[x[b] for x in pA], pB=[x[b] for x in pB], use_param_info_gain=True, I=I,
+            use_inductive=True, inductive_epsilon=1e-3)
+        np.testing.assert_allclose(G[b].cpu().numpy(), G_ref, rtol=G_RTOL, atol=G_ATOL * max(1.0, np.abs(G_ref).max()))
+        np.testing.assert_allclose(q_pi[b].cpu().numpy(), q_ref, rtol=Q_RTOL, atol=Q_ATOL)

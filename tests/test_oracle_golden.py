@@ -56,3 +56,33 @@ def test_efe_oracle_matches_reference(name):
     np.testing.assert_allclose(G, d["G"], rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(q_pi, d["q_pi"], rtol=1e-10, atol=1e-300)
     np.testing.assert_array_equal(oefe.sample_policy(pol, q_pi), d["action"])
+
+
+EFE_EXTRA = ["efe_pig", "efe_pigA", "efe_ind", "efe_all"]
+
+
+def extra_terms(d):
+    """Keyword arguments of the flag-gated terms stored in an extra golden case."""
+    return dict(pA=unpack(d, "pA") if int(d["has_pA"]) else None,
+                pB=unpack(d, "pB") if int(d["has_pB"]) else None,
+                use_param_info_gain=bool(int(d["use_param_info_gain"])),
+                I=unpack(d, "I"), use_inductive=bool(int(d["use_inductive"])),
+                inductive_epsilon=float(d["eps"]))
+
+
+@pytest.mark.parametrize("name", EFE_EXTRA)
+def test_efe_oracle_extra_terms_match_reference(name):
+    """Parameter information gain (pA / pB) and the inductive value, against
+    the reference's own update_posterior_policies_inductive (control.py:795-963)."""
+    d = load_golden(name)
+    A_deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    B_deps = deps_from(d["B_dep_flat"], d["B_dep_offsets"])
+    S, U, T = d["S"].tolist(), d["U"].tolist(), int(d["T"])
+    pol = oefe.construct_policies(S, U, T)
+    np.testing.assert_array_equal(pol, d["policies"])
+    q_pi, G = oefe.update_posterior_policies(pol, unpack(d, "qs"), unpack(d, "A"), unpack(d, "B"),
+                                             unpack(d, "C"), d["E"], A_deps, B_deps,
+                                             gamma=float(d["gamma"]), **extra_terms(d))
+    np.testing.assert_allclose(G, d["G"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(q_pi, d["q_pi"], rtol=1e-10, atol=1e-300)
+    np.testing.assert_array_equal(oefe.sample_policy(pol, q_pi), d["action"])
