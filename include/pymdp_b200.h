@@ -179,6 +179,38 @@ int32_t b2_neg_efe_noalloc(void* stream, const int32_t* policy_matrix, int64_t p
                            const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
                            const int64_t* B_dep_offsets, int32_t flags);
 
+/* ============================================================== adjoints ==
+ * No counterpart in the reference's native kernels: the reference obtains
+ * gradients with jax.grad of its JAX path (pymdp/ffi/_core.py:282-310,
+ * `with_jax_grad`). These are hand-written reverse passes of the same
+ * arithmetic, for model fitting.
+ *
+ * b2_neg_efe_bwd: given d_neg_efe = dL/dG [Bn, P], writes dL/dqs_init
+ * [Bn, qs_offsets[F]], dL/dA, dL/dB, dL/dC (laid out like A, B, C). Utility
+ * and state information gain only (flag bits 0 and 1). Arguments otherwise as
+ * b2_neg_efe (no I / pA / pB / epsilon). FP32 with atomic accumulation over
+ * policies; (T + 1) * total states <= 1024. */
+int32_t b2_neg_efe_bwd(void* stream, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+                       const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
+                       const float* B, int64_t B_count, const float* C, int64_t C_count,
+                       const float* d_neg_efe, int64_t dG_count, float* d_qs_init, float* d_A, float* d_B,
+                       float* d_C, int64_t Bn, int64_t P, int64_t T, int64_t F, int64_t M, const int64_t* S,
+                       const int64_t* O, const int64_t* U, const int64_t* qs_offsets, const int64_t* A_offsets,
+                       const int64_t* B_offsets, const int64_t* C_offsets, const int64_t* A_dep_flat,
+                       int64_t A_dep_flat_len, const int64_t* A_dep_offsets, const int64_t* B_dep_flat,
+                       int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int32_t flags);
+
+/* b2_fpi_obs_bwd: reverse pass of b2_fpi_obs (unrolled through all num_iter
+ * sweeps, FP64, every iterate recomputed on chip). Given d_q = dL/dq_out
+ * [batch, S_tot], writes dL/dA (laid out like A_flat; only the observed rows
+ * are non-zero; accumulated over agents when A_agent_stride = 0) and dL/dprior
+ * [batch, S_tot]. Other arguments as b2_fpi_obs. */
+int32_t b2_fpi_obs_bwd(void* stream, const float* A_flat, int64_t A_agent_stride, const int64_t* A_offsets,
+                       int64_t A_offsets_len, const int64_t* O, int64_t O_len, const int32_t* obs,
+                       const float* prior, const float* d_q, float* d_A, float* d_prior, int64_t batch,
+                       const int64_t* S, int64_t S_len, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                       const int64_t* A_dep_offsets, int64_t A_dep_offsets_len, int32_t num_iter);
+
 /* q_pi = softmax(gamma * neg_efe + log(clip(E, eps))) per agent — the step
  * the reference runs in XLA right after the FFI call
  * (pymdp/control.py:349 and :963). gamma is [Bn] (gamma_batched = 1) or a

@@ -73,6 +73,12 @@ _SIGS = {
                                      c_int64, _PF, c_int64, c_int64, c_int64, c_int64, c_int64, c_int64, _P64,
                                      _P64, _P64, _P64, _P64, _P64, _P64, _P64, _P64, _P64, c_int64, _P64, _P64,
                                      c_int64, _P64, c_int32]),
+    "b2_neg_efe_bwd": (c_int32, [c_void_p, c_void_p, c_int64, c_int32, _PF, c_int64, _PF, c_int64, _PF, c_int64,
+                                 _PF, c_int64, _PF, c_int64, _PF, _PF, _PF, _PF, c_int64, c_int64, c_int64, c_int64,
+                                 c_int64, _P64, _P64, _P64, _P64, _P64, _P64, _P64, _P64, c_int64, _P64, _P64,
+                                 c_int64, _P64, c_int32]),
+    "b2_fpi_obs_bwd": (c_int32, [c_void_p, _PF, c_int64, _P64, c_int64, _P64, c_int64, c_void_p, _PF, _PF, _PF,
+                                 _PF, c_int64, _P64, c_int64, _P64, c_int64, _P64, c_int64, c_int32]),
     "b2_policy_posterior": (c_int32, [c_void_p, _PF, _PF, c_int32, _PF, c_int32, _PF, c_int64, c_int64]),
     "b2_select_action": (c_int32, [c_void_p, _PF, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64]),
 }

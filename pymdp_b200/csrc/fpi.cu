@@ -773,6 +773,169 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
   }
 }
 
+
+// ------------------------------------------------------------ adjoint
+// Reverse pass of the fused-observation FPI for gradients of a loss on the
+// posteriors with respect to the observed A rows and the prior. The reference
+// differentiates its JAX scan (pymdp/ffi/_core.py:282-310 with_jax_grad over
+// pymdp/algos.py:88-155); this is the hand-written unrolled adjoint of the
+// same Jacobi sweeps, with every iterate recomputed and kept on chip:
+//   q_i = softmax(logq_i), logq_{i+1} = lp + sum_(g,ax) M_(g,ax)(q_i),
+//   M_(g,ax)(q)[s] = sum_{k: digit_ax(k) = s} ll_g[k] prod_{j != ax} q_{dep j}[digit_j(k)],
+// output softmax(logq_n). Backward: softmax adjoint, then for i = n-1..0
+// d lp += d logq_{i+1}, d ll_g[k] += c prod_{j != ax} q, d q_i += c ll_g[k]
+// prod_{l != ax, j} q with c = d logq_{i+1}[dep ax][digit ax(k)], and the
+// softmax adjoint for d logq_i. Finally d A[o_m, k] = d ll_g[k] / A (A >= eps)
+// for every source m of group g, d prior = d lp / prior (prior >= eps). FP64
+// throughout; one warp per agent; shared-memory double atomics for sums over k.
+struct FpiBwd {
+  int32_t ll_off[kMaxM + 1];  // group g's ll (and d ll) doubles inside the agent's smem block
+  int32_t words;              // doubles per agent
+};
+
+__device__ __forceinline__ void softmax_bwd_warp(const double* __restrict__ q, const double* __restrict__ gq,
+                                                 double* __restrict__ glogq, int n, int lane) {
+  double dot = 0.0;
+  for (int i = lane; i < n; i += 32) dot += q[i] * gq[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+  for (int i = lane; i < n; i += 32) glogq[i] = q[i] * (gq[i] - dot);
+}
+
+__global__ void __launch_bounds__(32)
+    fpi_bwd_kernel(const __grid_constant__ FpiParams p, const __grid_constant__ FpiBwd bw, const FpiIO io,
+                   const float* __restrict__ dq_out, float* __restrict__ dA, float* __restrict__ dprior) {
+  extern __shared__ double smem_d[];
+  const int lane = threadIdx.x;
+  const int64_t b = blockIdx.x;
+  if (b >= io.batch) return;
+  const int F = p.F, St = p.S_tot, n = p.num_iter;
+  double* ll = smem_d;                    // [sum_g K_g]
+  double* dll = ll + bw.ll_off[p.G];      // [sum_g K_g]
+  double* lp = dll + bw.ll_off[p.G];      // [St]
+  double* dlp = lp + St;                  // [St]
+  double* hist = dlp + St;                // [(n + 1) * St]: q_0 .. q_{n-1}, then softmax(logq_n)
+  double* logq = hist + (n + 1) * St;     // [St]
+  double* glogq = logq + St;              // [St]
+  double* gq = glogq + St;                // [St]
+  int64_t* rowoff = reinterpret_cast<int64_t*>(gq + St);  // [M]
+
+  for (int m = lane; m < p.M; m += 32) {
+    int o = io.obs[b * p.M + m];
+    o = (o < 0 || o >= p.src[m].O) ? 0 : o;
+    rowoff[m] = b * io.src_stride + p.src[m].src_off + (int64_t)o * p.src[m].K;
+  }
+  for (int i = lane; i < St; i += 32) {
+    lp[i] = log((double)fmaxf(__ldg(io.prior + b * St + i), kMinVal));
+    dlp[i] = 0.0;
+    logq[i] = 0.0;
+  }
+  __syncwarp();
+  for (int g = 0; g < p.G; ++g) {
+    const FpiGroup& gr = p.grp[g];
+    for (int k = lane; k < gr.K; k += 32) {
+      double v = 0.0;
+      for (int si = gr.src_begin; si < gr.src_end; ++si)
+        v += log((double)fmaxf(__ldg(io.src + rowoff[p.src_order[si]] + k), kMinVal));
+      ll[bw.ll_off[g] + k] = v;
+      dll[bw.ll_off[g] + k] = 0.0;
+    }
+  }
+  __syncwarp();
+  // forward with history
+  for (int it = 0; it <= n; ++it) {
+    for (int f = 0; f < F; ++f) softmax_warp(logq + p.lp_off[f], hist + it * St + p.lp_off[f], p.S[f], lane);
+    __syncwarp();
+    if (it == n) break;
+    const double* q = hist + it * St;
+    for (int i = lane; i < St; i += 32) logq[i] = lp[i];
+    __syncwarp();
+    for (int g = 0; g < p.G; ++g) {
+      const FpiGroup& gr = p.grp[g];
+      for (int k = lane; k < gr.K; k += 32) {
+        int dig[kMaxRank];
+        int rem = k;
+        for (int x = gr.rank - 1; x >= 0; --x) {
+          const int d = p.S[gr.dep[x]];
+          const int qd = rem / d;
+          dig[x] = rem - qd * d;
+          rem = qd;
+        }
+        const double L = ll[bw.ll_off[g] + k];
+        for (int ax = 0; ax < gr.rank; ++ax) {
+          double other = L;
+          for (int j = 0; j < gr.rank; ++j)
+            if (j != ax) other *= q[p.lp_off[gr.dep[j]] + dig[j]];
+          atomicAdd(&logq[p.lp_off[gr.dep[ax]] + dig[ax]], other);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // backward
+  for (int i = lane; i < St; i += 32) gq[i] = (double)__ldg(dq_out + b * St + i);
+  __syncwarp();
+  for (int f = 0; f < F; ++f)
+    softmax_bwd_warp(hist + n * St + p.lp_off[f], gq + p.lp_off[f], glogq + p.lp_off[f], p.S[f], lane);
+  __syncwarp();
+  for (int it = n - 1; it >= 0; --it) {
+    const double* q = hist + it * St;
+    for (int i = lane; i < St; i += 32) {
+      dlp[i] += glogq[i];
+      gq[i] = 0.0;
+    }
+    __syncwarp();
+    for (int g = 0; g < p.G; ++g) {
+      const FpiGroup& gr = p.grp[g];
+      for (int k = lane; k < gr.K; k += 32) {
+        int dig[kMaxRank];
+        int rem = k;
+        for (int x = gr.rank - 1; x >= 0; --x) {
+          const int d = p.S[gr.dep[x]];
+          const int qd = rem / d;
+          dig[x] = rem - qd * d;
+          rem = qd;
+        }
+        const double L = ll[bw.ll_off[g] + k];
+        double dl = 0.0;
+        for (int ax = 0; ax < gr.rank; ++ax) {
+          const double c = glogq[p.lp_off[gr.dep[ax]] + dig[ax]];
+          double prod = 1.0;
+          for (int j = 0; j < gr.rank; ++j)
+            if (j != ax) prod *= q[p.lp_off[gr.dep[j]] + dig[j]];
+          dl += c * prod;
+          for (int j = 0; j < gr.rank; ++j) {
+            if (j == ax) continue;
+            double pr = c * L;
+            for (int l = 0; l < gr.rank; ++l)
+              if (l != ax && l != j) pr *= q[p.lp_off[gr.dep[l]] + dig[l]];
+            atomicAdd(&gq[p.lp_off[gr.dep[j]] + dig[j]], pr);
+          }
+        }
+        dll[bw.ll_off[g] + k] += dl;  // one lane per k
+      }
+    }
+    __syncwarp();
+    for (int f = 0; f < F; ++f)
+      softmax_bwd_warp(q + p.lp_off[f], gq + p.lp_off[f], glogq + p.lp_off[f], p.S[f], lane);
+    __syncwarp();
+  }
+  // to the inputs
+  for (int i = lane; i < St; i += 32) {
+    const float pv = __ldg(io.prior + b * St + i);
+    dprior[b * St + i] = pv >= kMinVal ? (float)(dlp[i] / (double)pv) : 0.f;
+  }
+  for (int g = 0; g < p.G; ++g) {
+    const FpiGroup& gr = p.grp[g];
+    for (int k = lane; k < gr.K; k += 32)
+      for (int si = gr.src_begin; si < gr.src_end; ++si) {
+        const int64_t e = rowoff[p.src_order[si]] + k;
+        const float a = __ldg(io.src + e);
+        if (a >= kMinVal) atomicAdd(dA + e, (float)(dll[bw.ll_off[g] + k] / (double)a));
+      }
+  }
+}
+
 template <int TEAM, int APC, bool FUSED>
 int32_t launch_one(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const char* op) {
   const int bytes = APC * p.agent_words * 8;
@@ -900,4 +1063,59 @@ extern "C" int32_t b2_fpi_obs(void* stream, const float* A_flat, int64_t A_agent
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer");
   FpiIO io{A_flat, A_agent_stride, obs, prior, q_out, batch};
   return launch<true>(p, io, (cudaStream_t)stream, op);
+}
+
+extern "C" int32_t b2_fpi_obs_bwd(void* stream, const float* A_flat, int64_t A_agent_stride,
+                                  const int64_t* A_offsets, int64_t A_offsets_len, const int64_t* O, int64_t O_len,
+                                  const int32_t* obs, const float* prior, const float* d_q, float* d_A,
+                                  float* d_prior, int64_t batch, const int64_t* S, int64_t S_len,
+                                  const int64_t* A_dep_flat, int64_t A_dep_flat_len, const int64_t* A_dep_offsets,
+                                  int64_t A_dep_offsets_len, int32_t num_iter) {
+  const char* op = "fpi_obs bwd";
+  if (!S || !A_offsets || !O || !A_dep_flat || !A_dep_offsets)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null attribute array");
+  const int64_t M = A_dep_offsets_len - 1;
+  if (O_len != M || A_offsets_len != M + 1)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": O / A_offsets sizes inconsistent with M = " +
+                                             std::to_string(M));
+  FpiParams p;
+  std::vector<int64_t> K;
+  B2_TRY(build_params(&p, &K, S, S_len, nullptr, 0, A_dep_flat, A_dep_flat_len, A_dep_offsets, A_dep_offsets_len,
+                      num_iter, op));
+  if (A_offsets[0] != 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_offsets must start at zero");
+  for (int64_t m = 0; m < M; ++m) {
+    if (O[m] <= 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": " + idx("O", m) + " must be positive");
+    if (A_offsets[m + 1] - A_offsets[m] != O[m] * K[m])
+      return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_offsets inconsistent with O/deps for modality " +
+                                               std::to_string(m));
+    p.src[m].src_off = A_offsets[m];
+    p.src[m].O = (int32_t)O[m];
+  }
+  if (batch < 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": negative batch");
+  if (A_agent_stride != 0 && A_agent_stride < A_offsets[M])
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_agent_stride smaller than one agent's A");
+  FpiBwd bw;
+  std::memset(&bw, 0, sizeof(bw));
+  int64_t off = 0;
+  for (int g = 0; g < p.G; ++g) {
+    bw.ll_off[g] = (int32_t)off;
+    off += p.grp[g].K;
+  }
+  bw.ll_off[p.G] = (int32_t)off;
+  const int64_t words = 2 * off + 2LL * p.S_tot + (int64_t)(num_iter + 1) * p.S_tot + 3LL * p.S_tot + M;
+  if (words * 8 > kMaxSmemPerCta)
+    return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": per-agent working set of " + std::to_string(words * 8) +
+                                        " bytes exceeds shared memory");
+  bw.words = (int32_t)words;
+  if (batch == 0) return B2_OK;
+  if (!A_flat || !obs || !prior || !d_q || !d_A || !d_prior)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer");
+  if (batch > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
+  const int64_t a_words = A_agent_stride == 0 ? A_offsets[M] : batch * A_agent_stride;
+  B2_CUDA_TRY(op, cudaMemsetAsync(d_A, 0, (size_t)a_words * sizeof(float), (cudaStream_t)stream));
+  FpiIO io{A_flat, A_agent_stride, obs, prior, nullptr, batch};
+  const int bytes = (int)words * 8;
+  B2_TRY(ensure_smem_attr((const void*)fpi_bwd_kernel, bytes, op));
+  fpi_bwd_kernel<<<(unsigned)batch, 32, bytes, (cudaStream_t)stream>>>(p, bw, io, d_q, d_A, d_prior);
+  return check_launch(op);
 }
