@@ -159,3 +159,19 @@ def test_generate_I_matrix_matches_reference_fixture():
         I = generate_I_matrix(unpack(d, "H"), unpack(d, "B"), 0.1, 3)
         for got, want in zip(I, unpack(d, "I")):
             np.testing.assert_array_equal(got, want)
+
+
+def test_fit_model_multiaction_map_matches_oracle():
+    """Host logic of the fitting likelihood: the policy -> multi-action map
+    reproduces ``multiaction_probabilities`` (``pymdp/agent.py:908-937``)."""
+    import torch
+
+    from oracle import fitting as ofit
+    from pymdp_b200.fitting import FitModel
+    for S, U, T in (([8, 4], [4, 1], 2), ([3, 2, 2], [3, 1, 2], 2), ([4], [4], 3)):
+        fm = FitModel(S, [3] * len(S), U, policy_len=T, device="cpu")
+        rng = np.random.default_rng(1)
+        q = rng.dirichlet(np.ones(fm.P))
+        got = (torch.as_tensor(q, dtype=torch.float32) @ fm.policy_to_multi).numpy()
+        ref = ofit.multiaction_probabilities(q, fm.policies.numpy(), U)
+        np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
