@@ -133,6 +133,50 @@ def run_fpi_config(dev, steps: int, warmup: int, flush):
             "bytes_per_launch": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
 
 
+FIT_SUBJECTS, FIT_TRIALS = 1024, 64
+
+
+def run_fit_config(dev, steps: int, warmup: int, flush):
+    """Model fitting: the summed action log-likelihood of 1024 subjects x 64
+    trials (S=[8,4], O=[8,4,3] on both factors, U=[4,1], policy_len 2,
+    num_iter 16, logits ~ N(0,1), C ~ N(0,1), log gamma ~ N(log 8, 0.3),
+    actions sampled from each subject's own model) and its gradient w.r.t.
+    every parameter, forward + backward replayed as one CUDA graph. Device
+    time per evaluation (L2 flushed before each) and subject-steps/s."""
+    import torch
+
+    from pymdp_b200 import _lib
+    from pymdp_b200.fitting import FitModel, GraphedLogLikelihood
+
+    fm = FitModel([8, 4], [8, 4, 3], [4, 1], policy_len=2, num_iter=16, device=dev)
+    gen = torch.Generator(device=dev).manual_seed(3)
+    A, B, C, lg = fm.init_params(FIT_SUBJECTS, gen)
+    obs, acts = fm.simulate(A, B, C, lg, FIT_TRIALS, gen)
+    params = [x.clone().requires_grad_(True) for x in A + B + C + [lg]]
+    n0 = _lib.launch_count()
+    graphed = GraphedLogLikelihood(fm, params, obs, acts, warmup=max(warmup, 1))
+    native = _lib.launch_count() - n0  # native launches of the warm-up passes plus the captured one
+    for _ in range(warmup):
+        graphed()
+    torch.cuda.synchronize(dev)
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        graphed()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    return {"workload": f"model fitting, {FIT_SUBJECTS} subjects x {FIT_TRIALS} trials, S=[8,4], O=[8,4,3], "
+                        "U=[4,1], policy_len 2, num_iter 16: action log-likelihood + gradient w.r.t. A/B logits, "
+                        "C and log gamma (native FPI / neg-EFE adjoints, one CUDA graph), L2 flushed before each",
+            "subject_steps_per_s": FIT_SUBJECTS * FIT_TRIALS / (ms * 1e-3), "ms_per_evaluation": ms,
+            "native_launches_per_evaluation": native // (max(warmup, 1) + 1),
+            "log_likelihood": float(graphed.ll)}
+
+
 def efe_flops_per_agent() -> float:
     K = int(np.prod(S))
     P = int(np.prod(U)) ** T
@@ -310,6 +354,7 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     fpi_res = run_fpi_config(dev, args.steps, args.warmup, flush)
+    fit_res = run_fit_config(dev, args.steps, args.warmup, flush)
     efe_ev = []
 
     def step(timed_efe=False):
@@ -434,6 +479,7 @@ def run_b200(args, rank, world, local_rank):
         "error_vs_fp64": err,
         "fpi": dict(fpi_res, roofline={"bound": "hbm", "achieved": fpi_res["gbs"], "peak": peak_gbs, "unit": "GB/s",
                                        "frac": fpi_res["gbs"] / peak_gbs}),
+        "fit": fit_res,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -445,8 +491,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "fpi"],
-                    help="step: the agent step (default); fpi: only the 4096-agent FPI model (for profiling)")
+    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit"],
+                    help="step: the agent step (default); fpi: only the 4096-agent FPI model; fit: only the "
+                         "model-fitting gradient (for profiling)")
     ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
@@ -458,6 +505,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    if args.workload in ("fpi", "fit") and world > 1:
+        raise SystemExit("--workload fpi/fit runs on one GPU")
     if args.workload == "fpi":
         import torch
 
@@ -465,6 +514,14 @@ def main():
         torch.cuda.set_device(dev)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         print(json.dumps(run_fpi_config(dev, args.steps, args.warmup, flush)), flush=True)
+        return
+    if args.workload == "fit":
+        import torch
+
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        print(json.dumps(run_fit_config(dev, args.steps, args.warmup, flush)), flush=True)
         return
     if world > 1:
         import datetime

@@ -73,6 +73,8 @@ class FitModel:
         self.policy_to_multi = torch.as_tensor(onehot, device=self.device)
         self.log_E = torch.full((self.P,), -math.log(self.P), device=self.device)
         self.qs_offsets = np.cumsum([0] + self.S)
+        self.multi_stride = torch.as_tensor([int(np.prod(self.U[f + 1:])) for f in range(self.F)],
+                                            device=self.device)
 
     # ------------------------------------------------------------------ params
     def init_params(self, n_subjects: int, generator: torch.Generator | None = None, log_gamma_mean=math.log(8.0),
@@ -125,11 +127,10 @@ class FitModel:
         n = A_flat.shape[0]
         gamma = torch.exp(log_gamma)
         prior = torch.cat([torch.full((n, s), 1.0 / s, device=A_flat.device) for s in self.S], dim=1)
-        mult = torch.as_tensor([int(np.prod(self.U[f + 1:])) for f in range(self.F)], device=A_flat.device)
         ll = torch.zeros(n, device=A_flat.device)
         for t in range(obs.shape[0]):
             qs, probs = self._step_probs(A_flat, B_flat, C_flat, gamma, prior, obs[t])
-            k = (actions[t] * mult).sum(-1, keepdim=True)
+            k = (actions[t] * self.multi_stride).sum(-1, keepdim=True)
             lp = torch.log(probs) if form == "log" else torch.log_softmax(probs, dim=-1)
             ll = ll + lp.gather(1, k).squeeze(1)
             prior = self._prior_next(B, qs, actions[t])
@@ -166,3 +167,51 @@ class FitModel:
             s = torch.stack([torch.multinomial(B[f][ar, :, s[:, f], acts[t, :, f]], 1, generator=generator)[:, 0]
                              for f in range(self.F)], dim=1)
         return obs, acts
+
+
+class GraphedLogLikelihood:
+    """One forward + backward of :meth:`FitModel.log_likelihood` over fixed
+    trials, captured in a CUDA graph.
+
+    ``params`` are leaf tensors (A logits, B logits, C, log gamma, in that
+    order, as lists flattened into one list) that the caller updates IN
+    PLACE between calls; each call replays the graph and returns the static
+    likelihood tensor, with the gradients in ``p.grad`` (overwritten, not
+    accumulated). Every kernel of the step, the native FPI / neg-EFE forward
+    and adjoint launches included, is replayed without host work. No earlier
+    autograd graph over ``params`` may still be alive at construction (drop
+    any eager loss first): its gradient-accumulation nodes belong to another
+    stream and break the capture.
+    """
+
+    def __init__(self, model: FitModel, params: Sequence[torch.Tensor], obs, actions, form: str = "log",
+                 warmup: int = 3):
+        self.model, self.params = model, list(params)
+        nA, nB, nC = model.M, model.F, model.M
+        if len(self.params) != nA + nB + nC + 1:
+            raise ValueError("params must be A logits + B logits + C + [log_gamma]")
+        self.obs, self.actions = obs.contiguous(), actions.contiguous()
+        split = (self.params[:nA], self.params[nA:nA + nB], self.params[nA + nB:nA + nB + nC], self.params[-1])
+
+        def step():
+            ll = model.log_likelihood(*split, self.obs, self.actions, form=form)
+            ll.backward()
+            return ll
+
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                for p in self.params:
+                    p.grad = None
+                step()
+        torch.cuda.current_stream().wait_stream(side)
+        for p in self.params:
+            p.grad = None
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.ll = step()
+
+    def __call__(self) -> torch.Tensor:
+        self.graph.replay()
+        return self.ll

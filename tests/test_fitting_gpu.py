@@ -78,3 +78,27 @@ def test_fit_gradient_matches_finite_differences(form):
             worst = max(worst, err)
             assert err <= GRAD_REL, (i, key, got, fd, err)
     print(f"max relative gradient error ({form}): {worst:.2e}")
+
+
+def test_graphed_log_likelihood_matches_eager():
+    """The CUDA-graph replay of forward + backward gives the eager value and
+    gradients, and follows in-place parameter updates."""
+    from pymdp_b200.fitting import GraphedLogLikelihood
+    fm, A, B, C, lg, obs, acts = _setup(8, 6, 5)
+    params = [x.clone().requires_grad_(True) for x in A + B + C + [lg]]
+    split = lambda ps: (ps[:3], ps[3:5], ps[5:8], ps[8])  # noqa: E731
+    ll = fm.log_likelihood(*split(params), obs, acts)
+    ll.backward()
+    ref = float(ll.detach())
+    gref = [p.grad.clone() for p in params]
+    del ll
+    for p in params:
+        p.grad = None
+    graphed = GraphedLogLikelihood(fm, params, obs, acts)
+    assert abs(float(graphed()) - ref) <= LL_REL * abs(ref)
+    for p, g in zip(params, gref):
+        torch.testing.assert_close(p.grad, g, rtol=1e-5, atol=1e-6)
+    with torch.no_grad():
+        params[-1].add_(0.1)
+        ref2 = float(fm.log_likelihood(*split(params), obs, acts))
+    assert abs(float(graphed()) - ref2) <= LL_REL * abs(ref2)
