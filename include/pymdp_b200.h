@@ -226,6 +226,120 @@ int32_t b2_policy_posterior(void* stream, const float* neg_efe, const float* E, 
 int32_t b2_select_action(void* stream, const float* q_pi, const int32_t* policy_matrix,
                          int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F);
 
+
+/* ------------------------------------------------------ uneven-size rollout
+ * Closed-loop rollout of many agents of DIFFERENT sizes in one persistent
+ * launch. Replaces, for inference_algo="fpi", no learning and deterministic
+ * action selection, the reference's `rollout` (pymdp/envs/rollout.py:468-700)
+ * over a `PymdpEnv` built from each agent's own A / B / D: per step and agent
+ *   prior  = D at the first step, else B[..., a_prev] . qs_prev
+ *            (_resolve_empirical_prior, rollout.py:65-84; agent.py:825-851);
+ *   qs     = infer_states (FPI, algos.py:88-155), in FP64;
+ *   G      = neg-EFE of every policy (control.py:604-690; utility and state
+ *            information gain per `flags`), FP32 accumulation with the A
+ *            operand in FP32 or BF16;
+ *   q_pi   = softmax(gamma G + log E), E uniform (control.py:349);
+ *   action = first step of the first maximum of q_pi (control.py:115-150);
+ *   env    = state' ~ B[:, state, action], obs' ~ A[:, state'] (envs/env.py:
+ *            333-400); the environment's draws use a counter-based generator
+ *            (SplitMix64 over seed, agent, step, stream), not JAX's PRNG.
+ * Transitions are factor-local: B_f is [S_f, S_f, U_f]. Policies are all
+ * prod(U)^T action sequences in the order of control.construct_policies
+ * (control.py:152-195). */
+#define B2_RO_MAX_F 4
+#define B2_RO_MAX_M 8
+#define B2_RO_MAX_S 64
+#define B2_RO_MAX_O 32
+#define B2_RO_MAX_K 4096
+#define B2_RO_MAX_STOT 256
+#define B2_RO_MAX_P 1024
+#define B2_RO_MAX_COLS 64
+#define B2_RO_TAB_FLOATS 4096
+
+/* One agent. Offsets are element offsets into the b2_ro_buffers arrays. */
+typedef struct b2_ro_agent {
+  int32_t F, M, T, P;       /* factors, modalities, policy_len, prod(U)^T     */
+  int32_t n_multi, w0;      /* prod(U); prod(U)^(T-1)                         */
+  int32_t S_tot, sum_K;     /* sum S_f; sum K_m                               */
+  int32_t S[B2_RO_MAX_F], U[B2_RO_MAX_F];
+  int32_t qs_off[B2_RO_MAX_F];  /* start of factor f within the S_tot entries */
+  int32_t ustride[B2_RO_MAX_F]; /* prod(U[f+1:]) (row-major multi-action)     */
+  int32_t O[B2_RO_MAX_M], K[B2_RO_MAX_M], rank[B2_RO_MAX_M];
+  int32_t dep[B2_RO_MAX_M][B2_RO_MAX_F];     /* ascending factor indices      */
+  int32_t dstride[B2_RO_MAX_M][B2_RO_MAX_F]; /* stride of each dep axis in K  */
+  int64_t A_off[B2_RO_MAX_M]; /* [A_m; lin_m]: (O_m + 1) x K_m, row-major     */
+  int64_t C_off[B2_RO_MAX_M]; /* C_m: O_m log-preferences                     */
+  int64_t B_off[B2_RO_MAX_F]; /* B_f: S_f x S_f x U_f                          */
+  int64_t D_off;              /* S_tot                                         */
+  int64_t ll_off;             /* sum_K doubles of scratch                      */
+  int64_t qs_base;            /* S_tot entries of qs / qs64                    */
+  int64_t G_off;              /* P entries of G                                */
+  float gamma;
+  int32_t reserved;
+} b2_ro_agent;
+
+/* A unit of policy evaluation: policies [p_lo, p_hi) of one agent. */
+typedef struct b2_ro_tile {
+  int32_t agent, p_lo, p_hi, reserved;
+} b2_ro_tile;
+
+/* Device buffers of one rollout (counts in elements). */
+typedef struct b2_ro_buffers {
+  const b2_ro_agent* agents; /* device copy of the descriptors                */
+  const b2_ro_tile* tiles;   /* device copy of the tiles                       */
+  float* Aprime;             /* A rows filled by the caller; lin rows by setup */
+  uint16_t* Aprime_bf16;     /* BF16 image of Aprime (precision BF16 only)     */
+  int64_t Aprime_count;
+  const float* B;
+  int64_t B_count;
+  const float* C;
+  int64_t C_count;
+  const float* D;
+  int64_t D_count;
+  double* ll;
+  int64_t ll_count;
+  float* qs;                 /* FP32 posterior per agent                       */
+  double* qs64;              /* FP64 posterior per agent                       */
+  int64_t qs_count;
+  float* G;
+  int64_t G_count;
+  int32_t* env_state;        /* n_agents x B2_RO_MAX_F                         */
+  int32_t* obs;              /* n_agents x B2_RO_MAX_M                         */
+  int16_t* rec_obs;          /* optional: steps x n_agents x B2_RO_MAX_M       */
+  int16_t* rec_state;        /* optional: steps x n_agents x B2_RO_MAX_F       */
+  int16_t* rec_action;       /* optional: steps x n_agents x B2_RO_MAX_F       */
+  float* rec_qs;             /* optional: steps x qs_count                      */
+  float* rec_G;              /* optional: steps x G_count                       */
+  uint32_t* sync;            /* scratch, >= 2 * steps + 32 words               */
+  int64_t sync_count;
+} b2_ro_buffers;
+
+/* Launch shape: threads per CTA (128, 256, 512), K-chunk of the policy
+ * contraction (32, 64), largest tile (policies per tile, <= 64) and
+ * precision (B2_PRECISION_FP32 or B2_PRECISION_BF16). */
+typedef struct b2_ro_config {
+  int32_t threads, kc, cols, precision;
+} b2_ro_config;
+
+/* No counterpart in the reference (its rollout precomputes nothing): fills
+ * lin_m[k] = sum_o A_m[o, k] (C_m[o] [flag bit 0] + log A_m[o, k] [bit 1]),
+ * the row of [A_m; lin_m] that carries utility and -H_A . x, in FP64, and the
+ * BF16 image when `Aprime_bf16` is set. Run once after the A rows change. */
+int32_t b2_rollout_setup(void* stream, const b2_ro_agent* agents_host, int64_t n_agents,
+                         const b2_ro_buffers* buffers, int32_t flags);
+
+/* Runs `steps` rollout steps of every agent, from an environment reset (state ~
+ * D, first observation ~ A), in ONE cooperative persistent launch (plus a
+ * memset of `sync`), so a CUDA graph can hold the whole rollout. `agents_host`
+ * / `tiles_host` are host copies of buffers->agents / ->tiles and are
+ * validated on every call; the tiles must cover every policy of every agent
+ * exactly once. Device-side failures (a grid barrier that waited too long)
+ * are reported in sync[2] (non-zero) with a code in sync[3]. Overlapping
+ * calls on the same buffers race. */
+int32_t b2_rollout(void* stream, const b2_ro_agent* agents_host, int64_t n_agents, const b2_ro_tile* tiles_host,
+                   int64_t n_tiles, const b2_ro_buffers* buffers, int64_t steps, uint64_t seed, int32_t num_iter,
+                   int32_t flags, const b2_ro_config* config);
+
 #ifdef __cplusplus
 }
 #endif

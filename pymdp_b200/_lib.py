@@ -81,7 +81,51 @@ _SIGS = {
                                  _PF, c_int64, _P64, c_int64, _P64, c_int64, _P64, c_int64, c_int32]),
     "b2_policy_posterior": (c_int32, [c_void_p, _PF, _PF, c_int32, _PF, c_int32, _PF, c_int64, c_int64]),
     "b2_select_action": (c_int32, [c_void_p, _PF, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_int64]),
+    "b2_rollout_setup": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int32]),
+    "b2_rollout": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_int32,
+                             c_int32, c_void_p]),
 }
+
+# ------------------------------------------------ uneven-size rollout structs
+RO_MAX_F, RO_MAX_M, RO_MAX_S, RO_MAX_O = 4, 8, 64, 32
+RO_MAX_K, RO_MAX_STOT, RO_MAX_P, RO_MAX_COLS, RO_TAB_FLOATS = 4096, 256, 1024, 64, 4096
+
+
+class RoAgent(ctypes.Structure):
+    """``b2_ro_agent``."""
+
+    _fields_ = [("F", c_int32), ("M", c_int32), ("T", c_int32), ("P", c_int32), ("n_multi", c_int32),
+                ("w0", c_int32), ("S_tot", c_int32), ("sum_K", c_int32), ("S", c_int32 * RO_MAX_F),
+                ("U", c_int32 * RO_MAX_F), ("qs_off", c_int32 * RO_MAX_F), ("ustride", c_int32 * RO_MAX_F),
+                ("O", c_int32 * RO_MAX_M), ("K", c_int32 * RO_MAX_M), ("rank", c_int32 * RO_MAX_M),
+                ("dep", (c_int32 * RO_MAX_F) * RO_MAX_M), ("dstride", (c_int32 * RO_MAX_F) * RO_MAX_M),
+                ("A_off", c_int64 * RO_MAX_M), ("C_off", c_int64 * RO_MAX_M), ("B_off", c_int64 * RO_MAX_F),
+                ("D_off", c_int64), ("ll_off", c_int64), ("qs_base", c_int64), ("G_off", c_int64),
+                ("gamma", c_float), ("reserved", c_int32)]
+
+
+class RoTile(ctypes.Structure):
+    """``b2_ro_tile``."""
+
+    _fields_ = [("agent", c_int32), ("p_lo", c_int32), ("p_hi", c_int32), ("reserved", c_int32)]
+
+
+class RoBuffers(ctypes.Structure):
+    """``b2_ro_buffers`` (device addresses)."""
+
+    _fields_ = [("agents", c_void_p), ("tiles", c_void_p), ("Aprime", c_void_p), ("Aprime_bf16", c_void_p),
+                ("Aprime_count", c_int64), ("B", c_void_p), ("B_count", c_int64), ("C", c_void_p),
+                ("C_count", c_int64), ("D", c_void_p), ("D_count", c_int64), ("ll", c_void_p), ("ll_count", c_int64),
+                ("qs", c_void_p), ("qs64", c_void_p), ("qs_count", c_int64), ("G", c_void_p), ("G_count", c_int64),
+                ("env_state", c_void_p), ("obs", c_void_p), ("rec_obs", c_void_p), ("rec_state", c_void_p),
+                ("rec_action", c_void_p), ("rec_qs", c_void_p), ("rec_G", c_void_p), ("sync", c_void_p),
+                ("sync_count", c_int64)]
+
+
+class RoConfig(ctypes.Structure):
+    """``b2_ro_config``."""
+
+    _fields_ = [("threads", c_int32), ("kc", c_int32), ("cols", c_int32), ("precision", c_int32)]
 
 _lib = None
 _load_error: Exception | None = None

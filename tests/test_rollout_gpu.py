@@ -1,0 +1,129 @@
+"""Uneven-size persistent rollout (``b2_rollout``) against the FP64 oracle
+of ``pymdp/envs/rollout.py:468-700``: environment draws bit-exact, posteriors
+within 1e-5, neg-EFE within 1e-5 (FP32) / 1e-3 (BF16 A operand) relative
+to max(1, |G|), and the same actions; plus CUDA-graph replay, the autotuner
+and the full 2000-agent workload."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import rollout as oro
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 6
+SEED = 11
+
+
+def _small(n=32, seed=1):
+    from pymdp_b200.rollout import make_uneven_agents
+    return make_uneven_agents(n, seed, k_cap=512, p_cap=64, max_states=16, max_obs=12)
+
+
+def _check_agent(sp, i, rec, steps, seed, g_tol, q_tol):
+    ref = oro.rollout_agent(sp, i, steps, seed, actions=rec["action"])
+    np.testing.assert_array_equal(rec["obs"], np.asarray(ref["obs"]), err_msg=f"agent {i} observations")
+    np.testing.assert_array_equal(rec["state"], np.asarray(ref["state"]), err_msg=f"agent {i} states")
+    near_ties = 0
+    for t in range(steps):
+        for f in range(len(sp.S)):
+            err = float(np.max(np.abs(rec["qs"][t][f] - ref["qs"][t][f])))
+            assert err <= 1e-5, (i, t, f, err)
+        G, Gr = rec["G"][t], ref["G"][t]
+        gerr = float(np.max(np.abs(G - Gr))) / max(1.0, float(np.max(np.abs(Gr))))
+        assert gerr <= g_tol, (i, t, gerr)
+        p_gpu = int(np.argmax(G))
+        if list(rec["action"][t]) != ref["action"][t]:
+            q = ref["q_pi"][t]
+            assert q[p_gpu] >= q.max() * (1 - q_tol), (i, t, q[p_gpu], q.max())
+            near_ties += 1
+    return near_ties
+
+
+@pytest.mark.parametrize("precision,g_tol,q_tol", [("fp32", 1e-5, 1e-3), ("bf16", 1e-3, 0.2)])
+def test_rollout_matches_oracle(precision, g_tol, q_tol):
+    from pymdp_b200.rollout import UnevenRollout
+    specs = _small()
+    ro = UnevenRollout(specs, precision=precision, threads=256, kc=32, cols=16)
+    ro.run(STEPS, SEED, record=True)
+    ro.check_status()
+    recs = ro.records()
+    ties = sum(_check_agent(sp, i, recs[i], STEPS, SEED, g_tol, q_tol) for i, sp in enumerate(specs))
+    if precision == "fp32":
+        assert ties == 0
+
+
+@pytest.mark.parametrize("shape", [(128, 64, 64), (512, 32, 7), (256, 64, 1)])
+def test_rollout_launch_shapes_agree(shape):
+    """Every launch shape (threads, K chunk, tile width) gives the oracle's
+    trajectory; tile width 1 evaluates every policy without prefix sharing."""
+    from pymdp_b200.rollout import UnevenRollout
+    specs = _small(16, seed=2)
+    t, kc, cols = shape
+    ro = UnevenRollout(specs, threads=t, kc=kc, cols=cols)
+    ro.run(4, SEED, record=True)
+    ro.check_status()
+    recs = ro.records()
+    assert sum(_check_agent(sp, i, recs[i], 4, SEED, 1e-5, 1e-3) for i, sp in enumerate(specs)) == 0
+
+
+def test_rollout_graph_replay_reproduces_run():
+    from pymdp_b200.rollout import UnevenRollout
+    specs = _small(24, seed=3)
+    ro = UnevenRollout(specs)
+    g = ro.capture(5, SEED, record=True)
+    torch.cuda.synchronize()
+    ro.check_status()
+    direct = ro.records()
+    for r in ro._records.values():
+        if torch.is_tensor(r):
+            r.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    ro.check_status()
+    again = ro.records()
+    for a, b in zip(direct, again):
+        for k in ("obs", "state", "action"):
+            np.testing.assert_array_equal(a[k], b[k])
+        np.testing.assert_allclose(a["G"], b["G"], rtol=1e-5, atol=1e-5)
+    del g
+
+
+def test_autotune_picks_a_candidate_and_caches(tmp_path):
+    from pymdp_b200.rollout import UnevenRollout, autotune
+    specs = _small(16, seed=4)
+    ro = UnevenRollout(specs)
+    cands = [(128, 32, 16), (256, 64, 32)]
+    path = str(tmp_path / "tune.json")
+    best, timings = autotune(ro, steps=1, candidates=cands, cache_path=path)
+    assert tuple(best) in cands and len(timings) == 2
+    assert (ro.config.threads, ro.config.kc, ro.config.cols) == tuple(best)
+    best2, timings2 = autotune(ro, steps=1, candidates=cands, cache_path=path)
+    assert tuple(best2) == tuple(best) and timings2 == timings
+    ro.run(2, SEED, record=True)
+    ro.check_status()
+    recs = ro.records()
+    assert sum(_check_agent(sp, i, recs[i], 2, SEED, 1e-5, 1e-3) for i, sp in enumerate(specs)) == 0
+
+
+def test_rollout_full_workload_spot_checks():
+    """The 2000-agent uneven workload: 3 steps, properties of every agent and
+    the oracle on the agents of the three costliest tiles and two others."""
+    from pymdp_b200.rollout import UnevenRollout, make_uneven_agents
+    specs = make_uneven_agents(2000, seed=0)
+    ro = UnevenRollout(specs, threads=256, kc=64, cols=32)
+    steps = 3
+    ro.run(steps, SEED, record=True)
+    ro.check_status()
+    recs = ro.records()
+    for sp, r in zip(specs, recs):
+        assert (r["obs"] >= 0).all() and (r["obs"] < np.asarray(sp.O)).all()
+        assert (r["action"] >= 0).all() and (r["action"] < np.asarray(sp.U)).all()
+        assert np.isfinite(r["G"]).all()
+        for t in range(steps):
+            for q in r["qs"][t]:
+                assert abs(float(q.sum()) - 1.0) < 1e-5
+    picks = list(dict.fromkeys([int(x) for x in ro.tiles_np[:3, 0]] + [7, 1234]))
+    for i in picks:
+        assert _check_agent(specs[i], i, recs[i], steps, SEED, 1e-5, 1e-3) == 0
