@@ -177,6 +177,50 @@ def run_fit_config(dev, steps: int, warmup: int, flush):
             "log_likelihood": float(graphed.ll)}
 
 
+RO_AGENTS, RO_STEPS = 2000, 100
+FP32_SIMT_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA x 1965 MHz
+
+
+def run_rollout_config(dev, steps: int, warmup: int):
+    """Uneven-size closed-loop rollout: 2000 agents of random sizes, 100
+    steps of infer_states -> infer_policies -> action -> env step in one
+    CUDA-graph-captured persistent launch, launch shape autotuned, for the
+    FP32 and BF16 A operand. One replay is one timed step."""
+    import torch
+
+    from pymdp_b200.rollout import UnevenRollout, autotune, make_uneven_agents, tile_cost
+
+    specs = make_uneven_agents(RO_AGENTS, seed=0)
+    out = {"workload": f"uneven rollout, {RO_AGENTS} agents (F 1-4 of S 2-64, U 1-4, M 1-6 of O 2-32, policy_len "
+                       f"1-4, K_m <= 4096, P <= 256), {RO_STEPS} steps per replay of one CUDA graph holding one "
+                       "persistent launch; working set (A 237 MB) above L2"}
+    for prec in ("fp32", "bf16"):
+        ro = UnevenRollout(specs, precision=prec, device=dev)
+        best, _ = autotune(ro, steps=2)
+        graph = ro.capture(RO_STEPS, seed=1)
+        for _ in range(max(warmup, 1)):
+            graph.replay()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ro.check_status()
+        ms = e0.elapsed_time(e1) / steps
+        macs = sum(tile_cost(specs[a], lo, hi) for a, lo, hi, _ in ro.tiles_np) * RO_STEPS
+        tf = 2 * macs / (ms * 1e-3) / 1e12
+        out[prec] = {"agent_steps_per_s": RO_AGENTS * RO_STEPS / (ms * 1e-3), "ms_per_rollout": ms,
+                     "launch_shape": {"threads": best[0], "kc": best[1], "cols": best[2]},
+                     "efe_tflops": tf, "roofline": {"bound": "fp32 simt", "achieved": tf,
+                                                    "peak": FP32_SIMT_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                                                    "frac": tf / FP32_SIMT_NOMINAL_TFLOPS,
+                                                    "peak_source": "nominal"}}
+        del graph, ro
+    return out
+
+
 def efe_flops_per_agent() -> float:
     K = int(np.prod(S))
     P = int(np.prod(U)) ** T
@@ -355,6 +399,7 @@ def run_b200(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     fpi_res = run_fpi_config(dev, args.steps, args.warmup, flush)
     fit_res = run_fit_config(dev, args.steps, args.warmup, flush)
+    ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup)
     efe_ev = []
 
     def step(timed_efe=False):
@@ -480,6 +525,7 @@ def run_b200(args, rank, world, local_rank):
         "fpi": dict(fpi_res, roofline={"bound": "hbm", "achieved": fpi_res["gbs"], "peak": peak_gbs, "unit": "GB/s",
                                        "frac": fpi_res["gbs"] / peak_gbs}),
         "fit": fit_res,
+        "rollout": ro_res,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -491,9 +537,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit"],
+    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout"],
                     help="step: the agent step (default); fpi: only the 4096-agent FPI model; fit: only the "
-                         "model-fitting gradient (for profiling)")
+                         "model-fitting gradient; rollout: only the uneven-size rollout (for profiling)")
     ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
@@ -505,8 +551,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload in ("fpi", "fit") and world > 1:
-        raise SystemExit("--workload fpi/fit runs on one GPU")
+    if args.workload in ("fpi", "fit", "rollout") and world > 1:
+        raise SystemExit("--workload fpi/fit/rollout runs on one GPU")
     if args.workload == "fpi":
         import torch
 
@@ -522,6 +568,13 @@ def main():
         torch.cuda.set_device(dev)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         print(json.dumps(run_fit_config(dev, args.steps, args.warmup, flush)), flush=True)
+        return
+    if args.workload == "rollout":
+        import torch
+
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        print(json.dumps(run_rollout_config(dev, args.steps, args.warmup)), flush=True)
         return
     if world > 1:
         import datetime

@@ -264,6 +264,15 @@ typedef struct b2_ro_agent {
   int32_t S[B2_RO_MAX_F], U[B2_RO_MAX_F];
   int32_t qs_off[B2_RO_MAX_F];  /* start of factor f within the S_tot entries */
   int32_t ustride[B2_RO_MAX_F]; /* prod(U[f+1:]) (row-major multi-action)     */
+  /* Reduced policy space. A factor that no modality observes leaves neg-EFE
+   * unchanged, so policies that differ only in its actions have equal G; they
+   * are evaluated once, over the observed factors' actions, and expanded when
+   * q_pi is formed (ties then resolve to the first policy, as in the
+   * reference). */
+  int32_t obs_mask;             /* bit f: some modality depends on factor f    */
+  int32_t n_multi_r, P_r, w0_r; /* prod(U_observed); n_multi_r^T; ^(T-1)      */
+  int32_t ustride_r[B2_RO_MAX_F]; /* stride of f in the reduced multi-action,
+                                     0 for unobserved factors                 */
   int32_t O[B2_RO_MAX_M], K[B2_RO_MAX_M], rank[B2_RO_MAX_M];
   int32_t dep[B2_RO_MAX_M][B2_RO_MAX_F];     /* ascending factor indices      */
   int32_t dstride[B2_RO_MAX_M][B2_RO_MAX_F]; /* stride of each dep axis in K  */
@@ -278,7 +287,7 @@ typedef struct b2_ro_agent {
   int32_t reserved;
 } b2_ro_agent;
 
-/* A unit of policy evaluation: policies [p_lo, p_hi) of one agent. */
+/* A unit of policy evaluation: reduced policies [p_lo, p_hi) of one agent. */
 typedef struct b2_ro_tile {
   int32_t agent, p_lo, p_hi, reserved;
 } b2_ro_tile;
@@ -301,7 +310,7 @@ typedef struct b2_ro_buffers {
   float* qs;                 /* FP32 posterior per agent                       */
   double* qs64;              /* FP64 posterior per agent                       */
   int64_t qs_count;
-  float* G;
+  float* G;                  /* P per agent (the first P_r hold reduced G)     */
   int64_t G_count;
   int32_t* env_state;        /* n_agents x B2_RO_MAX_F                         */
   int32_t* obs;              /* n_agents x B2_RO_MAX_M                         */
@@ -332,8 +341,8 @@ int32_t b2_rollout_setup(void* stream, const b2_ro_agent* agents_host, int64_t n
  * D, first observation ~ A), in ONE cooperative persistent launch (plus a
  * memset of `sync`), so a CUDA graph can hold the whole rollout. `agents_host`
  * / `tiles_host` are host copies of buffers->agents / ->tiles and are
- * validated on every call; the tiles must cover every policy of every agent
- * exactly once. Device-side failures (a grid barrier that waited too long)
+ * validated on every call; the tiles must cover every reduced policy
+ * [0, P_r) of every agent exactly once. Device-side failures (a grid barrier that waited too long)
  * are reported in sync[2] (non-zero) with a code in sync[3]. Overlapping
  * calls on the same buffers race. */
 int32_t b2_rollout(void* stream, const b2_ro_agent* agents_host, int64_t n_agents, const b2_ro_tile* tiles_host,

@@ -97,7 +97,8 @@ class RoAgent(ctypes.Structure):
     _fields_ = [("F", c_int32), ("M", c_int32), ("T", c_int32), ("P", c_int32), ("n_multi", c_int32),
                 ("w0", c_int32), ("S_tot", c_int32), ("sum_K", c_int32), ("S", c_int32 * RO_MAX_F),
                 ("U", c_int32 * RO_MAX_F), ("qs_off", c_int32 * RO_MAX_F), ("ustride", c_int32 * RO_MAX_F),
-                ("O", c_int32 * RO_MAX_M), ("K", c_int32 * RO_MAX_M), ("rank", c_int32 * RO_MAX_M),
+                ("obs_mask", c_int32), ("n_multi_r", c_int32), ("P_r", c_int32), ("w0_r", c_int32),
+                ("ustride_r", c_int32 * RO_MAX_F), ("O", c_int32 * RO_MAX_M), ("K", c_int32 * RO_MAX_M), ("rank", c_int32 * RO_MAX_M),
                 ("dep", (c_int32 * RO_MAX_F) * RO_MAX_M), ("dstride", (c_int32 * RO_MAX_F) * RO_MAX_M),
                 ("A_off", c_int64 * RO_MAX_M), ("C_off", c_int64 * RO_MAX_M), ("B_off", c_int64 * RO_MAX_F),
                 ("D_off", c_int64), ("ll_off", c_int64), ("qs_base", c_int64), ("G_off", c_int64),

@@ -177,79 +177,94 @@ __device__ void ro_softmax_factors(const b2_ro_agent& ag, const double* x, doubl
   }
 }
 
-// acc[dep_i][k_i] += ll[k] * prod_{j != i} q[dep_j][k_j] over k (algos.py:26-51).
-// Each thread walks a contiguous chunk of k with mixed-radix digits (last axis
-// fastest) and flushes an axis' running sum when its digit changes.
+// Messages of one modality to its factors (algos.py:26-51),
+//   acc[dep_i][s] += sum_{k: k_i = s} ll[k] * prod_{j != i} q[dep_j][k_j],
+// without atomics: v[k] = ll[k] * prod_j q[dep_j][k_j] goes to shared memory
+// (each thread walks a contiguous chunk of k with mixed-radix digits, last
+// axis fastest); then for each dependency axis i, viewing v as
+// (pre, S_i, post), the R threads of state s sum a strided segment, combine
+// by shuffles in a fixed order and divide by q[dep_i][s]. The division is
+// safe: every log-likelihood and log-prior is >= log MINVAL, so log_q spans
+// less than 745 and no softmax entry underflows to zero.
 template <int NT>
-__device__ void ro_fpi_modality(const b2_ro_agent& ag, int m, const double* ll, const double* q, double* acc) {
+__device__ void ro_fpi_modality(const b2_ro_agent& ag, int m, const double* ll, const double* q, double* acc,
+                                double* v) {
   const int K = ag.K[m], r = ag.rank[m];
-  const int chunk = (K + NT - 1) / NT;
-  const int k0 = threadIdx.x * chunk;
-  const int k1 = min(K, k0 + chunk);
-  if (k0 >= k1) return;
-  int dig[kF], Sd[kF], base[kF];
-  double run[kF];
+  {
+    const int chunk = (K + NT - 1) / NT;
+    const int k0 = threadIdx.x * chunk;
+    const int k1 = min(K, k0 + chunk);
+    if (k0 < k1) {
+      int dig[kF], Sd[kF], base[kF];
 #pragma unroll
-  for (int i = 0; i < kF; ++i) {
-    if (i < r) {
-      const int f = ag.dep[m][i];
-      Sd[i] = ag.S[f];
-      base[i] = ag.qs_off[f];
-      dig[i] = (k0 / ag.dstride[m][i]) % Sd[i];
-    } else {
-      Sd[i] = 1;
-      base[i] = 0;
-      dig[i] = 0;
-    }
-    run[i] = 0.0;
-  }
-  for (int k = k0;;) {
-    const double l = ll[k];
-    double qv[kF], w[kF];
-#pragma unroll
-    for (int i = 0; i < kF; ++i) qv[i] = (i < r) ? q[base[i] + dig[i]] : 1.0;
-    double pre = 1.0;
-#pragma unroll
-    for (int i = 0; i < kF; ++i) {
-      w[i] = pre;
-      pre *= qv[i];
-    }
-    double suf = 1.0;
-#pragma unroll
-    for (int i = kF - 1; i >= 0; --i) {
-      w[i] *= suf;
-      suf *= qv[i];
-    }
-#pragma unroll
-    for (int i = 0; i < kF; ++i)
-      if (i < r) run[i] = fma(l, w[i], run[i]);
-    if (++k >= k1) break;
-    bool carry = true;
-#pragma unroll
-    for (int i = kF - 1; i >= 0; --i) {
-      if (carry && i < r) {
-        atomicAdd(&acc[base[i] + dig[i]], run[i]);
-        run[i] = 0.0;
-        if (++dig[i] < Sd[i])
-          carry = false;
-        else
+      for (int i = 0; i < kF; ++i) {
+        if (i < r) {
+          const int f = ag.dep[m][i];
+          Sd[i] = ag.S[f];
+          base[i] = ag.qs_off[f];
+          dig[i] = (k0 / ag.dstride[m][i]) % Sd[i];
+        } else {
+          Sd[i] = 1;
+          base[i] = 0;
           dig[i] = 0;
+        }
+      }
+      for (int k = k0;;) {
+        double w = ll[k];
+#pragma unroll
+        for (int i = 0; i < kF; ++i)
+          if (i < r) w *= q[base[i] + dig[i]];
+        v[k] = w;
+        if (++k >= k1) break;
+        bool carry = true;
+#pragma unroll
+        for (int i = kF - 1; i >= 0; --i) {
+          if (carry && i < r) {
+            if (++dig[i] < Sd[i])
+              carry = false;
+            else
+              dig[i] = 0;
+          }
+        }
       }
     }
   }
-#pragma unroll
-  for (int i = 0; i < kF; ++i)
-    if (i < r) atomicAdd(&acc[base[i] + dig[i]], run[i]);
+  __syncthreads();
+  for (int i = 0; i < r; ++i) {
+    const int f = ag.dep[m][i], S = ag.S[f], post = ag.dstride[m][i], pre = K / (S * post);
+    int R = 1;
+    while (R < 32 && S * R * 2 <= NT) R <<= 1;
+    const int s = threadIdx.x / R, rr = threadIdx.x & (R - 1);
+    double sum = 0.0;
+    if (s < S) {
+      if (post >= R) {
+        for (int pp = 0; pp < pre; ++pp) {
+          const double* row = v + ((int64_t)pp * S + s) * post;
+          for (int j = rr; j < post; j += R) sum += row[j];
+        }
+      } else {
+        for (int pp = rr; pp < pre; pp += R) {
+          const double* row = v + ((int64_t)pp * S + s) * post;
+          for (int j = 0; j < post; ++j) sum += row[j];
+        }
+      }
+    }
+    for (int o = R >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (s < S && rr == 0) acc[ag.qs_off[f] + s] += sum / q[ag.qs_off[f] + s];
+  }
+  __syncthreads();
 }
 
 // infer_states (algos.py:88-155): Jacobi sweeps from log_q = 0 with the log
 // prior in sm[0:256]; writes qs (FP32 and FP64) and the optional record.
+// Shared layout: lp | lq | q | acc (256 doubles each) | v (4096 doubles).
 template <int NT>
 __device__ void ro_fpi(const RoArgs& a, const b2_ro_agent& ag, const int* s_obs, double* sm, int rec_t) {
   double* lp = sm;
   double* lq = sm + B2_RO_MAX_STOT;
   double* q = sm + 2 * B2_RO_MAX_STOT;
   double* acc = sm + 3 * B2_RO_MAX_STOT;
+  double* v = sm + 4 * B2_RO_MAX_STOT;
   double* ll = a.buf.ll + ag.ll_off;
   const int tid = threadIdx.x;
   int koff = 0;
@@ -267,10 +282,9 @@ __device__ void ro_fpi(const RoArgs& a, const b2_ro_agent& ag, const int* s_obs,
     __syncthreads();
     koff = 0;
     for (int m = 0; m < ag.M; ++m) {
-      ro_fpi_modality<NT>(ag, m, ll + koff, q, acc);
+      ro_fpi_modality<NT>(ag, m, ll + koff, q, acc, v);
       koff += ag.K[m];
     }
-    __syncthreads();
     for (int j = tid; j < ag.S_tot; j += NT) lq[j] = acc[j] + lp[j];
     __syncthreads();
   }
@@ -313,6 +327,21 @@ __device__ void ro_reset_agent(const RoArgs& a, const b2_ro_agent& ag, int agent
   ro_fpi<NT>(a, ag, s_obs, sm, 0);
 }
 
+// Index of policy p in the reduced policy space (the observed factors'
+// actions only; see b2_ro_agent).
+__device__ __forceinline__ int ro_reduced_policy(const b2_ro_agent& ag, int p) {
+  if (ag.P_r == ag.P) return p;
+  int pr = 0, W = ag.w0;
+  for (int t = 0; t < ag.T; ++t) {
+    const int mt = (p / W) % ag.n_multi;
+    int mr = 0;
+    for (int f = 0; f < ag.F; ++f) mr += ((mt / ag.ustride[f]) % ag.U[f]) * ag.ustride_r[f];
+    pr = pr * ag.n_multi_r + mr;
+    W /= ag.n_multi;
+  }
+  return pr;
+}
+
 // q_pi, action, records, env step, empirical prior and the next FPI.
 template <int NT>
 __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent, int t, double* sm, int* s_state,
@@ -327,7 +356,7 @@ __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent,
   if (tid < ag.M) s_obs[tid] = a.buf.obs[agent * kM + tid];
   // q_pi = softmax(gamma G + log E), E uniform (control.py:349)
   float mx = -INFINITY;
-  for (int p = tid; p < ag.P; p += NT) mx = fmaxf(mx, gm * G[p]);
+  for (int p = tid; p < ag.P; p += NT) mx = fmaxf(mx, gm * G[ro_reduced_policy(ag, p)]);
   mx = warp_max(mx);
   if (lane == 0) s_rv[wid] = mx;
   __syncthreads();
@@ -340,7 +369,7 @@ __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent,
   mx = s_rv[0];
   __syncthreads();
   float sum = 0.f;
-  for (int p = tid; p < ag.P; p += NT) sum += expf(gm * G[p] - mx);
+  for (int p = tid; p < ag.P; p += NT) sum += expf(gm * G[ro_reduced_policy(ag, p)] - mx);
   sum = warp_sum(sum);
   if (lane == 0) s_rv[wid] = sum;
   __syncthreads();
@@ -356,7 +385,7 @@ __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent,
   float best = -INFINITY;
   int bi = 0x7fffffff;
   for (int p = tid; p < ag.P; p += NT) {
-    const float v = expf(gm * G[p] - mx) / sum;
+    const float v = expf(gm * G[ro_reduced_policy(ag, p)] - mx) / sum;
     if (v > best || (v == best && p < bi)) {
       best = v;
       bi = p;
@@ -394,7 +423,8 @@ __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent,
   if (tid < kF && a.buf.rec_state) a.buf.rec_state[rec * kF + tid] = (int16_t)(tid < ag.F ? s_state[tid] : -1);
   if (tid < kF && a.buf.rec_action) a.buf.rec_action[rec * kF + tid] = (int16_t)(tid < ag.F ? s_act[tid] : -1);
   if (a.buf.rec_G)
-    for (int p = tid; p < ag.P; p += NT) a.buf.rec_G[(int64_t)t * a.buf.G_count + ag.G_off + p] = G[p];
+    for (int p = tid; p < ag.P; p += NT)
+      a.buf.rec_G[(int64_t)t * a.buf.G_count + ag.G_off + p] = G[ro_reduced_policy(ag, p)];
   // env.step: state' ~ B[:, state, action], obs' ~ A[:, state'] (envs/env.py:352-378)
   const int hstep = t + 1;
   int* s_next = s_act + kF;
@@ -438,127 +468,151 @@ __device__ TileSmem ro_tile_smem(unsigned char* smem, int tab_floats) {
   s.sOut = s.sX + KC * kCols;
   s.g0 = s.sOut + kRpad * kCols;
   s.g1 = s.g0 + kCols;
-  s.sDig = reinterpret_cast<unsigned char*>(s.g1 + kCols);
-  s.sFac = s.sDig + KC * kF;
+  s.sDig = reinterpret_cast<unsigned char*>(s.g1 + kCols);  // 2 x KC x kF
+  s.sFac = s.sDig + 2 * KC * kF;
   return s;
 }
 
-// out[:R, :n] = [A_m; lin_m] (R x K) * X (K x n) into sOut (row stride kCols).
-// Thread = (4-row group, CB-column group, k slice). The KG k slices are
-// interleaved (k = kg mod KG) and KG depends on K alone, each slice sums in
-// increasing k, and slices are added in slice order: every column's arithmetic
-// is the same whatever the tile width or the column's position, so policies
-// with equal neg-EFE get bit-equal values and the first maximum wins, as in
-// the reference. Units (row group x column group, column-major) that do not
-// fit NT / KG threads run in passes.
-__device__ __forceinline__ int ro_kslices(int K) {
-  return K >= 1024 ? 16 : K >= 256 ? 8 : K >= 64 ? 4 : K >= 16 ? 2 : 1;
+// Digits of k0 .. k0 + KC - 1 along modality m's dependency axes.
+template <int NT, int KC>
+__device__ __forceinline__ void ro_digits(const b2_ro_agent& ag, int m, int k0, unsigned char* dst) {
+  const int K = ag.K[m], r = ag.rank[m];
+  for (int kk = threadIdx.x; kk < KC; kk += NT) {
+    const int k = k0 + kk;
+    if (k < K)
+      for (int i = 0; i < r; ++i) dst[kk * kF + i] = (unsigned char)((k / ag.dstride[m][i]) % ag.S[ag.dep[m][i]]);
+  }
 }
 
+template <int NT, int KC, bool BF16>
+__device__ __forceinline__ void ro_load_a(const float* Am, const __nv_bfloat16* Ab, int R, int K, int k0,
+                                          float* pa) {
+  constexpr int AE = (kRpad * KC + NT - 1) / NT;
+#pragma unroll
+  for (int j = 0; j < AE; ++j) {
+    const int idx = threadIdx.x + j * NT, row = idx / KC, kk = idx % KC;
+    float v = 0.f;
+    if (idx < kRpad * KC && row < R && k0 + kk < K) {
+      const int64_t g = (int64_t)row * K + k0 + kk;
+      v = (BF16 && row + 1 < R) ? __bfloat162float(Ab[g]) : __ldg(Am + g);
+    }
+    pa[j] = v;
+  }
+}
+
+// out[:R, :n] = [A_m; lin_m] (R x K) * X (K x n) into sOut (row stride kCols),
+// X[k, c] = prod_i tab[c][dep_i][k_i] (table row stride ts, odd). A thread
+// owns 4 rows x CB columns of one k slice; the KG slices of a unit are
+// adjacent lanes and combine by shuffles. The next A chunk is loaded into
+// registers while the current one is multiplied.
 template <int NT, int KC, bool BF16, int CB>
-__device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const float* tab, int n,
+__device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const float* tab, int ts, int n,
                             const TileSmem& s) {
-  const int K = ag.K[m], R = ag.O[m] + 1, r = ag.rank[m], St = ag.S_tot;
-  const int RG = (R + 3) >> 2, CG = (n + CB - 1) / CB, units = RG * CG;
-  const int KG = ro_kslices(K), upp = NT / KG;
-  const int tid = threadIdx.x, ul = tid / KG, kg = tid - (tid / KG) * KG;
+  constexpr int NW = NT / 32;
+  constexpr int AE = (kRpad * KC + NT - 1) / NT;
+  const int K = ag.K[m], R = ag.O[m] + 1, r = ag.rank[m];
+  const int RG = (R + 3) >> 2, CG = (n + CB - 1) / CB, units = RG * CG;  // units <= 9 x 8 <= NT
+  int KG = 1;
+  while (KG < 16 && units * KG * 2 <= NT) KG <<= 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int unit = tid / KG, kg = tid & (KG - 1);
+  const bool active = unit < units;
+  const int cg = active ? unit / RG : 0, rg = active ? unit - (unit / RG) * RG : 0;
+  const int colpad = CG * CB;
   const float* Am = a.buf.Aprime + ag.A_off[m];
   const __nv_bfloat16* Ab = BF16 ? reinterpret_cast<const __nv_bfloat16*>(a.buf.Aprime_bf16) + ag.A_off[m] : nullptr;
   int qoff[kF];
 #pragma unroll
   for (int i = 0; i < kF; ++i) qoff[i] = i < r ? ag.qs_off[ag.dep[m][i]] : 0;
-  for (int u0 = 0; u0 < units; u0 += upp) {
-    const int u1 = min(units, u0 + upp);
-    const int cg0 = u0 / RG, c0 = cg0 * CB, colpad = ((u1 - 1) / RG + 1 - cg0) * CB;
-    const int unit = u0 + ul;
-    const bool active = unit < u1;
-    const int cg = unit / RG, rg = unit - (unit / RG) * RG;
-    float acc[4][CB];
+  float acc[4][CB];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < CB; ++j) acc[i][j] = 0.f;
-    for (int k0 = 0; k0 < K; k0 += KC) {
-      const int kn = min(KC, K - k0);
-      for (int e = tid; e < kn * r; e += NT) {
-        const int kk = e / r, i = e - kk * r;
-        s.sDig[kk * kF + i] = (unsigned char)(((k0 + kk) / ag.dstride[m][i]) % ag.S[ag.dep[m][i]]);
-      }
-      for (int e = tid; e < kRpad * KC; e += NT) {
-        const int row = e / KC, kk = e - row * KC;
-        float v = 0.f;
-        if (row < R && kk < kn) {
-          const int64_t idx = (int64_t)row * K + k0 + kk;
-          v = (BF16 && row + 1 < R) ? __bfloat162float(Ab[idx]) : __ldg(Am + idx);
-        }
-        s.sA[kk * kRpad + row] = v;
-      }
-      __syncthreads();
-      for (int e = tid; e < KC * colpad; e += NT) {
-        const int kk = e / colpad, cl = e - kk * colpad, c = c0 + cl;
+    for (int j = 0; j < CB; ++j) acc[i][j] = 0.f;
+  float pa[AE];
+  ro_load_a<NT, KC, BF16>(Am, Ab, R, K, 0, pa);
+  ro_digits<NT, KC>(ag, m, 0, s.sDig);
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = 0; k0 < K; k0 += KC) {
+    const int kn = min(KC, K - k0);
+#pragma unroll
+    for (int j = 0; j < AE; ++j) {
+      const int idx = tid + j * NT;
+      if (idx < kRpad * KC) s.sA[(idx % KC) * kRpad + idx / KC] = pa[j];
+    }
+    const unsigned char* dg = s.sDig + buf * KC * kF;
+    for (int kk = warp; kk < KC; kk += NW) {
+      const unsigned char* d = dg + kk * kF;
+      for (int c = lane; c < colpad; c += 32) {
         float x = 0.f;
         if (kk < kn && c < n) {
-          const float* col = tab + c * St;
-          const unsigned char* d = s.sDig + kk * kF;
+          const float* col = tab + c * ts;
           x = col[qoff[0] + d[0]];
 #pragma unroll
           for (int i = 1; i < kF; ++i)
             if (i < r) x *= col[qoff[i] + d[i]];
         }
-        s.sX[kk * kCols + cl] = x;
+        s.sX[kk * kCols + c] = x;
       }
-      __syncthreads();
-      if (active) {
-        const float* xb = s.sX + CB * (cg - cg0);
-        for (int kk = kg; kk < kn; kk += KG) {
-          const float4 av = *reinterpret_cast<const float4*>(s.sA + kk * kRpad + 4 * rg);
-          const float* xr = xb + kk * kCols;
-          float xv[CB];
-#pragma unroll
-          for (int j = 0; j < CB; j += 4) {
-            const float4 x4 = *reinterpret_cast<const float4*>(xr + j);
-            xv[j] = x4.x;
-            xv[j + 1] = x4.y;
-            xv[j + 2] = x4.z;
-            xv[j + 3] = x4.w;
-          }
-#pragma unroll
-          for (int j = 0; j < CB; ++j) {
-            acc[0][j] = fmaf(av.x, xv[j], acc[0][j]);
-            acc[1][j] = fmaf(av.y, xv[j], acc[1][j]);
-            acc[2][j] = fmaf(av.z, xv[j], acc[2][j]);
-            acc[3][j] = fmaf(av.w, xv[j], acc[3][j]);
-          }
-        }
-      }
-      __syncthreads();
     }
-    // slices added in slice order
-    for (int j0 = 0; j0 < KG; ++j0) {
-      if (active && kg == j0) {
+    __syncthreads();
+    if (k0 + KC < K) {
+      ro_load_a<NT, KC, BF16>(Am, Ab, R, K, k0 + KC, pa);
+      ro_digits<NT, KC>(ag, m, k0 + KC, s.sDig + (buf ^ 1) * KC * kF);
+    }
+    if (active) {
+      const float* xb = s.sX + CB * cg;
+      for (int kk = kg; kk < kn; kk += KG) {
+        const float4 av = *reinterpret_cast<const float4*>(s.sA + kk * kRpad + 4 * rg);
+        const float* xr = xb + kk * kCols;
+        float xv[CB];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int row = 4 * rg + i;
+        for (int j = 0; j < CB; j += 4) {
+          const float4 x4 = *reinterpret_cast<const float4*>(xr + j);
+          xv[j] = x4.x;
+          xv[j + 1] = x4.y;
+          xv[j + 2] = x4.z;
+          xv[j + 3] = x4.w;
+        }
 #pragma unroll
-          for (int j = 0; j < CB; ++j) {
-            const int c = CB * cg + j;
-            if (row < R && c < n) {
-              float* o = &s.sOut[row * kCols + c];
-              *o = j0 == 0 ? acc[i][j] : *o + acc[i][j];
-            }
-          }
+        for (int j = 0; j < CB; ++j) {
+          acc[0][j] = fmaf(av.x, xv[j], acc[0][j]);
+          acc[1][j] = fmaf(av.y, xv[j], acc[1][j]);
+          acc[2][j] = fmaf(av.z, xv[j], acc[2][j]);
+          acc[3][j] = fmaf(av.w, xv[j], acc[3][j]);
         }
       }
-      __syncthreads();
+    }
+    buf ^= 1;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < CB; ++j)
+      for (int o = KG >> 1; o > 0; o >>= 1) acc[i][j] += __shfl_xor_sync(0xffffffffu, acc[i][j], o);
+  if (active && kg == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = 4 * rg + i;
+#pragma unroll
+      for (int j = 0; j < CB; ++j) {
+        const int c = CB * cg + j;
+        if (row < R && c < n) s.sOut[row * kCols + c] = acc[i][j];
+      }
     }
   }
+  __syncthreads();
 }
 
-// neg-EFE of policies [p_lo, p_hi) of one agent (control.py:604-690).
+// neg-EFE of reduced policies [p_lo, p_hi) of one agent (control.py:604-690).
 template <int NT, int KC, bool BF16>
 __device__ void ro_tile(const RoArgs& a, const b2_ro_agent& ag, const b2_ro_tile& tile, unsigned char* smem) {
+  constexpr int NW = NT / 32;
   const TileSmem s = ro_tile_smem<NT, KC>(smem, a.tab_floats);
-  const int tid = threadIdx.x, St = ag.S_tot, nu = ag.n_multi;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int St = ag.S_tot, ts = St | 1, nu = ag.n_multi_r;
   const bool ig = (a.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
   for (int j = tid; j < St; j += NT) {
     s.sFac[j] = (unsigned char)ro_factor_of(ag, j);
@@ -566,27 +620,32 @@ __device__ void ro_tile(const RoArgs& a, const b2_ro_agent& ag, const b2_ro_tile
   }
   __syncthreads();
   float *prev = s.tab1, *cur = s.tab0, *gp = s.g1, *gc = s.g0;
-  int W = ag.w0, prev_lo = 0;
+  int W = ag.w0_r, prev_lo = 0;
   for (int t = 0; t < ag.T; ++t) {
     const int c_lo = tile.p_lo / W, n = (tile.p_hi - 1) / W + 1 - c_lo;
-    for (int e = tid; e < n * St; e += NT) {
-      const int c = e / St, j = e - c * St;
-      const int f = s.sFac[j], S = ag.S[f], U = ag.U[f], sj = j - ag.qs_off[f];
+    for (int c = warp; c < n; c += NW) {
       const int pc = t == 0 ? 0 : (c_lo + c) / nu - prev_lo;
-      const int u = (((c_lo + c) % nu) / ag.ustride[f]) % U;
-      const float* Bf = a.buf.B + ag.B_off[f] + (int64_t)sj * S * U + u;
-      const float* pq = prev + pc * St + ag.qs_off[f];
-      float acc = 0.f;
-      for (int s2 = 0; s2 < S; ++s2) acc = fmaf(__ldg(Bf + (int64_t)s2 * U), pq[s2], acc);
-      cur[c * St + j] = acc;
+      const int mu = (c_lo + c) % nu;
+      const float* pq = prev + pc * ts;
+      for (int j = lane; j < St; j += 32) {
+        const int f = s.sFac[j];
+        if (!((ag.obs_mask >> f) & 1)) continue;  // unobserved: never read
+        const int S = ag.S[f], U = ag.U[f], sj = j - ag.qs_off[f];
+        const int u = (mu / ag.ustride_r[f]) % U;
+        const float* Bf = a.buf.B + ag.B_off[f] + (int64_t)sj * S * U + u;
+        const float* pf = pq + ag.qs_off[f];
+        float acc = 0.f;
+        for (int s2 = 0; s2 < S; ++s2) acc = fmaf(__ldg(Bf + (int64_t)s2 * U), pf[s2], acc);
+        cur[c * ts + j] = acc;
+      }
     }
     for (int c = tid; c < n; c += NT) gc[c] = t == 0 ? 0.f : gp[(c_lo + c) / nu - prev_lo];
     __syncthreads();
     for (int m = 0; m < ag.M; ++m) {
       if (n <= 4)
-        ro_contract<NT, KC, BF16, 4>(a, ag, m, cur, n, s);
+        ro_contract<NT, KC, BF16, 4>(a, ag, m, cur, ts, n, s);
       else
-        ro_contract<NT, KC, BF16, 8>(a, ag, m, cur, n, s);
+        ro_contract<NT, KC, BF16, 8>(a, ag, m, cur, ts, n, s);
       const int O = ag.O[m];
       for (int c = tid; c < n; c += NT) {
         float h = 0.f;
@@ -711,6 +770,26 @@ int32_t validate_agents(const b2_ro_agent* ags, int64_t n, const b2_ro_buffers& 
       if (P > B2_RO_MAX_P) return ro_unsup(at + "prod(U)^T above 1024");
     }
     if (P != g.P || w0 != g.w0) return ro_bad(at + "P / w0 inconsistent with U and T");
+    int mask = 0;
+    for (int m = 0; m < g.M && m < kM; ++m)
+      for (int j = 0; j < g.rank[m] && j < kF; ++j)
+        if (g.dep[m][j] >= 0 && g.dep[m][j] < g.F) mask |= 1 << g.dep[m][j];
+    if (mask != g.obs_mask) return ro_bad(at + "obs_mask != union of the dependencies");
+    int64_t nr = 1;
+    for (int f = g.F - 1; f >= 0; --f) {
+      if ((mask >> f) & 1) {
+        if (g.ustride_r[f] != nr) return ro_bad(at + "ustride_r inconsistent with U and obs_mask");
+        nr *= g.U[f];
+      } else if (g.ustride_r[f] != 0) {
+        return ro_bad(at + "ustride_r of an unobserved factor must be 0");
+      }
+    }
+    int64_t Pr = 1, w0r = 1;
+    for (int t = 0; t < g.T; ++t) {
+      if (t + 1 < g.T) w0r *= nr;
+      Pr *= nr;
+    }
+    if (nr != g.n_multi_r || Pr != g.P_r || w0r != g.w0_r) return ro_bad(at + "n_multi_r / P_r / w0_r inconsistent");
     int64_t sumK = 0;
     for (int m = 0; m < g.M; ++m) {
       if (g.O[m] < 1 || g.O[m] > B2_RO_MAX_O) return ro_unsup(at + "O_m must be in [1, 32]");
@@ -805,25 +884,27 @@ extern "C" int32_t b2_rollout(void* stream_, const b2_ro_agent* agents_host, int
   if (b.sync_count < 2 * steps + 32) return ro_bad("sync needs at least 2 * steps + 32 words");
   B2_TRY(validate_agents(agents_host, n_agents, b, true));
   // tiles: bounds, shape, and an exact cover of every agent's policies
-  int64_t tab = B2_RO_MAX_STOT;
+  int64_t tab = B2_RO_MAX_STOT + 1;
   std::vector<int64_t> covered(n_agents, 0);
   for (int64_t i = 0; i < n_tiles; ++i) {
     const b2_ro_tile& t = tiles_host[i];
     if (t.agent < 0 || t.agent >= n_agents) return ro_bad("tile agent out of range");
     const b2_ro_agent& g = agents_host[t.agent];
-    if (t.p_lo < 0 || t.p_hi <= t.p_lo || t.p_hi > g.P) return ro_bad("tile policy range out of range");
-    const int64_t n = t.p_hi - t.p_lo;
+    if (t.p_lo < 0 || t.p_hi <= t.p_lo || t.p_hi > g.P_r) return ro_bad("tile policy range out of range");
+    const int64_t n = t.p_hi - t.p_lo, ts = g.S_tot | 1;
     if (n > c.cols) return ro_bad("tile wider than cols");
-    if (n * g.S_tot > B2_RO_TAB_FLOATS) return ro_unsup("tile width x S_tot above the 4096-float table");
-    tab = std::max(tab, n * g.S_tot);
+    if (n * ts > B2_RO_TAB_FLOATS) return ro_unsup("tile width x (S_tot | 1) above the 4096-float table");
+    tab = std::max(tab, n * ts);
     covered[t.agent] += n;
   }
   for (int64_t i = 0; i < n_agents; ++i)
-    if (covered[i] != agents_host[i].P) return ro_bad("tiles do not cover agent " + std::to_string(i) + " once");
+    if (covered[i] != agents_host[i].P_r)
+      return ro_bad("tiles do not cover agent " + std::to_string(i) + " once");
   tab = (tab + 3) & ~int64_t(3);
   const size_t tile_bytes = (size_t)(2 * tab + c.kc * kRpad + c.kc * kCols + kRpad * kCols + 2 * kCols) * 4 +
-                            (size_t)c.kc * kF + B2_RO_MAX_STOT;
-  const size_t smem = std::max(tile_bytes, (size_t)4 * B2_RO_MAX_STOT * sizeof(double));
+                            (size_t)2 * c.kc * kF + B2_RO_MAX_STOT;
+  const size_t fpi_bytes = (size_t)(4 * B2_RO_MAX_STOT + B2_RO_MAX_K) * sizeof(double);
+  const size_t smem = std::max(tile_bytes, fpi_bytes);
   int dev = 0, n_sm = 0, coop = 0;
   B2_CUDA_TRY(kRoName, cudaGetDevice(&dev));
   B2_CUDA_TRY(kRoName, cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));

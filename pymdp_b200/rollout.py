@@ -80,6 +80,17 @@ class AgentSpec:
     def num_policies(self) -> int:
         return int(np.prod(self.U)) ** int(self.policy_len)
 
+    @property
+    def observed(self) -> list:
+        """Factors some modality depends on."""
+        return sorted({d for deps in self.A_dependencies for d in deps})
+
+    @property
+    def num_reduced_policies(self) -> int:
+        """Policies over the observed factors' actions only (unobserved
+        factors leave neg-EFE unchanged)."""
+        return int(np.prod([self.U[f] for f in self.observed])) ** int(self.policy_len)
+
 
 def make_uneven_agents(n_agents: int = 2000, seed: int = 0, k_cap: int = 4096, p_cap: int = 256,
                        gamma: float = 16.0, max_factors: int = 4, max_states: int = 64, max_modalities: int = 6,
@@ -137,6 +148,13 @@ def _descriptor(spec: AgentSpec, offs: dict) -> RoAgent:
     for f in range(F):
         g.S[f], g.U[f], g.qs_off[f] = spec.S[f], spec.U[f], int(qoff[f])
         g.ustride[f] = int(np.prod(spec.U[f + 1:]))
+    obs = set(spec.observed)
+    nr = 1
+    for f in range(F - 1, -1, -1):
+        g.ustride_r[f] = nr if f in obs else 0
+        nr *= spec.U[f] if f in obs else 1
+    g.obs_mask = sum(1 << f for f in obs)
+    g.n_multi_r, g.P_r, g.w0_r = nr, nr ** g.T, nr ** (g.T - 1)
     sumK = 0
     for m, deps in enumerate(spec.A_dependencies):
         K = int(np.prod([spec.S[d] for d in deps]))
@@ -157,10 +175,12 @@ def _descriptor(spec: AgentSpec, offs: dict) -> RoAgent:
 
 
 def tile_cost(spec: AgentSpec, p_lo: int, p_hi: int) -> float:
-    """Multiply-adds of one tile: per depth, its distinct prefixes times the
-    contraction rows x K plus the B roll-out."""
-    nu = int(np.prod(spec.U))
-    per_col = sum((o + 1) * int(a[0].size) for o, a in zip(spec.O, spec.A)) + sum(s * s for s in spec.S)
+    """Multiply-adds of one tile of reduced policies: per depth, its distinct
+    prefixes times the contraction rows x K plus the B roll-out of the
+    observed factors."""
+    nu = int(np.prod([spec.U[f] for f in spec.observed]))
+    per_col = (sum((o + 1) * int(a[0].size) for o, a in zip(spec.O, spec.A))
+               + sum(spec.S[f] ** 2 for f in spec.observed))
     cost, W = 0.0, nu ** (spec.policy_len - 1)
     for _t in range(spec.policy_len):
         cost += ((p_hi - 1) // W + 1 - p_lo // W) * per_col
@@ -169,13 +189,14 @@ def tile_cost(spec: AgentSpec, p_lo: int, p_hi: int) -> float:
 
 
 def make_tiles(specs: Sequence[AgentSpec], cols: int) -> np.ndarray:
-    """Cut each agent's policies into tiles of at most ``cols`` policies (and
-    at most 4096 / S_tot, the shared-memory table), largest cost first.
-    Returns ``(n_tiles, 4)`` int32 rows ``(agent, p_lo, p_hi, 0)``."""
+    """Cut each agent's reduced policies into tiles of at most ``cols``
+    policies (and at most 4096 / (S_tot | 1), the shared-memory table),
+    largest cost first. Returns ``(n_tiles, 4)`` int32 rows
+    ``(agent, p_lo, p_hi, 0)``."""
     rows, costs = [], []
     for i, sp in enumerate(specs):
-        P, St = sp.num_policies, int(sum(sp.S))
-        width = max(1, min(int(cols), P, _lib.RO_TAB_FLOATS // St))
+        P, ts = sp.num_reduced_policies, int(sum(sp.S)) | 1
+        width = max(1, min(int(cols), P, _lib.RO_TAB_FLOATS // ts))
         for lo in range(0, P, width):
             hi = min(P, lo + width)
             rows.append((i, lo, hi, 0))

@@ -25,7 +25,7 @@ int main(void) {
   printf("b2_ro_tile %zu\\n", sizeof(b2_ro_tile));
   printf("b2_ro_buffers %zu\\n", sizeof(b2_ro_buffers));
   printf("b2_ro_config %zu\\n", sizeof(b2_ro_config));
-  F(b2_ro_agent, S) F(b2_ro_agent, dep) F(b2_ro_agent, dstride) F(b2_ro_agent, A_off) F(b2_ro_agent, C_off)
+  F(b2_ro_agent, S) F(b2_ro_agent, obs_mask) F(b2_ro_agent, ustride_r) F(b2_ro_agent, O) F(b2_ro_agent, dep) F(b2_ro_agent, dstride) F(b2_ro_agent, A_off) F(b2_ro_agent, C_off)
   F(b2_ro_agent, B_off) F(b2_ro_agent, D_off) F(b2_ro_agent, G_off) F(b2_ro_agent, gamma)
   F(b2_ro_buffers, Aprime_count) F(b2_ro_buffers, qs64) F(b2_ro_buffers, rec_G) F(b2_ro_buffers, sync_count)
   return 0;
@@ -86,10 +86,10 @@ def test_tiles_cover_every_policy_once(cols):
     from pymdp_b200.rollout import make_tiles, make_uneven_agents, tile_cost
     specs = make_uneven_agents(60, seed=4)
     tiles = make_tiles(specs, cols)
-    cover = [np.zeros(sp.num_policies, np.int64) for sp in specs]
+    cover = [np.zeros(sp.num_reduced_policies, np.int64) for sp in specs]
     for a, lo, hi, _ in tiles:
-        assert 0 <= lo < hi <= specs[a].num_policies
-        assert hi - lo <= cols and (hi - lo) * sum(specs[a].S) <= _lib.RO_TAB_FLOATS
+        assert 0 <= lo < hi <= specs[a].num_reduced_policies
+        assert hi - lo <= cols and (hi - lo) * (sum(specs[a].S) | 1) <= _lib.RO_TAB_FLOATS
         cover[a][lo:hi] += 1
     assert all((c == 1).all() for c in cover)
     costs = [tile_cost(specs[a], lo, hi) for a, lo, hi, _ in tiles]
@@ -159,3 +159,29 @@ def test_rollout_validation_rejects_bad_input():
     tiles[0].p_hi = tiles[0].p_lo
     rc, msg = _call(descs, tiles, nt, b)
     assert rc == _lib.B2_ERR_INVALID_ARGUMENT and "tile" in msg
+
+
+def test_reduced_policy_space():
+    """Unobserved factors are dropped from the evaluated policy set; the map
+    from a full policy to its reduced index keeps the observed actions."""
+    from oracle.efe import construct_policies
+    from pymdp_b200.rollout import AgentSpec, _descriptor
+    rng = np.random.default_rng(0)
+    S, U, T = [3, 4, 2], [2, 3, 2], 2
+    A = [rng.dirichlet(np.ones(5), size=(3, 2)).transpose(2, 0, 1)]  # modality on factors 0 and 2
+    B = [rng.dirichlet(np.ones(s), size=(s, u)).transpose(2, 0, 1) for s, u in zip(S, U)]
+    sp = AgentSpec(A, B, [np.zeros(5)], [np.ones(s) / s for s in S], [[0, 2]], T)
+    assert sp.observed == [0, 2] and sp.num_reduced_policies == 4 ** T and sp.num_policies == 12 ** T
+    g = _descriptor(sp, {"A": [0], "C": [0], "B": [0, 0, 0], "D": 0, "ll": 0, "qs": 0, "G": 0})
+    assert (g.obs_mask, g.n_multi_r, g.P_r, g.w0_r, list(g.ustride_r)[:3]) == (0b101, 4, 16, 4, [2, 0, 1])
+    pol = construct_policies(S, U, T)
+    red = construct_policies([S[0], S[2]], [U[0], U[2]], T)
+    index = {tuple(r.reshape(-1)): i for i, r in enumerate(red)}
+    for p, row in enumerate(pol):
+        pr, W = 0, g.w0
+        for t in range(T):
+            mt = (p // W) % g.n_multi
+            mr = sum(((mt // g.ustride[f]) % g.U[f]) * g.ustride_r[f] for f in range(3))
+            pr = pr * g.n_multi_r + mr
+            W //= g.n_multi
+        assert pr == index[tuple(row[:, [0, 2]].reshape(-1))]
