@@ -44,6 +44,13 @@ enum {
 #define B2_FLAG_USE_INDUCTIVE 4
 #define B2_FLAG_USE_PARAM_INFO_GAIN 8
 #define B2_FLAG_MODEL_PARAMS_STATIC 16
+/* This build only (the reference ABI has no such bit): the policy matrix is the
+ * full product of every factor's controls over T steps in the order of
+ * control.construct_policies (pymdp/control.py:152-195), shared by all agents.
+ * The tensor-core paths then evaluate every distinct policy prefix once
+ * (depth t has prod(U)^(t+1) prefixes instead of P) and sum G along the tree.
+ * Ignored when P != prod(U)^T, when the matrix is per agent, or by the SIMT path. */
+#define B2_FLAG_POLICY_TREE 32
 /* Precision selector, bits 8-9 of `flags` (unused by the reference ABI). */
 #define B2_PRECISION_SHIFT 8
 #define B2_PRECISION_FP32 0   /* SIMT FP32, FP32 accumulate (default)         */

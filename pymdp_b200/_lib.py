@@ -26,6 +26,7 @@ FLAG_USE_STATES_INFO_GAIN = 1 << 1
 FLAG_USE_INDUCTIVE = 1 << 2
 FLAG_USE_PARAM_INFO_GAIN = 1 << 3
 FLAG_MODEL_PARAMS_STATIC = 1 << 4
+FLAG_POLICY_TREE = 1 << 5
 PRECISION_SHIFT = 8
 PRECISIONS = {"fp32": 0, "tf32x3": 1, "bf16": 2}
 

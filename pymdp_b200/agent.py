@@ -152,8 +152,10 @@ class Agent:
             if pB is not None else None
         self._pA_flat = ffi.flatten_ragged_f32(self.pA, 1, dev)[0] if (use_param_info_gain and self.pA) else None
         self._pB_flat = ffi.flatten_ragged_f32(self.pB, 1, dev)[0] if (use_param_info_gain and self.pB) else None
+        # policies built here are construct_policies' full product set: let the
+        # tensor-core paths share the evaluation of common policy prefixes
         self._flags = ffi.efe_flags(use_utility, use_states_info_gain, use_param_info_gain, use_inductive,
-                                    precision=precision)
+                                    precision=precision, policy_tree=policies is None)
         self.use_param_info_gain, self.use_inductive = use_param_info_gain, use_inductive
         self.A, self.B, self.C = A, B, C
 

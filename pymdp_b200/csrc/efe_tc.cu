@@ -63,6 +63,7 @@ constexpr int kTcMaxOuter = 3;       // tensor-core path: dependency rank <= 4
 constexpr int kTcMaxAStages = 8;     // A (X) stages in tensor memory
 constexpr int kTcWSlots = 2;         // W slots in shared memory
 constexpr int kTcWSlotTarget = 32768;  // preferred bytes per W bulk copy
+constexpr int kTcMaxT = 8;             // policy-tree mode: policy_len <= 8
 
 struct TcGroup {
   int64_t pack_off;  // per-agent byte offset of this group's W image
@@ -95,6 +96,12 @@ struct TcParams {
   int8_t b_tr[kEfeMaxF];    // 1: staged transposed as [k][u][s] (rank-1 parents, S % 4 == 0)
   int8_t mod_order[B2_MAX_MODALITIES];
   TcGroup grp[kTcMaxGroups];
+  // policy-tree mode (B2_FLAG_POLICY_TREE): CTA x of depth t covers prefixes
+  // [(x - tree_tiles[t]) * 128, +128) of the prod(U)^(t+1) prefixes at depth t
+  int32_t tree, tree_nu;
+  int32_t tree_tiles[kTcMaxT + 1];  // cumulative 128-row tiles per depth
+  int64_t tree_off[kTcMaxT + 1];    // cumulative prefixes per depth (per-agent offsets into Gt)
+  int64_t tree_w[kTcMaxT];          // prod(U)^(T-1-t): policies per prefix at depth t
 };
 
 template <int PREC>
@@ -658,7 +665,8 @@ template <int PREC>
 __global__ void __launch_bounds__(kThreadsAll, 1)
     efe_tc_kernel(const __grid_constant__ EfeParams p, const __grid_constant__ TcParams tp,
                   const int32_t* __restrict__ pm, int pm_batched, const float* __restrict__ qs_init,
-                  const float* __restrict__ B, const uint8_t* __restrict__ pack, float* __restrict__ G) {
+                  const float* __restrict__ B, const uint8_t* __restrict__ pack, float* __restrict__ G,
+                  double* __restrict__ Gt) {
   using Tr = TcTraits<PREC>;
   constexpr int kPl = Tr::kPlanes;
   constexpr int CPS = Tr::kCps;
@@ -682,6 +690,15 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t b = blockIdx.y;
+  // steps this CTA evaluates and its first row (a policy, or a prefix at depth t_lo in tree mode)
+  int t_lo = 0, t_hi = p.T, row0 = blockIdx.x * kTcTile;
+  if (tp.tree) {
+    int t = 0;
+    while (t + 1 < p.T && (int)blockIdx.x >= tp.tree_tiles[t + 1]) ++t;
+    t_lo = t;
+    t_hi = t + 1;
+    row0 = ((int)blockIdx.x - tp.tree_tiles[t]) * kTcTile;
+  }
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, (uint32_t)tp.tmem_cols);
   if (tid == 0) {
@@ -731,14 +748,14 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
   if (warp == kProducers / 32) {
     // ---------------- W loader: large bulk copies into the W slots
     if (lane == 0) {
-      const int T = p.T, G = tp.G, wch = tp.wch, ws_bytes = tp.ws_bytes;
+      const int G = tp.G, wch = tp.wch, ws_bytes = tp.ws_bytes;
       uint64_t* const w_full = sm.w_full;
       uint64_t* const w_free = sm.w_free;
       volatile int* const abort_flag = sm.abort_flag;
       const uint32_t ws0 = tc::smem_u32(sm.Ws);
       const uint8_t* const pack_b = pack + b * tp.pack_stride;
       Ring wr;
-      for (int t = 0; t < T; ++t)
+      for (int t = t_lo; t < t_hi; ++t)
         for (int g = 0; g < G; ++g) {
           const int nch = tp.grp[g].nch, chunk_bytes = tp.grp[g].chunk_bytes;
           const uint8_t* wimg = pack_b + tp.grp[g].pack_off;
@@ -760,7 +777,7 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     if (lane == 0) {
       const uint64_t wdesc0 = tc::desc_kmajor_sw128(tc::smem_u32(sm.Ws));
       const uint32_t acol0 = tmem + (uint32_t)tp.a_col;
-      const int T = p.T, G = tp.G, wch = tp.wch, nacc = tp.nacc;
+      const int G = tp.G, wch = tp.wch, nacc = tp.nacc;
       const uint32_t ws16 = (uint32_t)tp.ws_bytes >> 4;
       uint64_t* const x_full = sm.x_full;
       uint64_t* const done = sm.done;
@@ -776,7 +793,7 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
       // results of the look-ahead barrier tests made while issuing the
       // previous stage (false: wait here)
       uint32_t x_ready = 0, w_ready = 0;
-      for (int t = 0; t < T; ++t)
+      for (int t = t_lo; t < t_hi; ++t)
         for (int g = 0; g < G; ++g, ++j) {
           const uint32_t idesc = tp.grp[g].idesc;
           const int N = tp.grp[g].N, nch = tp.grp[g].nch;
@@ -833,20 +850,24 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     // ---------------- producers (warps 0-15): policy pl, quarter qt
     const int pl = tid & (kTcTile - 1);
     const int qt = tid >> 7;
-    const int pol = blockIdx.x * kTcTile + pl;
-    const bool active = pol < p.P;
+    const int pol = row0 + pl;  // policy, or prefix at depth t_lo in tree mode
+    const int n_rows = tp.tree ? (int)(tp.tree_off[t_lo + 1] - tp.tree_off[t_lo]) : p.P;
+    const bool active = pol < n_rows;
+    // the row's actions: a prefix's are those of its first policy
+    const int64_t pol_act = tp.tree ? (int64_t)pol * tp.tree_w[t_lo] : pol;
     const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
     double g_acc = 0.0;
     bool bad_action = false;
     int cur = 0;
     Ring ring;
     uint32_t j = 0;
-    const int32_t* u_base = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (int64_t)(active ? pol : 0) * p.T * p.F;
-    for (int t = 0; t < p.T; ++t) {
+    const int32_t* u_base = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (active ? pol_act : 0) * p.T * p.F;
+    for (int t = 0; t < t_hi; ++t) {
       rollout_step(p, tp, Bag, tp.b_words > 0, u_base + t * p.F, qsm + cur * p.S_tot * kTcTile,
                    qsm + (cur ^ 1) * p.S_tot * kTcTile, pl, qt, bad_action);
       producers_sync();
       cur ^= 1;
+      if (t < t_lo) continue;  // tree mode: roll out to this CTA's depth, evaluate only there
       const float* q = qsm + cur * p.S_tot * kTcTile;
       for (int g = 0; g < tp.G; ++g, ++j) {
         const TcGroup& gr = tp.grp[g];
@@ -904,7 +925,10 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     producers_sync();
     if (qt == 0 && active && !*sm.abort_flag) {
       const double gsum = ((red[pl] + red[kTcTile + pl]) + red[2 * kTcTile + pl]) + red[3 * kTcTile + pl];
-      G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : (float)gsum;
+      if (tp.tree)
+        Gt[b * tp.tree_off[p.T] + tp.tree_off[t_lo] + pol] = bad_action ? __longlong_as_double(0x7ff8000000000000ll) : gsum;
+      else
+        G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : (float)gsum;
     }
   }
   tc::fence_before_sync();
@@ -914,6 +938,19 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
 }
 
 }  // namespace
+
+// Policy-tree mode: G[p] = sum_t g_t[p / prod(U)^(T-1-t)] from the per-prefix
+// step values (FP64), NaN where a prefix held an out-of-range action.
+__global__ void efe_tree_combine_kernel(const __grid_constant__ TcParams tp, int T, int P,
+                                        const double* __restrict__ Gt, float* __restrict__ G) {
+  const int64_t b = blockIdx.y;
+  const int pol = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pol >= P) return;
+  const double* g = Gt + b * tp.tree_off[T];
+  double s = 0.0;
+  for (int t = 0; t < T; ++t) s += g[tp.tree_off[t] + pol / tp.tree_w[t]];
+  G[b * P + pol] = (float)s;
+}
 
 // Plan the tensor-core path; returns B2_ERR_UNSUPPORTED when the model falls
 // outside its limits (the caller then uses the SIMT kernel).
@@ -1054,19 +1091,45 @@ int32_t launch_tc_t(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_ba
   TcParams tp;
   int smem = 0;
   if (tc_plan_t<PREC>(p, &tp, &smem) != B2_OK) return B2_OK;
-  const size_t bytes = (size_t)Bn * (size_t)tp.pack_stride;
+  // policy tree: a shared full product policy set with T >= 2
+  if ((p.flags & B2_FLAG_POLICY_TREE) && !pm_batched && p.T >= 2 && p.T <= kTcMaxT) {
+    int64_t nu = 1, P = 1;
+    for (int f = 0; f < p.F; ++f) nu *= p.U[f];
+    for (int t = 0; t < p.T && P <= p.P; ++t) P *= nu;
+    if (P == p.P && nu > 1) {
+      tp.tree = 1;
+      tp.tree_nu = (int32_t)nu;
+      int64_t n = 1;
+      tp.tree_tiles[0] = 0;
+      tp.tree_off[0] = 0;
+      for (int t = 0; t < p.T; ++t) {
+        n *= nu;
+        tp.tree_tiles[t + 1] = tp.tree_tiles[t] + (int32_t)((n + kTcTile - 1) / kTcTile);
+        tp.tree_off[t + 1] = tp.tree_off[t] + n;
+        tp.tree_w[t] = p.P / n;
+      }
+    }
+  }
+  const size_t pack_bytes = (size_t)Bn * (size_t)tp.pack_stride;
+  const size_t gt_bytes = tp.tree ? (size_t)Bn * (size_t)tp.tree_off[p.T] * sizeof(double) : 0;
   uint8_t* pack = nullptr;
-  B2_TRY(ws_alloc((void**)&pack, bytes, stream, kEfeName));
+  B2_TRY(ws_alloc((void**)&pack, pack_bytes + gt_bytes, stream, kEfeName));
+  double* Gt = tp.tree ? reinterpret_cast<double*>(pack + pack_bytes) : nullptr;
   int Kmax = 0;
   for (int g = 0; g < tp.G; ++g) Kmax = tp.grp[g].Kpad > Kmax ? tp.grp[g].Kpad : Kmax;
   dim3 pgrid((unsigned)((Kmax + 127) / 128), (unsigned)tp.G, (unsigned)Bn);
-  dim3 grid((unsigned)((p.P + kTcTile - 1) / kTcTile), (unsigned)Bn);
+  dim3 grid((unsigned)(tp.tree ? tp.tree_tiles[p.T] : (p.P + kTcTile - 1) / kTcTile), (unsigned)Bn);
   efe_tc_pack_kernel<PREC><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
   int32_t rc = check_launch("efe_ffi tc pack");
   if (rc == B2_OK) rc = ensure_smem_attr((const void*)efe_tc_kernel<PREC>, smem, kEfeName);
   if (rc == B2_OK) {
-    efe_tc_kernel<PREC><<<grid, kThreadsAll, smem, stream>>>(p, tp, pm, pm_batched, qs, B, pack, G);
+    efe_tc_kernel<PREC><<<grid, kThreadsAll, smem, stream>>>(p, tp, pm, pm_batched, qs, B, pack, G, Gt);
     rc = check_launch("efe_ffi tc");
+  }
+  if (rc == B2_OK && tp.tree) {
+    efe_tree_combine_kernel<<<dim3((unsigned)((p.P + 255) / 256), (unsigned)Bn), 256, 0, stream>>>(tp, p.T, p.P, Gt,
+                                                                                                   G);
+    rc = check_launch("efe_ffi tc tree combine");
   }
   cudaError_t fe = cudaFreeAsync(pack, stream);
   if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);

@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (FLAG_MODEL_PARAMS_STATIC, FLAG_USE_INDUCTIVE, FLAG_USE_PARAM_INFO_GAIN,  # noqa: F401
+from ._lib import (FLAG_MODEL_PARAMS_STATIC, FLAG_POLICY_TREE, FLAG_USE_INDUCTIVE, FLAG_USE_PARAM_INFO_GAIN,  # noqa: F401
                    FLAG_USE_STATES_INFO_GAIN, FLAG_USE_UTILITY, MAX_DEP_RANK, PRECISIONS, PRECISION_SHIFT,
                    B2Error, InvalidArgumentError, UnsupportedError, check, i64, is_available)
 
@@ -239,8 +239,11 @@ def can_handle(A_dependencies, B_dependencies, use_param_info_gain: bool, *, num
 
 
 def efe_flags(use_utility=True, use_states_info_gain=True, use_param_info_gain=False, use_inductive=False,
-              ffi_cache_params_static=False, precision="fp32") -> int:
-    flags = 0
+              ffi_cache_params_static=False, precision="fp32", policy_tree=False) -> int:
+    """Flag word of ``b2_neg_efe``. ``policy_tree`` declares the policy matrix
+    to be ``construct_policies``' full product set (``B2_FLAG_POLICY_TREE``):
+    the tensor-core paths then evaluate each distinct prefix once."""
+    flags = FLAG_POLICY_TREE if policy_tree else 0
     flags |= FLAG_USE_UTILITY if use_utility else 0
     flags |= FLAG_USE_STATES_INFO_GAIN if use_states_info_gain else 0
     flags |= FLAG_USE_INDUCTIVE if use_inductive else 0
@@ -294,7 +297,7 @@ def neg_efe_all_policies_ffi(policy_matrix, qs_init, A, B, C, I, A_dependencies,
                              pA=None, pB=None, use_utility: bool = True, use_states_info_gain: bool = True,
                              use_param_info_gain: bool = False, use_inductive: bool = True,
                              inductive_epsilon: float = 1e-3, ffi_cache_params_static: bool = False,
-                             precision: str = "fp32") -> torch.Tensor:
+                             precision: str = "fp32", policy_tree: bool = False) -> torch.Tensor:
     """``pymdp/ffi/_efe.py:491-711``: ``neg_efe`` (G) of every policy.
 
     ``qs_init[f]``: ``(*batch, S_f)``; ``A[m]``: ``(*batch, O_m, *S_deps)``;
@@ -367,7 +370,7 @@ def neg_efe_all_policies_ffi(policy_matrix, qs_init, A, B, C, I, A_dependencies,
     eps = _dev_f32(torch.as_tensor(inductive_epsilon, dtype=torch.float32), dev).reshape(-1).contiguous()
     out = torch.empty(lead + (P,), dtype=torch.float32, device=dev)
     flags = efe_flags(use_utility, use_states_info_gain, use_param_info_gain, use_inductive,
-                      ffi_cache_params_static, precision)
+                      ffi_cache_params_static, precision, policy_tree=policy_tree)
     lay.call(None, pm, 0, qs_flat, A_flat, B_flat, C_flat, I_flat, pA_flat, pB_flat, eps, out, Bn, P, flags)
     return out
 

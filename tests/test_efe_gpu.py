@@ -246,3 +246,33 @@ def test_agent_with_param_info_gain_and_inductive_matches_oracle():
             use_inductive=True, inductive_epsilon=1e-3)
         np.testing.assert_allclose(G[b].cpu().numpy(), G_ref, rtol=G_RTOL, atol=G_ATOL * max(1.0, np.abs(G_ref).max()))
         np.testing.assert_allclose(q_pi[b].cpu().numpy(), q_ref, rtol=Q_RTOL, atol=Q_ATOL)
+
+
+# ----------------------------------------- policy-tree mode (B2_FLAG_POLICY_TREE)
+@pytest.mark.parametrize("precision", ["tf32x3", "bf16"])
+@pytest.mark.parametrize("case", [
+    dict(S=[3, 4, 2], O=[4, 5, 3], U=[2, 3, 2], T=2, A_deps=[[0, 2], [1, 2, 0], [1]], B_deps=[[0], [1, 0], [2, 1]]),
+    dict(S=[5, 3], O=[7], U=[3, 2], T=3, A_deps=[[1, 0]], B_deps=[[0], [1]], C2d=True),
+    dict(S=[32, 16, 8], O=[16, 16, 8, 8, 4], U=[4, 4, 1], T=3, A_deps=[[0, 1, 2]] * 5, B_deps=[[0], [1], [2]]),
+])
+def test_policy_tree_matches_oracle_and_full_evaluation(case, precision):
+    """Evaluating each distinct policy prefix once (T >= 2, the full product
+    policy set) gives the oracle's G, and the per-policy evaluation's."""
+    from pymdp_b200 import _lib, ffi
+    rng = np.random.default_rng(len(case["S"]) * 7 + case["T"])
+    batch = 2
+    A, B, C, qs = random_efe(rng, case["S"], case["O"], case["U"], case["T"], case["A_deps"], case["B_deps"],
+                             batch, case.get("C2d", False))
+    pol = oefe.construct_policies(case["S"], case["U"], case["T"])
+    I = [torch.zeros((batch, 1, s), device="cuda") for s in case["S"]]
+    args = (pol, [cuda(q) for q in qs], [cuda(a) for a in A], [cuda(b) for b in B], [cuda(c) for c in C], I,
+            case["A_deps"], case["B_deps"])
+    G_tree = ffi.neg_efe_all_policies_ffi(*args, use_inductive=False, precision=precision,
+                                          policy_tree=True).cpu().numpy()
+    G_full = ffi.neg_efe_all_policies_ffi(*args, use_inductive=False, precision=precision).cpu().numpy()
+    assert _lib.load().b2_device_error() == 0
+    for b in range(batch):
+        ref = oefe.neg_efe_all_policies(pol, [q[b] for q in qs], [a[b] for a in A], [x[b] for x in B],
+                                        [c[b] for c in C], case["A_deps"], case["B_deps"])
+        _g_close(G_tree[b], ref, precision)
+        _g_close(G_full[b], ref, precision)
