@@ -221,15 +221,19 @@ def run_rollout_config(dev, steps: int, warmup: int):
     return out
 
 
-def efe_flops_per_agent() -> float:
+def efe_flops_per_agent(tree: bool = False) -> float:
+    """Contraction flops per agent: every policy at every step (dense), or,
+    with the policy tree, every distinct prefix once: 2 * sum_t nu^(t+1) *
+    sum_m O_m K_m with nu = prod(U)."""
     K = int(np.prod(S))
-    P = int(np.prod(U)) ** T
-    return 2.0 * T * P * sum(o * K for o in O)
+    nu = int(np.prod(U))
+    cols = sum(nu ** (t + 1) for t in range(T)) if tree else T * nu ** T
+    return 2.0 * cols * sum(o * K for o in O)
 
 
-# DRAM bytes per agent of the neg-EFE tensor-core kernel, from an ncu capture of 160 agents (the W image is read
-# once per agent, so traffic scales with agents); None where no capture exists yet.
-EFE_TRAFFIC_PER_AGENT = {"tf32x3": 347.2e6 / 160}
+# DRAM bytes per agent of the neg-EFE tensor-core kernel (policy-tree mode), from an ncu capture of 160 agents (the
+# W image is read from DRAM once per agent, so traffic scales with agents); None where no capture exists yet.
+EFE_TRAFFIC_PER_AGENT = {"tf32x3": (339.3e6 + 8.8e6) / 160}
 
 
 def fpi_bytes_per_agent() -> float:
@@ -398,8 +402,8 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     fpi_res = run_fpi_config(dev, args.steps, args.warmup, flush)
-    fit_res = run_fit_config(dev, args.steps, args.warmup, flush)
-    ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup)
+    fit_res = run_fit_config(dev, args.steps, args.warmup, flush) if args.legs == "all" else None
+    ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if args.legs == "all" else None
     efe_ev = []
 
     def step(timed_efe=False):
@@ -481,7 +485,9 @@ def run_b200(args, rank, world, local_rank):
         pass
     peak_tf = peaks.get("bf16_tflops", 1590.0)
     peak_gbs = peaks.get("hbm_gbs", 6650.0)
-    flops = efe_flops_per_agent() * n_agents
+    tree = agent.precision != "fp32"  # the tensor-core paths evaluate each policy prefix once
+    flops = efe_flops_per_agent(tree) * n_agents
+    dense_flops = efe_flops_per_agent(False) * n_agents
     achieved_tf = flops / (efe_ms * 1e-3) / 1e12
     total_agents = n_agents * world
     value = total_agents * args.steps / (ms * 1e-3)
@@ -516,6 +522,8 @@ def run_b200(args, rank, world, local_rank):
                                  if agent.precision in EFE_TRAFFIC_PER_AGENT else None),
                      "kernel": f"neg-EFE launch over {n_agents} agents (W pack + policy evaluation + q_pi)",
                      "flops_per_launch": flops, "ms_per_launch": efe_ms,
+                     "policy_tree": tree, "dense_equivalent_flops_per_launch": dense_flops,
+                     "dense_equivalent_tflops": dense_flops / (efe_ms * 1e-3) / 1e12,
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"},
         "cpu_baseline": None if cpu_val is None else {
             "value": cpu_val, "unit": "agent-steps/s", "cores": min(sample, cpu_workers()), "kind": "port",
@@ -540,6 +548,8 @@ def main():
     ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout"],
                     help="step: the agent step (default); fpi: only the 4096-agent FPI model; fit: only the "
                          "model-fitting gradient; rollout: only the uneven-size rollout (for profiling)")
+    ap.add_argument("--legs", default="all", choices=["all", "step"],
+                    help="all: also the fitting and rollout workloads (default); step: the agent step and FPI only")
     ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
