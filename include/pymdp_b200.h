@@ -261,7 +261,7 @@ int32_t b2_select_action(void* stream, const float* q_pi, const int32_t* policy_
 #define B2_RO_MAX_STOT 256
 #define B2_RO_MAX_P 1024
 #define B2_RO_MAX_COLS 64
-#define B2_RO_TAB_FLOATS 4096
+#define B2_RO_TAB_FLOATS 6144
 
 /* One agent. Offsets are element offsets into the b2_ro_buffers arrays. */
 typedef struct b2_ro_agent {

@@ -89,7 +89,7 @@ _SIGS = {
 
 # ------------------------------------------------ uneven-size rollout structs
 RO_MAX_F, RO_MAX_M, RO_MAX_S, RO_MAX_O = 4, 8, 64, 32
-RO_MAX_K, RO_MAX_STOT, RO_MAX_P, RO_MAX_COLS, RO_TAB_FLOATS = 4096, 256, 1024, 64, 4096
+RO_MAX_K, RO_MAX_STOT, RO_MAX_P, RO_MAX_COLS, RO_TAB_FLOATS = 4096, 256, 1024, 64, 6144
 
 
 class RoAgent(ctypes.Structure):

@@ -453,9 +453,10 @@ __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent,
 }
 
 // ------------------------------------------------------- policy evaluation
+// Prefix tables are [state j][column c] with row stride NC = round_up(width, 8).
 struct TileSmem {
-  float *tab0, *tab1, *sA, *sX, *sOut, *g0, *g1;
-  unsigned char *sDig, *sFac;
+  float *tab0, *tab1, *sA, *sW, *sOut, *g0, *g1;
+  unsigned char* sFac;
 };
 
 template <int NT, int KC>
@@ -464,24 +465,12 @@ __device__ TileSmem ro_tile_smem(unsigned char* smem, int tab_floats) {
   s.tab0 = reinterpret_cast<float*>(smem);
   s.tab1 = s.tab0 + tab_floats;
   s.sA = s.tab1 + tab_floats;
-  s.sX = s.sA + KC * kRpad;
-  s.sOut = s.sX + KC * kCols;
+  s.sW = s.sA + KC * kRpad;
+  s.sOut = s.sW + (KC + 1) * kCols;
   s.g0 = s.sOut + kRpad * kCols;
   s.g1 = s.g0 + kCols;
-  s.sDig = reinterpret_cast<unsigned char*>(s.g1 + kCols);  // 2 x KC x kF
-  s.sFac = s.sDig + 2 * KC * kF;
+  s.sFac = reinterpret_cast<unsigned char*>(s.g1 + kCols);
   return s;
-}
-
-// Digits of k0 .. k0 + KC - 1 along modality m's dependency axes.
-template <int NT, int KC>
-__device__ __forceinline__ void ro_digits(const b2_ro_agent& ag, int m, int k0, unsigned char* dst) {
-  const int K = ag.K[m], r = ag.rank[m];
-  for (int kk = threadIdx.x; kk < KC; kk += NT) {
-    const int k = k0 + kk;
-    if (k < K)
-      for (int i = 0; i < r; ++i) dst[kk * kF + i] = (unsigned char)((k / ag.dstride[m][i]) % ag.S[ag.dep[m][i]]);
-  }
 }
 
 template <int NT, int KC, bool BF16>
@@ -501,19 +490,26 @@ __device__ __forceinline__ void ro_load_a(const float* Am, const __nv_bfloat16* 
 }
 
 // out[:R, :n] = [A_m; lin_m] (R x K) * X (K x n) into sOut (row stride kCols),
-// X[k, c] = prod_i tab[c][dep_i][k_i] (table row stride ts, odd). A thread
-// owns 4 rows x CB columns of one k slice; the KG slices of a unit are
+// with X[k, c] = prod_i q_c[dep_i][k_i] never formed: the innermost dependency
+// axis (stride 1 in K) is contracted directly against the prefix table,
+//   out[o, c] = sum_po w[po, c] * sum_s A[o, po * S_in + s] * q_c[dep_last][s],
+// and the outer axes enter as per-column weights w[po, c] = prod of the other
+// dependencies' marginals, S_in times fewer values than X. A thread owns 4 rows x
+// CB columns of one contiguous k slice per chunk; the KG slices of a unit are
 // adjacent lanes and combine by shuffles. The next A chunk is loaded into
 // registers while the current one is multiplied.
 template <int NT, int KC, bool BF16, int CB>
-__device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const float* tab, int ts, int n,
+__device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const float* tab, int NC, int n,
                             const TileSmem& s) {
   constexpr int NW = NT / 32;
   constexpr int AE = (kRpad * KC + NT - 1) / NT;
   const int K = ag.K[m], R = ag.O[m] + 1, r = ag.rank[m];
+  const int f_in = ag.dep[m][r - 1], S_in = ag.S[f_in];
+  const float* xin = tab + ag.qs_off[f_in] * NC;
   const int RG = (R + 3) >> 2, CG = (n + CB - 1) / CB, units = RG * CG;  // units <= 9 x 8 <= NT
   int KG = 1;
   while (KG < 16 && units * KG * 2 <= NT) KG <<= 1;
+  const int L = KC / KG;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int unit = tid / KG, kg = tid & (KG - 1);
   const bool active = unit < units;
@@ -521,9 +517,14 @@ __device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const
   const int colpad = CG * CB;
   const float* Am = a.buf.Aprime + ag.A_off[m];
   const __nv_bfloat16* Ab = BF16 ? reinterpret_cast<const __nv_bfloat16*>(a.buf.Aprime_bf16) + ag.A_off[m] : nullptr;
-  int qoff[kF];
+  int qo[kF - 1], So[kF - 1], ro[kF - 1];  // outer axes: table offset, size, stride in outer-index units
 #pragma unroll
-  for (int i = 0; i < kF; ++i) qoff[i] = i < r ? ag.qs_off[ag.dep[m][i]] : 0;
+  for (int i = 0; i < kF - 1; ++i) {
+    const bool on = i < r - 1;
+    qo[i] = on ? ag.qs_off[ag.dep[m][i]] : 0;
+    So[i] = on ? ag.S[ag.dep[m][i]] : 1;
+    ro[i] = on ? ag.dstride[m][i] / S_in : 1;
+  }
   float acc[4][CB];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -531,9 +532,6 @@ __device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const
     for (int j = 0; j < CB; ++j) acc[i][j] = 0.f;
   float pa[AE];
   ro_load_a<NT, KC, BF16>(Am, Ab, R, K, 0, pa);
-  ro_digits<NT, KC>(ag, m, 0, s.sDig);
-  __syncthreads();
-  int buf = 0;
   for (int k0 = 0; k0 < K; k0 += KC) {
     const int kn = min(KC, K - k0);
 #pragma unroll
@@ -541,31 +539,38 @@ __device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const
       const int idx = tid + j * NT;
       if (idx < kRpad * KC) s.sA[(idx % KC) * kRpad + idx / KC] = pa[j];
     }
-    const unsigned char* dg = s.sDig + buf * KC * kF;
-    for (int kk = warp; kk < KC; kk += NW) {
-      const unsigned char* d = dg + kk * kF;
-      for (int c = lane; c < colpad; c += 32) {
-        float x = 0.f;
-        if (kk < kn && c < n) {
-          const float* col = tab + c * ts;
-          x = col[qoff[0] + d[0]];
+    const int po0 = k0 / S_in, npo = (k0 + kn - 1) / S_in - po0 + 1;
+    if (r > 1) {
+      for (int pr = warp; pr < npo; pr += NW) {
+        const int po = po0 + pr;
+        int off[kF - 1];
 #pragma unroll
-          for (int i = 1; i < kF; ++i)
-            if (i < r) x *= col[qoff[i] + d[i]];
+        for (int i = 0; i < kF - 1; ++i) off[i] = (i < r - 1) ? (qo[i] + (po / ro[i]) % So[i]) * NC : 0;
+        for (int c = lane; c < colpad; c += 32) {
+          float w = 0.f;
+          if (c < n) {
+            w = tab[off[0] + c];
+#pragma unroll
+            for (int i = 1; i < kF - 1; ++i)
+              if (i < r - 1) w *= tab[off[i] + c];
+          }
+          s.sW[pr * kCols + c] = w;
         }
-        s.sX[kk * kCols + c] = x;
       }
     }
     __syncthreads();
-    if (k0 + KC < K) {
-      ro_load_a<NT, KC, BF16>(Am, Ab, R, K, k0 + KC, pa);
-      ro_digits<NT, KC>(ag, m, k0 + KC, s.sDig + (buf ^ 1) * KC * kF);
-    }
-    if (active) {
-      const float* xb = s.sX + CB * cg;
-      for (int kk = kg; kk < kn; kk += KG) {
+    if (k0 + KC < K) ro_load_a<NT, KC, BF16>(Am, Ab, R, K, k0 + KC, pa);
+    const int kb = kg * L, ke = min(kn, kb + L);
+    if (active && kb < ke) {
+      int si = (k0 + kb) % S_in, pr = (k0 + kb) / S_in - po0;
+      float inner[4][CB];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < CB; ++j) inner[i][j] = 0.f;
+      for (int kk = kb; kk < ke; ++kk) {
         const float4 av = *reinterpret_cast<const float4*>(s.sA + kk * kRpad + 4 * rg);
-        const float* xr = xb + kk * kCols;
+        const float* xr = xin + si * NC + CB * cg;
         float xv[CB];
 #pragma unroll
         for (int j = 0; j < CB; j += 4) {
@@ -577,14 +582,41 @@ __device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const
         }
 #pragma unroll
         for (int j = 0; j < CB; ++j) {
-          acc[0][j] = fmaf(av.x, xv[j], acc[0][j]);
-          acc[1][j] = fmaf(av.y, xv[j], acc[1][j]);
-          acc[2][j] = fmaf(av.z, xv[j], acc[2][j]);
-          acc[3][j] = fmaf(av.w, xv[j], acc[3][j]);
+          inner[0][j] = fmaf(av.x, xv[j], inner[0][j]);
+          inner[1][j] = fmaf(av.y, xv[j], inner[1][j]);
+          inner[2][j] = fmaf(av.z, xv[j], inner[2][j]);
+          inner[3][j] = fmaf(av.w, xv[j], inner[3][j]);
+        }
+        const bool wrap = ++si == S_in;
+        if (wrap || kk + 1 == ke) {  // this outer index ends here (or the slice does): weight and flush
+          if (r > 1) {
+            const float* wr = s.sW + pr * kCols + CB * cg;
+#pragma unroll
+            for (int j = 0; j < CB; j += 4) {
+              const float4 w4 = *reinterpret_cast<const float4*>(wr + j);
+              const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+              for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc[i][j + jj] = fmaf(inner[i][j + jj], wv[jj], acc[i][j + jj]);
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+              for (int j = 0; j < CB; ++j) acc[i][j] += inner[i][j];
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < CB; ++j) inner[i][j] = 0.f;
+          if (wrap) {
+            si = 0;
+            ++pr;
+          }
         }
       }
     }
-    buf ^= 1;
     __syncthreads();
   }
 #pragma unroll
@@ -612,11 +644,11 @@ __device__ void ro_tile(const RoArgs& a, const b2_ro_agent& ag, const b2_ro_tile
   constexpr int NW = NT / 32;
   const TileSmem s = ro_tile_smem<NT, KC>(smem, a.tab_floats);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int St = ag.S_tot, ts = St | 1, nu = ag.n_multi_r;
+  const int St = ag.S_tot, nu = ag.n_multi_r, NC = (tile.p_hi - tile.p_lo + 7) & ~7;
   const bool ig = (a.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
   for (int j = tid; j < St; j += NT) {
     s.sFac[j] = (unsigned char)ro_factor_of(ag, j);
-    s.tab1[j] = a.buf.qs[ag.qs_base + j];  // the root: the posterior
+    s.tab1[j * NC] = a.buf.qs[ag.qs_base + j];  // the root (column 0): the posterior
   }
   __syncthreads();
   float *prev = s.tab1, *cur = s.tab0, *gp = s.g1, *gc = s.g0;
@@ -626,26 +658,25 @@ __device__ void ro_tile(const RoArgs& a, const b2_ro_agent& ag, const b2_ro_tile
     for (int c = warp; c < n; c += NW) {
       const int pc = t == 0 ? 0 : (c_lo + c) / nu - prev_lo;
       const int mu = (c_lo + c) % nu;
-      const float* pq = prev + pc * ts;
       for (int j = lane; j < St; j += 32) {
         const int f = s.sFac[j];
         if (!((ag.obs_mask >> f) & 1)) continue;  // unobserved: never read
         const int S = ag.S[f], U = ag.U[f], sj = j - ag.qs_off[f];
         const int u = (mu / ag.ustride_r[f]) % U;
         const float* Bf = a.buf.B + ag.B_off[f] + (int64_t)sj * S * U + u;
-        const float* pf = pq + ag.qs_off[f];
+        const float* pf = prev + ag.qs_off[f] * NC + pc;
         float acc = 0.f;
-        for (int s2 = 0; s2 < S; ++s2) acc = fmaf(__ldg(Bf + (int64_t)s2 * U), pf[s2], acc);
-        cur[c * ts + j] = acc;
+        for (int s2 = 0; s2 < S; ++s2) acc = fmaf(__ldg(Bf + (int64_t)s2 * U), pf[s2 * NC], acc);
+        cur[j * NC + c] = acc;
       }
     }
     for (int c = tid; c < n; c += NT) gc[c] = t == 0 ? 0.f : gp[(c_lo + c) / nu - prev_lo];
     __syncthreads();
     for (int m = 0; m < ag.M; ++m) {
       if (n <= 4)
-        ro_contract<NT, KC, BF16, 4>(a, ag, m, cur, ts, n, s);
+        ro_contract<NT, KC, BF16, 4>(a, ag, m, cur, NC, n, s);
       else
-        ro_contract<NT, KC, BF16, 8>(a, ag, m, cur, ts, n, s);
+        ro_contract<NT, KC, BF16, 8>(a, ag, m, cur, NC, n, s);
       const int O = ag.O[m];
       for (int c = tid; c < n; c += NT) {
         float h = 0.f;
@@ -884,25 +915,25 @@ extern "C" int32_t b2_rollout(void* stream_, const b2_ro_agent* agents_host, int
   if (b.sync_count < 2 * steps + 32) return ro_bad("sync needs at least 2 * steps + 32 words");
   B2_TRY(validate_agents(agents_host, n_agents, b, true));
   // tiles: bounds, shape, and an exact cover of every agent's policies
-  int64_t tab = B2_RO_MAX_STOT + 1;
+  int64_t tab = 8 * B2_RO_MAX_STOT;
   std::vector<int64_t> covered(n_agents, 0);
   for (int64_t i = 0; i < n_tiles; ++i) {
     const b2_ro_tile& t = tiles_host[i];
     if (t.agent < 0 || t.agent >= n_agents) return ro_bad("tile agent out of range");
     const b2_ro_agent& g = agents_host[t.agent];
     if (t.p_lo < 0 || t.p_hi <= t.p_lo || t.p_hi > g.P_r) return ro_bad("tile policy range out of range");
-    const int64_t n = t.p_hi - t.p_lo, ts = g.S_tot | 1;
+    const int64_t n = t.p_hi - t.p_lo, nc = (n + 7) & ~int64_t(7);
     if (n > c.cols) return ro_bad("tile wider than cols");
-    if (n * ts > B2_RO_TAB_FLOATS) return ro_unsup("tile width x (S_tot | 1) above the 4096-float table");
-    tab = std::max(tab, n * ts);
+    if (nc * g.S_tot > B2_RO_TAB_FLOATS) return ro_unsup("round_up(tile width, 8) x S_tot above the table");
+    tab = std::max(tab, nc * g.S_tot);
     covered[t.agent] += n;
   }
   for (int64_t i = 0; i < n_agents; ++i)
     if (covered[i] != agents_host[i].P_r)
       return ro_bad("tiles do not cover agent " + std::to_string(i) + " once");
   tab = (tab + 3) & ~int64_t(3);
-  const size_t tile_bytes = (size_t)(2 * tab + c.kc * kRpad + c.kc * kCols + kRpad * kCols + 2 * kCols) * 4 +
-                            (size_t)2 * c.kc * kF + B2_RO_MAX_STOT;
+  const size_t tile_bytes = (size_t)(2 * tab + c.kc * kRpad + (c.kc + 1) * kCols + kRpad * kCols + 2 * kCols) * 4 +
+                            B2_RO_MAX_STOT;
   const size_t fpi_bytes = (size_t)(4 * B2_RO_MAX_STOT + B2_RO_MAX_K) * sizeof(double);
   const size_t smem = std::max(tile_bytes, fpi_bytes);
   int dev = 0, n_sm = 0, coop = 0;

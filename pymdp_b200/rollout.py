@@ -190,13 +190,13 @@ def tile_cost(spec: AgentSpec, p_lo: int, p_hi: int) -> float:
 
 def make_tiles(specs: Sequence[AgentSpec], cols: int) -> np.ndarray:
     """Cut each agent's reduced policies into tiles of at most ``cols``
-    policies (and at most 4096 / (S_tot | 1), the shared-memory table),
-    largest cost first. Returns ``(n_tiles, 4)`` int32 rows
+    policies (with round_up(width, 8) x S_tot within the shared-memory
+    prefix table), largest cost first. Returns ``(n_tiles, 4)`` int32 rows
     ``(agent, p_lo, p_hi, 0)``."""
     rows, costs = [], []
     for i, sp in enumerate(specs):
-        P, ts = sp.num_reduced_policies, int(sum(sp.S)) | 1
-        width = max(1, min(int(cols), P, _lib.RO_TAB_FLOATS // ts))
+        P, St = sp.num_reduced_policies, int(sum(sp.S))
+        width = max(1, min(int(cols), P, _lib.RO_TAB_FLOATS // St // 8 * 8))
         for lo in range(0, P, width):
             hi = min(P, lo + width)
             rows.append((i, lo, hi, 0))

@@ -89,7 +89,7 @@ def test_tiles_cover_every_policy_once(cols):
     cover = [np.zeros(sp.num_reduced_policies, np.int64) for sp in specs]
     for a, lo, hi, _ in tiles:
         assert 0 <= lo < hi <= specs[a].num_reduced_policies
-        assert hi - lo <= cols and (hi - lo) * (sum(specs[a].S) | 1) <= _lib.RO_TAB_FLOATS
+        assert hi - lo <= cols and (hi - lo + 7) // 8 * 8 * sum(specs[a].S) <= _lib.RO_TAB_FLOATS
         cover[a][lo:hi] += 1
     assert all((c == 1).all() for c in cover)
     costs = [tile_cost(specs[a], lo, hi) for a, lo, hi, _ in tiles]
