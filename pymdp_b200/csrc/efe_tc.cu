@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     efe_tc_kernel(const __grid_constant__ EfeParams p, const __grid_constant__ TcParams tp,
                   const int32_t* __restrict__ pm, int pm_batched, const float* __restrict__ qs_init,
                   const float* __restrict__ B, const uint8_t* __restrict__ pack, float* __restrict__ G,
-                  double* __restrict__ Gt) {
+                  double* __restrict__ Gt, const float* __restrict__ Qt) {
   using Tr = TcTraits<PREC>;
   constexpr int kPl = Tr::kPlanes;
   constexpr int CPS = Tr::kCps;
@@ -863,11 +863,23 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     uint32_t j = 0;
     const int32_t* u_base = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (active ? pol_act : 0) * p.T * p.F;
     for (int t = 0; t < t_hi; ++t) {
+      if (tp.tree) {
+        // the parents' marginals (depth t - 1) were rolled out once per agent by
+        // efe_tree_rollout_kernel; qsm already holds qs_init for depth 0
+        if (t < t_lo) continue;
+        if (t > 0) {
+          const int64_t prow = tp.tree_off[t - 1] + (active ? pol / tp.tree_nu : 0);
+          const float* qrow = Qt + (b * tp.tree_off[p.T - 1] + prow) * p.S_tot;
+          float* qd = qsm + cur * p.S_tot * kTcTile;
+          for (int s2 = qt; s2 < p.S_tot; s2 += 4) qd[s2 * kTcTile + pl] = __ldg(qrow + s2);
+          producers_sync();
+        }
+      }
       rollout_step(p, tp, Bag, tp.b_words > 0, u_base + t * p.F, qsm + cur * p.S_tot * kTcTile,
                    qsm + (cur ^ 1) * p.S_tot * kTcTile, pl, qt, bad_action);
       producers_sync();
       cur ^= 1;
-      if (t < t_lo) continue;  // tree mode: roll out to this CTA's depth, evaluate only there
+      if (t < t_lo) continue;  // (per-policy mode never skips)
       const float* q = qsm + cur * p.S_tot * kTcTile;
       for (int g = 0; g < tp.G; ++g, ++j) {
         const TcGroup& gr = tp.grp[g];
@@ -938,6 +950,71 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
 }
 
 }  // namespace
+
+// Policy-tree mode: the marginals of every distinct policy prefix of depth
+// 0 .. T-2, depth by depth, once per agent (one CTA): Qt[t][c][j] =
+// (B_f[..., u_t(c)] . joint of the parent prefix's marginals over f's B
+// dependencies)[s], the parent of prefix c at depth t being c / prod(U) at
+// depth t - 1 (qs_init at t = 0). The deepest level is rolled out inside
+// efe_tc_kernel, from these.
+__global__ void __launch_bounds__(512) efe_tree_rollout_kernel(const __grid_constant__ EfeParams p,
+                                                              const __grid_constant__ TcParams tp,
+                                                              const float* __restrict__ qs_init,
+                                                              const float* __restrict__ B, float* __restrict__ Qt) {
+  const int64_t b = blockIdx.x;
+  const int St = p.S_tot, nu = tp.tree_nu;
+  float* Qb = Qt + b * tp.tree_off[p.T - 1] * St;
+  const float* Bb = B + b * p.B_stride;
+  int ustride[kEfeMaxF];
+  int us = 1;
+  for (int f = p.F - 1; f >= 0; --f) {
+    ustride[f] = us;
+    us *= p.U[f];
+  }
+  for (int t = 0; t + 1 < p.T; ++t) {
+    const int n = (int)(tp.tree_off[t + 1] - tp.tree_off[t]);
+    float* out = Qb + tp.tree_off[t] * St;
+    for (int e = threadIdx.x; e < n * St; e += blockDim.x) {
+      const int c = e / St;
+      const int j = e - c * St;
+      int f = 0;
+      while (f + 1 < p.F && j >= p.qs_off[f + 1]) ++f;
+      const int s = j - p.qs_off[f], U = p.U[f];
+      const int u = ((c % nu) / ustride[f]) % U;
+      const float* q = t == 0 ? qs_init + b * St : Qb + (tp.tree_off[t - 1] + c / nu) * St;
+      const EfeFactor& fb = p.fac[f];
+      const float* Bs = Bb + fb.B_off + (int64_t)s * fb.K * U + u;
+      float acc = 0.f;
+      if (fb.rank == 1) {
+        const float* qv = q + p.qs_off[fb.dep[0]];
+        for (int k = 0; k < fb.K; ++k) acc = fmaf(__ldg(Bs + (int64_t)k * U), qv[k], acc);
+      } else {
+        int dig[B2_MAX_DEP_RANK];
+#pragma unroll
+        for (int i = 0; i < B2_MAX_DEP_RANK; ++i) dig[i] = 0;
+        for (int k = 0; k < fb.K; ++k) {
+          float w = 1.f;
+#pragma unroll
+          for (int i = 0; i < B2_MAX_DEP_RANK; ++i)
+            if (i < fb.rank) w *= q[p.qs_off[fb.dep[i]] + dig[i]];
+          acc = fmaf(__ldg(Bs + (int64_t)k * U), w, acc);
+          bool carry = true;
+#pragma unroll
+          for (int i = B2_MAX_DEP_RANK - 1; i >= 0; --i) {
+            if (carry && i < fb.rank) {
+              if (++dig[i] < p.S[fb.dep[i]])
+                carry = false;
+              else
+                dig[i] = 0;
+            }
+          }
+        }
+      }
+      out[(int64_t)c * St + j] = acc;
+    }
+    __syncthreads();
+  }
+}
 
 // Policy-tree mode: G[p] = sum_t g_t[p / prod(U)^(T-1-t)] from the per-prefix
 // step values (FP64), NaN where a prefix held an out-of-range action.
@@ -1108,22 +1185,31 @@ int32_t launch_tc_t(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_ba
         tp.tree_off[t + 1] = tp.tree_off[t] + n;
         tp.tree_w[t] = p.P / n;
       }
+      // the prefix roll-out kernel indexes (prefix, state) pairs of one depth in 32 bits
+      if ((double)tp.tree_off[p.T - 1] * p.S_tot >= 2.0e9) tp.tree = 0;
     }
   }
   const size_t pack_bytes = (size_t)Bn * (size_t)tp.pack_stride;
   const size_t gt_bytes = tp.tree ? (size_t)Bn * (size_t)tp.tree_off[p.T] * sizeof(double) : 0;
+  const size_t qt_bytes =
+      tp.tree ? ((size_t)Bn * (size_t)tp.tree_off[p.T - 1] * (size_t)p.S_tot * sizeof(float) + 255) / 256 * 256 : 0;
   uint8_t* pack = nullptr;
-  B2_TRY(ws_alloc((void**)&pack, pack_bytes + gt_bytes, stream, kEfeName));
+  B2_TRY(ws_alloc((void**)&pack, pack_bytes + gt_bytes + qt_bytes, stream, kEfeName));
   double* Gt = tp.tree ? reinterpret_cast<double*>(pack + pack_bytes) : nullptr;
+  float* Qt = tp.tree ? reinterpret_cast<float*>(pack + pack_bytes + gt_bytes) : nullptr;
   int Kmax = 0;
   for (int g = 0; g < tp.G; ++g) Kmax = tp.grp[g].Kpad > Kmax ? tp.grp[g].Kpad : Kmax;
   dim3 pgrid((unsigned)((Kmax + 127) / 128), (unsigned)tp.G, (unsigned)Bn);
   dim3 grid((unsigned)(tp.tree ? tp.tree_tiles[p.T] : (p.P + kTcTile - 1) / kTcTile), (unsigned)Bn);
   efe_tc_pack_kernel<PREC><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
   int32_t rc = check_launch("efe_ffi tc pack");
+  if (rc == B2_OK && tp.tree) {
+    efe_tree_rollout_kernel<<<(unsigned)Bn, 512, 0, stream>>>(p, tp, qs, B, Qt);
+    rc = check_launch("efe_ffi tc tree rollout");
+  }
   if (rc == B2_OK) rc = ensure_smem_attr((const void*)efe_tc_kernel<PREC>, smem, kEfeName);
   if (rc == B2_OK) {
-    efe_tc_kernel<PREC><<<grid, kThreadsAll, smem, stream>>>(p, tp, pm, pm_batched, qs, B, pack, G, Gt);
+    efe_tc_kernel<PREC><<<grid, kThreadsAll, smem, stream>>>(p, tp, pm, pm_batched, qs, B, pack, G, Gt, Qt);
     rc = check_launch("efe_ffi tc");
   }
   if (rc == B2_OK && tp.tree) {
