@@ -156,6 +156,41 @@ int32_t b2_neg_efe(void* stream, const int32_t* policy_matrix, int64_t pm_count,
                    const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
                    const int64_t* B_dep_offsets, int32_t flags);
 
+/* b2_neg_efe with a caller-owned cache of the tensor-core operand images (the
+ * W images packed from A and C). The reference's CUDA path keeps such caches
+ * inside the library, keyed by device pointer, when the caller sets
+ * B2_FLAG_MODEL_PARAMS_STATIC (pymdp/ffi/neg_efe/neg_efe_cuda_entry.cc:40-90);
+ * here the caller owns the buffer and its validity, so a reused address can
+ * never hit a stale entry. When *pack_cache_valid is 0 the call packs A and C
+ * into pack_cache (at least b2_neg_efe_pack_bytes bytes, 256-byte aligned) and
+ * sets *pack_cache_valid to 1; when it is 1 the images are reused. The images
+ * stay valid while A, C, Bn, the model layout and flag bits 0-1 and 8-9 are
+ * unchanged; use the cache on one stream (or order the streams). Calls that
+ * take the SIMT path ignore the cache. */
+int32_t b2_neg_efe_cached(void* stream, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+                          const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
+                          const float* B, int64_t B_count, const float* C, int64_t C_count,
+                          const float* I, int64_t I_count, const float* pA, int64_t pA_count,
+                          const float* pB, int64_t pB_count, const float* inductive_epsilon,
+                          int64_t eps_count, float* neg_efe_out, int64_t out_count, int64_t Bn, int64_t P,
+                          int64_t T, int64_t F, int64_t M, const int64_t* S, const int64_t* O,
+                          const int64_t* U, const int64_t* qs_offsets, const int64_t* A_offsets,
+                          const int64_t* B_offsets, const int64_t* C_offsets, const int64_t* I_offsets,
+                          const int64_t* I_depths, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                          const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
+                          const int64_t* B_dep_offsets, int32_t flags, uint8_t* pack_cache,
+                          int64_t pack_cache_bytes, int32_t* pack_cache_valid);
+
+/* Bytes of the pack cache b2_neg_efe_cached needs for these attributes, Bn and
+ * flags (0 when the call would take the SIMT path). Host only: needs no GPU. */
+int32_t b2_neg_efe_pack_bytes(int64_t Bn, int64_t P, int64_t T, int64_t F, int64_t M, const int64_t* S,
+                              const int64_t* O, const int64_t* U, const int64_t* qs_offsets,
+                              const int64_t* A_offsets, const int64_t* B_offsets, const int64_t* C_offsets,
+                              const int64_t* I_offsets, const int64_t* I_depths, const int64_t* A_dep_flat,
+                              int64_t A_dep_flat_len, const int64_t* A_dep_offsets, const int64_t* B_dep_flat,
+                              int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int32_t flags,
+                              int64_t* bytes);
+
 /* Size of the fixed device scratch behind b2_neg_efe_noalloc (16 MiB). */
 #define B2_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -16,6 +16,8 @@ else.
 
 from __future__ import annotations
 
+import ctypes
+
 from typing import Sequence
 
 import numpy as np
@@ -159,6 +161,16 @@ class Agent:
         self.use_param_info_gain, self.use_inductive = use_param_info_gain, use_inductive
         self.A, self.B, self.C = A, B, C
 
+    def _pack_cache(self, P: int):
+        """The tensor-core operand images of this agent's (immutable) A and C,
+        packed on the first call and reused (``b2_neg_efe_cached``); None
+        when the call takes the SIMT path."""
+        if not hasattr(self, "_pack"):
+            n = self._layout.pack_bytes(self.batch_size, P, self._flags)
+            self._pack = None if n == 0 else (torch.empty(n, dtype=torch.uint8, device=self.device),
+                                              ctypes.c_int32(0))
+        return self._pack
+
     # ------------------------------------------------------------------ API
     def infer_states(self, observations, empirical_prior: Sequence[torch.Tensor]):
         """``pymdp/agent.py:675-823`` (fpi): returns ``qs[f]`` of shape ``(batch, 1, S_f)``.
@@ -191,7 +203,8 @@ class Agent:
         P = self.policies.shape[0]
         G = torch.empty((self.batch_size, P), device=self.device)
         self._layout.call(None, self.policies, 0, qs_flat, self._A_flat, self._B_flat, self._C_flat,
-                          self._I_flat, self._pA_flat, self._pB_flat, self._eps, G, self.batch_size, P, self._flags)
+                          self._I_flat, self._pA_flat, self._pB_flat, self._eps, G, self.batch_size, P, self._flags,
+                          cache=self._pack_cache(P))
         q_pi = ffi.policy_posterior(G, self.E, self.gamma)
         return q_pi, G
 

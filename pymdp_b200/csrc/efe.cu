@@ -475,7 +475,10 @@ int32_t ws_alloc(void** ptr, size_t bytes, cudaStream_t stream, const char* op) 
 
 using namespace b2;
 
-extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+namespace b2 {
+namespace {
+
+int32_t neg_efe_impl(void* stream_, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
                               const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
                               const float* B, int64_t B_count, const float* C, int64_t C_count, const float* I,
                               int64_t I_count, const float* pA, int64_t pA_count, const float* pB,
@@ -486,7 +489,7 @@ extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64
                               const int64_t* C_offsets, const int64_t* I_offsets, const int64_t* I_depths,
                               const int64_t* A_dep_flat, int64_t A_dep_flat_len, const int64_t* A_dep_offsets,
                               const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets,
-                              int32_t flags) {
+                              int32_t flags, const PackCache* cache) {
   cudaStream_t stream = (cudaStream_t)stream_;
   if (Bn < 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": negative Bn");
   EfeParams p;
@@ -576,7 +579,8 @@ extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64
   if (prec != B2_PRECISION_FP32) {
     // tensor-core path; models outside its limits take the SIMT FP32 path
     bool used = false;
-    B2_TRY(launch_efe_tc(p, prec, Bn, policy_matrix, pm_batched, qs_init, A, B, C, neg_efe_out, stream, &used));
+    B2_TRY(launch_efe_tc(p, prec, Bn, policy_matrix, pm_batched, qs_init, A, B, C, neg_efe_out, stream, &used,
+                         cache));
     if (used) return B2_OK;
   }
   float* lin = nullptr;
@@ -587,6 +591,67 @@ extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64
   cudaError_t fe = cudaFreeAsync(lin, stream);
   if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
   return rc;
+}
+
+}  // namespace
+}  // namespace b2
+
+extern "C" int32_t b2_neg_efe(void* stream_, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+                              const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
+                              const float* B, int64_t B_count, const float* C, int64_t C_count, const float* I,
+                              int64_t I_count, const float* pA, int64_t pA_count, const float* pB,
+                              int64_t pB_count, const float* inductive_epsilon, int64_t eps_count,
+                              float* neg_efe_out, int64_t out_count, int64_t Bn, int64_t P, int64_t T, int64_t F,
+                              int64_t M, const int64_t* S, const int64_t* O, const int64_t* U,
+                              const int64_t* qs_offsets, const int64_t* A_offsets, const int64_t* B_offsets,
+                              const int64_t* C_offsets, const int64_t* I_offsets, const int64_t* I_depths,
+                              const int64_t* A_dep_flat, int64_t A_dep_flat_len, const int64_t* A_dep_offsets,
+                              const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets,
+                              int32_t flags) {
+  return neg_efe_impl(stream_, policy_matrix, pm_count, pm_batched, qs_init, qs_count, A, A_count, B, B_count, C, C_count, I,
+                      I_count, pA, pA_count, pB, pB_count, inductive_epsilon, eps_count, neg_efe_out, out_count, Bn, P,
+                      T, F, M, S, O, U, qs_offsets, A_offsets, B_offsets, C_offsets, I_offsets, I_depths, A_dep_flat,
+                      A_dep_flat_len, A_dep_offsets, B_dep_flat, B_dep_flat_len, B_dep_offsets, flags, nullptr);
+}
+
+extern "C" int32_t b2_neg_efe_cached(void* stream_, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
+                              const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
+                              const float* B, int64_t B_count, const float* C, int64_t C_count, const float* I,
+                              int64_t I_count, const float* pA, int64_t pA_count, const float* pB,
+                              int64_t pB_count, const float* inductive_epsilon, int64_t eps_count,
+                              float* neg_efe_out, int64_t out_count, int64_t Bn, int64_t P, int64_t T, int64_t F,
+                              int64_t M, const int64_t* S, const int64_t* O, const int64_t* U,
+                              const int64_t* qs_offsets, const int64_t* A_offsets, const int64_t* B_offsets,
+                              const int64_t* C_offsets, const int64_t* I_offsets, const int64_t* I_depths,
+                              const int64_t* A_dep_flat, int64_t A_dep_flat_len, const int64_t* A_dep_offsets,
+                              const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets,
+                              int32_t flags, uint8_t* pack_cache, int64_t pack_cache_bytes,
+                                     int32_t* pack_cache_valid) {
+  if (!pack_cache || !pack_cache_valid)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": null pack cache");
+  const PackCache cache{pack_cache, pack_cache_bytes, pack_cache_valid};
+  return neg_efe_impl(stream_, policy_matrix, pm_count, pm_batched, qs_init, qs_count, A, A_count, B, B_count, C, C_count, I,
+                      I_count, pA, pA_count, pB, pB_count, inductive_epsilon, eps_count, neg_efe_out, out_count, Bn, P,
+                      T, F, M, S, O, U, qs_offsets, A_offsets, B_offsets, C_offsets, I_offsets, I_depths, A_dep_flat,
+                      A_dep_flat_len, A_dep_offsets, B_dep_flat, B_dep_flat_len, B_dep_offsets, flags, &cache);
+}
+
+extern "C" int32_t b2_neg_efe_pack_bytes(int64_t Bn, int64_t P, int64_t T, int64_t F, int64_t M, const int64_t* S,
+                                         const int64_t* O, const int64_t* U, const int64_t* qs_offsets,
+                                         const int64_t* A_offsets, const int64_t* B_offsets,
+                                         const int64_t* C_offsets, const int64_t* I_offsets,
+                                         const int64_t* I_depths, const int64_t* A_dep_flat,
+                                         int64_t A_dep_flat_len, const int64_t* A_dep_offsets,
+                                         const int64_t* B_dep_flat, int64_t B_dep_flat_len,
+                                         const int64_t* B_dep_offsets, int32_t flags, int64_t* bytes) {
+  if (!bytes || Bn < 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": null bytes or negative Bn");
+  EfeParams p;
+  B2_TRY(build_efe_params(&p, P, T, F, M, S, O, U, qs_offsets, A_offsets, B_offsets, C_offsets, I_offsets,
+                          I_depths, A_dep_flat, A_dep_flat_len, A_dep_offsets, B_dep_flat, B_dep_flat_len,
+                          B_dep_offsets, flags));
+  const bool simt_terms = (flags & (B2_FLAG_USE_PARAM_INFO_GAIN | B2_FLAG_USE_INDUCTIVE)) != 0;
+  *bytes = simt_terms ? 0 : efe_tc_pack_bytes(p, (flags >> B2_PRECISION_SHIFT) & 3, Bn);
+  return B2_OK;
 }
 
 extern "C" int32_t b2_policy_posterior(void* stream, const float* neg_efe, const float* E, int32_t E_batched,

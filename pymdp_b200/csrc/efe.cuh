@@ -58,7 +58,17 @@ int32_t launch_efe_plain(const EfeParams& p, int64_t Bn, const int32_t* pm, int 
 int32_t ws_alloc(void** ptr, size_t bytes, cudaStream_t stream, const char* op);
 // Tensor-core path (efe_tc.cu); *used = false when the model is outside its
 // limits and nothing was launched.
+// Caller-owned cache of the tensor-core operand images (b2_neg_efe_cached).
+struct PackCache {
+  uint8_t* buf;
+  int64_t bytes;
+  int32_t* valid;  // host flag: 0 = pack into buf (then set to 1), 1 = reuse
+};
 int32_t launch_efe_tc(const EfeParams& p, int prec, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
-                      const float* A, const float* B, const float* C, float* G, cudaStream_t stream, bool* used);
+                      const float* A, const float* B, const float* C, float* G, cudaStream_t stream, bool* used,
+                      const PackCache* cache = nullptr);
+// Bytes of the tensor-core operand images for Bn agents at precision prec
+// (0 when the model takes the SIMT path).
+int64_t efe_tc_pack_bytes(const EfeParams& p, int prec, int64_t Bn);
 
 }  // namespace b2

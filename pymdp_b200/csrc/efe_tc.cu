@@ -1164,7 +1164,8 @@ int32_t tc_plan_t(const EfeParams& p, TcParams* tp, int* smem_bytes) {
 
 template <int PREC>
 int32_t launch_tc_t(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
-                    const float* A, const float* B, const float* C, float* G, cudaStream_t stream, bool* used) {
+                    const float* A, const float* B, const float* C, float* G, cudaStream_t stream, bool* used,
+                    const PackCache* cache) {
   TcParams tp;
   int smem = 0;
   if (tc_plan_t<PREC>(p, &tp, &smem) != B2_OK) return B2_OK;
@@ -1189,20 +1190,31 @@ int32_t launch_tc_t(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_ba
       if ((double)tp.tree_off[p.T - 1] * p.S_tot >= 2.0e9) tp.tree = 0;
     }
   }
-  const size_t pack_bytes = (size_t)Bn * (size_t)tp.pack_stride;
+  if (cache && (reinterpret_cast<uintptr_t>(cache->buf) & 255u) != 0)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": pack cache must be 256-byte aligned");
+  if (cache && cache->bytes < Bn * tp.pack_stride)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": pack cache of " + std::to_string(cache->bytes) +
+                                             " bytes, needs " + std::to_string(Bn * tp.pack_stride));
+  const size_t pack_bytes = cache ? 0 : (size_t)Bn * (size_t)tp.pack_stride;
   const size_t gt_bytes = tp.tree ? (size_t)Bn * (size_t)tp.tree_off[p.T] * sizeof(double) : 0;
   const size_t qt_bytes =
       tp.tree ? ((size_t)Bn * (size_t)tp.tree_off[p.T - 1] * (size_t)p.S_tot * sizeof(float) + 255) / 256 * 256 : 0;
-  uint8_t* pack = nullptr;
-  B2_TRY(ws_alloc((void**)&pack, pack_bytes + gt_bytes + qt_bytes, stream, kEfeName));
-  double* Gt = tp.tree ? reinterpret_cast<double*>(pack + pack_bytes) : nullptr;
-  float* Qt = tp.tree ? reinterpret_cast<float*>(pack + pack_bytes + gt_bytes) : nullptr;
+  uint8_t* ws = nullptr;
+  if (pack_bytes + gt_bytes + qt_bytes > 0)
+    B2_TRY(ws_alloc((void**)&ws, pack_bytes + gt_bytes + qt_bytes, stream, kEfeName));
+  uint8_t* pack = cache ? cache->buf : ws;
+  double* Gt = tp.tree ? reinterpret_cast<double*>(ws + pack_bytes) : nullptr;
+  float* Qt = tp.tree ? reinterpret_cast<float*>(ws + pack_bytes + gt_bytes) : nullptr;
   int Kmax = 0;
   for (int g = 0; g < tp.G; ++g) Kmax = tp.grp[g].Kpad > Kmax ? tp.grp[g].Kpad : Kmax;
   dim3 pgrid((unsigned)((Kmax + 127) / 128), (unsigned)tp.G, (unsigned)Bn);
   dim3 grid((unsigned)(tp.tree ? tp.tree_tiles[p.T] : (p.P + kTcTile - 1) / kTcTile), (unsigned)Bn);
-  efe_tc_pack_kernel<PREC><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
-  int32_t rc = check_launch("efe_ffi tc pack");
+  int32_t rc = B2_OK;
+  if (!cache || *cache->valid == 0) {
+    efe_tc_pack_kernel<PREC><<<pgrid, 128, 0, stream>>>(p, tp, A, C, pack);
+    rc = check_launch("efe_ffi tc pack");
+    if (rc == B2_OK && cache) *cache->valid = 1;
+  }
   if (rc == B2_OK && tp.tree) {
     efe_tree_rollout_kernel<<<(unsigned)Bn, 512, 0, stream>>>(p, tp, qs, B, Qt);
     rc = check_launch("efe_ffi tc tree rollout");
@@ -1217,20 +1229,31 @@ int32_t launch_tc_t(const EfeParams& p, int64_t Bn, const int32_t* pm, int pm_ba
                                                                                                    G);
     rc = check_launch("efe_ffi tc tree combine");
   }
-  cudaError_t fe = cudaFreeAsync(pack, stream);
-  if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
+  if (ws) {
+    cudaError_t fe = cudaFreeAsync(ws, stream);
+    if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
+  }
   *used = rc == B2_OK;
   return rc;
 }
 
+int64_t efe_tc_pack_bytes(const EfeParams& p, int prec, int64_t Bn) {
+  TcParams tp;
+  int smem = 0;
+  if (Bn > 65535 || (prec != B2_PRECISION_BF16 && prec != B2_PRECISION_TF32X3)) return 0;
+  const int32_t rc = prec == B2_PRECISION_BF16 ? tc_plan_t<B2_PRECISION_BF16>(p, &tp, &smem)
+                                               : tc_plan_t<B2_PRECISION_TF32X3>(p, &tp, &smem);
+  return rc == B2_OK ? Bn * tp.pack_stride : 0;
+}
+
 int32_t launch_efe_tc(const EfeParams& p, int prec, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
                       const float* A, const float* B, const float* C, float* G, cudaStream_t stream,
-                      bool* used) {
+                      bool* used, const PackCache* cache) {
   *used = false;
   if (Bn > 65535) return B2_OK;
   if (prec == B2_PRECISION_BF16)
-    return launch_tc_t<B2_PRECISION_BF16>(p, Bn, pm, pm_batched, qs, A, B, C, G, stream, used);
-  return launch_tc_t<B2_PRECISION_TF32X3>(p, Bn, pm, pm_batched, qs, A, B, C, G, stream, used);
+    return launch_tc_t<B2_PRECISION_BF16>(p, Bn, pm, pm_batched, qs, A, B, C, G, stream, used, cache);
+  return launch_tc_t<B2_PRECISION_TF32X3>(p, Bn, pm, pm_batched, qs, A, B, C, G, stream, used, cache);
 }
 
 }  // namespace b2

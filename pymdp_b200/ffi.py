@@ -13,6 +13,8 @@ over the batch internally (one launch per call).
 
 from __future__ import annotations
 
+import ctypes
+
 from typing import Sequence
 
 import numpy as np
@@ -277,7 +279,19 @@ class EfeLayout:
                                     self.C_offsets, self.I_offsets, self.I_depths, self.A_dep_flat,
                                     self.A_dep_offsets, self.B_dep_flat, self.B_dep_offsets)]
 
-    def call(self, stream, pm, pm_batched, qs, A, B, C, I, pA, pB, eps, out, Bn, P, flags):
+    def pack_bytes(self, Bn: int, P: int, flags: int) -> int:
+        """Bytes of the tensor-core pack cache (``b2_neg_efe_pack_bytes``)."""
+        c = self._c
+        n = ctypes.c_int64(0)
+        check(_lib.load().b2_neg_efe_pack_bytes(
+            int(Bn), int(P), self.T, self.F, self.M, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9],
+            len(self.A_dep_flat), c[10], c[11], len(self.B_dep_flat), c[12], int(flags), ctypes.byref(n)))
+        return int(n.value)
+
+    def call(self, stream, pm, pm_batched, qs, A, B, C, I, pA, pB, eps, out, Bn, P, flags, cache=None):
+        """``b2_neg_efe``; with ``cache = (uint8 device tensor, ctypes.c_int32
+        valid flag)`` the tensor-core operand images are packed once and
+        reused (``b2_neg_efe_cached``)."""
         c = self._c
         for t in (pm, qs, A, B, C, I, pA, pB, eps, out):
             if t is not None:
@@ -286,11 +300,16 @@ class EfeLayout:
             stream = _stream(out)
         ptr = (lambda t: 0 if t is None else t.data_ptr())
         cnt = (lambda t: 0 if t is None else t.numel())
-        check(_lib.load().b2_neg_efe(
-            stream, ptr(pm), cnt(pm), int(pm_batched), ptr(qs), cnt(qs), ptr(A), cnt(A), ptr(B), cnt(B), ptr(C),
-            cnt(C), ptr(I), cnt(I), ptr(pA), cnt(pA), ptr(pB), cnt(pB), ptr(eps), cnt(eps), ptr(out), cnt(out),
-            int(Bn), int(P), self.T, self.F, self.M, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9],
-            len(self.A_dep_flat), c[10], c[11], len(self.B_dep_flat), c[12], int(flags)))
+        args = (stream, ptr(pm), cnt(pm), int(pm_batched), ptr(qs), cnt(qs), ptr(A), cnt(A), ptr(B), cnt(B), ptr(C),
+                cnt(C), ptr(I), cnt(I), ptr(pA), cnt(pA), ptr(pB), cnt(pB), ptr(eps), cnt(eps), ptr(out), cnt(out),
+                int(Bn), int(P), self.T, self.F, self.M, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9],
+                len(self.A_dep_flat), c[10], c[11], len(self.B_dep_flat), c[12], int(flags))
+        if cache is None:
+            check(_lib.load().b2_neg_efe(*args))
+        else:
+            buf, valid = cache
+            _require_cuda(buf, "pack cache")
+            check(_lib.load().b2_neg_efe_cached(*args, buf.data_ptr(), buf.numel(), ctypes.byref(valid)))
 
 
 def neg_efe_all_policies_ffi(policy_matrix, qs_init, A, B, C, I, A_dependencies, B_dependencies, *,

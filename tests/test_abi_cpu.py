@@ -175,3 +175,17 @@ def test_fit_model_multiaction_map_matches_oracle():
         got = (torch.as_tensor(q, dtype=torch.float32) @ fm.policy_to_multi).numpy()
         ref = ofit.multiaction_probabilities(q, fm.policies.numpy(), U)
         np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
+
+
+def test_neg_efe_pack_bytes_host_query():
+    """b2_neg_efe_pack_bytes plans the tensor-core operand images on the host:
+    positive for the tensor-core precisions, 0 where the SIMT path runs."""
+    from pymdp_b200 import ffi
+    lay = ffi.EfeLayout([32, 16, 8], [16, 16, 8, 8, 4], [4, 4, 1], 3, [[0, 1, 2]] * 5, [[0], [1], [2]])
+    P = 16 ** 3
+    n_tf = lay.pack_bytes(4, P, ffi.efe_flags(precision="tf32x3"))
+    n_bf = lay.pack_bytes(4, P, ffi.efe_flags(precision="bf16"))
+    assert n_tf > n_bf > 0 and n_tf % 4 == 0 and n_bf % 4 == 0
+    assert lay.pack_bytes(8, P, ffi.efe_flags(precision="bf16")) == 2 * n_bf
+    assert lay.pack_bytes(4, P, ffi.efe_flags(precision="fp32")) == 0
+    assert lay.pack_bytes(4, P, ffi.efe_flags(use_inductive=True, precision="bf16")) == 0

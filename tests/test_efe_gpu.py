@@ -276,3 +276,43 @@ def test_policy_tree_matches_oracle_and_full_evaluation(case, precision):
                                         [c[b] for c in C], case["A_deps"], case["B_deps"])
         _g_close(G_tree[b], ref, precision)
         _g_close(G_full[b], ref, precision)
+
+
+@pytest.mark.parametrize("precision", ["tf32x3", "bf16"])
+def test_pack_cache_reuses_operand_images(precision):
+    """b2_neg_efe_cached: the first call packs (and sets the valid flag), the
+    second reuses the images; both equal b2_neg_efe bit for bit. Clearing the
+    flag after A changes repacks."""
+    import ctypes
+    from pymdp_b200 import ffi
+    case = dict(S=[9, 7, 5], O=[11, 3, 6], U=[4, 3, 1], T=2, A_deps=[[0, 1, 2], [0, 1, 2], [2, 0]],
+                B_deps=[[0], [1], [2]])
+    rng = np.random.default_rng(5)
+    batch = 3
+    A, B, C, qs = random_efe(rng, case["S"], case["O"], case["U"], case["T"], case["A_deps"], case["B_deps"], batch)
+    pol = torch.as_tensor(oefe.construct_policies(case["S"], case["U"], case["T"]), device="cuda").int().contiguous()
+    P = pol.shape[0]
+    lay = ffi.EfeLayout(case["S"], case["O"], case["U"], case["T"], case["A_deps"], case["B_deps"])
+    flat = lambda xs: ffi.flatten_ragged_f32([cuda(x) for x in xs], 1)[0]  # noqa: E731
+    qs_f, A_f, B_f, C_f = flat(qs), flat(A), flat(B), flat([np.repeat(c[:, None, :], case["T"], 1) for c in C])
+    I_f = torch.zeros((batch, int(lay.I_offsets[-1])), device="cuda")
+    eps = torch.full((1,), 1e-3, device="cuda")
+    flags = ffi.efe_flags(precision=precision, policy_tree=True)
+
+    def run(cache=None):
+        out = torch.empty((batch, P), device="cuda")
+        lay.call(None, pol, 0, qs_f, A_f, B_f, C_f, I_f, None, None, eps, out, batch, P, flags, cache=cache)
+        return out.cpu().numpy()
+
+    n = lay.pack_bytes(batch, P, flags)
+    assert n > 0
+    cache = (torch.empty(n, dtype=torch.uint8, device="cuda"), ctypes.c_int32(0))
+    ref = run()
+    first = run(cache)
+    assert cache[1].value == 1
+    second = run(cache)
+    np.testing.assert_array_equal(first, ref)
+    np.testing.assert_array_equal(second, ref)
+    A_f.mul_(0.5).add_(0.5 / 11)  # a different (still normalised for modality 0) A: repack
+    cache[1].value = 0
+    np.testing.assert_array_equal(run(cache), run())
