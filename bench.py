@@ -503,6 +503,8 @@ def run_b200(args, rank, world, local_rank):
             "agents": sample,
             "qs_max_rel": max(_max_rel(qs_g[f][b], ref[b][0][f], 1e-6) for b in range(sample) for f in range(len(S))),
             "G_max_rel": max(_max_rel(G_g[b], ref[b][1], 1e-6) for b in range(sample)),
+            "G_max_abs_over_max_G": max(float(np.max(np.abs(np.asarray(G_g[b], np.float64) - ref[b][1]))
+                                            / np.max(np.abs(ref[b][1]))) for b in range(sample)),
             "q_pi_max_abs": max(float(np.max(np.abs(q_pi_g[b] - ref[b][2]))) for b in range(sample)),
             "actions_equal": int(sum(bool(np.array_equal(act_g[b], ref[b][3])) for b in range(sample))),
         }
