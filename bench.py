@@ -349,6 +349,19 @@ def _max_rel(got, ref, floor):
     return float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), floor)))
 
 
+def reduce_max_over_ranks(values, world: int, device="cpu") -> list:
+    """Max over ranks of per-rank timings: the job takes as long as its slowest
+    rank (every rank calls this, in the same order)."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -402,8 +415,10 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     fpi_res = run_fpi_config(dev, args.steps, args.warmup, flush)
-    fit_res = run_fit_config(dev, args.steps, args.warmup, flush) if args.legs == "all" else None
-    ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if args.legs == "all" else None
+    # the fitting and rollout workloads are single-GPU measurements: run with N = 1 only
+    extras = args.legs == "all" and world == 1
+    fit_res = run_fit_config(dev, args.steps, args.warmup, flush) if extras else None
+    ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if extras else None
     efe_ev = []
 
     def step(timed_efe=False):
@@ -471,10 +486,7 @@ def run_b200(args, rank, world, local_rank):
     e2e_ms = ev0.elapsed_time(ev1)
     h2d = obs_h.numel() * 4 + sum(x.numel() * 4 for x in prior_h)
     d2h = act_h.numel() * 4
-    t = torch.tensor([ms, e2e_ms, efe_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms, efe_ms = [float(x) for x in t.tolist()]
+    ms, e2e_ms, efe_ms = reduce_max_over_ranks([ms, e2e_ms, efe_ms], world, dev)
     if rank != 0:
         return
     import json as _json
