@@ -583,6 +583,13 @@ int32_t neg_efe_impl(void* stream_, const int32_t* policy_matrix, int64_t pm_cou
                          cache));
     if (used) return B2_OK;
   }
+  {
+    // small models: all of an agent's policies in one CTA
+    bool used = false;
+    B2_TRY(launch_efe_small(p, Bn, false, policy_matrix, pm_batched, qs_init, A, B, C, neg_efe_out, nullptr,
+                            nullptr, nullptr, nullptr, nullptr, stream, &used));
+    if (used) return B2_OK;
+  }
   float* lin = nullptr;
   const size_t bytes = (size_t)Bn * p.T * p.K_tot * sizeof(float);
   B2_TRY(ws_alloc((void**)&lin, bytes, stream, kEfeName));

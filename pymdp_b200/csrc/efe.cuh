@@ -58,6 +58,14 @@ int32_t launch_efe_plain(const EfeParams& p, int64_t Bn, const int32_t* pm, int 
 int32_t ws_alloc(void** ptr, size_t bytes, cudaStream_t stream, const char* op);
 // Tensor-core path (efe_tc.cu); *used = false when the model is outside its
 // limits and nothing was launched.
+// Small-model path (efe_small.cu): one CTA per agent with every policy's
+// roll-out in shared memory; used when that working set fits kEfeSmallMaxSmem.
+constexpr int64_t kEfeSmallMaxSmem = 96 * 1024;
+int64_t efe_small_smem_bytes(const EfeParams& p);
+int32_t launch_efe_small(const EfeParams& p, int64_t Bn, bool bwd, const int32_t* pm, int pm_batched,
+                         const float* qs, const float* A, const float* B, const float* C, float* G, const float* dG,
+                         float* dqs, float* dA, float* dB, float* dC, cudaStream_t stream, bool* used);
+
 // Caller-owned cache of the tensor-core operand images (b2_neg_efe_cached).
 struct PackCache {
   uint8_t* buf;

@@ -209,7 +209,8 @@ extern "C" int32_t b2_neg_efe_bwd(void* stream_, const int32_t* policy_matrix, i
     if (c.actual != c.expected)
       return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": " + c.name + " element_count = " +
                                                std::to_string(c.actual) + ", expected " + std::to_string(c.expected));
-  if ((int64_t)(T + 1) * p.S_tot > kBwdMaxHist)
+  const bool small = efe_small_smem_bytes(p) <= kEfeSmallMaxSmem;
+  if (!small && (int64_t)(T + 1) * p.S_tot > kBwdMaxHist)
     return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": (T + 1) * total states exceeds " +
                                         std::to_string(kBwdMaxHist));
   if (Bn == 0) return B2_OK;
@@ -221,6 +222,12 @@ extern "C" int32_t b2_neg_efe_bwd(void* stream_, const int32_t* policy_matrix, i
   B2_CUDA_TRY(op, cudaMemsetAsync(d_A, 0, (size_t)Bn * p.A_stride * sizeof(float), stream));
   B2_CUDA_TRY(op, cudaMemsetAsync(d_B, 0, (size_t)Bn * p.B_stride * sizeof(float), stream));
   B2_CUDA_TRY(op, cudaMemsetAsync(d_C, 0, (size_t)Bn * p.C_stride * sizeof(float), stream));
+  if (small) {
+    bool used = false;
+    B2_TRY(launch_efe_small(p, Bn, true, policy_matrix, pm_batched, qs_init, A, B, C, nullptr, d_neg_efe, d_qs_init,
+                            d_A, d_B, d_C, stream, &used));
+    if (used) return B2_OK;
+  }
   dim3 grid((unsigned)((P + 127) / 128), (unsigned)Bn);
   efe_bwd_kernel<<<grid, 128, 0, stream>>>(p, policy_matrix, pm_batched, qs_init, A, B, C, d_neg_efe, d_qs_init,
                                            d_A, d_B, d_C);
