@@ -188,15 +188,27 @@ def tile_cost(spec: AgentSpec, p_lo: int, p_hi: int) -> float:
     return cost
 
 
-def make_tiles(specs: Sequence[AgentSpec], cols: int) -> np.ndarray:
+def make_tiles(specs: Sequence[AgentSpec], cols: int, balance_tiles: int | None = None) -> np.ndarray:
     """Cut each agent's reduced policies into tiles of at most ``cols``
     policies (with round_up(width, 8) x S_tot within the shared-memory
-    prefix table), largest cost first. Returns ``(n_tiles, 4)`` int32 rows
+    prefix table), largest cost first. With ``balance_tiles``, an agent whose
+    policies cost more than (total cost / balance_tiles) per tile gets
+    narrower tiles, so no tile dominates a step (off by default: on the
+    2000-agent workload, balancing to 1776 tiles cut the costliest tile 5x but
+    made the rollout 25% slower, as narrow tiles share fewer prefixes and
+    carry more fixed cost). Returns ``(n_tiles, 4)`` int32 rows
     ``(agent, p_lo, p_hi, 0)``."""
+    target = None
+    if balance_tiles:
+        total = sum(tile_cost(sp, 0, sp.num_reduced_policies) for sp in specs)
+        target = total / float(balance_tiles)
     rows, costs = [], []
     for i, sp in enumerate(specs):
         P, St = sp.num_reduced_policies, int(sum(sp.S))
         width = max(1, min(int(cols), P, _lib.RO_TAB_FLOATS // St // 8 * 8))
+        if target is not None:
+            per_policy = tile_cost(sp, 0, P) / P
+            width = max(1, min(width, int(target // max(per_policy, 1e-9))))
         for lo in range(0, P, width):
             hi = min(P, lo + width)
             rows.append((i, lo, hi, 0))
