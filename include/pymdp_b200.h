@@ -285,7 +285,8 @@ int32_t b2_select_action(void* stream, const float* q_pi, const int32_t* policy_
  *   env    = state' ~ B[:, state, action], obs' ~ A[:, state'] (envs/env.py:
  *            333-400); the environment's draws use a counter-based generator
  *            (SplitMix64 over seed, agent, step, stream), not JAX's PRNG.
- * Transitions are factor-local: B_f is [S_f, S_f, U_f]. Policies are all
+ * Transitions are factor-local: B_f[next, prev, u], stored action-major (see
+ * b2_ro_agent.B_off). Policies are all
  * prod(U)^T action sequences in the order of control.construct_policies
  * (control.py:152-195). */
 #define B2_RO_MAX_F 4
@@ -320,7 +321,9 @@ typedef struct b2_ro_agent {
   int32_t dstride[B2_RO_MAX_M][B2_RO_MAX_F]; /* stride of each dep axis in K  */
   int64_t A_off[B2_RO_MAX_M]; /* [A_m; lin_m]: (O_m + 1) x K_m, row-major     */
   int64_t C_off[B2_RO_MAX_M]; /* C_m: O_m log-preferences                     */
-  int64_t B_off[B2_RO_MAX_F]; /* B_f: S_f x S_f x U_f                          */
+  int64_t B_off[B2_RO_MAX_F]; /* B_f stored U_f x S_f x S_f (action, previous
+                                 state, next state): B[next, prev, u] at
+                                 (u * S_f + prev) * S_f + next                 */
   int64_t D_off;              /* S_tot                                         */
   int64_t ll_off;             /* sum_K doubles of scratch                      */
   int64_t qs_base;            /* S_tot entries of qs / qs64                    */

@@ -430,7 +430,7 @@ __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent,
   int* s_next = s_act + kF;
   if (tid < ag.F) {
     const int f = tid, S = ag.S[f], U = ag.U[f];
-    s_next[f] = ro_categorical(a.buf.B + ag.B_off[f] + (int64_t)s_state[f] * U + s_act[f], S, (int64_t)S * U,
+    s_next[f] = ro_categorical(a.buf.B + ag.B_off[f] + ((int64_t)s_act[f] * S + s_state[f]) * S, S, 1,
                                ro_u01(a.seed, agent, hstep, 128 + f));
   }
   __syncthreads();
@@ -443,9 +443,10 @@ __device__ void ro_step_agent(const RoArgs& a, const b2_ro_agent& ag, int agent,
   const double* qs64 = a.buf.qs64 + ag.qs_base;
   for (int j = tid; j < ag.S_tot; j += NT) {
     const int f = ro_factor_of(ag, j), S = ag.S[f], U = ag.U[f], s = j - ag.qs_off[f];
-    const float* Bf = a.buf.B + ag.B_off[f] + (int64_t)s * S * U + s_act[f];
+    (void)U;
+    const float* Bf = a.buf.B + ag.B_off[f] + (int64_t)s_act[f] * S * S + s;
     double acc = 0.0;
-    for (int s2 = 0; s2 < S; ++s2) acc = fma((double)Bf[(int64_t)s2 * U], qs64[ag.qs_off[f] + s2], acc);
+    for (int s2 = 0; s2 < S; ++s2) acc = fma((double)Bf[(int64_t)s2 * S], qs64[ag.qs_off[f] + s2], acc);
     sm[j] = log(fmax(acc, kMinValD));
   }
   __syncthreads();
@@ -638,6 +639,80 @@ __device__ void ro_contract(const RoArgs& a, const b2_ro_agent& ag, int m, const
   __syncthreads();
 }
 
+// The same contraction for narrow tiles (n <= NCOL <= 8 columns): warps own
+// 8-row groups and stream A straight from global memory, lanes over k
+// (coalesced along the rows), with no shared-memory chunks or barriers inside
+// the loop; each lane forms x[k, c] = w[po, c] q_c[dep_last][s] itself.
+// Partial sums combine by shuffles and shared-memory atomics into sOut.
+template <int NT, bool BF16, int NCOL>
+__device__ void ro_contract_narrow(const RoArgs& a, const b2_ro_agent& ag, int m, const float* tab, int NC, int n,
+                                   const TileSmem& s) {
+  constexpr int NW = NT / 32;
+  const int K = ag.K[m], R = ag.O[m] + 1, r = ag.rank[m];
+  const int f_in = ag.dep[m][r - 1], S_in = ag.S[f_in];
+  const float* xin = tab + ag.qs_off[f_in] * NC;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int RG8 = (R + 7) >> 3;
+  const int KS = NW >= RG8 ? NW / RG8 : 1;  // k splits per row group
+  const float* Am = a.buf.Aprime + ag.A_off[m];
+  const __nv_bfloat16* Ab = BF16 ? reinterpret_cast<const __nv_bfloat16*>(a.buf.Aprime_bf16) + ag.A_off[m] : nullptr;
+  int qo[kF - 1], So[kF - 1], ro[kF - 1];
+#pragma unroll
+  for (int i = 0; i < kF - 1; ++i) {
+    const bool on = i < r - 1;
+    qo[i] = on ? ag.qs_off[ag.dep[m][i]] : 0;
+    So[i] = on ? ag.S[ag.dep[m][i]] : 1;
+    ro[i] = on ? ag.dstride[m][i] / S_in : 1;
+  }
+  for (int e = tid; e < kRpad * kCols; e += NT) s.sOut[e] = 0.f;
+  __syncthreads();
+  for (int item = warp; item < RG8 * KS; item += NW) {
+    const int rg8 = item % RG8, ks = item / RG8;
+    float acc[8][NCOL];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int c = 0; c < NCOL; ++c) acc[i][c] = 0.f;
+    for (int k = ks * 32 + lane; k < K; k += 32 * KS) {
+      const int po = k / S_in, si = k - po * S_in;
+      float xv[NCOL];
+#pragma unroll
+      for (int c = 0; c < NCOL; ++c) xv[c] = c < n ? xin[si * NC + c] : 0.f;
+      if (r > 1) {
+#pragma unroll
+        for (int i = 0; i < kF - 1; ++i)
+          if (i < r - 1) {
+            const float* row = tab + (qo[i] + (po / ro[i]) % So[i]) * NC;
+#pragma unroll
+            for (int c = 0; c < NCOL; ++c) xv[c] *= c < n ? row[c] : 0.f;
+          }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int row = 8 * rg8 + i;
+        float av = 0.f;
+        if (row < R) {
+          const int64_t g = (int64_t)row * K + k;
+          av = (BF16 && row + 1 < R) ? __bfloat162float(Ab[g]) : __ldg(Am + g);
+        }
+#pragma unroll
+        for (int c = 0; c < NCOL; ++c) acc[i][c] = fmaf(av, xv[c], acc[i][c]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int c = 0; c < NCOL; ++c) {
+        float v = acc[i][c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        const int row = 8 * rg8 + i;
+        if (lane == 0 && row < R && c < n) atomicAdd(&s.sOut[row * kCols + c], v);
+      }
+  }
+  __syncthreads();
+}
+
 // neg-EFE of reduced policies [p_lo, p_hi) of one agent (control.py:604-690).
 template <int NT, int KC, bool BF16>
 __device__ void ro_tile(const RoArgs& a, const b2_ro_agent& ag, const b2_ro_tile& tile, unsigned char* smem) {
@@ -663,10 +738,10 @@ __device__ void ro_tile(const RoArgs& a, const b2_ro_agent& ag, const b2_ro_tile
         if (!((ag.obs_mask >> f) & 1)) continue;  // unobserved: never read
         const int S = ag.S[f], U = ag.U[f], sj = j - ag.qs_off[f];
         const int u = (mu / ag.ustride_r[f]) % U;
-        const float* Bf = a.buf.B + ag.B_off[f] + (int64_t)sj * S * U + u;
+        const float* Bf = a.buf.B + ag.B_off[f] + (int64_t)u * S * S + sj;  // lanes: consecutive next states
         const float* pf = prev + ag.qs_off[f] * NC + pc;
         float acc = 0.f;
-        for (int s2 = 0; s2 < S; ++s2) acc = fmaf(__ldg(Bf + (int64_t)s2 * U), pf[s2 * NC], acc);
+        for (int s2 = 0; s2 < S; ++s2) acc = fmaf(__ldg(Bf + (int64_t)s2 * S), pf[s2 * NC], acc);
         cur[j * NC + c] = acc;
       }
     }
@@ -674,7 +749,9 @@ __device__ void ro_tile(const RoArgs& a, const b2_ro_agent& ag, const b2_ro_tile
     __syncthreads();
     for (int m = 0; m < ag.M; ++m) {
       if (n <= 4)
-        ro_contract<NT, KC, BF16, 4>(a, ag, m, cur, NC, n, s);
+        ro_contract_narrow<NT, BF16, 4>(a, ag, m, cur, NC, n, s);
+      else if (n <= 8)
+        ro_contract_narrow<NT, BF16, 8>(a, ag, m, cur, NC, n, s);
       else
         ro_contract<NT, KC, BF16, 8>(a, ag, m, cur, NC, n, s);
       const int O = ag.O[m];

@@ -271,7 +271,9 @@ class UnevenRollout:
                 nC += c.size
             for b in sp.B:
                 offs["B"].append(nB)
-                B_parts.append(b.reshape(-1))
+                # stored action-major: [u][prev][next], so a transition column and
+                # a roll-out row are contiguous
+                B_parts.append(np.ascontiguousarray(b.transpose(2, 1, 0)).reshape(-1))
                 nB += b.size
             offs["D"] = nD
             D_parts.append(np.concatenate(sp.D))
