@@ -269,6 +269,22 @@ int32_t b2_select_action(void* stream, const float* q_pi, const int32_t* policy_
                          int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F);
 
 
+/* Action selection with the reference's modes (pymdp/agent.py:939-967):
+ * sampling_mode 0 = "full" (a policy, then its first step: control.py:115-150),
+ * 1 = "marginal" (per control factor, from its first-step action marginal:
+ * control.py:42-113; marginal mode needs U, host int64 [F], each <= 1024);
+ * action_selection 0 = deterministic (first maximum), 1 = stochastic (a draw
+ * from the categorical with logits alpha * log clip(x), by the Gumbel-max
+ * trick, with uniforms from SplitMix64 over (seed, agent, factor, index): a
+ * different generator from JAX's, and one stream per factor where the
+ * reference reuses one key for every factor). policy_matrix [P, T, F] int32
+ * (shared); alpha: device [Bn] (alpha_batched = 1) or a single value (read
+ * only when stochastic); action [Bn, F] int32. */
+#define B2_SAMPLE_MAX_U 1024
+int32_t b2_sample_action(void* stream, const float* q_pi, const int32_t* policy_matrix, const int64_t* U,
+                         int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F, int32_t sampling_mode,
+                         int32_t action_selection, const float* alpha, int32_t alpha_batched, uint64_t seed);
+
 /* ------------------------------------------------------ uneven-size rollout
  * Closed-loop rollout of many agents of DIFFERENT sizes in one persistent
  * launch. Replaces, for inference_algo="fpi", no learning and deterministic

@@ -182,3 +182,41 @@ def update_posterior_policies(policies, qs_init, A, B, C, E, A_deps, B_deps, gam
 def sample_policy(policies, q_pi):
     """``control.py:115-150`` deterministic branch: first argmax, first step."""
     return np.asarray(policies)[int(np.argmax(q_pi)), 0]
+
+
+def get_marginals(q_pi, policies, num_controls):
+    """``control.py:42-67``: first-step action marginals, one per factor."""
+    policies = np.asarray(policies)
+    q_pi = np.asarray(q_pi, np.float64)
+    return [np.array([q_pi[policies[:, 0, f] == a].sum() for a in range(int(u))])
+            for f, u in enumerate(num_controls)]
+
+
+def sample_action_marginal(policies, num_controls, q_pi):
+    """Deterministic ``sample_action`` (``control.py:69-113``): first maximum
+    of each factor's marginal."""
+    return np.array([int(np.argmax(m)) for m in get_marginals(q_pi, policies, num_controls)])
+
+
+def gumbel(seed, agent, factor, index):
+    """Gumbel(0, 1) noise of the CUDA kernel's counter-based generator:
+    u = (top 24 bits of SplitMix64 over (seed, agent, factor, index) + 0.5)
+    / 2^24, g = -log(-log u)."""
+    from .rollout import MASK, sm64
+    h = sm64(seed & MASK)
+    h = sm64(h ^ (agent & MASK))
+    for x in (factor, index):
+        h = sm64(h ^ (x & 0xFFFFFFFF))
+    u = (np.float32(h >> 40) + np.float32(0.5)) * np.float32(1.0 / 16777216.0)
+    return -np.log(-np.log(np.float64(u)))
+
+
+def sample_stochastic(logits_base, alpha, seed, agent, factor):
+    """Gumbel-max draw from the categorical with logits alpha * log clip(x)
+    (the method of jax.random.categorical), with the kernel's noise. Returns
+    (index, gap between the two largest perturbed logits)."""
+    x = np.asarray(logits_base, np.float64)
+    z = alpha * log_stable(x) + np.array([gumbel(seed, agent, factor, i) for i in range(len(x))])
+    top = np.sort(z)
+    gap = top[-1] - top[-2] if len(top) > 1 else np.inf
+    return int(np.argmax(z)), gap

@@ -90,6 +90,8 @@ _SIGS = {
     "b2_neg_efe_pack_bytes": (c_int32, [c_int64, c_int64, c_int64, c_int64, c_int64, _P64, _P64, _P64, _P64, _P64,
                                         _P64, _P64, _P64, _P64, _P64, c_int64, _P64, _P64, c_int64, _P64, c_int32,
                                         POINTER(c_int64)]),
+    "b2_sample_action": (c_int32, [c_void_p, _PF, c_void_p, _P64, c_void_p, c_int64, c_int64, c_int64, c_int64,
+                                   c_int32, c_int32, _PF, c_int32, c_uint64]),
     "b2_rollout_setup": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int32]),
     "b2_rollout": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_int32,
                              c_int32, c_void_p]),

@@ -3,7 +3,7 @@
 Keeps the signatures and return shapes of ``Agent.infer_states``
 (``pymdp/agent.py:675-823``), ``Agent.infer_policies`` (``:853-906``) and
 ``Agent.sample_action`` (``:939-967``) for ``inference_algo="fpi"``,
-``sampling_mode="full"`` and deterministic action selection, with the
+either ``sampling_mode`` and either action selection, with the
 batch-broadcasting rules of ``pymdp/agent.py:228-330`` (unbatched A/B/C/D/E
 are broadcast to ``batch_size``; defaults C = uniform 1/O, D = uniform,
 E = uniform).
@@ -52,8 +52,10 @@ class Agent:
             raise ValueError("use_param_info_gain=True requires at least one of pA or pB.")
         if use_inductive and inductive_depth < 1:
             raise ValueError("`inductive_depth` must be >= 1")
-        if action_selection != "deterministic" or sampling_mode != "full":
-            raise NotImplementedError("only deterministic action selection with sampling_mode='full'")
+        if action_selection not in ("deterministic", "stochastic"):
+            raise ValueError("action_selection must be 'deterministic' or 'stochastic'")
+        if sampling_mode not in ("full", "marginal"):
+            raise ValueError("sampling_mode must be 'full' or 'marginal'")
         dev = torch.device(device)
         self.device = dev
         self.batch_size = int(batch_size)
@@ -209,5 +211,11 @@ class Agent:
         return q_pi, G
 
     def sample_action(self, q_pi: torch.Tensor, rng_key=None) -> torch.Tensor:
-        """``pymdp/agent.py:939-967`` (full, deterministic): ``(batch, F)`` int32."""
-        return ffi.select_action(q_pi, self.policies)
+        """``pymdp/agent.py:939-967``: ``(batch, F)`` int32 actions by this
+        agent's ``sampling_mode`` and ``action_selection``. For stochastic
+        selection ``rng_key`` is an integer seed (a counter-based generator
+        stands in for JAX's key)."""
+        if self.sampling_mode == "full" and self.action_selection == "deterministic":
+            return ffi.select_action(q_pi, self.policies)
+        return ffi.sample_action(q_pi, self.policies, self.num_controls, self.sampling_mode, self.action_selection,
+                                 self.alpha, rng_key)

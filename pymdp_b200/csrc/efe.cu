@@ -684,3 +684,152 @@ extern "C" int32_t b2_select_action(void* stream, const float* q_pi, const int32
                                                                         (int)T, (int)F);
   return check_launch("select_action");
 }
+
+// -------------------------------------------------------------------------
+// Action selection with the reference's four modes (pymdp/agent.py:939-967):
+// sampling_mode "full" picks a policy (control.py:115-150) and returns its
+// first step; "marginal" forms each control factor's first-step action
+// marginal (get_marginals, control.py:42-67) and picks from it
+// (control.py:69-113). Deterministic selection takes the first maximum;
+// stochastic selection draws from the categorical with logits
+// alpha * log clip(x) by the Gumbel-max trick (argmax of logits + Gumbel
+// noise, the method jax.random.categorical uses), with u from SplitMix64 over
+// (seed, agent, factor, index) instead of JAX's PRNG.
+namespace b2 {
+namespace {
+
+__device__ __forceinline__ uint64_t sa_mix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Gumbel(0, 1) from u in (0, 1): u = (top 24 bits + 0.5) / 2^24.
+__device__ __forceinline__ float sa_gumbel(uint64_t seed, int64_t agent, int factor, int index) {
+  uint64_t h = sa_mix(seed);
+  h = sa_mix(h ^ (uint64_t)agent);
+  h = sa_mix(h ^ (uint64_t)(uint32_t)factor);
+  h = sa_mix(h ^ (uint64_t)(uint32_t)index);
+  const float u = ((float)(h >> 40) + 0.5f) * (1.0f / 16777216.0f);
+  return -logf(-logf(u));
+}
+
+// argmax over a block (first index on ties); s_v / s_i: 32 slots each.
+__device__ int sa_block_argmax(float v, int i, float* s_v, int* s_i) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (ov > v || (ov == v && oi < i)) {
+      v = ov;
+      i = oi;
+    }
+  }
+  if (lane == 0) {
+    s_v[wid] = v;
+    s_i[wid] = i;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < nw; ++w)
+      if (s_v[w] > s_v[0] || (s_v[w] == s_v[0] && s_i[w] < s_i[0])) {
+        s_v[0] = s_v[w];
+        s_i[0] = s_i[w];
+      }
+  }
+  __syncthreads();
+  const int r = s_i[0];
+  __syncthreads();
+  return r;
+}
+
+struct SampleDims {
+  int32_t U[B2_MAX_FACTORS];
+};
+
+__global__ void sample_action_kernel(const float* __restrict__ q_pi, const int32_t* __restrict__ pm,
+                                     const __grid_constant__ SampleDims U, int32_t* __restrict__ action, int P,
+                                     int T, int F, int marginal, int stochastic, const float* __restrict__ alpha_p,
+                                     int alpha_batched, uint64_t seed) {
+  __shared__ float s_v[32];
+  __shared__ int s_i[32];
+  __shared__ float s_m[B2_SAMPLE_MAX_U];
+  const int64_t b = blockIdx.x;
+  const float* q = q_pi + b * P;
+  const float alpha = stochastic ? alpha_p[alpha_batched ? b : 0] : 0.f;
+  if (!marginal) {
+    float best = -INFINITY;
+    int bi = 0x7fffffff;
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+      const float v = stochastic ? alpha * log_stable(q[p]) + sa_gumbel(seed, b, -1, p) : q[p];
+      if (v > best || (v == best && p < bi) || (bi == 0x7fffffff && v != v)) {
+        best = v;
+        bi = p;
+      }
+    }
+    int p = sa_block_argmax(best, bi, s_v, s_i);
+    if (p == 0x7fffffff) p = 0;
+    for (int f = threadIdx.x; f < F; f += blockDim.x) action[b * F + f] = pm[(int64_t)p * T * F + f];
+    return;
+  }
+  for (int f = 0; f < F; ++f) {
+    const int Uf = U.U[f];
+    // first-step action marginal of factor f, summed in policy order (deterministic)
+    for (int a = threadIdx.x; a < Uf; a += blockDim.x) {
+      float acc = 0.f;
+      for (int p = 0; p < P; ++p)
+        if (pm[(int64_t)p * T * F + f] == a) acc += q[p];
+      s_m[a] = acc;
+    }
+    __syncthreads();
+    float best = -INFINITY;
+    int bi = 0x7fffffff;
+    for (int a = threadIdx.x; a < Uf; a += blockDim.x) {
+      const float v = stochastic ? alpha * log_stable(s_m[a]) + sa_gumbel(seed, b, f, a) : s_m[a];
+      if (v > best || (v == best && a < bi)) {
+        best = v;
+        bi = a;
+      }
+    }
+    int a = sa_block_argmax(best, bi, s_v, s_i);
+    if (threadIdx.x == 0) action[b * F + f] = a == 0x7fffffff ? 0 : a;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+}  // namespace b2
+
+extern "C" int32_t b2_sample_action(void* stream, const float* q_pi, const int32_t* policy_matrix, const int64_t* U,
+                                    int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F,
+                                    int32_t sampling_mode, int32_t action_selection, const float* alpha,
+                                    int32_t alpha_batched, uint64_t seed) {
+  const char* op = "sample_action";
+  if (Bn < 0 || P <= 0 || T <= 0 || F <= 0 || P > 0x7fffffff || T * F > 0x7fffffff)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": invalid sizes");
+  if (sampling_mode != 0 && sampling_mode != 1)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": sampling_mode must be 0 (full) or 1 (marginal)");
+  if (action_selection != 0 && action_selection != 1)
+    return fail(B2_ERR_INVALID_ARGUMENT,
+                std::string(op) + ": action_selection must be 0 (deterministic) or 1 (stochastic)");
+  if (F > B2_MAX_FACTORS) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": more than 16 factors");
+  b2::SampleDims dims{};
+  if (sampling_mode == 1) {
+    if (!U) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": marginal mode needs U");
+    for (int64_t f = 0; f < F; ++f) {
+      if (U[f] < 1) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": U must be positive");
+      if (U[f] > B2_SAMPLE_MAX_U) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": U above 1024");
+      dims.U[f] = (int32_t)U[f];
+    }
+  }
+  if (Bn == 0) return B2_OK;
+  if (!q_pi || !policy_matrix || !action || (action_selection == 1 && !alpha))
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer");
+  if (Bn > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": Bn too large");
+  b2::sample_action_kernel<<<(unsigned)Bn, 256, 0, (cudaStream_t)stream>>>(
+      q_pi, policy_matrix, dims, action, (int)P, (int)T, (int)F, sampling_mode, action_selection, alpha,
+      alpha_batched, seed);
+  return check_launch(op);
+}

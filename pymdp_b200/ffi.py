@@ -410,6 +410,33 @@ def policy_posterior(neg_efe: torch.Tensor, E: torch.Tensor, gamma) -> torch.Ten
     return q
 
 
+def sample_action(q_pi: torch.Tensor, policy_matrix, num_controls, sampling_mode: str = "full",
+                  action_selection: str = "deterministic", alpha=16.0, seed: int | None = None):
+    """``Agent.sample_action`` (``pymdp/agent.py:939-967``): ``sampling_mode``
+    "full" (``control.sample_policy``) or "marginal" (``control.sample_action``
+    over ``get_marginals``), ``action_selection`` "deterministic" or
+    "stochastic" (needs ``seed``: a counter-based generator stands in for
+    JAX's key). Returns ``(batch, F)`` int32."""
+    if sampling_mode not in ("full", "marginal"):
+        raise ValueError("sampling_mode must be 'full' or 'marginal'")
+    if action_selection not in ("deterministic", "stochastic"):
+        raise ValueError("action_selection must be 'deterministic' or 'stochastic'")
+    if action_selection == "stochastic" and seed is None:
+        raise ValueError("Please provide a random number generator key to sample actions stochastically")
+    q_pi = q_pi.contiguous()
+    pm = torch.as_tensor(policy_matrix, device=q_pi.device).to(torch.int32).contiguous()
+    P, T, F = pm.shape
+    Bn = q_pi.numel() // P
+    act = torch.empty(q_pi.shape[:-1] + (F,), dtype=torch.int32, device=q_pi.device)
+    _require_cuda(q_pi, "q_pi")
+    a = _dev_f32(torch.as_tensor(alpha, dtype=torch.float32), q_pi.device).reshape(-1).contiguous()
+    check(_lib.load().b2_sample_action(_stream(act), q_pi.data_ptr(), pm.data_ptr(), i64(list(num_controls)),
+                                       act.data_ptr(), Bn, P, T, F, int(sampling_mode == "marginal"),
+                                       int(action_selection == "stochastic"), a.data_ptr(), int(a.numel() != 1),
+                                       int(seed or 0) & ((1 << 64) - 1)))
+    return act
+
+
 def select_action(q_pi: torch.Tensor, policy_matrix: torch.Tensor) -> torch.Tensor:
     """Deterministic ``sample_policy`` (``control.py:115-150``): ``(batch, F)`` int32."""
     q_pi = q_pi.contiguous()

@@ -189,3 +189,19 @@ def test_neg_efe_pack_bytes_host_query():
     assert lay.pack_bytes(8, P, ffi.efe_flags(precision="bf16")) == 2 * n_bf
     assert lay.pack_bytes(4, P, ffi.efe_flags(precision="fp32")) == 0
     assert lay.pack_bytes(4, P, ffi.efe_flags(use_inductive=True, precision="bf16")) == 0
+
+
+def test_sample_action_validation():
+    """b2_sample_action rejects bad modes and sizes before touching a GPU."""
+    import ctypes
+    lib = _lib.load()
+    U = (ctypes.c_int64 * 2)(3, 2)
+    rc = lib.b2_sample_action(None, 0x1000, 0x1000, U, 0x1000, 4, 6, 1, 2, 2, 0, 0x1000, 0, 0)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT and b"sampling_mode" in lib.b2_last_error()
+    rc = lib.b2_sample_action(None, 0x1000, 0x1000, U, 0x1000, 4, 6, 1, 2, 0, 3, 0x1000, 0, 0)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT and b"action_selection" in lib.b2_last_error()
+    big = (ctypes.c_int64 * 2)(3, 4096)
+    rc = lib.b2_sample_action(None, 0x1000, 0x1000, big, 0x1000, 4, 6, 1, 2, 1, 0, 0x1000, 0, 0)
+    assert rc == _lib.B2_ERR_UNSUPPORTED
+    rc = lib.b2_sample_action(None, 0x1000, 0x1000, None, 0x1000, 4, 6, 1, 2, 1, 0, 0x1000, 0, 0)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT

@@ -316,3 +316,74 @@ def test_pack_cache_reuses_operand_images(precision):
     A_f.mul_(0.5).add_(0.5 / 11)  # a different (still normalised for modality 0) A: repack
     cache[1].value = 0
     np.testing.assert_array_equal(run(cache), run())
+
+
+# ------------------------------------------------ action selection modes
+def _random_qpi(rng, batch, P, alpha=2.0):
+    g = rng.gamma(alpha, size=(batch, P))
+    return (g / g.sum(1, keepdims=True)).astype(np.float32)
+
+
+def test_sample_action_modes_match_oracle():
+    """b2_sample_action: deterministic "full" and "marginal" equal the
+    reference's argmax rules; stochastic draws equal the oracle's restatement
+    of the same Gumbel-max draw (except where the perturbed logits tie within
+    1e-4)."""
+    from pymdp_b200 import ffi
+    rng = np.random.default_rng(21)
+    U, T, batch, alpha, seed = [3, 2, 1], 2, 64, 3.0, 1234
+    pol = oefe.construct_policies([3, 2, 2], U, T)
+    q = _random_qpi(rng, batch, len(pol))
+    qd = cuda(q)
+    full_det = ffi.sample_action(qd, pol, U, "full", "deterministic").cpu().numpy()
+    marg_det = ffi.sample_action(qd, pol, U, "marginal", "deterministic").cpu().numpy()
+    full_sto = ffi.sample_action(qd, pol, U, "full", "stochastic", alpha, seed).cpu().numpy()
+    marg_sto = ffi.sample_action(qd, pol, U, "marginal", "stochastic", alpha, seed).cpu().numpy()
+    ties = 0
+    for b in range(batch):
+        np.testing.assert_array_equal(full_det[b], oefe.sample_policy(pol, q[b]))
+        np.testing.assert_array_equal(marg_det[b], oefe.sample_action_marginal(pol, U, q[b]))
+        p, gap = oefe.sample_stochastic(q[b], alpha, seed, b, -1)
+        if gap > 1e-4:
+            np.testing.assert_array_equal(full_sto[b], pol[p, 0])
+        else:
+            ties += 1
+        for f, m in enumerate(oefe.get_marginals(q[b], pol, U)):
+            a, gap = oefe.sample_stochastic(m, alpha, seed, b, f)
+            if gap > 1e-4:
+                assert marg_sto[b, f] == a, (b, f)
+    assert ties <= 1
+
+
+@pytest.mark.parametrize("mode", ["full", "marginal"])
+@pytest.mark.parametrize("alpha", [1.0, 4.0])
+def test_stochastic_selection_follows_the_softmax(mode, alpha):
+    """Stochastic draws across many agents with the same q_pi follow
+    softmax(alpha * log q) (total variation below 0.015 over 40000 draws)."""
+    from pymdp_b200 import ffi
+    U, T, batch = [6], 1, 40000
+    pol = oefe.construct_policies([6], U, T)
+    q1 = np.array([0.05, 0.1, 0.15, 0.2, 0.22, 0.28], np.float32)
+    q = np.broadcast_to(q1, (batch, 6)).copy()
+    act = ffi.sample_action(cuda(q), pol, U, mode, "stochastic", alpha, 99).cpu().numpy()[:, 0]
+    freq = np.bincount(act, minlength=6) / batch
+    p = np.exp(alpha * np.log(q1.astype(np.float64)))
+    p /= p.sum()
+    assert 0.5 * np.abs(freq - p).sum() < 0.015, (freq, p)
+
+
+def test_agent_stochastic_marginal_mode_runs():
+    from pymdp_b200 import Agent
+    rng = np.random.default_rng(3)
+    A = [rng.dirichlet(np.ones(3), size=(3, 2)).transpose(2, 0, 1).astype(np.float32)]
+    B = [rng.dirichlet(np.ones(3), size=(3, 3)).transpose(2, 0, 1).astype(np.float32),
+         rng.dirichlet(np.ones(2), size=(2, 2)).transpose(2, 0, 1).astype(np.float32)]
+    agent = Agent(A, B, policy_len=2, batch_size=5, alpha=8.0, action_selection="stochastic",
+                  sampling_mode="marginal")
+    qs = agent.infer_states(torch.zeros((5, 1), dtype=torch.int32, device="cuda"),
+                            [torch.full((5, 3), 1 / 3, device="cuda"), torch.full((5, 2), 0.5, device="cuda")])
+    q_pi, _ = agent.infer_policies(qs)
+    with pytest.raises(ValueError):
+        agent.sample_action(q_pi)
+    act = agent.sample_action(q_pi, rng_key=7).cpu().numpy()
+    assert act.shape == (5, 2) and (act[:, 0] < 3).all() and (act[:, 1] < 2).all()
