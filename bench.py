@@ -133,6 +133,70 @@ def run_fpi_config(dev, steps: int, warmup: int, flush):
             "bytes_per_launch": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
 
 
+LEARN_AGENTS = 256
+
+
+def learn_bytes_per_agent(S, O, U, A_deps, B_deps) -> float:
+    """Algorithmic HBM bytes of one online learning step of one agent (T = 1
+    observation, one transition): every pA / pB element read and every A / B
+    element written; pA written in the observed row of each column, pB in the
+    taken action's slice; beliefs, observations and actions in."""
+    KA = [int(np.prod([S[d] for d in dp])) for dp in A_deps]
+    KB = [int(np.prod([S[d] for d in dp])) for dp in B_deps]
+    a = 8.0 * sum(o * k for o, k in zip(O, KA)) + 4.0 * sum(KA)
+    b = 8.0 * sum(s * k * u for s, k, u in zip(S, KB, U)) + 4.0 * sum(s * k for s, k in zip(S, KB))
+    return a + b + 4.0 * (2 * sum(S) + len(O) + len(S) + 2)
+
+
+def run_learn_config(dev, steps: int, warmup: int, flush):
+    """Online Dirichlet learning (pA -> A and pB -> B, one observation and one
+    transition per agent) on the 256-agent benchmark model: device time per
+    step (both launches; L2 flushed before each), agent-steps/s and
+    algorithmic HBM GB/s."""
+    import torch
+
+    from pymdp_b200 import ffi
+
+    S, O, U = [32, 16, 8], [16, 16, 8, 8, 4], [4, 4, 1]
+    A_deps, B_deps = [[0, 1, 2]] * 5, [[0], [1], [2]]
+    Bn = LEARN_AGENTS
+    lay = ffi.EfeLayout(S, O, U, 1, A_deps, B_deps)
+    g = torch.Generator(device=dev).manual_seed(7)
+    pA = torch.rand((Bn, int(lay.A_offsets[-1])), device=dev, generator=g) + 0.5
+    pB = torch.rand((Bn, int(lay.B_offsets[-1])), device=dev, generator=g) + 0.5
+    A, Bm = torch.empty_like(pA), torch.empty_like(pB)
+    q = torch.cat([torch.softmax(torch.randn((Bn, 2, s), device=dev, generator=g) * 3, -1) for s in S], -1)
+    q1 = q[:, 1:].contiguous()
+    obs = torch.stack([torch.randint(0, o, (Bn, 1), device=dev, generator=g) for o in O], -1).to(torch.int32)
+    act = torch.stack([torch.randint(0, u, (Bn, 1), device=dev, generator=g) for u in U], -1).to(torch.int32)
+    obs, act = obs.contiguous(), act.contiguous()
+    lr = torch.full((Bn,), 1e-3, device=dev)
+    work = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def launch():
+        lay.learn_A(pA, A, obs, q1, lr, Bn, 1)
+        lay.learn_B(pB, Bm, q, act, lr, work, Bn, 2)
+
+    for _ in range(warmup):
+        launch()
+    torch.cuda.synchronize(dev)
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launch()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    nbytes = learn_bytes_per_agent(S, O, U, A_deps, B_deps) * Bn
+    return {"workload": f"online Dirichlet learning of A and B, {Bn} agents, S={S}, O={O}, U={U}, every modality "
+                        f"on every factor, 1 observation + 1 transition per agent, L2 flushed before each step",
+            "agent_steps_per_s": Bn / (ms * 1e-3), "ms_per_step": ms, "launches_per_step": 3,
+            "bytes_per_step": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
+
+
 FIT_SUBJECTS, FIT_TRIALS = 1024, 64
 
 
@@ -419,6 +483,7 @@ def run_b200(args, rank, world, local_rank):
     extras = args.legs == "all" and world == 1
     fit_res = run_fit_config(dev, args.steps, args.warmup, flush) if extras else None
     ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if extras else None
+    learn_res = run_learn_config(dev, args.steps, args.warmup, flush) if extras else None
     efe_ev = []
 
     def step(timed_efe=False):
@@ -548,6 +613,7 @@ def run_b200(args, rank, world, local_rank):
                                        "frac": fpi_res["gbs"] / peak_gbs}),
         "fit": fit_res,
         "rollout": ro_res,
+        "learn": learn_res,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -559,7 +625,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout"],
+    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout", "learn"],
                     help="step: the agent step (default); fpi: only the 4096-agent FPI model; fit: only the "
                          "model-fitting gradient; rollout: only the uneven-size rollout (for profiling)")
     ap.add_argument("--legs", default="all", choices=["all", "step"],
@@ -575,8 +641,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload in ("fpi", "fit", "rollout") and world > 1:
-        raise SystemExit("--workload fpi/fit/rollout runs on one GPU")
+    if args.workload in ("fpi", "fit", "rollout", "learn") and world > 1:
+        raise SystemExit("--workload fpi/fit/rollout/learn runs on one GPU")
     if args.workload == "fpi":
         import torch
 
@@ -599,6 +665,14 @@ def main():
         dev = torch.device("cuda", local_rank)
         torch.cuda.set_device(dev)
         print(json.dumps(run_rollout_config(dev, args.steps, args.warmup)), flush=True)
+        return
+    if args.workload == "learn":
+        import torch
+
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        print(json.dumps(run_learn_config(dev, args.steps, args.warmup, flush)), flush=True)
         return
     if world > 1:
         import datetime

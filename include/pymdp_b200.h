@@ -285,6 +285,48 @@ int32_t b2_sample_action(void* stream, const float* q_pi, const int32_t* policy_
                          int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F, int32_t sampling_mode,
                          int32_t action_selection, const float* alpha, int32_t alpha_batched, uint64_t seed);
 
+/* ------------------------------------------------ online Dirichlet learning
+ * In-place Dirichlet updates of the flattened model buffers the FPI and EFE
+ * entry points read (A_offsets / B_offsets / qs_offsets / dependency lists as
+ * in b2_neg_efe; every agent's row holds its own copy). One launch updates
+ * every agent and every modality (factor); one thread owns one column of one
+ * agent's tensor. The reference runs these in JAX
+ * (pymdp/learning.py:11-233, called from Agent.infer_parameters,
+ * pymdp/agent.py:416-620, inference_algo "fpi"/"mmp"/"vmp" branch :564-567);
+ * it has no FFI for them, so the entry points follow those functions'
+ * arguments. lr is device [Bn] (lr_batched = 1) or a single device value.
+ *
+ * Observation model (learning.py:11-117):
+ *   pA_m += lr * sum_t o_{m,t} (x) qs_{A_dep[m][0],t} (x) ...
+ *   A_m   = clip(pA_m, MINVAL) / sum over the outcome axis
+ * for every m with bit m of modality_mask set (unset = pA_m is None: neither
+ * pA_m nor A_m is touched). qs: [Bn, T, S_tot]; obs: int32 [Bn, T, M] indices
+ * (an index outside [0, O_m) adds nothing: jax.nn.one_hot gives zeros), or,
+ * when obs_cat is non-null, float [Bn, T, sum O] distributions
+ * (categorical_obs=True); obs_count counts the array passed. */
+int32_t b2_update_obs_likelihood_dirichlet(
+    void* stream, float* pA, float* A, int64_t A_count, const int32_t* obs, const float* obs_cat, int64_t obs_count,
+    const float* qs, int64_t qs_count, const float* lr, int32_t lr_batched, int64_t Bn, int64_t T, int64_t F,
+    int64_t M, const int64_t* S, const int64_t* O, const int64_t* qs_offsets, const int64_t* A_offsets,
+    const int64_t* A_dep_flat, int64_t A_dep_flat_len, const int64_t* A_dep_offsets, int64_t modality_mask);
+
+/* Transition model (learning.py:119-233 with the joints of
+ * agent.py:539-543, :567): for transitions t < T-1 whose actions are all >= 0
+ * (valid_transition_mask, agent.py:480-483),
+ *   pB_f += lr * sum_t qs_{f,t+1} (x) qs_{B_dep[f][0],t} (x) ... (x) onehot(actions[t, f])
+ *   B_f   = clip(pB_f, MINVAL) / sum over the next-state axis.
+ * pB_f / B_f are [S_f, S_dep..., U_f] per agent; qs [Bn, T, S_tot] is the
+ * belief sequence; actions int32 [Bn, T-1, F]. Factors without their bit in
+ * factor_mask (factors_to_update) only get B_f renormalised from pB_f
+ * (learning.py:201-215). When no agent has a valid transition, or T < 2,
+ * nothing is written (the skip branch, agent.py:495-500, :603-604).
+ * workspace: one device int32 of scratch (the any-valid flag); two launches. */
+int32_t b2_update_state_transition_dirichlet(
+    void* stream, float* pB, float* B, int64_t B_count, const float* qs, int64_t qs_count, const int32_t* actions,
+    int64_t actions_count, const float* lr, int32_t lr_batched, int32_t* workspace, int64_t Bn, int64_t T, int64_t F,
+    const int64_t* S, const int64_t* U, const int64_t* qs_offsets, const int64_t* B_offsets,
+    const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int64_t factor_mask);
+
 /* ------------------------------------------------------ uneven-size rollout
  * Closed-loop rollout of many agents of DIFFERENT sizes in one persistent
  * launch. Replaces, for inference_algo="fpi", no learning and deterministic

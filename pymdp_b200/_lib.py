@@ -92,6 +92,12 @@ _SIGS = {
                                         POINTER(c_int64)]),
     "b2_sample_action": (c_int32, [c_void_p, _PF, c_void_p, _P64, c_void_p, c_int64, c_int64, c_int64, c_int64,
                                    c_int32, c_int32, _PF, c_int32, c_uint64]),
+    "b2_update_obs_likelihood_dirichlet": (c_int32, [c_void_p, _PF, _PF, c_int64, c_void_p, _PF, c_int64, _PF,
+                                                     c_int64, _PF, c_int32, c_int64, c_int64, c_int64, c_int64,
+                                                     _P64, _P64, _P64, _P64, _P64, c_int64, _P64, c_int64]),
+    "b2_update_state_transition_dirichlet": (c_int32, [c_void_p, _PF, _PF, c_int64, _PF, c_int64, c_void_p,
+                                                       c_int64, _PF, c_int32, c_void_p, c_int64, c_int64, c_int64,
+                                                       _P64, _P64, _P64, _P64, _P64, c_int64, _P64, c_int64]),
     "b2_rollout_setup": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int32]),
     "b2_rollout": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_int32,
                              c_int32, c_void_p]),

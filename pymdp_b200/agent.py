@@ -27,6 +27,11 @@ from . import ffi
 from .control import construct_policies, generate_I_matrix
 
 
+def _views(flat: torch.Tensor, offsets, shapes) -> list[torch.Tensor]:
+    """Per-array views ``[batch, *shape]`` of a flattened ``[batch, total]`` buffer."""
+    return [flat[:, int(offsets[i]):int(offsets[i + 1])].unflatten(1, tuple(sh)) for i, sh in enumerate(shapes)]
+
+
 def _t(x, dev) -> torch.Tensor:
     if isinstance(x, torch.Tensor):
         return x.to(device=dev, dtype=torch.float32)
@@ -45,11 +50,16 @@ class Agent:
                  sampling_mode: str = "full", inference_algo: str = "fpi", num_iter: int = 16,
                  batch_size: int = 1, precision: str = "fp32", device="cuda", pA: Sequence | None = None,
                  pB: Sequence | None = None, H: Sequence | None = None, I: Sequence | None = None,
-                 inductive_depth: int = 1, inductive_threshold: float = 0.1, inductive_epsilon=1e-3):
+                 inductive_depth: int = 1, inductive_threshold: float = 0.1, inductive_epsilon=1e-3,
+                 learn_A: bool = False, learn_B: bool = False):
         if inference_algo.lower() != "fpi":
             raise NotImplementedError("only inference_algo='fpi' is on the accelerated path")
         if use_param_info_gain and pA is None and pB is None:
             raise ValueError("use_param_info_gain=True requires at least one of pA or pB.")
+        if learn_A and pA is None:
+            raise ValueError("pA is required for A learning")
+        if learn_B and pB is None:
+            raise ValueError("pB is required for B learning")
         if use_inductive and inductive_depth < 1:
             raise ValueError("`inductive_depth` must be >= 1")
         if action_selection not in ("deterministic", "stochastic"):
@@ -150,18 +160,36 @@ class Agent:
                                      self.B_dependencies, [int(i.shape[1]) for i in I])
         self._I_flat, _ = ffi.flatten_ragged_f32(I, 1, dev)
         self._eps = _t(np.broadcast_to(np.asarray(inductive_epsilon, np.float32), (nbat,)).copy(), dev)
-        self.pA = [batched(_t(x, dev), len(self.A_dependencies[m]) + 1, f"pA[{m}]") for m, x in enumerate(pA)] \
-            if pA is not None else None
-        self.pB = [batched(_t(x, dev), len(self.B_dependencies[f]) + 2, f"pB[{f}]") for f, x in enumerate(pB)] \
-            if pB is not None else None
-        self._pA_flat = ffi.flatten_ragged_f32(self.pA, 1, dev)[0] if (use_param_info_gain and self.pA) else None
-        self._pB_flat = ffi.flatten_ragged_f32(self.pB, 1, dev)[0] if (use_param_info_gain and self.pB) else None
+        # Dirichlet parameters (pymdp/agent.py:201-250); a None entry of pA is a
+        # modality that neither informs the parameter information gain nor learns
+        self._pA_mask = 0 if pA is None else sum(1 << m for m, x in enumerate(pA) if x is not None)
+        if use_param_info_gain and pA is not None and self._pA_mask != (1 << M) - 1:
+            raise NotImplementedError("use_param_info_gain with a None entry in pA")
+        pA_b = None if pA is None else [
+            A[m] * 0 if x is None else batched(_t(x, dev), len(self.A_dependencies[m]) + 1, f"pA[{m}]")
+            for m, x in enumerate(pA)]
+        pB_b = None if pB is None else [batched(_t(x, dev), len(self.B_dependencies[f]) + 2, f"pB[{f}]")
+                                        for f, x in enumerate(pB)]
+        self._pA_flat = ffi.flatten_ragged_f32(pA_b, 1, dev)[0] if pA_b is not None else None
+        self._pB_flat = ffi.flatten_ragged_f32(pB_b, 1, dev)[0] if pB_b is not None else None
+        self.learn_A, self.learn_B = bool(learn_A), bool(learn_B)
+        self._H = H if (use_inductive and H is not None) else None
+        self.inductive_depth, self.inductive_threshold = int(inductive_depth), float(inductive_threshold)
         # policies built here are construct_policies' full product set: let the
         # tensor-core paths share the evaluation of common policy prefixes
         self._flags = ffi.efe_flags(use_utility, use_states_info_gain, use_param_info_gain, use_inductive,
                                     precision=precision, policy_tree=policies is None)
         self.use_param_info_gain, self.use_inductive = use_param_info_gain, use_inductive
-        self.A, self.B, self.C = A, B, C
+        # A, B (and pA, pB) are views of the flattened buffers the kernels read,
+        # so learning updates them in place
+        self._B_offsets = np.cumsum([0] + [int(np.prod(b.shape[1:])) for b in B])
+        self.A = _views(self._A_flat, self._A_offsets, [a.shape[1:] for a in A])
+        self.B = _views(self._B_flat, self._B_offsets, [b.shape[1:] for b in B])
+        self.pA = None if pA is None else [
+            None if x is None else v
+            for x, v in zip(pA, _views(self._pA_flat, self._A_offsets, [a.shape[1:] for a in A]))]
+        self.pB = None if pB is None else _views(self._pB_flat, self._B_offsets, [b.shape[1:] for b in B])
+        self.C = C
 
     def _pack_cache(self, P: int):
         """The tensor-core operand images of this agent's (immutable) A and C,
@@ -204,9 +232,10 @@ class Agent:
         qs_flat, _ = ffi.flatten_ragged_f32(latest, 1, self.device)
         P = self.policies.shape[0]
         G = torch.empty((self.batch_size, P), device=self.device)
+        pig = self.use_param_info_gain
         self._layout.call(None, self.policies, 0, qs_flat, self._A_flat, self._B_flat, self._C_flat,
-                          self._I_flat, self._pA_flat, self._pB_flat, self._eps, G, self.batch_size, P, self._flags,
-                          cache=self._pack_cache(P))
+                          self._I_flat, self._pA_flat if pig else None, self._pB_flat if pig else None, self._eps, G,
+                          self.batch_size, P, self._flags, cache=self._pack_cache(P))
         q_pi = ffi.policy_posterior(G, self.E, self.gamma)
         return q_pi, G
 
@@ -219,3 +248,72 @@ class Agent:
             return ffi.select_action(q_pi, self.policies)
         return ffi.sample_action(q_pi, self.policies, self.num_controls, self.sampling_mode, self.action_selection,
                                  self.alpha, rng_key)
+
+    def infer_parameters(self, beliefs_A, observations, actions, beliefs_B=None, lr_pA=1.0, lr_pB=1.0):
+        """``pymdp/agent.py:416-620`` for ``inference_algo="fpi"``: Dirichlet
+        updates of pA -> A (``learn_A``) and pB -> B (``learn_B``), in place on
+        the device buffers (``b2_update_obs_likelihood_dirichlet``,
+        ``b2_update_state_transition_dirichlet``); returns ``self``.
+
+        ``beliefs_A[f]``: ``(batch, T, S_f)`` (or ``(batch, S_f)``, T = 1);
+        ``observations``: per modality ``(batch,)`` / ``(batch, T)`` indices, or
+        float ``(batch, T, O_m)`` distributions (categorical observations);
+        ``actions``: ``(batch, F)`` or ``(batch, T', F)``, sliced to T-1 steps
+        of the B belief sequence (``beliefs_B`` if given, else ``beliefs_A``).
+        B learns only when some agent of the batch has a transition whose
+        actions are all >= 0 (``agent.py:480-500``); with ``use_inductive``
+        and H, I is then regenerated from the new B (``agent.py:606-615``)."""
+        dev, nbat = self.device, self.batch_size
+
+        def seq(beliefs):
+            qs = [_t(q, dev) for q in beliefs]
+            qs = [q.reshape(nbat, -1, self.num_states[f]) for f, q in enumerate(qs)]
+            return torch.cat(qs, dim=-1).contiguous()
+
+        def rate(lr):
+            return _t(np.broadcast_to(np.asarray(lr, np.float32), (nbat,)).copy(), dev) \
+                if not isinstance(lr, torch.Tensor) else lr.to(dev, torch.float32).expand(nbat).contiguous()
+
+        if self.learn_A:
+            qa = seq(beliefs_A)
+            T = qa.shape[1]
+            obs = [torch.as_tensor(o, device=dev) for o in (observations if isinstance(observations, (list, tuple))
+                                                             else list(torch.as_tensor(observations).unbind(-1)))]
+            categorical = obs[0].is_floating_point()
+            if categorical:
+                o = torch.cat([x.to(torch.float32).reshape(nbat, T, self.num_obs[m]) for m, x in enumerate(obs)], -1)
+            else:
+                o = torch.stack([x.reshape(nbat, T) for x in obs], dim=-1).to(torch.int32)
+            self._layout.learn_A(self._pA_flat, self._A_flat, o.contiguous(), qa, rate(lr_pA), nbat, T,
+                                 modality_mask=self._pA_mask, categorical=categorical)
+        if self.learn_B and actions is not None:
+            qb = seq(beliefs_A if beliefs_B is None else beliefs_B)
+            T = qb.shape[1]
+            act = torch.as_tensor(actions, device=dev).to(torch.int32)
+            if act.ndim == 2:
+                act = act.unsqueeze(1)
+            act = act[:, :max(T - 1, 0)].contiguous()
+            if T > 1 and act.shape[1] == T - 1:
+                if not hasattr(self, "_learn_work"):
+                    self._learn_work = torch.zeros(1, dtype=torch.int32, device=dev)
+                self._layout.learn_B(self._pB_flat, self._B_flat, qb, act, rate(lr_pB), self._learn_work, nbat, T)
+                if self._H is not None:
+                    self._regenerate_I()
+        if getattr(self, "_pack", None) is not None:  # the tensor-core operand images hold the old A
+            self._pack[1].value = 0
+        return self
+
+    def _regenerate_I(self):
+        """``control.generate_I_matrix`` on the learned B (``agent.py:606-615``);
+        a host computation, as in the constructor."""
+        F, nbat = self.num_factors, self.batch_size
+        H_b = [np.broadcast_to(np.asarray(_t(h, "cpu")), (nbat, self.num_states[f])) for f, h in enumerate(self._H)]
+        B_host = [b.cpu().numpy() for b in self.B]
+        per = [generate_I_matrix([H_b[f][b_] for f in range(F)], [B_host[f][b_] for f in range(F)],
+                                 self.inductive_threshold, self.inductive_depth) for b_ in range(nbat)]
+        I = [torch.as_tensor(np.stack([per[b_][f] for b_ in range(nbat)]), device=self.device, dtype=torch.float32)
+             for f in range(F)]
+        if [int(i.shape[1]) for i in I] != [int(d) for d in self._layout.I_depths]:
+            raise NotImplementedError("the learned B changed the inductive depth of I")
+        self.I = I
+        self._I_flat, _ = ffi.flatten_ragged_f32(I, 1, self.device)

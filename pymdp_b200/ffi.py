@@ -311,6 +311,36 @@ class EfeLayout:
             _require_cuda(buf, "pack cache")
             check(_lib.load().b2_neg_efe_cached(*args, buf.data_ptr(), buf.numel(), ctypes.byref(valid)))
 
+    def learn_A(self, pA: torch.Tensor, A: torch.Tensor, obs: torch.Tensor, qs: torch.Tensor, lr: torch.Tensor,
+                Bn: int, T: int, modality_mask: int | None = None, categorical: bool = False):
+        """``b2_update_obs_likelihood_dirichlet`` in place on the flattened
+        ``pA`` / ``A`` ([Bn, A_offsets[M]]): ``obs`` int32 [Bn, T, M] (or float
+        [Bn, T, sum O] when ``categorical``), ``qs`` [Bn, T, S_tot], ``lr`` [Bn]
+        or one value (device)."""
+        for t in (pA, A, obs, qs, lr):
+            _require_cuda(t, "learning buffer")
+        c = self._c
+        mask = (1 << self.M) - 1 if modality_mask is None else int(modality_mask)
+        check(_lib.load().b2_update_obs_likelihood_dirichlet(
+            _stream(pA), pA.data_ptr(), A.data_ptr(), A.numel(), 0 if categorical else obs.data_ptr(),
+            obs.data_ptr() if categorical else 0, obs.numel(), qs.data_ptr(), qs.numel(), lr.data_ptr(),
+            int(lr.numel() != 1), int(Bn), int(T), self.F, self.M, c[0], c[1], c[3], c[4], c[9], len(self.A_dep_flat),
+            c[10], mask))
+
+    def learn_B(self, pB: torch.Tensor, B: torch.Tensor, qs: torch.Tensor, actions: torch.Tensor, lr: torch.Tensor,
+                workspace: torch.Tensor, Bn: int, T: int, factor_mask: int | None = None):
+        """``b2_update_state_transition_dirichlet`` in place on the flattened
+        ``pB`` / ``B`` ([Bn, B_offsets[F]]): ``qs`` [Bn, T, S_tot] belief
+        sequence, ``actions`` int32 [Bn, T-1, F], ``workspace`` one device int32."""
+        for t in (pB, B, qs, actions, lr, workspace):
+            _require_cuda(t, "learning buffer")
+        c = self._c
+        mask = (1 << self.F) - 1 if factor_mask is None else int(factor_mask)
+        check(_lib.load().b2_update_state_transition_dirichlet(
+            _stream(pB), pB.data_ptr(), B.data_ptr(), B.numel(), qs.data_ptr(), qs.numel(), actions.data_ptr(),
+            actions.numel(), lr.data_ptr(), int(lr.numel() != 1), workspace.data_ptr(), int(Bn), int(T), self.F,
+            c[0], c[2], c[3], c[5], c[11], len(self.B_dep_flat), c[12], mask))
+
 
 def neg_efe_all_policies_ffi(policy_matrix, qs_init, A, B, C, I, A_dependencies, B_dependencies, *,
                              pA=None, pB=None, use_utility: bool = True, use_states_info_gain: bool = True,

@@ -102,6 +102,12 @@ def _vmap(fn, in_axes=0, out_axes=0):
     return mapped
 
 
+def _cond(pred, true_fn, false_fn, *operands, operand=None):
+    """``lax.cond`` evaluated eagerly (the predicate is a concrete value)."""
+    args = operands if operands else (() if operand is None else (operand,))
+    return true_fn(*args) if bool(pred) else false_fn(*args)
+
+
 def _jit(fn=None, **_kw):
     if fn is None:
         return lambda f: f
@@ -114,8 +120,9 @@ def _softmax(x, axis=-1):
     return e / np.sum(e, axis=axis, keepdims=True)
 
 
-def _one_hot(x, n, dtype=np.float64):
-    return (np.asarray(x)[..., None] == np.arange(n)).astype(dtype)
+def _one_hot(x, n, dtype=np.float64, axis=-1):
+    out = (np.asarray(x)[..., None] == np.arange(n)).astype(dtype)
+    return out if axis == -1 else np.moveaxis(out, -1, axis)
 
 
 def _contract(*args, backend=None, **_kw):
@@ -197,7 +204,7 @@ def install_shims():
                         tree_leaves=_tree_leaves, Partial=functools.partial)
     nn = _module("jax.nn", softmax=_softmax, one_hot=_one_hot,
                  log_softmax=lambda x, axis=-1: np.log(_softmax(x, axis)))
-    lax = _module("jax.lax", scan=_scan, stop_gradient=lambda x: x,
+    lax = _module("jax.lax", scan=_scan, cond=_cond, stop_gradient=lambda x: x,
                   Precision=types.SimpleNamespace(HIGHEST=None, DEFAULT=None))
     random = _module("jax.random")
     special = _module("jax.scipy.special", xlogy=sps.xlogy, digamma=sps.digamma, gammaln=sps.gammaln)
@@ -224,7 +231,7 @@ def install_shims():
     mpl.pyplot = _module("matplotlib.pyplot")
 
 
-def load_reference(ref_root: str):
+def load_reference(ref_root: str, modules=("utils", "maths", "algos", "control")):
     """Load the reference's utils/maths/algos/control modules on the shims.
 
     Returns a namespace with attributes ``utils``, ``maths``, ``algos``,
@@ -240,7 +247,7 @@ def load_reference(ref_root: str):
                   neg_efe_ffi_beneficial=lambda *a, **k: False)
     pkg.ffi = ffi
     loaded = {}
-    for name in ("utils", "maths", "algos", "control"):
+    for name in modules:
         spec = importlib.util.spec_from_file_location(f"pymdp.{name}", f"{ref_root}/pymdp/{name}.py")
         mod = importlib.util.module_from_spec(spec)
         sys.modules[f"pymdp.{name}"] = mod
