@@ -1,8 +1,9 @@
 """``Agent`` — the reference's ``pymdp.agent.Agent`` surface for the FPI + EFE path.
 
 Keeps the signatures and return shapes of ``Agent.infer_states``
-(``pymdp/agent.py:675-823``), ``Agent.infer_policies`` (``:853-906``) and
-``Agent.sample_action`` (``:939-967``) for ``inference_algo="fpi"``,
+(``pymdp/agent.py:675-823``), ``Agent.infer_policies`` (``:853-906``),
+``Agent.sample_action`` (``:939-967``) and ``Agent.infer_parameters``
+(``:416-620``, Dirichlet learning of A and B) for ``inference_algo="fpi"``,
 either ``sampling_mode`` and either action selection, with the
 batch-broadcasting rules of ``pymdp/agent.py:228-330`` (unbatched A/B/C/D/E
 are broadcast to ``batch_size``; defaults C = uniform 1/O, D = uniform,
