@@ -197,6 +197,61 @@ def run_learn_config(dev, steps: int, warmup: int, flush):
             "bytes_per_step": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
 
 
+HMM_AGENTS, HMM_T, HMM_K, HMM_U, HMM_O = 4096, 64, 32, 4, [16, 8]
+
+
+def hmm_bytes_per_agent(T, K, U, O) -> float:
+    """Algorithmic HBM bytes of one agent's exact filter + smoother: A, B,
+    prior, observations and actions in; mll, filtered, predicted, smoothed
+    and the pairwise posteriors (joint and conditional) out."""
+    ins = 4.0 * (sum(O) * K + K * K * U + K + T * len(O) + (T - 1))
+    outs = 4.0 * (1 + 3 * T * K + 2 * (T - 1) * K * K)
+    return ins + outs
+
+
+def run_hmm_config(dev, steps: int, warmup: int, flush):
+    """Exact single-factor HMM filtering + smoothing (run_exact_single_factor_hmm_scan
+    with the joint posteriors) for 4096 agents: device time per launch (L2
+    flushed before each), agent-sequences/s and algorithmic HBM GB/s."""
+    import torch
+
+    from pymdp_b200 import hmm
+
+    Bn, T, K, U, O = HMM_AGENTS, HMM_T, HMM_K, HMM_U, HMM_O
+    g = torch.Generator(device=dev).manual_seed(11)
+    A = [torch.softmax(torch.randn((Bn, o, K), device=dev, generator=g) * 2, dim=1) for o in O]
+    B = torch.softmax(torch.randn((Bn, K, K, U), device=dev, generator=g) * 2, dim=1).contiguous()
+    prior = torch.softmax(torch.randn((Bn, K), device=dev, generator=g), dim=1)
+    obs = [torch.randint(0, o, (Bn, T), device=dev, generator=g, dtype=torch.int32) for o in O]
+    acts = torch.randint(0, U, (Bn, T - 1), device=dev, generator=g, dtype=torch.int32)
+    A_flat = torch.cat([a.reshape(Bn, -1) for a in A], dim=-1).contiguous()
+    obs_i = torch.stack(obs, dim=-1).contiguous()
+    out = hmm.hmm_outputs(Bn, T, K, ("mll", "filtered", "predicted", "smoothed", "joint", "cond"), dev)
+
+    def launch():
+        hmm.hmm_smoother_packed(A_flat, 1, O, obs_i, False, prior, B, 1, U, acts, "index", out)
+
+    for _ in range(warmup):
+        launch()
+    torch.cuda.synchronize(dev)
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launch()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    nbytes = hmm_bytes_per_agent(T, K, U, O) * Bn
+    return {"workload": f"exact single-factor HMM filter + smoother, {Bn} agents, T={T}, K={K}, U={U}, O={O}, "
+                        f"index observations, all outputs incl. joint and conditional pairwise posteriors, L2 "
+                        f"flushed before each launch",
+            "agent_sequences_per_s": Bn / (ms * 1e-3), "ms_per_launch": ms, "bytes_per_launch": nbytes,
+            "gbs": nbytes / (ms * 1e-3) / 1e9}
+
+
 FIT_SUBJECTS, FIT_TRIALS = 1024, 64
 
 
@@ -484,6 +539,7 @@ def run_b200(args, rank, world, local_rank):
     fit_res = run_fit_config(dev, args.steps, args.warmup, flush) if extras else None
     ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if extras else None
     learn_res = run_learn_config(dev, args.steps, args.warmup, flush) if extras else None
+    hmm_res = run_hmm_config(dev, args.steps, args.warmup, flush) if extras else None
     efe_ev = []
 
     def step(timed_efe=False):
@@ -614,6 +670,7 @@ def run_b200(args, rank, world, local_rank):
         "fit": fit_res,
         "rollout": ro_res,
         "learn": learn_res,
+        "hmm": hmm_res,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -625,7 +682,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout", "learn"],
+    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout", "learn", "hmm"],
                     help="step: the agent step (default); fpi: only the 4096-agent FPI model; fit: only the "
                          "model-fitting gradient; rollout: only the uneven-size rollout (for profiling)")
     ap.add_argument("--legs", default="all", choices=["all", "step"],
@@ -641,8 +698,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload in ("fpi", "fit", "rollout", "learn") and world > 1:
-        raise SystemExit("--workload fpi/fit/rollout/learn runs on one GPU")
+    if args.workload in ("fpi", "fit", "rollout", "learn", "hmm") and world > 1:
+        raise SystemExit("--workload fpi/fit/rollout/learn/hmm runs on one GPU")
     if args.workload == "fpi":
         import torch
 
@@ -665,6 +722,14 @@ def main():
         dev = torch.device("cuda", local_rank)
         torch.cuda.set_device(dev)
         print(json.dumps(run_rollout_config(dev, args.steps, args.warmup)), flush=True)
+        return
+    if args.workload == "hmm":
+        import torch
+
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        print(json.dumps(run_hmm_config(dev, args.steps, args.warmup, flush)), flush=True)
         return
     if args.workload == "learn":
         import torch

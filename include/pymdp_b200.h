@@ -327,6 +327,45 @@ int32_t b2_update_state_transition_dirichlet(
     const int64_t* S, const int64_t* U, const int64_t* qs_offsets, const int64_t* B_offsets,
     const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int64_t factor_mask);
 
+/* ------------------------------------------- exact single-factor HMM smoothing
+ * A batch of single-factor HMMs (pymdp's column-stochastic orientation,
+ * B[next, current(, action)]), one agent per CTA, recurrences in FP64.
+ *
+ * b2_hmm_smoother = run_exact_single_factor_hmm_scan (pymdp/algos.py:1132-1208):
+ * log-likelihoods from A and the observations (compute_log_likelihood,
+ * pymdp/maths.py:214-263; obs int32 [Bn, T, M] indices, or, when obs_dist is
+ * non-null, float [Bn, T, sum O] distributions as distr_obs=True), the filter
+ * (hmm_filter_scan_colstoch, :959-988) and the smoother from the filtered
+ * marginals (hmm_smoother_from_filtered_colstoch, :1049-1130).
+ *   A      [Bn (A_batched) or 1, sum_m O_m * K]: A_m[o, k] row-major per modality
+ *   prior  [Bn, K]
+ *   B      U >= 1: [Bn (B_batched) or 1, K, K, U] with actions int32 [Bn, T-1]
+ *          (null allowed when U == 1); U == 0: time-varying [Bn or 1, T-1, K, K]
+ *   action_mode 0: jnp indexing (negative from the end, then clamped), as
+ *          B0[:, :, u] in run_exact_single_factor_hmm_scan; 1: a negative
+ *          action is the identity transition (invalid_action_mode="identity",
+ *          pymdp/inference.py:112-163, used by smoothing_exact)
+ *   outputs (float, null = not written; filtered is required):
+ *          mll [Bn], filtered / predicted / smoothed [Bn, T, K],
+ *          joint [Bn, T-1, K, K] (joint[t, j, i] = p(s_{t+1}=j, s_t=i | o)),
+ *          cond  [Bn, T-1, K, K] (cond[t, j, i] = p(s_t=i | s_{t+1}=j, o), the
+ *          reference's qss). K <= 128. */
+int32_t b2_hmm_smoother(void* stream, const float* A, int64_t A_count, int32_t A_batched, const int64_t* O,
+                        int64_t M, const int32_t* obs, const float* obs_dist, int64_t obs_count,
+                        const float* prior, int64_t prior_count, const float* B, int64_t B_count,
+                        int32_t B_batched, int64_t U, const int32_t* actions, int64_t actions_count,
+                        int32_t action_mode, int64_t Bn, int64_t T, int64_t K, float* mll, float* filtered,
+                        float* predicted, float* smoothed, float* joint, float* cond);
+
+/* hmm_smoother_from_filtered_colstoch (pymdp/algos.py:1049-1130) and
+ * smoothing_exact (pymdp/inference.py:595-634, action_mode 1) from given
+ * filtered marginals [Bn, T, K]; B, actions and outputs as above. */
+int32_t b2_hmm_smoother_from_filtered(void* stream, const float* filtered, int64_t filtered_count,
+                                      const float* B, int64_t B_count, int32_t B_batched, int64_t U,
+                                      const int32_t* actions, int64_t actions_count, int32_t action_mode,
+                                      int64_t Bn, int64_t T, int64_t K, float* smoothed, float* joint,
+                                      float* cond);
+
 /* ------------------------------------------------------ uneven-size rollout
  * Closed-loop rollout of many agents of DIFFERENT sizes in one persistent
  * launch. Replaces, for inference_algo="fpi", no learning and deterministic

@@ -98,6 +98,11 @@ _SIGS = {
     "b2_update_state_transition_dirichlet": (c_int32, [c_void_p, _PF, _PF, c_int64, _PF, c_int64, c_void_p,
                                                        c_int64, _PF, c_int32, c_void_p, c_int64, c_int64, c_int64,
                                                        _P64, _P64, _P64, _P64, _P64, c_int64, _P64, c_int64]),
+    "b2_hmm_smoother": (c_int32, [c_void_p, _PF, c_int64, c_int32, _P64, c_int64, c_void_p, _PF, c_int64, _PF,
+                                  c_int64, _PF, c_int64, c_int32, c_int64, c_void_p, c_int64, c_int32, c_int64,
+                                  c_int64, c_int64, _PF, _PF, _PF, _PF, _PF, _PF]),
+    "b2_hmm_smoother_from_filtered": (c_int32, [c_void_p, _PF, c_int64, _PF, c_int64, c_int32, c_int64, c_void_p,
+                                                c_int64, c_int32, c_int64, c_int64, c_int64, _PF, _PF, _PF]),
     "b2_rollout_setup": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int32]),
     "b2_rollout": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_int32,
                              c_int32, c_void_p]),

@@ -1,0 +1,368 @@
+// Exact single-factor HMM filtering and smoothing for a batch of agents:
+// the reference's run_exact_single_factor_hmm_scan (pymdp/algos.py:1132-1208)
+// = hmm_filter_scan_colstoch (:959-988) + hmm_smoother_from_filtered_colstoch
+// (:1049-1130), and smoothing_exact (pymdp/inference.py:595-634).
+//
+// The reference parallelises over time with lax.associative_scan because one
+// sequence is its unit of work. Here the unit is one agent's sequence, and a
+// batch holds thousands of them: one CTA per agent runs the recurrences in
+// time order (each step a K x K matrix-vector product in FP64 from shared
+// memory), which is the same algebra as the scan without its log2(T) extra
+// matrix products. B lives in shared memory (all actions of a stationary B
+// once per agent; a time-varying B step by step), rows padded by one float so
+// both the row and the column walks are conflict-free.
+//
+// Forward (filter), with p_0 = prior and, for t >= 1, p_t = B_{t-1} f_{t-1}:
+//   ll_t[k] = sum_m log clip(A_m[o_{m,t}, k])   (or sum_o o[o] log clip(A_m[o, k]))
+//   w = exp(ll_t - max ll_t), u = p_t * w, c = sum u
+//   f_t = u / c,  mll += log c + max ll_t        (_condition_on, algos.py:750-775)
+// Backward (smoother from filtered), s_{T-1} = f_{T-1}:
+//   pn_t = B_t f_t, cond_t[j, i] = B_t[j, i] f_t[i] / clip(pn_t[j])
+//   s_t[i] = sum_j cond_t[j, i] s_{t+1}[j]; smoothed_t = s_t / clip(sum s_t)
+//   joint_t[j, i] = cond_t[j, i] * smoothed_{t+1}[j]
+#include "common.cuh"
+
+namespace b2 {
+namespace {
+
+constexpr int kHmmThreads = 128;
+constexpr int kHmmMaxK = 128;
+constexpr double kHmmMinVal = 2.220446049250313e-16;
+
+struct HmmParams {
+  int32_t T, K, U;       // U = 0: time-varying B [T-1, K, K]
+  int32_t M;             // modalities (forward only)
+  int32_t obs_stride;    // M (index observations) or sum O (distributions)
+  int32_t action_mode;   // 0: jnp indexing (negative from the end, clamped); 1: negative -> identity
+  int32_t stage_all;     // stationary B staged once per agent
+  int64_t A_stride;      // A floats per agent (0: shared by every agent)
+  int64_t B_stride;      // B floats per agent (0: shared)
+  int32_t O[B2_MAX_MODALITIES];
+  int64_t A_off[B2_MAX_MODALITIES];
+  int32_t O_off[B2_MAX_MODALITIES];  // start of modality m in a distribution row
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int i = 0; i < kHmmThreads / 32; ++i) s += red[i];
+  return s;
+}
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double s = red[0];
+  for (int i = 1; i < kHmmThreads / 32; ++i) s = fmax(s, red[i]);
+  return s;
+}
+
+// Action of transition t of agent b as an index into B's last axis, or -1 for
+// the identity transition.
+__device__ __forceinline__ int hmm_action(const HmmParams& p, const int32_t* act, int64_t b, int t) {
+  if (p.U <= 0) return 0;
+  int u = act ? act[b * (p.T - 1) + t] : 0;
+  if (p.action_mode == 1) return u < 0 ? -1 : (u >= p.U ? p.U - 1 : u);
+  if (u < 0) u += p.U;  // jnp indexing: negative from the end, then clamped
+  return u < 0 ? 0 : (u >= p.U ? p.U - 1 : u);
+}
+
+// Shared tile of transition t: pointer to a K x (K+1) padded [next][current]
+// matrix, staging it first when B is time-varying or not staged whole. Ends
+// with a barrier when it stages. Returns nullptr for the identity transition.
+__device__ const float* hmm_stage(const HmmParams& p, const float* Bb, float* tile, const int32_t* act, int64_t b,
+                                  int t) {
+  const int K = p.K, ld = K + 1;
+  const int u = hmm_action(p, act, b, t);
+  if (u < 0) return nullptr;
+  if (p.U > 0 && p.stage_all) return tile + (int64_t)u * K * ld;
+  __syncthreads();  // the previous step's readers are done with the tile
+  if (p.U == 0) {
+    const float* src = Bb + (int64_t)t * K * K;
+    for (int e = threadIdx.x; e < K * K; e += kHmmThreads) tile[(e / K) * ld + e % K] = src[e];
+  } else {
+    for (int e = threadIdx.x; e < K * K; e += kHmmThreads) tile[(e / K) * ld + e % K] = Bb[(int64_t)e * p.U + u];
+  }
+  __syncthreads();
+  return tile;
+}
+
+// One agent's backward pass from its filtered marginals (global, FP32; each
+// thread reads back only the entries it wrote in the forward pass).
+__device__ void hmm_backward(const HmmParams& p, const float* Bb, float* tile, const int32_t* act, int64_t b,
+                             const float* filt, float* smoothed, float* joint, float* cond, double* f, double* inv_pn,
+                             double* s_next, double* red) {
+  const int K = p.K, ld = K + 1, T = p.T, j = threadIdx.x;
+  const bool own = j < K;
+  double s = own ? (double)filt[(int64_t)(T - 1) * K + j] : 0.0;  // s_{T-1} = f_{T-1}
+  double tot = block_sum(s, red);
+  if (own) {
+    s_next[j] = s;
+    if (smoothed) smoothed[(int64_t)(T - 1) * K + j] = (float)(s / fmax(tot, kHmmMinVal));
+  }
+  double sn_norm = tot;  // normaliser of s_{t+1}
+  for (int t = T - 2; t >= 0; --t) {
+    const float* Bt = hmm_stage(p, Bb, tile, act, b, t);
+    if (own) f[j] = (double)filt[(int64_t)t * K + j];
+    __syncthreads();
+    if (own) {
+      double pn = 0.0;  // pn_t[j] = sum_i B_t[j, i] f_t[i]
+      if (Bt) {
+        for (int i = 0; i < K; ++i) pn += (double)Bt[j * ld + i] * f[i];
+      } else {
+        pn = f[j];
+      }
+      inv_pn[j] = 1.0 / fmax(pn, kHmmMinVal);
+    }
+    __syncthreads();
+    double si = 0.0;
+    if (own) {  // s_t[i] = f_t[i] * sum_j B_t[j, i] inv_pn[j] s_{t+1}[j]  (thread = i)
+      double acc = 0.0;
+      if (Bt) {
+        for (int jj = 0; jj < K; ++jj) acc += (double)Bt[jj * ld + j] * inv_pn[jj] * s_next[jj];
+      } else {
+        acc = inv_pn[j] * s_next[j];
+      }
+      si = f[j] * acc;
+    }
+    // pairwise outputs of step t use the normalised s_{t+1}
+    const double inv_sn = 1.0 / fmax(sn_norm, kHmmMinVal);
+    if (joint || cond) {
+      float* jo = joint ? joint + (int64_t)t * K * K : nullptr;
+      float* co = cond ? cond + (int64_t)t * K * K : nullptr;
+      for (int e = threadIdx.x; e < K * K; e += kHmmThreads) {
+        const int r = e / K, c = e % K;  // [next r][current c]
+        const double bt = Bt ? (double)Bt[r * ld + c] : (r == c ? 1.0 : 0.0);
+        const double cd = bt * f[c] * inv_pn[r];
+        if (co) co[e] = (float)cd;
+        if (jo) jo[e] = (float)(cd * (s_next[r] * inv_sn));
+      }
+    }
+    tot = block_sum(si, red);  // its barriers order the reads of s_next / f / tile above before the writes below
+    if (own) {
+      s_next[j] = si;
+      if (smoothed) smoothed[(int64_t)t * K + j] = (float)(si / fmax(tot, kHmmMinVal));
+    }
+    sn_norm = tot;
+  }
+}
+
+// Stages every action of a stationary B once (ends with a barrier).
+__device__ void hmm_stage_all(const HmmParams& p, const float* Bb, float* tile) {
+  const int K = p.K, ld = K + 1;
+  const int64_t n = (int64_t)K * K * p.U;
+  for (int64_t e = threadIdx.x; e < n; e += kHmmThreads) {
+    const int u = (int)(e % p.U);
+    const int64_t jk = e / p.U;  // B[j, i, u] at (j * K + i) * U + u
+    tile[(int64_t)u * K * ld + (jk / K) * ld + jk % K] = Bb[e];
+  }
+  __syncthreads();
+}
+
+size_t hmm_smem_bytes(const HmmParams& p) {
+  const int64_t tiles = (p.U > 0 && p.stage_all) ? p.U : 1;
+  return (size_t)(tiles * p.K * (p.K + 1)) * sizeof(float) + 4 * kHmmMaxK * sizeof(double) + 64 * sizeof(double);
+}
+
+__device__ __forceinline__ double* hmm_vectors(unsigned char* smem, const HmmParams& p) {
+  const int64_t tiles = (p.U > 0 && p.stage_all) ? p.U : 1;
+  return reinterpret_cast<double*>(smem + ((tiles * p.K * (p.K + 1) * sizeof(float) + 15) & ~size_t(15)));
+}
+
+__global__ void __launch_bounds__(kHmmThreads)
+hmm_smoother_kernel(const HmmParams p, const float* __restrict__ A, const int32_t* __restrict__ obs,
+                    const float* __restrict__ obs_dist, const float* __restrict__ prior, const float* __restrict__ B,
+                    const int32_t* __restrict__ act, float* __restrict__ mll, float* __restrict__ filtered,
+                    float* __restrict__ predicted, float* __restrict__ smoothed, float* __restrict__ joint,
+                    float* __restrict__ cond) {
+  extern __shared__ __align__(16) unsigned char hmm_smem[];
+  const int64_t b = blockIdx.x;
+  const int K = p.K, ld = K + 1, T = p.T, j = threadIdx.x;
+  const bool own = j < K;
+  float* tile = reinterpret_cast<float*>(hmm_smem);
+  double* vec = hmm_vectors(hmm_smem, p);
+  double* f = vec;
+  double* red = vec + 4 * kHmmMaxK;
+  const float* Ab = A + b * p.A_stride;
+  const float* Bb = B + b * p.B_stride;
+  float* filt = filtered + b * (int64_t)T * K;
+  if (p.U > 0 && p.stage_all) hmm_stage_all(p, Bb, tile);
+  double m_ll = 0.0;
+  for (int t = 0; t < T; ++t) {
+    const float* Bt = t > 0 ? hmm_stage(p, Bb, tile, act, b, t - 1) : nullptr;
+    double pj = 0.0;
+    if (own) {
+      if (t == 0) {
+        pj = (double)prior[b * K + j];
+      } else if (Bt) {
+        for (int i = 0; i < K; ++i) pj += (double)Bt[j * ld + i] * f[i];
+      } else {
+        pj = f[j];
+      }
+    }
+    // log-likelihood of state j (compute_log_likelihood, maths.py:214-263)
+    double ll = -INFINITY;
+    if (own) {
+      ll = 0.0;
+      for (int m = 0; m < p.M; ++m) {
+        const float* Am = Ab + p.A_off[m];
+        if (obs_dist) {
+          const float* od = obs_dist + (b * T + t) * p.obs_stride + p.O_off[m];
+          double s = 0.0;
+          for (int o = 0; o < p.O[m]; ++o) s += (double)od[o] * log(fmax((double)Am[(int64_t)o * K + j], kHmmMinVal));
+          ll += s;
+        } else {
+          int o = obs[(b * T + t) * p.obs_stride + m];
+          if (o < 0) o += p.O[m];  // jnp indexing: negative from the end, then clamped
+          o = o < 0 ? 0 : (o >= p.O[m] ? p.O[m] - 1 : o);
+          ll += log(fmax((double)Am[(int64_t)o * K + j], kHmmMinVal));
+        }
+      }
+    }
+    const double lmax = block_max(ll, red);
+    const double u = own ? pj * exp(ll - lmax) : 0.0;
+    double c = block_sum(u, red);
+    if (c == 0.0) c = 1.0;  // _normalize_preserve_zeros: an all-zero row stays zero
+    m_ll += log(fmax(c, kHmmMinVal)) + lmax;
+    if (own) {
+      const double fj = u / c;
+      f[j] = fj;  // every read of f for this step happened before block_max's barriers
+      filt[(int64_t)t * K + j] = (float)fj;
+      if (predicted) predicted[(b * T + t) * K + j] = (float)pj;
+    }
+    __syncthreads();
+  }
+  if (mll && threadIdx.x == 0) mll[b] = (float)m_ll;
+  if (!smoothed && !joint && !cond) return;
+  hmm_backward(p, Bb, tile, act, b, filt, smoothed ? smoothed + b * (int64_t)T * K : nullptr,
+               joint ? joint + b * (int64_t)(T - 1) * K * K : nullptr,
+               cond ? cond + b * (int64_t)(T - 1) * K * K : nullptr, vec + 3 * kHmmMaxK, vec + kHmmMaxK,
+               vec + 2 * kHmmMaxK, red);
+}
+
+__global__ void __launch_bounds__(kHmmThreads)
+hmm_from_filtered_kernel(const HmmParams p, const float* __restrict__ filtered, const float* __restrict__ B,
+                         const int32_t* __restrict__ act, float* __restrict__ smoothed, float* __restrict__ joint,
+                         float* __restrict__ cond) {
+  extern __shared__ __align__(16) unsigned char hmm_smem[];
+  const int64_t b = blockIdx.x;
+  const int K = p.K, T = p.T;
+  float* tile = reinterpret_cast<float*>(hmm_smem);
+  double* vec = hmm_vectors(hmm_smem, p);
+  const float* Bb = B + b * p.B_stride;
+  if (p.U > 0 && p.stage_all) hmm_stage_all(p, Bb, tile);
+  hmm_backward(p, Bb, tile, act, b, filtered + b * (int64_t)T * K, smoothed ? smoothed + b * (int64_t)T * K : nullptr,
+               joint ? joint + b * (int64_t)(T - 1) * K * K : nullptr,
+               cond ? cond + b * (int64_t)(T - 1) * K * K : nullptr, vec + 3 * kHmmMaxK, vec + kHmmMaxK,
+               vec + 2 * kHmmMaxK, vec + 4 * kHmmMaxK);
+}
+
+constexpr size_t kHmmMaxSmem = 200 * 1024;
+
+// Validates the transition layout; fills p.U / p.B_stride / p.stage_all.
+int32_t hmm_transitions(const char* op, HmmParams& p, int64_t Bn, int64_t U, int32_t B_batched, int64_t B_count,
+                        const int32_t* actions, int64_t actions_count) {
+  const int64_t K = p.K, T = p.T;
+  if (U < 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": U must be >= 0");
+  const int64_t per = U == 0 ? (T - 1) * K * K : K * K * U;
+  p.U = (int32_t)U;
+  p.B_stride = B_batched ? per : 0;
+  if (B_count != (B_batched ? Bn : 1) * per)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": B_count mismatch");
+  if (U > 0 && actions && actions_count != Bn * (T - 1))
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": actions_count mismatch (expected Bn * (T-1))");
+  if (U > 1 && !actions && T > 1)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": actions are required when B has an action axis");
+  p.stage_all = 0;
+  if (U > 0) {
+    HmmParams q = p;
+    q.stage_all = 1;
+    p.stage_all = hmm_smem_bytes(q) <= kHmmMaxSmem ? 1 : 0;
+  }
+  if (hmm_smem_bytes(p) > kHmmMaxSmem) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": K too large");
+  return B2_OK;
+}
+
+}  // namespace
+}  // namespace b2
+
+using namespace b2;
+
+extern "C" int32_t b2_hmm_smoother(void* stream, const float* A, int64_t A_count, int32_t A_batched, const int64_t* O,
+                                   int64_t M, const int32_t* obs, const float* obs_dist, int64_t obs_count,
+                                   const float* prior, int64_t prior_count, const float* B, int64_t B_count,
+                                   int32_t B_batched, int64_t U, const int32_t* actions, int64_t actions_count,
+                                   int32_t action_mode, int64_t Bn, int64_t T, int64_t K, float* mll,
+                                   float* filtered, float* predicted, float* smoothed, float* joint, float* cond) {
+  const char* op = "hmm_smoother";
+  if (Bn < 0 || T < 1 || K < 1 || M < 1) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": invalid sizes");
+  if (K > kHmmMaxK) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": K above 128");
+  if (M > B2_MAX_MODALITIES) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": too many modalities");
+  if (Bn > 0x7fffffff || T * K > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": too large");
+  if (action_mode != 0 && action_mode != 1) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": action_mode");
+  if (!O) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null O");
+  HmmParams p{};
+  p.T = (int32_t)T;
+  p.K = (int32_t)K;
+  p.M = (int32_t)M;
+  p.action_mode = action_mode;
+  int64_t a_off = 0, o_tot = 0;
+  for (int64_t m = 0; m < M; ++m) {
+    if (O[m] <= 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": num_obs must be positive");
+    p.O[m] = (int32_t)O[m];
+    p.A_off[m] = a_off;
+    p.O_off[m] = (int32_t)o_tot;
+    a_off += O[m] * K;
+    o_tot += O[m];
+  }
+  p.A_stride = A_batched ? a_off : 0;
+  p.obs_stride = (int32_t)(obs_dist ? o_tot : M);
+  if (A_count != (A_batched ? Bn : 1) * a_off)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": A_count mismatch");
+  if (obs_count != Bn * T * p.obs_stride)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": obs_count mismatch");
+  if (prior_count != Bn * K) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": prior_count mismatch");
+  B2_TRY(hmm_transitions(op, p, Bn, U, B_batched, B_count, actions, actions_count));
+  if (Bn == 0) return B2_OK;
+  if (!A || !prior || !B || !filtered || (!obs && !obs_dist))
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer (filtered is required)");
+  const size_t smem = hmm_smem_bytes(p);
+  B2_TRY(ensure_smem_attr((const void*)hmm_smoother_kernel, (int)kHmmMaxSmem, op));
+  hmm_smoother_kernel<<<(unsigned)Bn, kHmmThreads, smem, (cudaStream_t)stream>>>(
+      p, A, obs_dist ? nullptr : obs, obs_dist, prior, B, actions, mll, filtered, predicted, smoothed,
+      T > 1 ? joint : nullptr, T > 1 ? cond : nullptr);
+  return check_launch(op);
+}
+
+extern "C" int32_t b2_hmm_smoother_from_filtered(void* stream, const float* filtered, int64_t filtered_count,
+                                                 const float* B, int64_t B_count, int32_t B_batched, int64_t U,
+                                                 const int32_t* actions, int64_t actions_count, int32_t action_mode,
+                                                 int64_t Bn, int64_t T, int64_t K, float* smoothed, float* joint,
+                                                 float* cond) {
+  const char* op = "hmm_smoother_from_filtered";
+  if (Bn < 0 || T < 1 || K < 1) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": invalid sizes");
+  if (K > kHmmMaxK) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": K above 128");
+  if (Bn > 0x7fffffff || T * K > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": too large");
+  if (action_mode != 0 && action_mode != 1) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": action_mode");
+  HmmParams p{};
+  p.T = (int32_t)T;
+  p.K = (int32_t)K;
+  p.action_mode = action_mode;
+  if (filtered_count != Bn * T * K)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": filtered_count mismatch");
+  B2_TRY(hmm_transitions(op, p, Bn, U, B_batched, B_count, actions, actions_count));
+  if (Bn == 0) return B2_OK;
+  if (!filtered || !B) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer");
+  const size_t smem = hmm_smem_bytes(p);
+  B2_TRY(ensure_smem_attr((const void*)hmm_from_filtered_kernel, (int)kHmmMaxSmem, op));
+  hmm_from_filtered_kernel<<<(unsigned)Bn, kHmmThreads, smem, (cudaStream_t)stream>>>(
+      p, filtered, B, actions, smoothed, T > 1 ? joint : nullptr, T > 1 ? cond : nullptr);
+  return check_launch(op);
+}

@@ -46,6 +46,8 @@ def _tree_map(f, tree, *rest, is_leaf=None):
         return f(tree, *rest)
     if isinstance(tree, (list, tuple)):
         out = [_tree_map(f, t, *[r[i] for r in rest], is_leaf=is_leaf) for i, t in enumerate(tree)]
+        if hasattr(tree, "_fields"):  # NamedTuple
+            return type(tree)(*out)
         return type(tree)(out) if isinstance(tree, tuple) else out
     if isinstance(tree, dict):
         return {k: _tree_map(f, v, *[r[k] for r in rest], is_leaf=is_leaf) for k, v in tree.items()}
@@ -93,6 +95,12 @@ def _vmap(fn, in_axes=0, out_axes=0):
                 break
             if n is not None:
                 break
+        if n == 0:  # an empty mapped axis: JAX returns empty outputs of the per-element shape
+            probe = [a if ax is None else _tree_map(lambda x, ax=ax: np.zeros(np.delete(np.shape(x), ax)), a)
+                     for a, ax in zip(args, axes)]
+            with np.errstate(all="ignore"):
+                out = fn(*probe, **kwargs)
+            return _tree_map(lambda leaf: np.zeros((0,) + np.shape(leaf)), out)
         outs = []
         for i in range(n):
             sl = [a if ax is None else _tree_map(lambda x, ax=ax: np.take(x, i, axis=ax), a)
@@ -100,6 +108,25 @@ def _vmap(fn, in_axes=0, out_axes=0):
             outs.append(fn(*sl, **kwargs))
         return _tree_map(lambda *leaves: np.stack([np.asarray(l) for l in leaves]), outs[0], *outs[1:])
     return mapped
+
+
+def _associative_scan(fn, elems, reverse=False, axis=0):
+    """``lax.associative_scan`` as a left fold in time order:
+    ``out[i] = fn(out[i - 1], elems[i])`` (the same result for an associative
+    ``fn``; JAX evaluates it as a tree). ``fn`` sees a leading axis of 1, as it
+    would see a batch of pairs."""
+    if axis != 0:
+        raise NotImplementedError("associative_scan over axis != 0")
+    n = np.shape(_tree_leaves(elems)[0])[0]
+    take = lambda i: _tree_map(lambda x: np.asarray(x)[i], elems)  # noqa: E731
+    expand = lambda t: _tree_map(lambda x: np.asarray(x)[None], t)  # noqa: E731
+    squeeze = lambda t: _tree_map(lambda x: np.asarray(x)[0], t)  # noqa: E731
+    out, acc = [None] * n, None
+    for i in (range(n - 1, -1, -1) if reverse else range(n)):
+        cur = take(i)
+        acc = cur if acc is None else squeeze(fn(expand(acc), expand(cur)))
+        out[i] = acc
+    return _tree_map(lambda *leaves: np.stack(leaves), out[0], *out[1:])
 
 
 def _cond(pred, true_fn, false_fn, *operands, operand=None):
@@ -200,11 +227,12 @@ def install_shims():
                  "asarray", "arange", "eye", "stack", "concatenate"):
         setattr(jnp, name, _immutable(getattr(np, name)))
     jnp.clip = _immutable(_clip)
+    jnp.matmul = lambda a, b, precision=None: np.matmul(a, b)
     tree_util = _module("jax.tree_util", tree_map=_tree_map, tree_reduce=_tree_reduce,
                         tree_leaves=_tree_leaves, Partial=functools.partial)
     nn = _module("jax.nn", softmax=_softmax, one_hot=_one_hot,
                  log_softmax=lambda x, axis=-1: np.log(_softmax(x, axis)))
-    lax = _module("jax.lax", scan=_scan, cond=_cond, stop_gradient=lambda x: x,
+    lax = _module("jax.lax", scan=_scan, cond=_cond, associative_scan=_associative_scan, stop_gradient=lambda x: x,
                   Precision=types.SimpleNamespace(HIGHEST=None, DEFAULT=None))
     random = _module("jax.random")
     special = _module("jax.scipy.special", xlogy=sps.xlogy, digamma=sps.digamma, gammaln=sps.gammaln)
