@@ -209,7 +209,7 @@ def hmm_bytes_per_agent(T, K, U, O) -> float:
     return ins + outs
 
 
-def run_hmm_config(dev, steps: int, warmup: int, flush):
+def run_hmm_config(dev, steps: int, warmup: int, flush, agents: int = HMM_AGENTS):
     """Exact single-factor HMM filtering + smoothing (run_exact_single_factor_hmm_scan
     with the joint posteriors) for 4096 agents: device time per launch (L2
     flushed before each), agent-sequences/s and algorithmic HBM GB/s."""
@@ -217,7 +217,7 @@ def run_hmm_config(dev, steps: int, warmup: int, flush):
 
     from pymdp_b200 import hmm
 
-    Bn, T, K, U, O = HMM_AGENTS, HMM_T, HMM_K, HMM_U, HMM_O
+    Bn, T, K, U, O = agents, HMM_T, HMM_K, HMM_U, HMM_O
     g = torch.Generator(device=dev).manual_seed(11)
     A = [torch.softmax(torch.randn((Bn, o, K), device=dev, generator=g) * 2, dim=1) for o in O]
     B = torch.softmax(torch.randn((Bn, K, K, U), device=dev, generator=g) * 2, dim=1).contiguous()
@@ -687,6 +687,7 @@ def main():
                          "model-fitting gradient; rollout: only the uneven-size rollout (for profiling)")
     ap.add_argument("--legs", default="all", choices=["all", "step"],
                     help="all: also the fitting and rollout workloads (default); step: the agent step and FPI only")
+    ap.add_argument("--hmm-agents", type=int, default=HMM_AGENTS, help="agents of the hmm workload")
     ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
@@ -729,7 +730,7 @@ def main():
         dev = torch.device("cuda", local_rank)
         torch.cuda.set_device(dev)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        print(json.dumps(run_hmm_config(dev, args.steps, args.warmup, flush)), flush=True)
+        print(json.dumps(run_hmm_config(dev, args.steps, args.warmup, flush, args.hmm_agents)), flush=True)
         return
     if args.workload == "learn":
         import torch
