@@ -5,7 +5,7 @@
 //
 // The reference parallelises over time with lax.associative_scan because one
 // sequence is its unit of work. Here the unit is one agent's sequence, and a
-// batch holds thousands of them: one CTA per agent runs the recurrences in
+// batch holds thousands of them: one warp (K <= 32) or CTA per agent runs the recurrences in
 // time order (each step a K x K matrix-vector product in FP64 from shared
 // memory), which is the same algebra as the scan without its log2(T) extra
 // matrix products. B lives in shared memory (all actions of a stationary B
@@ -264,6 +264,200 @@ hmm_from_filtered_kernel(const HmmParams p, const float* __restrict__ filtered, 
                vec + 2 * kHmmMaxK, vec + 4 * kHmmMaxK);
 }
 
+// ------------------------------------------------------------ K <= 32
+// One warp per agent: lane j owns state j, the vectors live in registers and
+// move between lanes by shuffles, so a step has no block barrier (the CTA
+// kernel above spends most of its time waiting at them when K <= 32, where
+// only one of its four warps does the K x K products). Pairwise outputs are
+// written a row per iteration, lane = column: coalesced, no index division.
+constexpr size_t kHmmWarpStageMax = 48 * 1024;  // all actions of B per agent, else one tile per step
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Padded [next][current] tile of transition t (nullptr = identity).
+template <bool ALL>
+__device__ __forceinline__ const float* hmm_wtile(const HmmParams& p, const float* Bb, float* tile,
+                                                  const int32_t* act, int64_t b, int t) {
+  const int K = p.K, ld = K + 1, c = threadIdx.x;
+  const int u = hmm_action(p, act, b, t);
+  if (u < 0) return nullptr;
+  if (ALL && p.U > 0) return tile + (int64_t)u * K * ld;
+  __syncwarp();  // the lanes are done reading the previous tile
+  if (c < K) {
+    if (p.U == 0) {
+      const float* src = Bb + (int64_t)t * K * K;
+      for (int r = 0; r < K; ++r) tile[r * ld + c] = src[r * K + c];
+    } else {
+      for (int r = 0; r < K; ++r) tile[r * ld + c] = Bb[((int64_t)r * K + c) * p.U + u];
+    }
+  }
+  __syncwarp();
+  return tile;
+}
+
+// Backward pass of one agent from its filtered marginals (each lane reads
+// back only its own entries).
+template <bool ALL>
+__device__ void hmm_wbackward(const HmmParams& p, const float* Bb, float* tile, const int32_t* act, int64_t b,
+                              const float* filt, float* smoothed, float* joint, float* cond) {
+  const int K = p.K, ld = K + 1, T = p.T, j = threadIdx.x;
+  const bool own = j < K;
+  double s_next = own ? (double)filt[(int64_t)(T - 1) * K + j] : 0.0;  // s_{T-1} = f_{T-1}
+  double sn_norm = warp_sum_d(s_next);
+  if (own && smoothed) smoothed[(int64_t)(T - 1) * K + j] = (float)(s_next / fmax(sn_norm, kHmmMinVal));
+  for (int t = T - 2; t >= 0; --t) {
+    const float* Bt = hmm_wtile<ALL>(p, Bb, tile, act, b, t);
+    const double ft = own ? (double)filt[(int64_t)t * K + j] : 0.0;
+    double pn = ft;  // pn_t[j] = sum_i B_t[j, i] f_t[i]
+    if (Bt) {
+      pn = 0.0;
+      for (int i = 0; i < K; ++i) {
+        const double fi = __shfl_sync(0xffffffffu, ft, i);
+        if (own) pn += (double)Bt[j * ld + i] * fi;
+      }
+    }
+    const double ipn = own ? 1.0 / fmax(pn, kHmmMinVal) : 0.0;
+    const double w = ipn * s_next;  // row weight of s_t = cond^T s_{t+1}
+    double acc = w;                 // s_t[i] = f_t[i] * sum_j B_t[j, i] w_j  (lane = i)
+    if (Bt) {
+      acc = 0.0;
+      for (int r = 0; r < K; ++r) {
+        const double wr = __shfl_sync(0xffffffffu, w, r);
+        if (own) acc += (double)Bt[r * ld + j] * wr;
+      }
+    }
+    const double si = own ? ft * acc : 0.0;
+    if (joint || cond) {  // cond[t, r, c] = B[r, c] f[c] / pn[r]; joint = cond * smoothed_{t+1}[r]
+      float* co = cond ? cond + (int64_t)t * K * K : nullptr;
+      float* jo = joint ? joint + (int64_t)t * K * K : nullptr;
+      const double inv_sn = 1.0 / fmax(sn_norm, kHmmMinVal);
+      const float fc = (float)ft;
+      for (int r = 0; r < K; ++r) {
+        const float rc = (float)__shfl_sync(0xffffffffu, ipn, r);
+        const float rj = (float)(__shfl_sync(0xffffffffu, w, r) * inv_sn);
+        if (own) {
+          const float base = (Bt ? Bt[r * ld + j] : (r == j ? 1.f : 0.f)) * fc;
+          if (co) co[r * K + j] = base * rc;
+          if (jo) jo[r * K + j] = base * rj;
+        }
+      }
+    }
+    const double tot = warp_sum_d(si);
+    if (own && smoothed) smoothed[(int64_t)t * K + j] = (float)(si / fmax(tot, kHmmMinVal));
+    s_next = si;
+    sn_norm = tot;
+  }
+}
+
+template <bool ALL>
+__device__ void hmm_wstage_all(const HmmParams& p, const float* Bb, float* tile) {
+  const int K = p.K, ld = K + 1, c = threadIdx.x;
+  if (ALL && p.U > 0 && c < K)
+    for (int u = 0; u < p.U; ++u)
+      for (int r = 0; r < K; ++r) tile[((int64_t)u * K + r) * ld + c] = Bb[((int64_t)r * K + c) * p.U + u];
+  __syncwarp();
+}
+
+template <bool ALL>
+__global__ void __launch_bounds__(32)
+hmm_smoother_warp_kernel(const HmmParams p, const float* __restrict__ A, const int32_t* __restrict__ obs,
+                         const float* __restrict__ obs_dist, const float* __restrict__ prior,
+                         const float* __restrict__ B, const int32_t* __restrict__ act, float* __restrict__ mll,
+                         float* __restrict__ filtered, float* __restrict__ predicted, float* __restrict__ smoothed,
+                         float* __restrict__ joint, float* __restrict__ cond) {
+  extern __shared__ __align__(16) unsigned char hmm_smem[];
+  float* tile = reinterpret_cast<float*>(hmm_smem);
+  const int64_t b = blockIdx.x;
+  const int K = p.K, ld = K + 1, T = p.T, j = threadIdx.x;
+  const bool own = j < K;
+  const float* Ab = A + b * p.A_stride;
+  const float* Bb = B + b * p.B_stride;
+  float* filt = filtered + b * (int64_t)T * K;
+  hmm_wstage_all<ALL>(p, Bb, tile);
+  double f = 0.0, m_ll = 0.0;
+  for (int t = 0; t < T; ++t) {
+    double pj;
+    if (t == 0) {
+      pj = own ? (double)prior[b * K + j] : 0.0;
+    } else {
+      const float* Bt = hmm_wtile<ALL>(p, Bb, tile, act, b, t - 1);
+      pj = f;
+      if (Bt) {
+        pj = 0.0;
+        for (int i = 0; i < K; ++i) {
+          const double fi = __shfl_sync(0xffffffffu, f, i);
+          if (own) pj += (double)Bt[j * ld + i] * fi;
+        }
+      }
+    }
+    double ll = -INFINITY;
+    if (own) {
+      ll = 0.0;
+      for (int m = 0; m < p.M; ++m) {
+        const float* Am = Ab + p.A_off[m];
+        if (obs_dist) {
+          const float* od = obs_dist + (b * T + t) * p.obs_stride + p.O_off[m];
+          double s = 0.0;
+          for (int o = 0; o < p.O[m]; ++o) s += (double)od[o] * log(fmax((double)Am[(int64_t)o * K + j], kHmmMinVal));
+          ll += s;
+        } else {
+          int o = obs[(b * T + t) * p.obs_stride + m];
+          if (o < 0) o += p.O[m];  // jnp indexing: negative from the end, then clamped
+          o = o < 0 ? 0 : (o >= p.O[m] ? p.O[m] - 1 : o);
+          ll += log(fmax((double)Am[(int64_t)o * K + j], kHmmMinVal));
+        }
+      }
+    }
+    const double lmax = warp_max_d(ll);
+    const double u = own ? pj * exp(ll - lmax) : 0.0;
+    double c = warp_sum_d(u);
+    if (c == 0.0) c = 1.0;  // _normalize_preserve_zeros: an all-zero row stays zero
+    m_ll += log(fmax(c, kHmmMinVal)) + lmax;
+    f = u / c;
+    if (own) {
+      filt[(int64_t)t * K + j] = (float)f;
+      if (predicted) predicted[(b * T + t) * K + j] = (float)pj;
+    }
+  }
+  if (mll && j == 0) mll[b] = (float)m_ll;
+  if (!smoothed && !joint && !cond) return;
+  hmm_wbackward<ALL>(p, Bb, tile, act, b, filt, smoothed ? smoothed + b * (int64_t)T * K : nullptr,
+                     joint ? joint + b * (int64_t)(T - 1) * K * K : nullptr,
+                     cond ? cond + b * (int64_t)(T - 1) * K * K : nullptr);
+}
+
+template <bool ALL>
+__global__ void __launch_bounds__(32)
+hmm_from_filtered_warp_kernel(const HmmParams p, const float* __restrict__ filtered, const float* __restrict__ B,
+                              const int32_t* __restrict__ act, float* __restrict__ smoothed,
+                              float* __restrict__ joint, float* __restrict__ cond) {
+  extern __shared__ __align__(16) unsigned char hmm_smem[];
+  float* tile = reinterpret_cast<float*>(hmm_smem);
+  const int64_t b = blockIdx.x;
+  const int K = p.K, T = p.T;
+  const float* Bb = B + b * p.B_stride;
+  hmm_wstage_all<ALL>(p, Bb, tile);
+  hmm_wbackward<ALL>(p, Bb, tile, act, b, filtered + b * (int64_t)T * K,
+                     smoothed ? smoothed + b * (int64_t)T * K : nullptr,
+                     joint ? joint + b * (int64_t)(T - 1) * K * K : nullptr,
+                     cond ? cond + b * (int64_t)(T - 1) * K * K : nullptr);
+}
+
+// Shared memory of the warp kernels; *all = every action of B staged once.
+size_t hmm_warp_smem(const HmmParams& p, bool* all) {
+  const size_t one = (size_t)p.K * (p.K + 1) * sizeof(float);
+  *all = p.U > 0 && one * p.U <= kHmmWarpStageMax;
+  return *all ? one * p.U : one;
+}
+
 constexpr size_t kHmmMaxSmem = 200 * 1024;
 
 // Validates the transition layout; fills p.U / p.B_stride / p.stage_all.
@@ -333,6 +527,19 @@ extern "C" int32_t b2_hmm_smoother(void* stream, const float* A, int64_t A_count
   if (Bn == 0) return B2_OK;
   if (!A || !prior || !B || !filtered || (!obs && !obs_dist))
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer (filtered is required)");
+  if (K <= 32) {
+    bool all = false;
+    const size_t wsmem = hmm_warp_smem(p, &all);
+    if (all)
+      hmm_smoother_warp_kernel<true><<<(unsigned)Bn, 32, wsmem, (cudaStream_t)stream>>>(
+          p, A, obs_dist ? nullptr : obs, obs_dist, prior, B, actions, mll, filtered, predicted, smoothed,
+          T > 1 ? joint : nullptr, T > 1 ? cond : nullptr);
+    else
+      hmm_smoother_warp_kernel<false><<<(unsigned)Bn, 32, wsmem, (cudaStream_t)stream>>>(
+          p, A, obs_dist ? nullptr : obs, obs_dist, prior, B, actions, mll, filtered, predicted, smoothed,
+          T > 1 ? joint : nullptr, T > 1 ? cond : nullptr);
+    return check_launch(op);
+  }
   const size_t smem = hmm_smem_bytes(p);
   B2_TRY(ensure_smem_attr((const void*)hmm_smoother_kernel, (int)kHmmMaxSmem, op));
   hmm_smoother_kernel<<<(unsigned)Bn, kHmmThreads, smem, (cudaStream_t)stream>>>(
@@ -360,6 +567,17 @@ extern "C" int32_t b2_hmm_smoother_from_filtered(void* stream, const float* filt
   B2_TRY(hmm_transitions(op, p, Bn, U, B_batched, B_count, actions, actions_count));
   if (Bn == 0) return B2_OK;
   if (!filtered || !B) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer");
+  if (K <= 32) {
+    bool all = false;
+    const size_t wsmem = hmm_warp_smem(p, &all);
+    if (all)
+      hmm_from_filtered_warp_kernel<true><<<(unsigned)Bn, 32, wsmem, (cudaStream_t)stream>>>(
+          p, filtered, B, actions, smoothed, T > 1 ? joint : nullptr, T > 1 ? cond : nullptr);
+    else
+      hmm_from_filtered_warp_kernel<false><<<(unsigned)Bn, 32, wsmem, (cudaStream_t)stream>>>(
+          p, filtered, B, actions, smoothed, T > 1 ? joint : nullptr, T > 1 ? cond : nullptr);
+    return check_launch(op);
+  }
   const size_t smem = hmm_smem_bytes(p);
   B2_TRY(ensure_smem_attr((const void*)hmm_from_filtered_kernel, (int)kHmmMaxSmem, op));
   hmm_from_filtered_kernel<<<(unsigned)Bn, kHmmThreads, smem, (cudaStream_t)stream>>>(
