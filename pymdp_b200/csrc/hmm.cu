@@ -35,6 +35,7 @@ struct HmmParams {
   int32_t obs_stride;    // M (index observations) or sum O (distributions)
   int32_t action_mode;   // 0: jnp indexing (negative from the end, clamped); 1: negative -> identity
   int32_t stage_all;     // stationary B staged once per agent
+  int32_t wstage;        // warp kernels: A, observations and actions staged in shared memory
   int64_t A_stride;      // A floats per agent (0: shared by every agent)
   int64_t B_stride;      // B floats per agent (0: shared)
   int32_t O[B2_MAX_MODALITIES];
@@ -283,11 +284,20 @@ __device__ __forceinline__ double warp_max_d(double v) {
 }
 
 // Padded [next][current] tile of transition t (nullptr = identity).
+// Action of transition t from one agent's action row (nullptr = action 0).
+__device__ __forceinline__ int hmm_waction(const HmmParams& p, const int32_t* ab, int t) {
+  if (p.U <= 0) return 0;
+  int u = ab ? ab[t] : 0;
+  if (p.action_mode == 1) return u < 0 ? -1 : (u >= p.U ? p.U - 1 : u);
+  if (u < 0) u += p.U;  // jnp indexing: negative from the end, then clamped
+  return u < 0 ? 0 : (u >= p.U ? p.U - 1 : u);
+}
+
 template <bool ALL>
 __device__ __forceinline__ const float* hmm_wtile(const HmmParams& p, const float* Bb, float* tile,
-                                                  const int32_t* act, int64_t b, int t) {
+                                                  const int32_t* ab, int t) {
   const int K = p.K, ld = K + 1, c = threadIdx.x;
-  const int u = hmm_action(p, act, b, t);
+  const int u = hmm_waction(p, ab, t);
   if (u < 0) return nullptr;
   if (ALL && p.U > 0) return tile + (int64_t)u * K * ld;
   __syncwarp();  // the lanes are done reading the previous tile
@@ -306,16 +316,18 @@ __device__ __forceinline__ const float* hmm_wtile(const HmmParams& p, const floa
 // Backward pass of one agent from its filtered marginals (each lane reads
 // back only its own entries).
 template <bool ALL>
-__device__ void hmm_wbackward(const HmmParams& p, const float* Bb, float* tile, const int32_t* act, int64_t b,
+__device__ void hmm_wbackward(const HmmParams& p, const float* Bb, float* tile, const int32_t* ab,
                               const float* filt, float* smoothed, float* joint, float* cond) {
   const int K = p.K, ld = K + 1, T = p.T, j = threadIdx.x;
   const bool own = j < K;
   double s_next = own ? (double)filt[(int64_t)(T - 1) * K + j] : 0.0;  // s_{T-1} = f_{T-1}
+  double ft_next = (own && T >= 2) ? (double)filt[(int64_t)(T - 2) * K + j] : 0.0;
   double sn_norm = warp_sum_d(s_next);
   if (own && smoothed) smoothed[(int64_t)(T - 1) * K + j] = (float)(s_next / fmax(sn_norm, kHmmMinVal));
   for (int t = T - 2; t >= 0; --t) {
-    const float* Bt = hmm_wtile<ALL>(p, Bb, tile, act, b, t);
-    const double ft = own ? (double)filt[(int64_t)t * K + j] : 0.0;
+    const double ft = ft_next;
+    if (own && t > 0) ft_next = (double)filt[(int64_t)(t - 1) * K + j];  // one step ahead: hides its latency
+    const float* Bt = hmm_wtile<ALL>(p, Bb, tile, ab, t);
     double pn = ft;  // pn_t[j] = sum_i B_t[j, i] f_t[i]
     if (Bt) {
       pn = 0.0;
@@ -382,13 +394,36 @@ hmm_smoother_warp_kernel(const HmmParams p, const float* __restrict__ A, const i
   const float* Bb = B + b * p.B_stride;
   float* filt = filtered + b * (int64_t)T * K;
   hmm_wstage_all<ALL>(p, Bb, tile);
+  // this agent's A, observations and actions: staged once, so no step waits on
+  // a chain of global loads (observation -> row of A, action -> tile)
+  const int64_t a_words = p.A_off[p.M - 1] + (int64_t)p.O[p.M - 1] * K;
+  const int64_t o_words = (int64_t)T * p.obs_stride;
+  const float* Aw = Ab;
+  const int32_t* obw = obs ? obs + b * o_words : nullptr;
+  const float* odw = obs_dist ? obs_dist + b * o_words : nullptr;
+  const int32_t* aw = act ? act + b * (T - 1) : nullptr;
+  if (p.wstage) {
+    const size_t tile_bytes = ((size_t)((ALL && p.U > 0) ? p.U : 1) * K * ld * sizeof(float) + 15) & ~size_t(15);
+    float* As = reinterpret_cast<float*>(hmm_smem + tile_bytes);
+    uint32_t* Os = reinterpret_cast<uint32_t*>(As + a_words);
+    int32_t* Ws = reinterpret_cast<int32_t*>(Os + o_words);
+    for (int64_t e = j; e < a_words; e += 32) As[e] = Ab[e];
+    const uint32_t* osrc = obs_dist ? reinterpret_cast<const uint32_t*>(odw) : reinterpret_cast<const uint32_t*>(obw);
+    for (int64_t e = j; e < o_words; e += 32) Os[e] = osrc[e];
+    if (aw)
+      for (int e = j; e < T - 1; e += 32) Ws[e] = aw[e];
+    __syncwarp();
+    Aw = As;
+    if (obs_dist) odw = reinterpret_cast<const float*>(Os); else obw = reinterpret_cast<const int32_t*>(Os);
+    if (aw) aw = Ws;
+  }
   double f = 0.0, m_ll = 0.0;
   for (int t = 0; t < T; ++t) {
     double pj;
     if (t == 0) {
       pj = own ? (double)prior[b * K + j] : 0.0;
     } else {
-      const float* Bt = hmm_wtile<ALL>(p, Bb, tile, act, b, t - 1);
+      const float* Bt = hmm_wtile<ALL>(p, Bb, tile, aw, t - 1);
       pj = f;
       if (Bt) {
         pj = 0.0;
@@ -402,14 +437,14 @@ hmm_smoother_warp_kernel(const HmmParams p, const float* __restrict__ A, const i
     if (own) {
       ll = 0.0;
       for (int m = 0; m < p.M; ++m) {
-        const float* Am = Ab + p.A_off[m];
+        const float* Am = Aw + p.A_off[m];
         if (obs_dist) {
-          const float* od = obs_dist + (b * T + t) * p.obs_stride + p.O_off[m];
+          const float* od = odw + (int64_t)t * p.obs_stride + p.O_off[m];
           double s = 0.0;
           for (int o = 0; o < p.O[m]; ++o) s += (double)od[o] * log(fmax((double)Am[(int64_t)o * K + j], kHmmMinVal));
           ll += s;
         } else {
-          int o = obs[(b * T + t) * p.obs_stride + m];
+          int o = obw[(int64_t)t * p.obs_stride + m];
           if (o < 0) o += p.O[m];  // jnp indexing: negative from the end, then clamped
           o = o < 0 ? 0 : (o >= p.O[m] ? p.O[m] - 1 : o);
           ll += log(fmax((double)Am[(int64_t)o * K + j], kHmmMinVal));
@@ -429,7 +464,7 @@ hmm_smoother_warp_kernel(const HmmParams p, const float* __restrict__ A, const i
   }
   if (mll && j == 0) mll[b] = (float)m_ll;
   if (!smoothed && !joint && !cond) return;
-  hmm_wbackward<ALL>(p, Bb, tile, act, b, filt, smoothed ? smoothed + b * (int64_t)T * K : nullptr,
+  hmm_wbackward<ALL>(p, Bb, tile, aw, filt, smoothed ? smoothed + b * (int64_t)T * K : nullptr,
                      joint ? joint + b * (int64_t)(T - 1) * K * K : nullptr,
                      cond ? cond + b * (int64_t)(T - 1) * K * K : nullptr);
 }
@@ -445,17 +480,26 @@ hmm_from_filtered_warp_kernel(const HmmParams p, const float* __restrict__ filte
   const int K = p.K, T = p.T;
   const float* Bb = B + b * p.B_stride;
   hmm_wstage_all<ALL>(p, Bb, tile);
-  hmm_wbackward<ALL>(p, Bb, tile, act, b, filtered + b * (int64_t)T * K,
+  hmm_wbackward<ALL>(p, Bb, tile, act ? act + b * (T - 1) : nullptr, filtered + b * (int64_t)T * K,
                      smoothed ? smoothed + b * (int64_t)T * K : nullptr,
                      joint ? joint + b * (int64_t)(T - 1) * K * K : nullptr,
                      cond ? cond + b * (int64_t)(T - 1) * K * K : nullptr);
 }
 
+constexpr size_t kHmmWarpInputMax = 40 * 1024;  // staged A + observations + actions per agent
+
 // Shared memory of the warp kernels; *all = every action of B staged once.
-size_t hmm_warp_smem(const HmmParams& p, bool* all) {
+// With `inputs`, also decides p.wstage (A, observations and actions staged).
+size_t hmm_warp_smem(HmmParams& p, bool* all, bool inputs) {
   const size_t one = (size_t)p.K * (p.K + 1) * sizeof(float);
   *all = p.U > 0 && one * p.U <= kHmmWarpStageMax;
-  return *all ? one * p.U : one;
+  const size_t tile = ((*all ? one * p.U : one) + 15) & ~size_t(15);
+  p.wstage = 0;
+  if (!inputs) return tile;
+  const size_t a_words = (size_t)(p.A_off[p.M - 1] + (int64_t)p.O[p.M - 1] * p.K);
+  const size_t extra = 4 * (a_words + (size_t)p.T * p.obs_stride + (size_t)p.T);
+  p.wstage = extra <= kHmmWarpInputMax ? 1 : 0;
+  return tile + (p.wstage ? extra : 0);
 }
 
 constexpr size_t kHmmMaxSmem = 200 * 1024;
@@ -529,7 +573,10 @@ extern "C" int32_t b2_hmm_smoother(void* stream, const float* A, int64_t A_count
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer (filtered is required)");
   if (K <= 32) {
     bool all = false;
-    const size_t wsmem = hmm_warp_smem(p, &all);
+    const size_t wsmem = hmm_warp_smem(p, &all, true);
+    const int wmax = (int)(kHmmWarpStageMax + kHmmWarpInputMax + 16);
+    B2_TRY(ensure_smem_attr((const void*)hmm_smoother_warp_kernel<true>, wmax, op));
+    B2_TRY(ensure_smem_attr((const void*)hmm_smoother_warp_kernel<false>, wmax, op));
     if (all)
       hmm_smoother_warp_kernel<true><<<(unsigned)Bn, 32, wsmem, (cudaStream_t)stream>>>(
           p, A, obs_dist ? nullptr : obs, obs_dist, prior, B, actions, mll, filtered, predicted, smoothed,
@@ -569,7 +616,7 @@ extern "C" int32_t b2_hmm_smoother_from_filtered(void* stream, const float* filt
   if (!filtered || !B) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer");
   if (K <= 32) {
     bool all = false;
-    const size_t wsmem = hmm_warp_smem(p, &all);
+    const size_t wsmem = hmm_warp_smem(p, &all, false);
     if (all)
       hmm_from_filtered_warp_kernel<true><<<(unsigned)Bn, 32, wsmem, (cudaStream_t)stream>>>(
           p, filtered, B, actions, smoothed, T > 1 ? joint : nullptr, T > 1 ? cond : nullptr);
