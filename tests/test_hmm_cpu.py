@@ -78,3 +78,33 @@ def test_hmm_abi_validation():
     # an empty batch is a valid no-op
     rc = lib.b2_hmm_smoother_from_filtered(None, fake, 0, fake, 50, 0, 2, fake, 0, 1, 0, 3, 5, fake, 0, 0)
     assert rc == _lib.B2_OK
+
+
+def test_transition_layout_rules():
+    """The host classifies B as the reference's per-sequence shapes plus an
+    optional batch axis (no device work)."""
+    import torch
+
+    from pymdp_b200.hmm import _transitions
+    Bn, T, K = 3, 5, 4
+    # action axis: shared (K, K, U) or batched (Bn, K, K, U), actions reshaped to (Bn, T-1)
+    t, batched, U, a = _transitions(torch.zeros(K, K, 2), np.zeros((Bn, T - 1, 1), np.int64), Bn, T, K)
+    assert (batched, U, tuple(a.shape), a.dtype) == (0, 2, (Bn, T - 1), torch.int32)
+    t, batched, U, a = _transitions(torch.zeros(Bn, K, K, 2), np.zeros((Bn, T - 1)), Bn, T, K)
+    assert (batched, U) == (1, 2)
+    # stationary without actions: one action
+    t, batched, U, a = _transitions(torch.zeros(K, K), None, Bn, T, K)
+    assert (batched, U, a, tuple(t.shape)) == (0, 1, None, (K, K, 1))
+    t, batched, U, a = _transitions(torch.zeros(Bn, K, K), None, Bn, T, K)
+    assert (batched, U, tuple(t.shape)) == (1, 1, (Bn, K, K, 1))
+    # time-varying (T-1, K, K), shared or batched
+    t, batched, U, a = _transitions(torch.zeros(T - 1, K, K), None, Bn, T, K)
+    assert (batched, U) == (0, 0)
+    t, batched, U, a = _transitions(torch.zeros(Bn, T - 1, K, K), None, Bn, T, K)
+    assert (batched, U) == (1, 0)
+    # several actions and no action history: the reference's error
+    with pytest.raises(ValueError):
+        _transitions(torch.zeros(K, K, 3), None, Bn, T, K)
+    # one observation: no transition is taken, any action axis is accepted
+    t, batched, U, a = _transitions(torch.zeros(K, K, 3), None, Bn, 1, K)
+    assert U == 3
