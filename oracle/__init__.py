@@ -14,6 +14,8 @@ JAX implementation (the branch its CI runs):
   sampling, empirical prior, planning, action).
 * ``oracle.learning`` — ``pymdp/learning.py:11-233`` and the filtering branch
   of ``Agent.infer_parameters`` (``pymdp/agent.py:416-620``).
+* ``oracle.mmp`` — sequence inference, ``run_mmp`` / ``run_vmp``
+  (``pymdp/algos.py:157-571``): the checker for a sequence-inference kernel.
 * ``oracle.hmm`` — ``run_exact_single_factor_hmm_scan`` /
   ``hmm_smoother_from_filtered_colstoch`` (``pymdp/algos.py:959-1208``) and
   ``smoothing_exact`` (``pymdp/inference.py:595-634``).
@@ -21,7 +23,8 @@ JAX implementation (the branch its CI runs):
 Parity pin: the functions are checked against golden vectors produced by
 running the reference's own Python code (``tests/golden/make_golden*.py``
 through ``tests/golden/refshim.py``): ``tests/test_oracle_golden.py``,
-``tests/test_learning_cpu.py``, ``tests/test_hmm_cpu.py``. The same
+``tests/test_learning_cpu.py``, ``tests/test_hmm_cpu.py``,
+``tests/test_seq_oracle_cpu.py``. The same
 functions, run on a spawned process pool over the host cores, are the timed
 CPU baseline of ``bench.py``.
 
