@@ -4,6 +4,8 @@
 * ``update_state_transition_dirichlet``  ``pymdp/learning.py:119-233``
 * ``dirichlet_expected_value``           ``pymdp/maths.py:843-862`` (clip at
   MINVAL, normalise over axis 0)
+* ``update_state_transition_from_joint`` ``learning.py:119-157`` with given
+  pairwise joints (the smoothing algorithms' form)
 * ``infer_parameters``                   ``pymdp/agent.py:416-620`` for the
   filtering algorithms (``fpi`` / ``mmp`` / ``vmp``): A learns from the
   marginal beliefs, B from joints built out of the belief sequence
@@ -83,6 +85,17 @@ def update_state_transition_dirichlet(pB, B, joint_beliefs, actions, num_control
         qB.append(pb)
         E_qB.append(dirichlet_expected_value(pb))
     return qB, E_qB
+
+
+def update_state_transition_from_joint(pB_f, joint, actions_f, num_controls_f, lr=1.0):
+    """``learning.py:119-157`` with a joint array (the smoothing algorithms'
+    form, ``:153``): ``joint`` ``(T-1, S_f, S_prev...)`` pairwise posteriors,
+    ``actions_f`` ``(T-1,)``; ``pB_f += lr * sum_t joint_t (x) onehot(a_t)``.
+    Returns ``(qB_f, E_qB_f)``."""
+    a = one_hot(np.asarray(actions_f), num_controls_f)
+    d = sum(outer([np.asarray(joint[t], np.float64), a[t]]) for t in range(a.shape[0]))
+    qb = np.asarray(pB_f, np.float64) + lr * d
+    return qb, dirichlet_expected_value(qb)
 
 
 def infer_parameters(pA, A, pB, B, beliefs_A, observations, actions, A_dependencies, B_dependencies, num_obs,

@@ -127,18 +127,52 @@ def make_B_case(ref, cfg, seed):
     return out
 
 
-def main(ref_root):
+# name -> (S_f, S_prev, U, T, lr, Bn): learning from given pairwise joints, the
+# smoothing algorithms' form (a joint array per factor, learning.py:153)
+JOINT_CASES = {
+    "learn_B_joint": (5, 5, 3, 6, [0.7, 1.4], 2),
+}
+
+
+def make_joint_case(ref, cfg, seed):
+    S, Sp, U, T, lr, Bn = cfg
+    rng = np.random.default_rng(seed)
+    B = np.stack([dirichlet_cols(rng, (S, Sp, U)) for _ in range(Bn)])
+    pB = f32(rng.uniform(0.05, 3.0, size=B.shape))
+    g = np.maximum(rng.gamma(1.0, size=(Bn, T - 1, S, Sp)), 1e-30)
+    joint = f32(g / g.sum(axis=(2, 3), keepdims=True))
+    actions = rng.integers(0, U, size=(Bn, T - 1, 1)).astype(np.int64)
+    actions[0, 1, 0] = -1  # one_hot gives zeros: this transition adds nothing
+    lr = f32(lr)
+    qB, EB = [], []
+    for b in range(Bn):
+        q, e = ref.learning.update_state_transition_dirichlet(
+            [pB[b]], [B[b]], [joint[b]], actions[b], num_controls=[U], lr=lr[b])
+        qB.append(q[0])
+        EB.append(e[0])
+    return {"U": np.array(U), "lr": lr, "Bn": np.array(Bn), "B": B, "pB": pB, "joint": joint, "actions": actions,
+            "qB": np.stack(qB), "EB": np.stack(EB)}
+
+
+def main(ref_root, names=None):
     sys.path.insert(0, HERE)
     import refshim
 
     ref = refshim.load_reference(ref_root, modules=("utils", "maths", "learning"))
+    want = (lambda n: names is None or n in names)  # noqa: E731
     for i, (name, cfg) in enumerate(A_CASES.items()):
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_A_case(ref, cfg, 100 + i))
-        print("wrote", name)
+        if want(name):
+            np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_A_case(ref, cfg, 100 + i))
+            print("wrote", name)
     for i, (name, cfg) in enumerate(B_CASES.items()):
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_B_case(ref, cfg, 200 + i))
-        print("wrote", name)
+        if want(name):
+            np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_B_case(ref, cfg, 200 + i))
+            print("wrote", name)
+    for i, (name, cfg) in enumerate(JOINT_CASES.items()):
+        if want(name):
+            np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_joint_case(ref, cfg, 250 + i))
+            print("wrote", name)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)

@@ -151,3 +151,15 @@ def test_learning_abi_validation():
 def test_layout_learning_wrappers_exist():
     lay = ffi.EfeLayout([4, 3], [5], [2, 1], 1, [[0, 1]], [[0], [1]])
     assert callable(lay.learn_A) and callable(lay.learn_B)
+
+
+def test_oracle_transition_model_from_joints_matches_reference_fixture():
+    """The smoothing algorithms' form: pB learns from given pairwise joints
+    (learning.py:153, a joint array per factor) — the checker for a
+    joint-input transition update."""
+    d = load_golden("learn_B_joint")
+    for b in range(int(d["Bn"])):
+        qb, eb = ol.update_state_transition_from_joint(d["pB"][b], d["joint"][b], d["actions"][b][:, 0],
+                                                       int(d["U"]), lr=d["lr"][b])
+        np.testing.assert_allclose(qb, d["qB"][b], rtol=1e-13, atol=0)
+        np.testing.assert_allclose(eb, d["EB"][b], rtol=1e-13, atol=1e-300)
