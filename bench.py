@@ -87,9 +87,10 @@ def fpi_bytes_per_agent_cfg(S, O, deps) -> float:
     return 4.0 * sum(K) + 8.0 * sum(S) + 4.0 * len(O)
 
 
-def run_fpi_config(dev, steps: int, warmup: int, flush):
-    """FPI alone on the 4096-agent model: device time per launch (L2 flushed
-    before each), agent-steps/s and algorithmic HBM GB/s."""
+def run_fpi_config(dev, steps: int, warmup: int, flush, agents: int = FPI_AGENTS):
+    """FPI alone on the FPI benchmark model (4096 agents; more for the
+    throughput sweep): device time per launch (L2 flushed before each),
+    agent-steps/s and algorithmic HBM GB/s."""
     import torch
 
     from pymdp_b200 import ffi
@@ -102,11 +103,11 @@ def run_fpi_config(dev, steps: int, warmup: int, flush):
         g = torch._standard_gamma(torch.full(shape, alpha, device=dev), generator=gen) + 1e-30
         return g / g.sum(1, keepdim=True)
 
-    A = [dirichlet((FPI_AGENTS, o) + tuple(FPI_S[d] for d in dp), 0.5) for o, dp in zip(FPI_O, deps)]
+    A = [dirichlet((agents, o) + tuple(FPI_S[d] for d in dp), 0.5) for o, dp in zip(FPI_O, deps)]
     A_flat, A_off = ffi.flatten_ragged_f32(A, 1, dev)
     del A
-    prior = torch.cat([dirichlet((FPI_AGENTS, s), 1.0) for s in FPI_S], dim=1).contiguous()
-    obs = torch.stack([torch.randint(0, o, (FPI_AGENTS,), device=dev, generator=gen) for o in FPI_O],
+    prior = torch.cat([dirichlet((agents, s), 1.0) for s in FPI_S], dim=1).contiguous()
+    obs = torch.stack([torch.randint(0, o, (agents,), device=dev, generator=gen) for o in FPI_O],
                       dim=1).to(torch.int32).contiguous()
     out = torch.empty_like(prior)
 
@@ -126,10 +127,10 @@ def run_fpi_config(dev, steps: int, warmup: int, flush):
         evs.append((e0, e1))
     torch.cuda.synchronize(dev)
     ms = sum(a.elapsed_time(b) for a, b in evs) / steps
-    nbytes = fpi_bytes_per_agent_cfg(FPI_S, FPI_O, deps) * FPI_AGENTS
-    return {"workload": f"FPI only, {FPI_AGENTS} agents, S={FPI_S}, O={FPI_O}, A_m on 2 random factors (K=256), "
+    nbytes = fpi_bytes_per_agent_cfg(FPI_S, FPI_O, deps) * agents
+    return {"workload": f"FPI only, {agents} agents, S={FPI_S}, O={FPI_O}, A_m on 2 random factors (K=256), "
                         f"{FPI_ITERS} iterations, L2 flushed before each launch",
-            "agent_steps_per_s": FPI_AGENTS / (ms * 1e-3), "ms_per_launch": ms,
+            "agent_steps_per_s": agents / (ms * 1e-3), "ms_per_launch": ms,
             "bytes_per_launch": nbytes, "gbs": nbytes / (ms * 1e-3) / 1e9}
 
 
@@ -293,7 +294,7 @@ def run_fit_config(dev, steps: int, warmup: int, flush):
                         "C and log gamma (native FPI / neg-EFE adjoints, one CUDA graph), L2 flushed before each",
             "subject_steps_per_s": FIT_SUBJECTS * FIT_TRIALS / (ms * 1e-3), "ms_per_evaluation": ms,
             "native_launches_per_evaluation": native // (max(warmup, 1) + 1),
-            "log_likelihood": float(graphed.ll)}
+            "log_likelihood": float(graphed.ll.detach())}
 
 
 RO_AGENTS, RO_STEPS = 2000, 100
@@ -481,43 +482,253 @@ def reduce_max_over_ranks(values, world: int, device="cpu") -> list:
     return [float(x) for x in t.tolist()]
 
 
+MINVAL = float(np.finfo(np.float64).eps)
+
+
+class RefCpuStep:
+    """The agent step on the reference's own CPU FFI kernels (``oracle/_ref``):
+    the observed log-likelihood slices (``compute_log_likelihood_per_modality``,
+    done here in NumPy as the reference does it in XLA before its FFI call),
+    FpiCpu (16 iterations), NegEfeCpu over all 4096 policies (utility + state
+    information gain, policy matrix broadcast over the batch as JAX's
+    ``vmap_method="broadcast_all"`` passes it), q_pi = softmax(gamma G + log E)
+    and the first-max action. The model is flattened once, outside the timed
+    calls, as the GPU path does at ``Agent`` construction."""
+
+    def __init__(self, model, idx):
+        from oracle import efe as oefe
+        from oracle import refcpu
+
+        self.refcpu = refcpu
+        A, B, C, D, obs = model
+        idx = np.asarray(list(idx))
+        n = len(idx)
+        self.n = n
+        flat = lambda xs: np.ascontiguousarray(np.concatenate(  # noqa: E731
+            [np.asarray(x[idx], np.float32).reshape(n, -1) for x in xs], axis=1))
+        self.A = [np.ascontiguousarray(a[idx]) for a in A]
+        self.obs = obs[idx]
+        self.A_flat, self.B_flat = flat(A), flat(B)
+        self.C_flat = flat([np.repeat(c[:, None, :], T, 1) for c in C])
+        self.lp = np.log(np.maximum(flat(D), MINVAL)).astype(np.float32)
+        self.I = np.zeros((n, sum(S)), np.float32)
+        self.pol = oefe.construct_policies(S, U, T).astype(np.int32)
+        self.pm = np.ascontiguousarray(np.broadcast_to(self.pol, (n,) + self.pol.shape))
+        F, M = len(S), len(O)
+        self.A_deps, self.B_deps = [list(range(F))] * M, [[f] for f in range(F)]
+        self.spans = refcpu.efe_spans(S, O, U, T, self.A_deps, self.B_deps)
+        K = int(np.prod(S))
+        self.ll_off = np.cumsum([0] + [K] * M)
+        self.logE = np.log(np.full(len(self.pol), 1.0 / len(self.pol)))
+
+    def __call__(self):
+        n, K = self.n, int(np.prod(S))
+        rows = np.arange(n)
+        ll = np.concatenate([np.log(np.maximum(a[rows, self.obs[:, m]].reshape(n, K), MINVAL))
+                             for m, a in enumerate(self.A)], axis=1).astype(np.float32)
+        qs = self.refcpu.fpi_cpu(ll, self.lp, S, self.ll_off, self.A_deps, NUM_ITER)
+        G = self.refcpu.neg_efe_cpu(self.pm, qs, self.A_flat, self.B_flat, self.C_flat, self.I, self.spans)
+        z = GAMMA * G.astype(np.float64) + self.logE
+        z -= z.max(axis=1, keepdims=True)
+        q_pi = np.exp(z)
+        q_pi /= q_pi.sum(axis=1, keepdims=True)
+        return qs, G, q_pi, self.pol[np.argmax(q_pi, axis=1), 0]
+
+
+def ref_cpu_available() -> bool:
+    try:
+        from oracle import ref_build
+
+        ref_build.load()
+        return True
+    except Exception:  # noqa: BLE001
+        return False
+
+
+def ref_cpu_desc() -> str:
+    from oracle import ref_build
+
+    return (f"reference NegEfeCpu + FpiCpu (pymdp/ffi CPU kernels compiled from the reference's sources, "
+            f"-O3 -ffast-math -march={ref_build.VARIANTS[ref_build.variant()]} -fopenmp, FP32), OpenMP on "
+            f"{os.cpu_count()} host threads")
+
+
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the agent step on the same
+    256-agent model, all of its agents every step (rank 0 only)."""
     if rank != 0:
         return
-    workers = cpu_workers()
     n_agents = args.agents
     model = make_model(1234, n_agents)
-    pool = OraclePool(workers)
-    try:
-        per_step = min(workers, n_agents)  # one agent per worker per step (bounded sample)
-        pool.run(model, range(per_step))
-        for _ in range(max(0, args.warmup - 1)):
-            pool.run(model, range(per_step))
-        times = [pool.run(model, [(i * per_step + k) % n_agents for k in range(per_step)])[1]
-                 for i in range(args.steps)]
-    finally:
-        pool.close()
+    if not ref_cpu_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU FFI kernels) "
+                          "was not built: run python -m oracle.ref_build where the reference sources are"}))
+        return
+    step = RefCpuStep(model, range(n_agents))
+    for _ in range(max(1, args.warmup)):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
     total = sum(times)
-    value = args.steps * per_step / total
+    value = args.steps * n_agents / total
     line = {
         "impl": "reference", "metric": "agent-steps/s", "value": value, "unit": "agent-steps/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload(n_agents), "agents_per_step": per_step},
-        "cpu_baseline": {"value": value, "unit": "agent-steps/s", "cores": workers, "kind": "port",
-                         "sample": f"{per_step} agents per step of the same model, one per worker process "
-                                   f"(FP64 NumPy oracle: FPI + EFE over 4096 policies + q_pi + action)"},
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload(n_agents), "agents_per_step": n_agents, "same_config": True},
+        "cpu_baseline": {"value": value, "unit": "agent-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": f"all {n_agents} agents of the workload per step: " + ref_cpu_desc()},
         "e2e": {"value": value, "unit": "agent-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def measure_peaks(dev) -> dict:
+    """Dense-matmul peaks of this GPU measured in the run (best of 5 after
+    warm-up, CUDA events): TF32 tensor cores (torch.matmul on FP32 with TF32
+    allowed) and FP32 SIMT (the same matmul with TF32 disallowed). They are
+    the roofline denominators of the TF32 and FP32-SIMT kernels; the HBM and
+    BF16 figures come from MEASURED_PEAKS.json."""
+    import torch
+
+    n = 8192
+    a = torch.randn((n, n), device=dev)
+    b = torch.randn((n, n), device=dev)
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    try:
+        for name, tf32 in (("tf32_tflops", True), ("fp32_simt_tflops", False)):
+            torch.backends.cuda.matmul.allow_tf32 = tf32
+            for _ in range(2):
+                torch.matmul(a, b)
+            best = float("inf")
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                torch.matmul(a, b)
+                e1.record()
+                torch.cuda.synchronize(dev)
+                best = min(best, e0.elapsed_time(e1))
+            out[name] = 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    out["how"] = f"torch.matmul FP32 {n}^3, TF32 allowed / disallowed, best of 5 (CUDA events)"
+    return out
+
+
+# Config 1: the plain single agent (S=[3,2], O=[3,5], U=[3,1], policy_len 1, 16 iterations, gamma 16).
+C1_S, C1_O, C1_U = [3, 2], [3, 5], [3, 1]
+
+
+def make_config1(seed: int):
+    rng = np.random.default_rng(seed)
+
+    def norm0(shape):
+        x = rng.uniform(0, 1, size=shape)
+        return (x / x.sum(0, keepdims=True)).astype(np.float32)
+
+    A = [norm0((o, 3, 2)) for o in C1_O]
+    B = [norm0((3, 3, 3)), norm0((2, 2, 1))]
+    obs = rng.integers(0, np.array(C1_O), size=(1, len(C1_O))).astype(np.int32)
+    return A, B, obs
+
+
+def run_config1(dev, steps: int, warmup: int):
+    """The plain single agent: one agent step (infer_states -> infer_policies
+    -> sample_action) through ``Agent``, captured once in a CUDA graph and
+    replayed; agent-steps/s = replays per second (launch/latency bound)."""
+    import torch
+
+    from pymdp_b200 import Agent
+
+    A, B, obs = make_config1(5)
+    agent = Agent(A, B, policy_len=1, gamma=16.0, batch_size=1, num_iter=NUM_ITER, device=dev)
+    obs_d = torch.as_tensor(obs, device=dev)
+    prior = [torch.full((1, s), 1.0 / s, device=dev) for s in C1_S]
+    stream = torch.cuda.Stream(dev)
+
+    def step():
+        qs = agent.infer_states(obs_d, prior)
+        q_pi, _ = agent.infer_policies(qs)
+        return agent.sample_action(q_pi)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(warmup, 1)):
+            step()
+    torch.cuda.synchronize(dev)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        act = step()
+    reps = 200
+    for _ in range(max(warmup, 1)):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps * reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    us = e0.elapsed_time(e1) * 1e3 / (steps * reps)
+    # eager (no graph): the same calls launched one by one from Python
+    t0 = time.perf_counter()
+    for _ in range(steps * 20):
+        step()
+    torch.cuda.synchronize(dev)
+    eager_us = (time.perf_counter() - t0) * 1e6 / (steps * 20)
+    return {"workload": "plain single agent: S=[3,2], O=[3,5], U=[3,1], A/B uniform(0,1) normalised, C/D/E uniform, "
+                        "policy_len 1, 16 FPI iterations, gamma 16; infer_states -> infer_policies -> sample_action",
+            "agent_steps_per_s": 1e6 / us, "us_per_step_graph": us, "us_per_step_eager": eager_us,
+            "action": act.cpu().tolist()}
+
+
+def run_plain_config(dev, model, steps: int, warmup: int, flush):
+    """The same agent step over the same 256 agents with the plain per-policy
+    kernel: one thread per (agent, policy) in FP32 SIMT, every policy's full
+    roll-out and contraction (no tensor cores, no shared policy prefixes). Its
+    agent-steps/s is the denominator of the fused-vs-plain ratio."""
+    import torch
+
+    from pymdp_b200 import Agent
+
+    A, B, C, D, obs = model
+    agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=len(obs), num_iter=NUM_ITER, device=dev,
+                  precision="fp32")
+    obs_d = torch.as_tensor(obs, device=dev)
+    prior_d = [torch.as_tensor(d, device=dev) for d in D]
+
+    def step():
+        qs = agent.infer_states(obs_d, prior_d)
+        q_pi, _ = agent.infer_policies(qs)
+        return agent.sample_action(q_pi)
+
+    for _ in range(max(1, warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        act = step()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    return {"kernel": "efe_plain_kernel (FP32 SIMT, one thread per agent and policy) after the same fused FPI",
+            "agent_steps_per_s": len(obs) / (ms * 1e-3), "ms_per_step": ms, "actions": act.cpu().numpy()}
 
 
 def run_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
 
-    from pymdp_b200 import Agent, _lib, ffi
+    from pymdp_b200 import Agent, _lib
 
     sample = 0 if world > 1 else (cpu_workers() if args.cpu_sample is None else args.cpu_sample)
     n_agents = args.agents
@@ -534,12 +745,16 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     fpi_res = run_fpi_config(dev, args.steps, args.warmup, flush)
-    # the fitting and rollout workloads are single-GPU measurements: run with N = 1 only
+    fpi_big = run_fpi_config(dev, args.steps, args.warmup, flush, 65536) if world == 1 else None
+    # single-GPU side measurements: run with N = 1 only
     extras = args.legs == "all" and world == 1
+    peaks_run = measure_peaks(dev) if world == 1 else {}
     fit_res = run_fit_config(dev, args.steps, args.warmup, flush) if extras else None
     ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if extras else None
     learn_res = run_learn_config(dev, args.steps, args.warmup, flush) if extras else None
     hmm_res = run_hmm_config(dev, args.steps, args.warmup, flush) if extras else None
+    c1_res = run_config1(dev, args.steps, args.warmup) if world == 1 else None
+    plain_res = run_plain_config(dev, model, min(args.steps, 3), 1, flush) if world == 1 else None
     efe_ev = []
 
     def step(timed_efe=False):
@@ -609,28 +824,34 @@ def run_b200(args, rank, world, local_rank):
     d2h = act_h.numel() * 4
     ms, e2e_ms, efe_ms = reduce_max_over_ranks([ms, e2e_ms, efe_ms], world, dev)
     if rank != 0:
+        if pool is not None:
+            pool.close()
         return
-    import json as _json
     peaks = {}
     try:
-        peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:  # noqa: BLE001
         pass
-    peak_tf = peaks.get("bf16_tflops", 1590.0)
-    peak_gbs = peaks.get("hbm_gbs", 6650.0)
     tree = agent.precision != "fp32"  # the tensor-core paths evaluate each policy prefix once
+    if agent.precision == "tf32x3" and "tf32_tflops" in peaks_run:
+        peak_tf, peak_src = peaks_run["tf32_tflops"], "TF32 dense matmul measured in this run (torch.matmul, TF32)"
+    elif agent.precision == "fp32" and "fp32_simt_tflops" in peaks_run:
+        peak_tf, peak_src = peaks_run["fp32_simt_tflops"], "FP32 SIMT matmul measured in this run"
+    else:
+        peak_tf = peaks.get("bf16_tflops", 1590.0)
+        peak_src = "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"
+    peak_gbs = peaks.get("hbm_gbs", 6650.0)
     flops = efe_flops_per_agent(tree) * n_agents
     dense_flops = efe_flops_per_agent(False) * n_agents
     achieved_tf = flops / (efe_ms * 1e-3) / 1e12
     total_agents = n_agents * world
     value = total_agents * args.steps / (ms * 1e-3)
-    cpu_val = cpu_dt = err = None
+    err = None
     if pool is not None:
         try:
-            ref, cpu_dt = pool.run(model, range(sample))
+            ref, _ = pool.run(model, range(sample))
         finally:
             pool.close()
-        cpu_val = sample / cpu_dt
         qs_g, G_g, q_pi_g, act_g = chk
         err = {
             "agents": sample,
@@ -641,6 +862,24 @@ def run_b200(args, rank, world, local_rank):
             "q_pi_max_abs": max(float(np.max(np.abs(q_pi_g[b] - ref[b][2]))) for b in range(sample)),
             "actions_equal": int(sum(bool(np.array_equal(act_g[b], ref[b][3])) for b in range(sample))),
         }
+    cpu_base = None
+    if world == 1 and ref_cpu_available() and args.cpu_sample != 0:
+        # the reference's own CPU agent step on a bounded sample of the same agents (about 10-30 s of CPU work)
+        n_ref = min(n_agents, args.ref_sample)
+        rstep = RefCpuStep(model, range(n_ref))
+        rstep()
+        reps, t0 = 0, time.perf_counter()
+        while reps < 2 or (time.perf_counter() - t0 < 10.0 and reps < 20):
+            rstep()
+            reps += 1
+        dt = time.perf_counter() - t0
+        cpu_base = {"value": reps * n_ref / dt, "unit": "agent-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                    "sample": f"agents 0..{n_ref - 1} of the timed model x {reps} steps ({dt:.1f} s): "
+                              + ref_cpu_desc()}
+    fused_over_plain = None
+    if plain_res is not None:
+        fused_over_plain = value / plain_res["agent_steps_per_s"]
+        plain_res["actions_equal_fused"] = int((plain_res.pop("actions") == chk[3]).all(axis=1).sum())
     line = {
         "metric": "agent-steps/s", "value": value, "unit": "agent-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -651,22 +890,27 @@ def run_b200(args, rank, world, local_rank):
         "e2e": {"value": total_agents * args.steps / (e2e_ms * 1e-3), "unit": "agent-steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
+        "fused_over_plain": fused_over_plain,
+        "plain": plain_res,
+        "config1": c1_res,
         "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": achieved_tf / peak_tf,
                      "traffic": (EFE_TRAFFIC_PER_AGENT[agent.precision] * n_agents
                                  if agent.precision in EFE_TRAFFIC_PER_AGENT else None),
-                     "kernel": f"neg-EFE launch over {n_agents} agents (W pack + policy evaluation + q_pi)",
+                     "kernel": f"neg-EFE launch over {n_agents} agents (policy evaluation + q_pi)",
                      "flops_per_launch": flops, "ms_per_launch": efe_ms,
                      "policy_tree": tree, "dense_equivalent_flops_per_launch": dense_flops,
                      "dense_equivalent_tflops": dense_flops / (efe_ms * 1e-3) / 1e12,
-                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"},
-        "cpu_baseline": None if cpu_val is None else {
-            "value": cpu_val, "unit": "agent-steps/s", "cores": min(sample, cpu_workers()), "kind": "port",
-            "sample": f"agents 0..{sample - 1} of the timed model, full agent step, FP64 NumPy oracle, one worker "
-                      f"process per core ({cpu_dt:.1f} s wall)"},
+                     "dense_equivalent_frac": dense_flops / (efe_ms * 1e-3) / 1e12 / peak_tf,
+                     "peak_source": peak_src},
+        "peaks_measured": peaks_run or None,
+        "cpu_baseline": cpu_base,
         "error_vs_fp64": err,
         "fpi": dict(fpi_res, roofline={"bound": "hbm", "achieved": fpi_res["gbs"], "peak": peak_gbs, "unit": "GB/s",
                                        "frac": fpi_res["gbs"] / peak_gbs}),
+        "fpi_65536": None if fpi_big is None else dict(
+            fpi_big, roofline={"bound": "hbm", "achieved": fpi_big["gbs"], "peak": peak_gbs, "unit": "GB/s",
+                               "frac": fpi_big["gbs"] / peak_gbs}),
         "fit": fit_res,
         "rollout": ro_res,
         "learn": learn_res,
@@ -674,6 +918,19 @@ def run_b200(args, rank, world, local_rank):
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
+
+
+def relaunch_under_torchrun(n: int):
+    """``--gpus N`` without a torchrun environment: run this same command as N
+    ranks (one process per GPU) under torch.distributed.run on 127.0.0.1."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    raise SystemExit(subprocess.call(cmd))
 
 
 def main():
@@ -688,57 +945,45 @@ def main():
     ap.add_argument("--legs", default="all", choices=["all", "step"],
                     help="all: also the fitting and rollout workloads (default); step: the agent step and FPI only")
     ap.add_argument("--hmm-agents", type=int, default=HMM_AGENTS, help="agents of the hmm workload")
+    ap.add_argument("--fpi-agents", type=int, default=FPI_AGENTS, help="agents of the fpi workload")
     ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
-    ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the CPU-baseline sample (0 = skip)")
+    ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the FP64 check sample (0 = skip)")
+    ap.add_argument("--ref-sample", type=int, default=64,
+                    help="agents per step of the reference CPU baseline sample (b200 arm)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
                     help="EFE contraction: fp32 (SIMT), tf32x3 or bf16 (tcgen05 tensor cores)")
     args = ap.parse_args()
+    if args.gpus < 1:
+        raise SystemExit("--gpus must be >= 1")
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        relaunch_under_torchrun(args.gpus)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}: launch one rank per GPU")
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload in ("fpi", "fit", "rollout", "learn", "hmm") and world > 1:
+    if args.workload != "step" and world > 1:
         raise SystemExit("--workload fpi/fit/rollout/learn/hmm runs on one GPU")
-    if args.workload == "fpi":
+    if args.workload != "step":
         import torch
 
         dev = torch.device("cuda", local_rank)
         torch.cuda.set_device(dev)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        print(json.dumps(run_fpi_config(dev, args.steps, args.warmup, flush)), flush=True)
-        return
-    if args.workload == "fit":
-        import torch
-
-        dev = torch.device("cuda", local_rank)
-        torch.cuda.set_device(dev)
-        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        print(json.dumps(run_fit_config(dev, args.steps, args.warmup, flush)), flush=True)
-        return
-    if args.workload == "rollout":
-        import torch
-
-        dev = torch.device("cuda", local_rank)
-        torch.cuda.set_device(dev)
-        print(json.dumps(run_rollout_config(dev, args.steps, args.warmup)), flush=True)
-        return
-    if args.workload == "hmm":
-        import torch
-
-        dev = torch.device("cuda", local_rank)
-        torch.cuda.set_device(dev)
-        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        print(json.dumps(run_hmm_config(dev, args.steps, args.warmup, flush, args.hmm_agents)), flush=True)
-        return
-    if args.workload == "learn":
-        import torch
-
-        dev = torch.device("cuda", local_rank)
-        torch.cuda.set_device(dev)
-        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        print(json.dumps(run_learn_config(dev, args.steps, args.warmup, flush)), flush=True)
+        if args.workload == "fpi":
+            res = run_fpi_config(dev, args.steps, args.warmup, flush, args.fpi_agents)
+        elif args.workload == "fit":
+            res = run_fit_config(dev, args.steps, args.warmup, flush)
+        elif args.workload == "rollout":
+            res = run_rollout_config(dev, args.steps, args.warmup)
+        elif args.workload == "hmm":
+            res = run_hmm_config(dev, args.steps, args.warmup, flush, args.hmm_agents)
+        else:
+            res = run_learn_config(dev, args.steps, args.warmup, flush)
+        print(json.dumps(res), flush=True)
         return
     if world > 1:
         import datetime

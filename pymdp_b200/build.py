@@ -40,17 +40,40 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _compile(args):
+    cmd, src = args
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    return src, res.returncode, res.stdout + res.stderr
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(ROOT, "include", "pymdp_b200.h")]
+    """Compile each source to an object in ``_build/`` (in parallel; only the
+    stale ones), then link the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(ROOT, "include", "pymdp_b200.h")]
+    deps = sources() + headers
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-Wall", "-Xptxas", "-v" if verbose else "-O3", "-o", LIB + ".tmp", *sources()]
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    obj_dir = os.path.join(ROOT, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+             "-Xptxas", "-v" if verbose else "-O3"]
+    jobs, objs = [], []
+    for src in sources():
+        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + headers):
+            jobs.append(([nvcc_path(), *flags, "-c", "-o", obj, src], src))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for src, rc, log in ex.map(_compile, jobs):
+            if rc != 0:
+                raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n" + log)
+            if verbose:
+                sys.stderr.write(f"== {os.path.basename(src)}\n" + log)
+    res = subprocess.run([nvcc_path(), *ARCH, "--shared", "-o", LIB + ".tmp", *objs], capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose:
-        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

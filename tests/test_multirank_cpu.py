@@ -68,3 +68,39 @@ def test_reduce_is_identity_on_one_rank(world):
     sys.path.insert(0, ROOT)
     import bench
     assert bench.reduce_max_over_ranks([3.0, 1.5], world) == [3.0, 1.5]
+
+
+def _run_bench(args, env_extra=None, timeout=240):
+    import json
+    import subprocess
+
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                              "MASTER_PORT")}
+    env.update(env_extra or {})
+    res = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], capture_output=True, text=True,
+                         env=env, timeout=timeout, cwd=ROOT)
+    lines = [json.loads(l) for l in res.stdout.splitlines() if l.startswith("{")]
+    return res, lines
+
+
+def test_gpus_flag_launches_one_rank_per_gpu_for_the_reference_arm():
+    """``bench.py --gpus 2`` outside torchrun relaunches itself as 2 ranks
+    (torch.distributed.run on 127.0.0.1); the reference arm runs on rank 0
+    alone and prints one line whose n_gpus is the world size."""
+    from oracle import ref_build
+    if not ref_build.build():
+        pytest.skip("reference CPU kernels not built")
+    res, lines = _run_bench(["--impl", "reference", "--gpus", "2", "--agents", "4", "--steps", "1",
+                             "--warmup", "1"])
+    assert res.returncode == 0, res.stderr[-2000:]
+    assert len(lines) == 1, res.stdout
+    line = lines[0]
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "reference" and line["config"]["same_config"]
+
+
+def test_gpus_flag_must_match_the_launched_world():
+    res, lines = _run_bench(["--impl", "reference", "--gpus", "2", "--agents", "4"],
+                            env_extra={"WORLD_SIZE": "1", "RANK": "0", "LOCAL_RANK": "0"})
+    assert res.returncode != 0 and not lines
+    assert "launch one rank per GPU" in res.stderr
