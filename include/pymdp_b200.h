@@ -107,7 +107,9 @@ int32_t b2_fpi(void* stream, const float* ll_flat, int64_t ll_count, const float
  *             shape (O[m], *S[A_dep[m]]) row-major. A_agent_stride = 0
  *             shares one A across the batch.
  *   obs       [batch, M] int32 observation indices, 0 <= obs < O[m].
- *             Out-of-range indices produce NaN posteriors for that agent.
+ *             An index outside [0, O[m]) is the reference's all-zero one-hot
+ *             (jax.nn.one_hot, pymdp/agent.py:673): modality m then adds
+ *             nothing to that agent's update (pymdp/maths.py:233-235).
  *   prior     [batch, lp_offsets[F]] prior probabilities (not logs).
  *   q_out     [batch, lp_offsets[F]]
  *
@@ -141,8 +143,9 @@ int32_t b2_fpi_obs(void* stream, const float* A_flat, int64_t A_agent_stride,
  * weight of pymdp/maths.py:783-808; pA and pB each 0 elements or
  * Bn * A_offsets[M] / Bn * B_offsets[F]) on the SIMT FP32 kernel whatever
  * precision bits 8-9 request. Bits 8-9 pick the contraction precision
- * (B2_PRECISION_*) of the other calls. Out-of-range actions in policy_matrix
- * give NaN for that policy. */
+ * (B2_PRECISION_*) of the other calls. An action in policy_matrix is read as
+ * jnp indexing reads B_f[..., u] (pymdp/control.py:386): a negative one counts
+ * from the end, then it is clamped to [0, U_f - 1]. */
 int32_t b2_neg_efe(void* stream, const int32_t* policy_matrix, int64_t pm_count, int32_t pm_batched,
                    const float* qs_init, int64_t qs_count, const float* A, int64_t A_count,
                    const float* B, int64_t B_count, const float* C, int64_t C_count,
@@ -199,12 +202,15 @@ int32_t b2_neg_efe_pack_bytes(int64_t Bn, int64_t P, int64_t T, int64_t F, int64
  * whole GPU through its own arena, a real-time loop that keeps allocator
  * latency out of its step, a runtime that forbids allocation inside its
  * handlers). Same arguments, validation and results as b2_neg_efe at
- * B2_PRECISION_FP32 (the SIMT kernel), but its workspace of
+ * B2_PRECISION_FP32 (the SIMT kernel) for the utility and state
+ * information-gain terms (flag bits 0 and 1), but its workspace of
  * Bn * T * sum_m K_m floats lives in one fixed device array of
  * B2_NOALLOC_SCRATCH_BYTES, held by every device that loads the library until
  * exit, and it calls no allocating routine. Calls whose workspace would
- * exceed that size, and tensor-core precision selectors, return
- * B2_ERR_UNSUPPORTED. All calls on a device share the array: calls that
+ * exceed that size, calls with B2_FLAG_USE_PARAM_INFO_GAIN or
+ * B2_FLAG_USE_INDUCTIVE, and tensor-core precision selectors return
+ * B2_ERR_UNSUPPORTED; an unknown precision selector returns
+ * B2_ERR_INVALID_ARGUMENT, as in b2_neg_efe. All calls on a device share the array: calls that
  * overlap on the GPU race and give wrong results, so order them (one
  * stream). The first call on each device looks up the array's address with
  * that device current; make it before any stream capture begins. */

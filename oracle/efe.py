@@ -68,6 +68,15 @@ def _joint(qs, deps):
     return np.ascontiguousarray(x)
 
 
+def jnp_index(u, n):
+    """The element ``x[u]`` reads under JAX on an axis of size ``n``: a negative
+    index counts from the end, then an out-of-bounds index is clamped (JAX's
+    gather semantics; NumPy would raise)."""
+    u = np.asarray(u)
+    u = np.where(u < 0, u + n, u)
+    return np.clip(u, 0, n - 1)
+
+
 def expected_state(qs, B, u_t, B_deps):
     """``control.py:351-389`` for all policies at once.
 
@@ -75,8 +84,9 @@ def expected_state(qs, B, u_t, B_deps):
     """
     out = []
     for f, (B_f, deps) in enumerate(zip(B, B_deps)):
-        # B_f[..., u] per policy: move the action axis first, gather.
-        Bsel = np.moveaxis(np.asarray(B_f, np.float64), -1, 0)[u_t[:, f]]  # (P, S_f, *S_deps)
+        # B_f[..., u] per policy: move the action axis first, gather. The index
+        # is read as a JAX gather reads it: negative from the end, then clamped.
+        Bsel = np.moveaxis(np.asarray(B_f, np.float64), -1, 0)[jnp_index(u_t[:, f], B_f.shape[-1])]
         r = len(deps)
         sub = _LET[: r + 1]
         subs = ["z" + sub] + ["z" + sub[j + 1] for j in range(r)]

@@ -85,6 +85,12 @@ def run_factorized_fpi(A, obs, prior, A_deps, num_iter):
     return fpi_from_ll(ll, [log_stable(p) for p in prior], A_deps, num_iter)
 
 
+def one_hot(o, n):
+    """``jax.nn.one_hot(o, n)`` as ``Agent.make_categorical`` uses it
+    (``pymdp/agent.py:659-673``): all zeros for an index outside [0, n)."""
+    return (np.arange(n) == int(o)).astype(np.float64)
+
+
 def run_fpi_batch(A, obs_idx, prior, A_deps, num_iter):
     """Batched convenience wrapper (one-hot observations given as indices).
 
@@ -97,7 +103,7 @@ def run_fpi_batch(A, obs_idx, prior, A_deps, num_iter):
     out = [np.zeros((batch, np.shape(prior[f])[-1])) for f in range(F)]
     for b in range(batch):
         A_b = [a[b] if a.ndim == len(A_deps[m]) + 2 else a for m, a in enumerate(A)]
-        obs = [np.eye(A_b[m].shape[0])[obs_idx[b, m]] for m in range(len(A))]
+        obs = [one_hot(obs_idx[b, m], A_b[m].shape[0]) for m in range(len(A))]
         pr = [p[b] for p in prior]
         qs = run_factorized_fpi(A_b, obs, pr, A_deps, num_iter)
         for f in range(F):

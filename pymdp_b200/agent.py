@@ -298,7 +298,8 @@ class Agent:
                 if not hasattr(self, "_learn_work"):
                     self._learn_work = torch.zeros(1, dtype=torch.int32, device=dev)
                 self._layout.learn_B(self._pB_flat, self._B_flat, qb, act, rate(lr_pB), self._learn_work, nbat, T)
-                if self._H is not None:
+                # B is unchanged when no agent had a valid transition: keep I
+                if self._H is not None and bool((act >= 0).all(dim=-1).any()):
                     self._regenerate_I()
         if getattr(self, "_pack", None) is not None:  # the tensor-core operand images hold the old A
             self._pack[1].value = 0

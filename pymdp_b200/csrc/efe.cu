@@ -186,18 +186,13 @@ __global__ void __launch_bounds__(128)
   const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (int64_t)pol * p.T * p.F;
   const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
   float g = 0.f;
-  bool bad_action = false;
   for (int t = 0; t < p.T; ++t) {
     // expected states
     const float* qc = qs[cur];
     float* qn = qs[cur ^ 1];
     for (int f = 0; f < p.F; ++f) {
       const EfeFactor& fb = p.fac[f];
-      int u = u_pol[t * p.F + f];
-      if (u < 0 || u >= p.U[f]) {
-        bad_action = true;
-        u = 0;
-      }
+      const int u = jnp_action(u_pol[t * p.F + f], p.U[f]);
       const float* Bf = B + b * p.B_stride + fb.B_off;
       const float* wBf = wB ? wB + b * p.B_stride + fb.B_off : nullptr;
       const int U = p.U[f];
@@ -255,7 +250,7 @@ __global__ void __launch_bounds__(128)
       g += h + la;
     }
   }
-  G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : g;
+  G[b * p.P + pol] = g;
 }
 
 // digamma(x) for x > 0 in FP64: the recurrence psi(x) = psi(x + 1) - 1/x up

@@ -8,6 +8,14 @@
 namespace b2 {
 
 constexpr int kEfeMaxF = B2_MAX_FACTORS;
+
+// The action index as jnp indexing reads B_f[..., u] (pymdp/control.py:386):
+// a negative index counts from the end, then an out-of-range index clamps to
+// [0, U - 1] (JAX's gather semantics for out-of-bounds indices).
+__host__ __device__ __forceinline__ int jnp_action(int u, int U) {
+  if (u < 0) u += U;
+  return u < 0 ? 0 : (u >= U ? U - 1 : u);
+}
 constexpr int kEfeMaxM = B2_MAX_MODALITIES;
 constexpr int kEfePlainMaxStot = 256;  // per-policy state vector kept per thread
 constexpr int kEfePlainMaxO = 128;

@@ -52,9 +52,6 @@ __global__ void __launch_bounds__(128)
   const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
   const bool ut = (p.flags & B2_FLAG_USE_UTILITY) != 0;
   const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (int64_t)pol * p.T * p.F;
-  for (int t = 0; t < p.T; ++t)
-    for (int f = 0; f < p.F; ++f)
-      if (u_pol[t * p.F + f] < 0 || u_pol[t * p.F + f] >= p.U[f]) return;  // NaN policy: no gradient
   const float* Ab = A + b * p.A_stride;
   const float* Bb = B + b * p.B_stride;
   const float* Cb = C + b * p.C_stride;
@@ -71,7 +68,7 @@ __global__ void __launch_bounds__(128)
     float* qn = hist + (t + 1) * St;
     for (int f = 0; f < p.F; ++f) {
       const EfeFactor& fb = p.fac[f];
-      const int u = u_pol[t * p.F + f], U = p.U[f];
+      const int U = p.U[f], u = jnp_action(u_pol[t * p.F + f], U);
       const float* Bf = Bb + fb.B_off;
       for (int s = 0; s < p.S[f]; ++s) {
         float acc = 0.f;
@@ -137,7 +134,7 @@ __global__ void __launch_bounds__(128)
     for (int i = 0; i < St; ++i) gqp[i] = 0.f;
     for (int f = 0; f < p.F; ++f) {
       const EfeFactor& fb = p.fac[f];
-      const int u = u_pol[t * p.F + f], U = p.U[f];
+      const int U = p.U[f], u = jnp_action(u_pol[t * p.F + f], U);
       const float* Bf = Bb + fb.B_off;
       float* dBf = dBb + fb.B_off;
       int dig[B2_MAX_DEP_RANK];

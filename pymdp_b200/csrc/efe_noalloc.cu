@@ -106,6 +106,7 @@ extern "C" int32_t b2_neg_efe_noalloc(
       return noalloc_bad(std::string(c.name) + " element_count = " + std::to_string(c.actual) + ", expected " +
                          std::to_string(c.expected));
   if (eps_count != 1 && eps_count != Bn) return noalloc_bad("inductive_epsilon must have 1 or Bn elements");
+  if (((flags >> B2_PRECISION_SHIFT) & 3) > B2_PRECISION_BF16) return noalloc_bad("unknown precision selector");
   if (flags & (B2_FLAG_USE_PARAM_INFO_GAIN | B2_FLAG_USE_INDUCTIVE))
     return fail(B2_ERR_UNSUPPORTED,
                 std::string(kNoAllocName) + ": only the utility and state-information-gain terms are built");

@@ -97,7 +97,6 @@ __global__ void __launch_bounds__(kSmallThreads)
   float* wv = gqp + P * St;            // P
   float* lin = wv + P;                 // Kx
   float* la = lin + Kx;                // Omax x Kx: log clip A [ig] + C_t [ut] of one (step, modality)
-  int* bad = reinterpret_cast<int*>(la + Omax * Kx);  // P
   const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
   const bool ut = (p.flags & B2_FLAG_USE_UTILITY) != 0;
   const int32_t* pmb = pm + (pm_batched ? b * (int64_t)P * T * F : 0);
@@ -105,16 +104,7 @@ __global__ void __launch_bounds__(kSmallThreads)
   const float* Bb = B + b * p.B_stride;
   const float* Cb = C + b * p.C_stride;
 
-  for (int pp = tid; pp < P; pp += NT) {
-    int bd = 0;
-    for (int t = 0; t < T; ++t)
-      for (int f = 0; f < F; ++f) {
-        const int u = pmb[((int64_t)pp * T + t) * F + f];
-        if (u < 0 || u >= p.U[f]) bd = 1;
-      }
-    bad[pp] = bd;
-    wv[pp] = BWD ? (bd ? 0.f : dG[b * P + pp]) : 0.f;
-  }
+  for (int pp = tid; pp < P; pp += NT) wv[pp] = BWD ? dG[b * P + pp] : 0.f;
   for (int e = tid; e < P * St; e += NT) hist[e] = __ldg(qs_init + b * St + e % St);
   __syncthreads();
   // forward roll-out of every policy: hist[t + 1] = B(u_t) . joint(hist[t])
@@ -124,8 +114,7 @@ __global__ void __launch_bounds__(kSmallThreads)
     for (int e = tid; e < P * St; e += NT) {
       const int pp = e / St, j = e - pp * St;
       const int f = small_factor_of(p, j), s = j - p.qs_off[f], U = p.U[f];
-      int u = pmb[((int64_t)pp * T + t) * F + f];
-      if (u < 0 || u >= U) u = 0;
+      const int u = jnp_action(pmb[((int64_t)pp * T + t) * F + f], U);
       const EfeFactor& fb = p.fac[f];
       const float* Bs = Bb + fb.B_off + (int64_t)s * fb.K * U + u;
       float acc = 0.f;
@@ -180,7 +169,7 @@ __global__ void __launch_bounds__(kSmallThreads)
         __syncthreads();
       }
     }
-    for (int pp = tid; pp < P; pp += NT) G[b * P + pp] = bad[pp] ? __int_as_float(0x7fc00000) : wv[pp];
+    for (int pp = tid; pp < P; pp += NT) G[b * P + pp] = wv[pp];
     return;
   }
 
@@ -247,8 +236,7 @@ __global__ void __launch_bounds__(kSmallThreads)
       __syncthreads();
       for (int e = tid; e < P * K; e += NT) {
         const int pp = e / K, k = e - pp * K;
-        int u = pmb[((int64_t)pp * T + t) * F + f];
-        if (u < 0 || u >= U) u = 0;
+        const int u = jnp_action(pmb[((int64_t)pp * T + t) * F + f], U);
         float acc = 0.f;
         for (int s = 0; s < S; ++s) acc = fmaf(__ldg(Bf + ((int64_t)s * K + k) * U + u), gq[pp * St + p.qs_off[f] + s], acc);
         gx[pp * Kx + k] = acc;
@@ -257,8 +245,7 @@ __global__ void __launch_bounds__(kSmallThreads)
         const int u = e % U, sk = e / U, k = sk % K, s = sk / K;
         float acc = 0.f;
         for (int pp = 0; pp < P; ++pp) {
-          int up = pmb[((int64_t)pp * T + t) * F + f];
-          if (up < 0 || up >= U) up = 0;
+          const int up = jnp_action(pmb[((int64_t)pp * T + t) * F + f], U);
           if (up == u) acc = fmaf(gq[pp * St + p.qs_off[f] + s], x[pp * Kx + k], acc);
         }
         dBb[fb.B_off + e] += acc;
@@ -293,7 +280,7 @@ int64_t efe_small_smem_bytes(const EfeParams& p) {
   int Kx = 0, Omax = 0;
   small_dims(p, &Kx, &Omax);
   const int64_t P = p.P, St = p.S_tot;
-  return ((p.T + 1) * P * St + 2 * P * Kx + 2 * P * Omax + 2 * P * St + P + Kx + (int64_t)Omax * Kx) * 4 + P * 4;
+  return ((p.T + 1) * P * St + 2 * P * Kx + 2 * P * Omax + 2 * P * St + P + Kx + (int64_t)Omax * Kx) * 4;
 }
 
 int32_t launch_efe_small(const EfeParams& p, int64_t Bn, bool bwd, const int32_t* pm, int pm_batched,

@@ -87,6 +87,10 @@ struct TcParams {
   int32_t wch;        // chunks per W slot (a multiple of kCps)
   int32_t ws_bytes;   // bytes per W slot
   int32_t nacc;       // TMEM accumulators the A stages rotate over (summed in FP64)
+  int32_t corr;       // 3xTF32: accumulator slot of the hi*lo + lo*hi correction products (-1: none, they
+                      // go with the hi*hi products)
+  int32_t drain;      // 1: each A stage's hi*hi products go to a fresh accumulator tied to its ring slot, which
+                      // the producers fold into FP64 registers before reusing the slot (N <= 64)
   int32_t b_words;    // floats of B staged in shared memory per CTA (0 = read B from global)
   int32_t a_col;      // first TMEM column of the A (X) stages; accumulators start at column 0
   int32_t tmem_cols;  // allocated TMEM columns
@@ -352,18 +356,22 @@ __device__ __forceinline__ void issue_stage_bf16(uint32_t dt, uint32_t a0, uint6
       : "memory");
 }
 
-__device__ __forceinline__ void issue_stage_tf32x3(uint32_t dt, uint32_t a0, uint64_t wd, uint32_t chunk16,
-                                                   uint32_t idesc, uint32_t first, uint32_t nx, uint32_t nxp,
-                                                   uint32_t nw, uint32_t nwp, uint32_t lo16, uint32_t& rx,
-                                                   uint32_t& rw) {
+// 3xTF32 stage: per K-step hi*hi into the accumulator dt (accumulate flag
+// `first` on the stage's first K-step), hi*lo and lo*hi into dc (`firstc` on
+// the stage's first K-step). dc may equal dt.
+__device__ __forceinline__ void issue_stage_tf32x3(uint32_t dt, uint32_t dc, uint32_t a0, uint64_t wd,
+                                                   uint32_t chunk16, uint32_t idesc, uint32_t first, uint32_t firstc,
+                                                   uint32_t nx, uint32_t nxp, uint32_t nw, uint32_t nwp,
+                                                   uint32_t lo16, uint32_t& rx, uint32_t& rw) {
   asm volatile(
       "{\n\t"
-      ".reg .pred px, pw, pa, pt;\n\t"
+      ".reg .pred px, pw, pa, pc, pt;\n\t"
       ".reg .b32 at, atl;\n\t"
       ".reg .b64 bh, bd, bdl, c16, cl;\n\t"
       "mbarrier.test_wait.parity.shared::cta.b64 px, [%2], %3;\n\t"
       "mbarrier.test_wait.parity.shared::cta.b64 pw, [%4], %5;\n\t"
       "setp.ne.b32 pa, %6, 0;\n\t"
+      "setp.ne.b32 pc, %14, 0;\n\t"
       "setp.eq.b32 pt, 0, 0;\n\t"
       "cvt.u64.u32 c16, %10;\n\t"
       "cvt.u64.u32 cl, %12;\n\t"
@@ -372,36 +380,36 @@ __device__ __forceinline__ void issue_stage_tf32x3(uint32_t dt, uint32_t a0, uin
       "add.u64 bd, bh, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pa;\n\t"
       "add.u64 bdl, bd, cl;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [at], bdl, %11, pc;\n\t"
       "add.u32 atl, at, 32;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 8;\n\t"
       "add.u64 bd, bh, 2;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pt;\n\t"
       "add.u64 bdl, bd, cl;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [at], bdl, %11, pt;\n\t"
       "add.u32 atl, at, 32;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 16;\n\t"
       "add.u64 bd, bh, 4;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pt;\n\t"
       "add.u64 bdl, bd, cl;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [at], bdl, %11, pt;\n\t"
       "add.u32 atl, at, 32;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 24;\n\t"
       "add.u64 bd, bh, 6;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bd, %11, pt;\n\t"
       "add.u64 bdl, bd, cl;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [at], bdl, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [at], bdl, %11, pt;\n\t"
       "add.u32 atl, at, 32;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%7], [atl], bd, %11, pt;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%13], [atl], bd, %11, pt;\n\t"
       "selp.u32 %0, 1, 0, px;\n\t"
       "selp.u32 %1, 1, 0, pw;\n\t"
       "}"
       : "=r"(rx), "=r"(rw)
       : "r"(nx), "r"(nxp), "r"(nw), "r"(nwp), "r"(first), "r"(dt), "r"(a0), "l"(wd), "r"(chunk16), "r"(idesc),
-        "r"(lo16)
+        "r"(lo16), "r"(dc), "r"(firstc)
       : "memory");
 }
 
@@ -433,7 +441,8 @@ struct TcSmem {
 template <int PREC, int MODE, int DLP>
 __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams& tp, const EfeParams& p,
                                               const float* __restrict__ q, const TcSmem sm, uint32_t tmem, int warp,
-                                              int pl, int qt, int lane, bool active, Ring& ring) {
+                                              int pl, int qt, int lane, bool active, Ring& ring,
+                                              double (&dsum)[16]) {
   using Tr = TcTraits<PREC>;
   constexpr int CH = Tr::kChunk;
   constexpr int Q = CH / 4;
@@ -461,11 +470,24 @@ __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams&
   }
   const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const int nstages = gr.nch / CPS;
+  // drain mode: this warp's 16 accumulator columns (qt * 16 ..) exist when qt * 16 < N
+  const bool drain = PREC == B2_PRECISION_TF32X3 && tp.drain && qt * 16 < gr.N;
+  const uint32_t dcol = (uint32_t)(qt * 16);
+  const int N = gr.N;
   for (int c = 0; c < nstages; ++c) {
     const int st = ring.slot;
     if (ring.wrapped) {
       warp_wait(&done[st], ring.phase ^ 1u, abort_flag, lane);
       tc::fence_after_sync();
+    }
+    if (drain && c >= nst) {
+      // slot st holds the hi*hi partial sums of stage c - nst of this GEMM
+      // (its MMAs are done): fold them into FP64 before stage c reuses it
+      uint32_t r[16];
+      tc::tmem_ld16(lane_base + (uint32_t)(st * N) + dcol, r);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int k = 0; k < 16; ++k) dsum[k] += (double)__uint_as_float(r[k]);
     }
     const uint32_t ta_st = lane_base + (uint32_t)(a_col + st * 32 * kPl * CPS + qt * 8);
 #pragma unroll
@@ -521,21 +543,22 @@ __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams&
 template <int PREC>
 __device__ __forceinline__ void produce_dispatch(const TcGroup& gr, const TcParams& tp, const EfeParams& p,
                                                  const float* __restrict__ q, const TcSmem sm, uint32_t tmem, int warp,
-                                                 int pl, int qt, int lane, bool active, Ring& ring) {
+                                                 int pl, int qt, int lane, bool active, Ring& ring,
+                                                 double (&dsum)[16]) {
   constexpr int CH = TcTraits<PREC>::kChunk;
   constexpr int Q = CH / 4;
   const int dlp = 1 << gr.lg;
   if (dlp > CH) {
-    produce_group<PREC, 2, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
+    produce_group<PREC, 2, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum);
   } else if (dlp > Q) {
-    produce_group<PREC, 1, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
+    produce_group<PREC, 1, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum);
   } else {
     switch (gr.lg) {
-      case 0: produce_group<PREC, 0, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
-      case 1: produce_group<PREC, 0, 2>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
-      case 2: produce_group<PREC, 0, 4>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
-      case 3: produce_group<PREC, 0, (Q >= 8 ? 8 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring); break;
-      default: produce_group<PREC, 0, (Q >= 16 ? 16 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
+      case 0: produce_group<PREC, 0, 1>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum); break;
+      case 1: produce_group<PREC, 0, 2>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum); break;
+      case 2: produce_group<PREC, 0, 4>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum); break;
+      case 3: produce_group<PREC, 0, (Q >= 8 ? 8 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum); break;
+      default: produce_group<PREC, 0, (Q >= 16 ? 16 : 1)>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum);
     }
   }
 }
@@ -547,17 +570,13 @@ __device__ __forceinline__ void produce_dispatch(const TcGroup& gr, const TcPara
 // load of the parent marginal. Other factors use the generic strided loop.
 __device__ __forceinline__ void rollout_step(const EfeParams& p, const TcParams& tp, const float* __restrict__ Bag,
                                              bool b_staged, const int32_t* __restrict__ u_pol, const float* qc,
-                                             float* qn, int pl, int qt, bool& bad_action) {
+                                             float* qn, int pl, int qt) {
   for (int f = 0; f < p.F; ++f) {
     const EfeFactor& fb = p.fac[f];
     const int U = p.U[f];
     const int S = p.S[f];
     const int K = fb.K;
-    int u = u_pol[f];
-    if (u < 0 || u >= U) {
-      bad_action = true;
-      u = 0;
-    }
+    const int u = jnp_action(u_pol[f], U);
     float* qnf = qn + p.qs_off[f] * kTcTile + pl;
     if (b_staged && tp.b_tr[f]) {
       const float* qv = qc + p.qs_off[fb.dep[0]] * kTcTile + pl;
@@ -777,7 +796,7 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     if (lane == 0) {
       const uint64_t wdesc0 = tc::desc_kmajor_sw128(tc::smem_u32(sm.Ws));
       const uint32_t acol0 = tmem + (uint32_t)tp.a_col;
-      const int G = tp.G, wch = tp.wch, nacc = tp.nacc;
+      const int G = tp.G, wch = tp.wch, nacc = tp.nacc, corr = tp.corr, drain = tp.drain;
       const uint32_t ws16 = (uint32_t)tp.ws_bytes >> 4;
       uint64_t* const x_full = sm.x_full;
       uint64_t* const done = sm.done;
@@ -821,14 +840,20 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
               tc::fence_after_sync();
               // stage c accumulates into accumulator c % nacc: shorter FP32
               // accumulation chains inside the tensor core
-              const uint32_t dt = tmem + (uint32_t)(acc_slot * N);
-              const uint32_t first = c < nacc ? 0u : 1u;
+              // drain mode: a fresh accumulator per stage, the stage's own ring slot
+              const uint32_t dt = tmem + (uint32_t)((drain ? st : acc_slot) * N);
+              const uint32_t first = drain ? 0u : (c < nacc ? 0u : 1u);
               const uint64_t wd = wdesc0 + (uint64_t)((uint32_t)wr.slot * ws16 + (uint32_t)wk * chunk16);
               const uint32_t a0 = acol0 + (uint32_t)(st * 32 * kPl * CPS);
-              if (PREC == B2_PRECISION_BF16)
+              if (PREC == B2_PRECISION_BF16) {
                 issue_stage_bf16(dt, a0, wd, chunk16, idesc, first, nx, nar.phase, nw, nwr.phase, rx, rw);
-              else
-                issue_stage_tf32x3(dt, a0, wd, chunk16, idesc, first, nx, nar.phase, nw, nwr.phase, lo16, rx, rw);
+              } else {
+                // correction products: their own accumulator (first use at stage 0), or dt's chain
+                const uint32_t dc = corr >= 0 ? tmem + (uint32_t)(corr * N) : dt;
+                const uint32_t firstc = corr >= 0 ? (c == 0 ? 0u : 1u) : 1u;
+                issue_stage_tf32x3(dt, dc, a0, wd, chunk16, idesc, first, firstc, nx, nar.phase, nw, nwr.phase,
+                                   lo16, rx, rw);
+              }
             }
             x_ready = rx;
             w_ready = w_last ? rw : 1u;
@@ -857,7 +882,6 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     const int64_t pol_act = tp.tree ? (int64_t)pol * tp.tree_w[t_lo] : pol;
     const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
     double g_acc = 0.0;
-    bool bad_action = false;
     int cur = 0;
     Ring ring;
     uint32_t j = 0;
@@ -876,7 +900,7 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
         }
       }
       rollout_step(p, tp, Bag, tp.b_words > 0, u_base + t * p.F, qsm + cur * p.S_tot * kTcTile,
-                   qsm + (cur ^ 1) * p.S_tot * kTcTile, pl, qt, bad_action);
+                   qsm + (cur ^ 1) * p.S_tot * kTcTile, pl, qt);
       producers_sync();
       cur ^= 1;
       if (t < t_lo) continue;  // (per-policy mode never skips)
@@ -885,36 +909,24 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
         const TcGroup& gr = tp.grp[g];
         build_prefix(gr, p, q, sm.pre, pl, qt, active);
         producers_sync();
-        produce_dispatch<PREC>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring);
+        double dsum[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) dsum[k] = 0.0;
+        const int s_first = ring.slot;  // ring slot of this GEMM's first A stage
+        produce_dispatch<PREC>(gr, tp, p, q, sm, tmem, warp, pl, qt, lane, active, ring, dsum);
         // epilogue: warp w reads TMEM lane quarter (w & 3) = its 32 policies,
         // 16-column blocks qt*16, qt*16 + 64, ... of every accumulator
         const int N = gr.N, n_obs = gr.n_obs;
+        // accumulators in use: main slots 0 .. nacc-1, then the correction slot
         const int nacc = gr.nch / CPS < tp.nacc ? gr.nch / CPS : tp.nacc;
+        const int corr = tp.corr;
+        const int nsum = nacc + (corr >= 0 ? 1 : 0);
         warp_wait(sm.acc_full, j & 1, sm.abort_flag, lane);
         tc::fence_after_sync();
         {
           const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
           double h = 0.0, lin = 0.0;
-          for (int n0 = qt * 16; n0 < N; n0 += 64) {
-            double sum[16];
-#pragma unroll
-            for (int k = 0; k < 16; ++k) sum[k] = 0.0;
-            int a = 0;
-            for (; a + 1 < nacc; a += 2) {
-              uint32_t r0[16], r1[16];
-              tc::tmem_ld16(taddr + (uint32_t)(a * N + n0), r0);
-              tc::tmem_ld16(taddr + (uint32_t)((a + 1) * N + n0), r1);
-              tc::tmem_wait_ld();
-#pragma unroll
-              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r0[k]) + (double)__uint_as_float(r1[k]);
-            }
-            if (a < nacc) {
-              uint32_t r0[16];
-              tc::tmem_ld16(taddr + (uint32_t)(a * N + n0), r0);
-              tc::tmem_wait_ld();
-#pragma unroll
-              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r0[k]);
-            }
+          auto consume = [&](int n0, const double (&sum)[16]) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
               const int n = n0 + k;
@@ -924,6 +936,50 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
                 lin = sum[k];
               }
             }
+          };
+          if (PREC == B2_PRECISION_TF32X3 && tp.drain) {
+            if (qt * 16 < N) {
+              // the stages still in their slots (the last nst), then the correction accumulator
+              const int nst = tp.nst, nstages = gr.nch / CPS;
+              for (int c = nstages > nst ? nstages - nst : 0; c < nstages; ++c) {
+                uint32_t r[16];
+                tc::tmem_ld16(taddr + (uint32_t)(((s_first + c) % nst) * N + qt * 16), r);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int k = 0; k < 16; ++k) dsum[k] += (double)__uint_as_float(r[k]);
+              }
+              uint32_t r[16];
+              tc::tmem_ld16(taddr + (uint32_t)(corr * N + qt * 16), r);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int k = 0; k < 16; ++k) dsum[k] += (double)__uint_as_float(r[k]);
+              consume(qt * 16, dsum);
+            }
+          } else {
+          for (int n0 = qt * 16; n0 < N; n0 += 64) {
+            double sum[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) sum[k] = 0.0;
+            int a = 0;
+            for (; a + 1 < nsum; a += 2) {
+              const int s0 = a, s1 = a + 1 < nacc ? a + 1 : corr;
+              uint32_t r0[16], r1[16];
+              tc::tmem_ld16(taddr + (uint32_t)(s0 * N + n0), r0);
+              tc::tmem_ld16(taddr + (uint32_t)(s1 * N + n0), r1);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r0[k]) + (double)__uint_as_float(r1[k]);
+            }
+            if (a < nsum) {
+              const int s0 = a < nacc ? a : corr;
+              uint32_t r0[16];
+              tc::tmem_ld16(taddr + (uint32_t)(s0 * N + n0), r0);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int k = 0; k < 16; ++k) sum[k] += (double)__uint_as_float(r0[k]);
+            }
+            consume(n0, sum);
+          }
           }
           g_acc += h + lin;
         }
@@ -938,9 +994,9 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
     if (qt == 0 && active && !*sm.abort_flag) {
       const double gsum = ((red[pl] + red[kTcTile + pl]) + red[2 * kTcTile + pl]) + red[3 * kTcTile + pl];
       if (tp.tree)
-        Gt[b * tp.tree_off[p.T] + tp.tree_off[t_lo] + pol] = bad_action ? __longlong_as_double(0x7ff8000000000000ll) : gsum;
+        Gt[b * tp.tree_off[p.T] + tp.tree_off[t_lo] + pol] = gsum;
       else
-        G[b * p.P + pol] = bad_action ? __int_as_float(0x7fc00000) : (float)gsum;
+        G[b * p.P + pol] = (float)gsum;
     }
   }
   tc::fence_before_sync();
@@ -1017,7 +1073,7 @@ __global__ void __launch_bounds__(512) efe_tree_rollout_kernel(const __grid_cons
 }
 
 // Policy-tree mode: G[p] = sum_t g_t[p / prod(U)^(T-1-t)] from the per-prefix
-// step values (FP64), NaN where a prefix held an out-of-range action.
+// step values (FP64).
 __global__ void efe_tree_combine_kernel(const __grid_constant__ TcParams tp, int T, int P,
                                         const double* __restrict__ Gt, float* __restrict__ G) {
   const int64_t b = blockIdx.y;
@@ -1121,17 +1177,43 @@ int32_t tc_plan_t(const EfeParams& p, TcParams* tp, int* smem_bytes) {
   // accumulators (BF16) / 5 (3xTF32, whose FP32 accumulation chains must stay
   // short), within the trait's maximum.
   const int stage_cols = 32 * planes * cps;  // 128 lanes x 128 bytes per plane per chunk
-  const int want_acc = PREC == B2_PRECISION_BF16 ? 2 : 5;
-  int nst = Tr::kMaxNst;
-  while (nst > 2 && 512 - nst * stage_cols < want_acc * Nmax) --nst;
-  int nacc = (512 - nst * stage_cols) / Nmax;
-  nacc = nacc > 8 ? 8 : nacc;
-  if (nacc < 1) return B2_ERR_UNSUPPORTED;
-  tp->nst = nst;
-  tp->nacc = nacc;
-  tp->a_col = (nacc * Nmax + 31) / 32 * 32;
-  if (tp->a_col + nst * stage_cols > 512) return B2_ERR_UNSUPPORTED;
+  tp->drain = 0;
+  tp->corr = -1;
   tp->tmem_cols = 512;
+  if (PREC == B2_PRECISION_TF32X3 && Nmax <= 64 &&
+      (Tr::kMaxNst + 1) * Nmax + Tr::kMaxNst * stage_cols <= 512) {
+    // 3xTF32 drain mode: stage s's hi*hi products go to accumulator slot
+    // (ring slot of s), fresh each stage, and the producers fold it into FP64
+    // before the slot's next use; one more accumulator holds the correction
+    // products (hi*lo + lo*hi, about 2^-11 of the result) of the whole GEMM.
+    // The tensor core's FP32 accumulation (which does not round to nearest)
+    // then runs over the 4 MMAs of one stage instead of the whole K range.
+    tp->drain = 1;
+    tp->nst = Tr::kMaxNst;
+    tp->nacc = Tr::kMaxNst;
+    tp->corr = Tr::kMaxNst;
+    tp->a_col = ((Tr::kMaxNst + 1) * Nmax + 31) / 32 * 32;
+  } else {
+    // Rotation mode: A stages in tensor memory, as many as leave room for at
+    // least 2 accumulators (BF16) / 5 (3xTF32) within the trait's maximum;
+    // consecutive stages rotate over the accumulators (shorter FP32 chains).
+    const int want_acc = PREC == B2_PRECISION_BF16 ? 2 : 5;
+    int nst = Tr::kMaxNst;
+    while (nst > 2 && 512 - nst * stage_cols < want_acc * Nmax) --nst;
+    int nacc = (512 - nst * stage_cols) / Nmax;
+    nacc = nacc > 8 ? 8 : nacc;
+    if (nacc < 1) return B2_ERR_UNSUPPORTED;
+    tp->nst = nst;
+    tp->a_col = (nacc * Nmax + 31) / 32 * 32;
+    // 3xTF32: the correction products share one accumulator of their own, so
+    // the main chains hold hi*hi products only (a third of the MMAs)
+    if (PREC == B2_PRECISION_TF32X3 && nacc >= 3) {
+      tp->corr = nacc - 1;
+      nacc -= 1;
+    }
+    tp->nacc = nacc;
+  }
+  if (tp->a_col + tp->nst * stage_cols > 512) return B2_ERR_UNSUPPORTED;
   // W slots: whole A stages, about kTcWSlotTarget bytes per bulk copy
   const int chunk_max = planes * Nmax * 128;
   int wch = kTcWSlotTarget / chunk_max / cps * cps;

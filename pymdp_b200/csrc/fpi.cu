@@ -219,6 +219,16 @@ __device__ __forceinline__ void team_sync() {
 // TEAM > 32 runs one agent per CTA of TEAM threads. GENERIC adds the
 // rank >= 4 contraction path (kept out of the rank <= 3 instantiations so
 // their hot loop has no call and no local memory).
+// Bit m set when agent b's observation of modality m lies in [0, O_m).
+__device__ __forceinline__ uint32_t obs_valid_mask(const FpiParams& p, const FpiIO& io, int64_t b) {
+  uint32_t ok = 0;
+  for (int m = 0; m < p.M; ++m) {
+    const int o = io.obs[b * p.M + m];
+    if (o >= 0 && o < p.src[m].O) ok |= 1u << m;
+  }
+  return ok;
+}
+
 template <int TEAM, int APC, bool FUSED, bool GENERIC>
 __global__ void __launch_bounds__(TEAM * APC)
     fpi_kernel(const __grid_constant__ FpiParams p, const FpiIO io) {
@@ -238,13 +248,10 @@ __global__ void __launch_bounds__(TEAM * APC)
   // Each source's row start (agent offset + observed slice) is resolved once
   // into shared memory before the element loop.
   int64_t* rowoff = reinterpret_cast<int64_t*>(q + p.S_tot);
-  bool bad_obs = false;
-  if (FUSED) {
-    for (int m = 0; m < p.M; ++m) {
-      const int o = io.obs[b * p.M + m];
-      bad_obs |= (o < 0 || o >= p.src[m].O);
-    }
-  }
+  // An observation outside [0, O_m) is the reference's all-zero one-hot
+  // (jax.nn.one_hot, pymdp/agent.py:673): its log-likelihood tensordot is 0,
+  // so that modality adds nothing (pymdp/maths.py:233-235).
+  const uint32_t obs_ok = FUSED ? obs_valid_mask(p, io, b) : 0xffffffffu;
   for (int m = t; m < p.M; m += TEAM) {
     int64_t r = b * io.src_stride + p.src[m].src_off;
     if (FUSED) {
@@ -260,7 +267,9 @@ __global__ void __launch_bounds__(TEAM * APC)
     for (int k = t; k < gr.K; k += TEAM) {
       double v = 0.0;
       for (int si = gr.src_begin; si < gr.src_end; ++si) {
-        const float a = __ldg(io.src + rowoff[p.src_order[si]] + k);
+        const int m = p.src_order[si];
+        if (!((obs_ok >> m) & 1u)) continue;
+        const float a = __ldg(io.src + rowoff[m] + k);
         v += FUSED ? log((double)fmaxf(a, kMinVal)) : (double)a;
       }
       int rem = k, addr = 0;
@@ -308,10 +317,6 @@ __global__ void __launch_bounds__(TEAM * APC)
   // ---- posterior marginals
   float* out = io.q_out + b * p.S_tot;
   for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp(logq + p.lp_off[f], out + p.lp_off[f], p.S[f], lane);
-  if (FUSED && bad_obs) {
-    team_sync<TEAM>();
-    for (int i = t; i < p.S_tot; i += TEAM) out[i] = __int_as_float(0x7fc00000);
-  }
 }
 
 // --------------------------------------------------------------- host side
@@ -602,13 +607,8 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
   int64_t* rowoff = reinterpret_cast<int64_t*>(qbuf + 2 * F * kR2MaxS);
 
   // ---- load phase
-  bool bad_obs = false;
-  if (FUSED) {
-    for (int m = 0; m < p.M; ++m) {
-      const int o = io.obs[b * p.M + m];
-      bad_obs |= (o < 0 || o >= p.src[m].O);
-    }
-  }
+  // out-of-range observation: that modality adds nothing (see fpi_kernel)
+  const uint32_t obs_ok = FUSED ? obs_valid_mask(p, io, b) : 0xffffffffu;
   for (int m = tid; m < p.M; m += nthr) {
     int64_t ro = b * io.src_stride + p.src[m].src_off;
     if (FUSED) {
@@ -661,10 +661,13 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
           const FpiGroup& gr = p.grp[g];
           gi[x] = g;
           ki[x] = k4;
-          va[x][0] = __ldg(reinterpret_cast<const float4*>(io.src + rowoff[p.src_order[gr.src_begin]]) + k4);
-          va[x][1] = gr.src_end - gr.src_begin > 1
-                         ? __ldg(reinterpret_cast<const float4*>(io.src + rowoff[p.src_order[gr.src_begin + 1]]) + k4)
-                         : make_float4(0.f, 0.f, 0.f, 0.f);
+          const int m0 = p.src_order[gr.src_begin];
+          const int m1 = gr.src_end - gr.src_begin > 1 ? p.src_order[gr.src_begin + 1] : -1;
+          va[x][0] = (obs_ok >> m0) & 1u ? __ldg(reinterpret_cast<const float4*>(io.src + rowoff[m0]) + k4)
+                                        : make_float4(1.f, 1.f, 1.f, 1.f);
+          va[x][1] = m1 >= 0 && ((obs_ok >> m1) & 1u)
+                         ? __ldg(reinterpret_cast<const float4*>(io.src + rowoff[m1]) + k4)
+                         : make_float4(1.f, 1.f, 1.f, 1.f);
           n = x + 1;
           k4 += nthr;
           while (g < p.G && 4 * k4 >= p.grp[g].K) {
@@ -694,7 +697,9 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
       for (int k = tid; k < gr.K; k += nthr) {
         double v = 0.0;
         for (int si = gr.src_begin; si < gr.src_end; ++si) {
-          const float a = __ldg(io.src + rowoff[p.src_order[si]] + k);
+          const int m = p.src_order[si];
+          if (!((obs_ok >> m) & 1u)) continue;
+          const float a = __ldg(io.src + rowoff[m] + k);
           v += FUSED ? log((double)fmaxf(a, kMinVal)) : (double)a;
         }
         store(g, k, v);
@@ -767,10 +772,6 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
     }
     __syncwarp();
   }
-  if (FUSED && bad_obs) {
-    __syncthreads();
-    for (int k = tid; k < p.S_tot; k += nthr) io.q_out[b * p.S_tot + k] = __int_as_float(0x7fc00000);
-  }
 }
 
 
@@ -820,6 +821,8 @@ __global__ void __launch_bounds__(32)
   double* gq = glogq + St;                // [St]
   int64_t* rowoff = reinterpret_cast<int64_t*>(gq + St);  // [M]
 
+  // out-of-range observation: that modality adds nothing and gets no gradient (see fpi_kernel)
+  const uint32_t obs_ok = obs_valid_mask(p, io, b);
   for (int m = lane; m < p.M; m += 32) {
     int o = io.obs[b * p.M + m];
     o = (o < 0 || o >= p.src[m].O) ? 0 : o;
@@ -835,8 +838,10 @@ __global__ void __launch_bounds__(32)
     const FpiGroup& gr = p.grp[g];
     for (int k = lane; k < gr.K; k += 32) {
       double v = 0.0;
-      for (int si = gr.src_begin; si < gr.src_end; ++si)
-        v += log((double)fmaxf(__ldg(io.src + rowoff[p.src_order[si]] + k), kMinVal));
+      for (int si = gr.src_begin; si < gr.src_end; ++si) {
+        const int m = p.src_order[si];
+        if ((obs_ok >> m) & 1u) v += log((double)fmaxf(__ldg(io.src + rowoff[m] + k), kMinVal));
+      }
       ll[bw.ll_off[g] + k] = v;
       dll[bw.ll_off[g] + k] = 0.0;
     }
@@ -929,6 +934,7 @@ __global__ void __launch_bounds__(32)
     const FpiGroup& gr = p.grp[g];
     for (int k = lane; k < gr.K; k += 32)
       for (int si = gr.src_begin; si < gr.src_end; ++si) {
+        if (!((obs_ok >> p.src_order[si]) & 1u)) continue;
         const int64_t e = rowoff[p.src_order[si]] + k;
         const float a = __ldg(io.src + e);
         if (a >= kMinVal) atomicAdd(dA + e, (float)(dll[bw.ll_off[g] + k] / (double)a));

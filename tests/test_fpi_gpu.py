@@ -2,8 +2,8 @@
 golden vectors made by the reference's own code and against the FP64 oracle.
 
 Tolerance (FP32 path vs FP64 reference): rtol 1e-5, atol 1e-7 per posterior
-entry; bit-level properties (normalisation, NaN on bad observations) at full
-benchmark size."""
+entry; size-independent properties (normalisation) at full benchmark size;
+out-of-range observations as the reference's all-zero one-hot."""
 
 import numpy as np
 import pytest
@@ -120,14 +120,37 @@ def test_fpi_full_size_cfg2_properties_and_sample_parity():
         np.testing.assert_allclose(qs[f].cpu().numpy()[idx], ref[f], rtol=RTOL, atol=ATOL)
 
 
-def test_fpi_bad_observation_gives_nan_for_that_agent_only():
+@pytest.mark.parametrize("name", ["fpi_bad_obs", "fpi_bad_obs_single"])
+def test_fpi_out_of_range_observation_matches_reference(name):
+    """An observation outside [0, O_m) is the reference's all-zero one-hot:
+    that modality adds nothing (fixture from the reference's own
+    run_factorized_fpi, tests/golden/make_golden_edges.py). The fast rank-2
+    kernel and the general kernel both see such agents."""
     from pymdp_b200 import ffi
-    S, O, deps = [4, 3], [5, 2], [[0, 1], [1]]
-    A, prior, obs = random_model(np.random.default_rng(9), S, O, deps, 3)
-    obs[1, 0] = 5  # out of range
-    qs = ffi.fpi_obs([cuda(a) for a in A], cuda(obs, torch.int32), [cuda(p) for p in prior], deps, 4)
-    q = torch.cat(qs, 1).cpu().numpy()
-    assert np.isnan(q[1]).all() and np.isfinite(q[[0, 2]]).all()
+    d = load_golden(name)
+    deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    qs = ffi.fpi_obs([cuda(a) for a in unpack(d, "A")], cuda(d["obs"], torch.int32),
+                     [cuda(p) for p in unpack(d, "prior")], deps, int(d["num_iter"]))
+    for f, q_ref in enumerate(unpack(d, "qs")):
+        np.testing.assert_allclose(qs[f].cpu().numpy(), q_ref, rtol=RTOL, atol=ATOL)
+
+
+def test_fpi_out_of_range_observation_on_the_rank2_fast_path():
+    """The benchmark FPI model (the fast rank-2 kernel, 16-byte slice loads):
+    agents with out-of-range observations equal the oracle with zero one-hots."""
+    from pymdp_b200 import ffi
+    rng = np.random.default_rng(12)
+    S, O = [16] * 4, [32] * 6
+    deps = [sorted(rng.choice(4, 2, replace=False).tolist()) for _ in O]
+    A, prior, obs = random_model(rng, S, O, deps, 6)
+    obs[1, 0], obs[2, 3], obs[3, :] = -1, 32, 1000
+    obs[4, 1], obs[4, 2] = -7, 40
+    qs = ffi.fpi_obs([cuda(a) for a in A], cuda(obs, torch.int32), [cuda(p) for p in prior], deps, 16)
+    ref = ofpi.run_fpi_batch([a.astype(np.float64) for a in A], obs, [p.astype(np.float64) for p in prior], deps, 16)
+    for f in range(4):
+        np.testing.assert_allclose(qs[f].cpu().numpy(), ref[f], rtol=RTOL, atol=ATOL)
+    # all observations out of range: the posterior is the FPI of the prior alone
+    np.testing.assert_allclose(qs[0].cpu().numpy()[3], prior[0][3], rtol=1e-5, atol=1e-7)
 
 
 def test_fpi_empty_batch_and_errors():

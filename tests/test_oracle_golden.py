@@ -86,3 +86,31 @@ def test_efe_oracle_extra_terms_match_reference(name):
     np.testing.assert_allclose(G, d["G"], rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(q_pi, d["q_pi"], rtol=1e-10, atol=1e-300)
     np.testing.assert_array_equal(oefe.sample_policy(pol, q_pi), d["action"])
+
+
+@pytest.mark.parametrize("name", ["fpi_bad_obs", "fpi_bad_obs_single"])
+def test_fpi_oracle_out_of_range_observation_matches_reference(name):
+    """An observation outside [0, O_m) is an all-zero one-hot in the reference
+    (jax.nn.one_hot): that modality adds nothing (tests/golden/make_golden_edges.py)."""
+    d = load_golden(name)
+    deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    obs = d["obs"]
+    assert ((obs < 0) | (obs >= d["O"][None, :])).any()
+    qs = ofpi.run_fpi_batch([a.astype(np.float64) for a in unpack(d, "A")], obs,
+                            [p.astype(np.float64) for p in unpack(d, "prior")], deps, int(d["num_iter"]))
+    for f, q in enumerate(unpack(d, "qs")):
+        np.testing.assert_allclose(qs[f], q, rtol=1e-12, atol=1e-14)
+
+
+def test_efe_oracle_out_of_range_action_matches_reference():
+    """Actions outside [0, U_f) are read as JAX's gather reads them (negative
+    from the end, then clamped), as in the reference's B_f[..., u_f]."""
+    d = load_golden("efe_bad_action")
+    A_deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    B_deps = deps_from(d["B_dep_flat"], d["B_dep_offsets"])
+    pol = d["policies"]
+    np.testing.assert_array_equal(oefe.jnp_index(pol, d["U"][None, None, :]), d["policies_as_read"])
+    q_pi, G = oefe.update_posterior_policies(pol, unpack(d, "qs"), unpack(d, "A"), unpack(d, "B"), unpack(d, "C"),
+                                             d["E"], A_deps, B_deps, gamma=float(d["gamma"]))
+    np.testing.assert_allclose(G, d["G"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(q_pi, d["q_pi"], rtol=1e-10, atol=1e-300)

@@ -118,3 +118,36 @@ def test_noalloc_rejects_tensor_core_precision():
     rc = _host_call(1, _lib.FLAG_USE_UTILITY | (_lib.PRECISIONS["bf16"] << _lib.PRECISION_SHIFT))
     assert rc == _lib.B2_ERR_UNSUPPORTED
     assert "B2_PRECISION_FP32" in _lib.last_error()
+
+
+def test_noalloc_rejects_the_flag_gated_terms():
+    for flag in (_lib.FLAG_USE_PARAM_INFO_GAIN, _lib.FLAG_USE_INDUCTIVE):
+        rc = _host_call(1, _lib.FLAG_USE_UTILITY | flag)
+        assert rc == _lib.B2_ERR_UNSUPPORTED
+        assert "utility and state-information-gain" in _lib.last_error()
+
+
+def test_noalloc_unknown_precision_is_an_invalid_argument():
+    rc = _host_call(1, _lib.FLAG_USE_UTILITY | (3 << _lib.PRECISION_SHIFT))
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "unknown precision selector" in _lib.last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_at_the_size_limit_matches_neg_efe():
+    """170 agents of two K = 4096 modalities at T = 3 fill 15.9 of the 16 MiB:
+    the whole fixed array is addressable and the result equals b2_neg_efe's."""
+    lib = _lib.load()
+    flags = _lib.FLAG_USE_UTILITY | _lib.FLAG_USE_STATES_INFO_GAIN
+    stream = torch.cuda.current_stream().cuda_stream
+    S, O, U, T = [32, 16, 8], [16, 16], [2, 1, 1], 3
+    batch = 170
+    lay, host, P = _flat_model(13, S, O, U, T, [[0, 1, 2], [0, 1, 2]], [[0], [1], [2]], batch)
+    assert _workspace_floats(lay, batch) * 4 <= _lib.NOALLOC_SCRATCH_BYTES < _workspace_floats(lay, 171) * 4
+    buf = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    ref = torch.empty((batch, P), device="cuda")
+    _lib.check(lib.b2_neg_efe(*_args(lay, buf, ref, batch, P, flags, stream)))
+    for _ in range(2):
+        out = torch.full((batch, P), float("nan"), device="cuda")
+        _lib.check(lib.b2_neg_efe_noalloc(*_args(lay, buf, out, batch, P, flags, stream)))
+        np.testing.assert_allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=G_RTOL, atol=G_ATOL)
