@@ -356,6 +356,31 @@ def efe_flops_per_agent(tree: bool = False) -> float:
 EFE_TRAFFIC_PER_AGENT = {"tf32x3": (339.3e6 + 8.8e6) / 160}
 
 
+def efe_bytes_per_agent() -> float:
+    """Algorithmic HBM bytes of one agent's neg-EFE + q_pi on the benchmark
+    model: A, B, C (T x O per modality), the beliefs and E read once; G and
+    q_pi written once."""
+    K = int(np.prod(S))
+    P = int(np.prod(U)) ** T
+    a = 4.0 * sum(O) * K
+    b = 4.0 * sum(s * s * u for s, u in zip(S, U))
+    return a + b + 4.0 * (T * sum(O) + sum(S)) + 4.0 * 3 * P
+
+
+def efe_factored_flops_per_agent() -> float:
+    """Multiply-add flops the factored path executes per agent on the
+    benchmark model (contraction order: factor 2, then 0, then 1): level 1 over
+    A for each depth, level 2 per factor-0 history, level 3 per pair."""
+    n = sum(O) + 1
+    K = int(np.prod(S))
+    total = 0
+    for t in range(T):
+        h1 = U[0] ** (t + 1)
+        h2 = U[1] ** (t + 1)
+        total += n * K + h1 * n * S[0] * S[1] + h1 * h2 * n * S[1]
+    return 2.0 * total
+
+
 def fpi_bytes_per_agent() -> float:
     K = int(np.prod(S))
     return 4.0 * len(O) * K + 8.0 * sum(S) + 4.0 * len(O)
@@ -698,7 +723,7 @@ def run_plain_config(dev, model, steps: int, warmup: int, flush):
 
     A, B, C, D, obs = model
     agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=len(obs), num_iter=NUM_ITER, device=dev,
-                  precision="fp32")
+                  precision="fp32", efe_algorithm="dense")
     obs_d = torch.as_tensor(obs, device=dev)
     prior_d = [torch.as_tensor(d, device=dev) for d in D]
 
@@ -739,22 +764,23 @@ def run_b200(args, rank, world, local_rank):
     model = make_model(1234 + rank, n_agents)
     A, B, C, D, obs = model
     agent = Agent(A, B, C=C, D=D, policy_len=T, gamma=GAMMA, batch_size=n_agents, num_iter=NUM_ITER, device=dev,
-                  precision=args.precision)
+                  precision=args.precision, efe_algorithm=args.efe)
     obs_d = torch.as_tensor(obs, device=dev)
     prior_d = [torch.as_tensor(d, device=dev) for d in D]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    fpi_res = run_fpi_config(dev, args.steps, args.warmup, flush)
-    fpi_big = run_fpi_config(dev, args.steps, args.warmup, flush, 65536) if world == 1 else None
+    main_only = args.legs == "main"
+    fpi_res = None if main_only else run_fpi_config(dev, args.steps, args.warmup, flush)
+    fpi_big = run_fpi_config(dev, args.steps, args.warmup, flush, 65536) if world == 1 and not main_only else None
     # single-GPU side measurements: run with N = 1 only
     extras = args.legs == "all" and world == 1
-    peaks_run = measure_peaks(dev) if world == 1 else {}
+    peaks_run = measure_peaks(dev) if world == 1 and not main_only else {}
     fit_res = run_fit_config(dev, args.steps, args.warmup, flush) if extras else None
     ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if extras else None
     learn_res = run_learn_config(dev, args.steps, args.warmup, flush) if extras else None
     hmm_res = run_hmm_config(dev, args.steps, args.warmup, flush) if extras else None
-    c1_res = run_config1(dev, args.steps, args.warmup) if world == 1 else None
-    plain_res = run_plain_config(dev, model, min(args.steps, 3), 1, flush) if world == 1 else None
+    c1_res = run_config1(dev, args.steps, args.warmup) if world == 1 and not main_only else None
+    plain_res = run_plain_config(dev, model, min(args.steps, 3), 1, flush) if world == 1 and not main_only else None
     efe_ev = []
 
     def step(timed_efe=False):
@@ -832,6 +858,7 @@ def run_b200(args, rank, world, local_rank):
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:  # noqa: BLE001
         pass
+    factored = args.efe == "factored"
     tree = agent.precision != "fp32"  # the tensor-core paths evaluate each policy prefix once
     if agent.precision == "tf32x3" and "tf32_tflops" in peaks_run:
         peak_tf, peak_src = peaks_run["tf32_tflops"], "TF32 dense matmul measured in this run (torch.matmul, TF32)"
@@ -885,7 +912,7 @@ def run_b200(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload(n_agents), "agents_per_gpu": n_agents, "fpi_iters": NUM_ITER, "policies": 4096,
-                   "precision": agent.precision, "l2": "flushed (256 MiB write) between timed steps",
+                   "efe_algorithm": args.efe, "precision": "fp32 (factored)" if factored else agent.precision, "l2": "flushed (256 MiB write) between timed steps",
                    "parallelism": f"agents sharded over {world} GPU(s), no collective"},
         "e2e": {"value": total_agents * args.steps / (e2e_ms * 1e-3), "unit": "agent-steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -893,21 +920,34 @@ def run_b200(args, rank, world, local_rank):
         "fused_over_plain": fused_over_plain,
         "plain": plain_res,
         "config1": c1_res,
-        "roofline": {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
-                     "frac": achieved_tf / peak_tf,
-                     "traffic": (EFE_TRAFFIC_PER_AGENT[agent.precision] * n_agents
-                                 if agent.precision in EFE_TRAFFIC_PER_AGENT else None),
-                     "kernel": f"neg-EFE launch over {n_agents} agents (policy evaluation + q_pi)",
-                     "flops_per_launch": flops, "ms_per_launch": efe_ms,
-                     "policy_tree": tree, "dense_equivalent_flops_per_launch": dense_flops,
-                     "dense_equivalent_tflops": dense_flops / (efe_ms * 1e-3) / 1e12,
-                     "dense_equivalent_frac": dense_flops / (efe_ms * 1e-3) / 1e12 / peak_tf,
-                     "peak_source": peak_src},
+        "roofline": ({"bound": "hbm", "achieved": efe_bytes_per_agent() * n_agents / (efe_ms * 1e-3) / 1e9,
+                      "peak": peak_gbs, "unit": "GB/s",
+                      "frac": efe_bytes_per_agent() * n_agents / (efe_ms * 1e-3) / 1e9 / peak_gbs,
+                      "traffic": (EFE_TRAFFIC_PER_AGENT["factored"] * n_agents
+                                  if "factored" in EFE_TRAFFIC_PER_AGENT else None),
+                      "kernel": f"factored neg-EFE launch over {n_agents} agents (history marginals, level 1, "
+                                f"tail, combine) + q_pi",
+                      "bytes_per_launch": efe_bytes_per_agent() * n_agents, "ms_per_launch": efe_ms,
+                      "executed_flops_per_launch": efe_factored_flops_per_agent() * n_agents,
+                      "dense_equivalent_flops_per_launch": dense_flops,
+                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"}
+                     if factored else
+                     {"bound": "tensor", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                      "frac": achieved_tf / peak_tf,
+                      "traffic": (EFE_TRAFFIC_PER_AGENT[agent.precision] * n_agents
+                                  if agent.precision in EFE_TRAFFIC_PER_AGENT else None),
+                      "kernel": f"neg-EFE launch over {n_agents} agents (policy evaluation + q_pi)",
+                      "flops_per_launch": flops, "ms_per_launch": efe_ms,
+                      "policy_tree": tree, "dense_equivalent_flops_per_launch": dense_flops,
+                      "dense_equivalent_tflops": dense_flops / (efe_ms * 1e-3) / 1e12,
+                      "dense_equivalent_frac": dense_flops / (efe_ms * 1e-3) / 1e12 / peak_tf,
+                      "peak_source": peak_src}),
         "peaks_measured": peaks_run or None,
         "cpu_baseline": cpu_base,
         "error_vs_fp64": err,
-        "fpi": dict(fpi_res, roofline={"bound": "hbm", "achieved": fpi_res["gbs"], "peak": peak_gbs, "unit": "GB/s",
-                                       "frac": fpi_res["gbs"] / peak_gbs}),
+        "fpi": None if fpi_res is None else dict(
+            fpi_res, roofline={"bound": "hbm", "achieved": fpi_res["gbs"], "peak": peak_gbs, "unit": "GB/s",
+                               "frac": fpi_res["gbs"] / peak_gbs}),
         "fpi_65536": None if fpi_big is None else dict(
             fpi_big, roofline={"bound": "hbm", "achieved": fpi_big["gbs"], "peak": peak_gbs, "unit": "GB/s",
                                "frac": fpi_big["gbs"] / peak_gbs}),
@@ -942,16 +982,20 @@ def main():
     ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout", "learn", "hmm"],
                     help="step: the agent step (default); fpi: only the 4096-agent FPI model; fit: only the "
                          "model-fitting gradient; rollout: only the uneven-size rollout (for profiling)")
-    ap.add_argument("--legs", default="all", choices=["all", "step"],
-                    help="all: also the fitting and rollout workloads (default); step: the agent step and FPI only")
+    ap.add_argument("--legs", default="all", choices=["all", "step", "main"],
+                    help="all: also the fitting, rollout, learning and HMM workloads (default); step: the agent step "
+                         "with its FPI, config-1, plain-kernel and peak legs; main: the agent step alone (profiling)")
     ap.add_argument("--hmm-agents", type=int, default=HMM_AGENTS, help="agents of the hmm workload")
     ap.add_argument("--fpi-agents", type=int, default=FPI_AGENTS, help="agents of the fpi workload")
     ap.add_argument("--agents", type=int, default=AGENTS, help="agents per GPU (256 = the benchmark workload)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="agents in the FP64 check sample (0 = skip)")
     ap.add_argument("--ref-sample", type=int, default=64,
                     help="agents per step of the reference CPU baseline sample (b200 arm)")
+    ap.add_argument("--efe", default="factored", choices=["factored", "dense"],
+                    help="neg-EFE algorithm: factored (contraction factor by factor over the per-factor marginals "
+                         "of the policy tree) or dense (one contraction per policy prefix, at --precision)")
     ap.add_argument("--precision", default="tf32x3", choices=["fp32", "tf32x3", "bf16"],
-                    help="EFE contraction: fp32 (SIMT), tf32x3 or bf16 (tcgen05 tensor cores)")
+                    help="dense EFE contraction: fp32 (SIMT), tf32x3 or bf16 (tcgen05 tensor cores)")
     args = ap.parse_args()
     if args.gpus < 1:
         raise SystemExit("--gpus must be >= 1")

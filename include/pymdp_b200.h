@@ -51,11 +51,22 @@ enum {
  * (depth t has prod(U)^(t+1) prefixes instead of P) and sum G along the tree.
  * Ignored when P != prod(U)^T, when the matrix is per agent, or by the SIMT path. */
 #define B2_FLAG_POLICY_TREE 32
+/* This build only: with B2_FLAG_POLICY_TREE and factor-local transitions
+ * (B_dependencies[f] == [f] for every f), contract A one factor at a time over
+ * the distinct predicted marginals of each factor (factor f has U_f^(t+1) of
+ * them after step t, one per history of its own actions) instead of once per
+ * policy prefix. Same G in another summation order, in FP32 with FP64
+ * accumulation of G; the precision bits are not used. Ignored (the other
+ * paths run) when the tree conditions do not hold, a dependency tuple has
+ * rank above 3, a factor has more than 64 states, or the flag-gated terms
+ * (bits 2 and 3) are on. */
+#define B2_FLAG_FACTORED 64
 /* Precision selector, bits 8-9 of `flags` (unused by the reference ABI). */
 #define B2_PRECISION_SHIFT 8
 #define B2_PRECISION_FP32 0   /* SIMT FP32, FP32 accumulate (default)         */
 #define B2_PRECISION_TF32X3 1 /* tcgen05 kind::tf32, 3-pass hi/lo split        */
-#define B2_PRECISION_BF16 2   /* tcgen05 kind::f16 BF16 operands, FP32 accum   */
+#define B2_PRECISION_BF16 2   /* tcgen05 kind::f16, 3-pass BF16 hi/lo split,   */
+                              /* FP32 accumulate                              */
 /* The two tensor-core selectors fall back to the SIMT FP32 kernel when the
  * model exceeds their limits (more than 8 distinct dependency tuples, a
  * dependency tuple of rank above 4, more than 256 - T observation rows per
@@ -227,6 +238,31 @@ int32_t b2_neg_efe_noalloc(void* stream, const int32_t* policy_matrix, int64_t p
                            const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
                            const int64_t* B_dep_offsets, int32_t flags);
 
+/* ================================================= sequence inference ==
+ * Drop-in for the reference's run_mmp / run_vmp (pymdp/algos.py:392-430,
+ * :512-571, reached from inference.update_posterior_states for
+ * inference_algo "mmp" / "vmp", pymdp/inference.py), batched over agents:
+ * marginal message passing (vmp = 0) or variational message passing
+ * (vmp = 1) over a window of T steps, num_iter mirror-descent iterations of
+ * step tau (update_marginals, :170-238), in FP64.
+ *
+ *   A        A_m of agent b at A + b * sum_m O[m] * K_m (A_batched = 1) or
+ *            shared (0); each (O[m], *S[A_dep[m]]) row-major
+ *   obs_idx  [Bn, T, M] int32 index observations (jnp indexing: clamped), or
+ *   obs_distr [Bn, T, sum_m O[m]] distributions (exactly one of the two)
+ *   B_seq    per agent, per factor the action-conditioned transitions
+ *            (T - 1, S_f, *S[B_dep[f]]) row-major, factors concatenated
+ *   prior    [Bn, sum_f S_f]; qs_out [Bn, T, sum_f S_f]
+ * The FP64 window state (T x (sum_m K_m + 5 sum_f S_f) doubles) must fit
+ * 200 KB of shared memory, else B2_ERR_UNSUPPORTED. */
+int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, int64_t A_count, int32_t A_batched,
+                          const int64_t* O, int64_t M, const int32_t* obs_idx, const float* obs_distr,
+                          int64_t obs_count, const float* B_seq, int64_t B_count, const float* prior,
+                          int64_t prior_count, float* qs_out, int64_t qs_count, int64_t Bn, int64_t T, int64_t F,
+                          const int64_t* S, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                          const int64_t* A_dep_offsets, const int64_t* B_dep_flat, int64_t B_dep_flat_len,
+                          const int64_t* B_dep_offsets, int32_t num_iter, float tau);
+
 /* ============================================================== adjoints ==
  * No counterpart in the reference's native kernels: the reference obtains
  * gradients with jax.grad of its JAX path (pymdp/ffi/_core.py:282-310,
@@ -291,6 +327,31 @@ int32_t b2_sample_action(void* stream, const float* q_pi, const int32_t* policy_
                          int32_t* action, int64_t Bn, int64_t P, int64_t T, int64_t F, int32_t sampling_mode,
                          int32_t action_selection, const float* alpha, int32_t alpha_batched, uint64_t seed);
 
+/* Agent.update_empirical_prior for inference_algo="fpi" (pymdp/agent.py:825-851):
+ * out[b] = compute_expected_state(qs[b], B[b], action[b], B_dependencies)
+ * (pymdp/control.py:351-389), the prior of the next step. qs [Bn,
+ * qs_offsets[F]], B [Bn, B_offsets[F]] (B_f as (S_f, *S[B_dep[f]], U_f)),
+ * action [Bn, F] int32 (read as jnp indexing reads B_f[..., u]: negative from
+ * the end, then clamped to [0, U_f - 1]), out like qs. Attributes as
+ * b2_neg_efe's. */
+int32_t b2_expected_state(void* stream, const float* qs, int64_t qs_count, const float* B, int64_t B_count,
+                          const int32_t* action, int64_t action_count, float* out, int64_t Bn, int64_t F,
+                          const int64_t* S, const int64_t* U, const int64_t* qs_offsets, const int64_t* B_offsets,
+                          const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets);
+
+/* Agent.multiaction_probabilities (pymdp/agent.py:908-937), batched:
+ * out [Bn, n_unique]. marginal = 0 ("full"): out[b, i] = sum of q_pi[b, p]
+ * over the policies p whose first-step actions equal unique_actions[i]
+ * ([n_unique, F] int32; the reference's unique_multiactions,
+ * pymdp/agent.py:396-399: the sorted distinct rows of policy_matrix[:, 0],
+ * padded to prod(U) rows with -1). marginal = 1: the outer product of the
+ * per-factor first-step action marginals (get_marginals,
+ * pymdp/control.py:42-67), row-major over factors, n_unique = prod(U)
+ * (unique_actions unused). policy_matrix [P, T, F] int32 (shared). */
+int32_t b2_multiaction_probabilities(void* stream, const float* q_pi, const int32_t* policy_matrix,
+                                     const int32_t* unique_actions, int64_t n_unique, int32_t marginal, int64_t Bn,
+                                     int64_t P, int64_t T, int64_t F, const int64_t* U, float* out);
+
 /* ------------------------------------------------ online Dirichlet learning
  * In-place Dirichlet updates of the flattened model buffers the FPI and EFE
  * entry points read (A_offsets / B_offsets / qs_offsets / dependency lists as
@@ -331,6 +392,22 @@ int32_t b2_update_state_transition_dirichlet(
     void* stream, float* pB, float* B, int64_t B_count, const float* qs, int64_t qs_count, const int32_t* actions,
     int64_t actions_count, const float* lr, int32_t lr_batched, int32_t* workspace, int64_t Bn, int64_t T, int64_t F,
     const int64_t* S, const int64_t* U, const int64_t* qs_offsets, const int64_t* B_offsets,
+    const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int64_t factor_mask);
+
+/* The same update with the pairwise posteriors given instead of formed from
+ * the belief sequence: the smoothing algorithms' branch of
+ * Agent.infer_parameters (inference_algo "ovf" / "exact",
+ * pymdp/agent.py:530-567, joints from inference.smoothing_ovf /
+ * smoothing_exact) into update_state_transition_dirichlet
+ * (pymdp/learning.py:119-157). joint: per agent, per factor the (T-1, S_f,
+ * *S[B_dep[f]]) joints row-major, factors concatenated. A transition counts
+ * when every action of that step is >= 0 (the reference's
+ * _apply_transition_mask); the batch-wide skip and factor_mask as
+ * b2_update_state_transition_dirichlet. */
+int32_t b2_update_state_transition_from_joint(
+    void* stream, float* pB, float* B, int64_t B_count, const float* joint, int64_t joint_count,
+    const int32_t* actions, int64_t actions_count, const float* lr, int32_t lr_batched, int32_t* workspace, int64_t Bn,
+    int64_t T, int64_t F, const int64_t* S, const int64_t* U, const int64_t* qs_offsets, const int64_t* B_offsets,
     const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int64_t factor_mask);
 
 /* ------------------------------------------- exact single-factor HMM smoothing

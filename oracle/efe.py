@@ -230,3 +230,30 @@ def sample_stochastic(logits_base, alpha, seed, agent, factor):
     top = np.sort(z)
     gap = top[-1] - top[-2] if len(top) > 1 else np.inf
     return int(np.argmax(z)), gap
+
+
+def unique_multiactions(policies, num_controls):
+    """``Agent.unique_multiactions`` (``pymdp/agent.py:396-399``): sorted distinct
+    rows of ``policies[:, 0]``, padded with -1 rows to ``prod(num_controls)``."""
+    first = np.unique(np.asarray(policies)[:, 0], axis=0)
+    size = int(np.prod(num_controls))
+    out = np.full((size, first.shape[1]), -1, dtype=np.int64)
+    out[:min(size, len(first))] = first[:size]
+    return out
+
+
+def multiaction_probabilities(q_pi, policies, num_controls, sampling_mode="full"):
+    """``Agent.multiaction_probabilities`` (``pymdp/agent.py:908-937``) for one
+    agent: "marginal" = the outer products of ``get_marginals``
+    (``control.py:42-67``) reduced left to right; "full" = q_pi summed where
+    ``policies[:, 0]`` equals each unique multi-action."""
+    q_pi = np.asarray(q_pi, np.float64)
+    if sampling_mode == "marginal":
+        m = get_marginals(q_pi, policies, num_controls)
+        out = m[0]
+        for x in m[1:]:
+            out = np.outer(out, x).reshape(-1)
+        return out
+    uniq = unique_multiactions(policies, num_controls)
+    locs = np.all(np.asarray(policies)[:, 0] == uniq[:, None, :], axis=-1)  # (n_unique, P)
+    return np.where(locs, q_pi[None, :], 0.0).sum(-1)

@@ -27,6 +27,7 @@ FLAG_USE_INDUCTIVE = 1 << 2
 FLAG_USE_PARAM_INFO_GAIN = 1 << 3
 FLAG_MODEL_PARAMS_STATIC = 1 << 4
 FLAG_POLICY_TREE = 1 << 5
+FLAG_FACTORED = 1 << 6
 PRECISION_SHIFT = 8
 PRECISIONS = {"fp32": 0, "tf32x3": 1, "bf16": 2}
 
@@ -98,11 +99,21 @@ _SIGS = {
     "b2_update_state_transition_dirichlet": (c_int32, [c_void_p, _PF, _PF, c_int64, _PF, c_int64, c_void_p,
                                                        c_int64, _PF, c_int32, c_void_p, c_int64, c_int64, c_int64,
                                                        _P64, _P64, _P64, _P64, _P64, c_int64, _P64, c_int64]),
+    "b2_update_state_transition_from_joint": (c_int32, [c_void_p, _PF, _PF, c_int64, _PF, c_int64, c_void_p,
+                                                        c_int64, _PF, c_int32, c_void_p, c_int64, c_int64, c_int64,
+                                                        _P64, _P64, _P64, _P64, _P64, c_int64, _P64, c_int64]),
     "b2_hmm_smoother": (c_int32, [c_void_p, _PF, c_int64, c_int32, _P64, c_int64, c_void_p, _PF, c_int64, _PF,
                                   c_int64, _PF, c_int64, c_int32, c_int64, c_void_p, c_int64, c_int32, c_int64,
                                   c_int64, c_int64, _PF, _PF, _PF, _PF, _PF, _PF]),
     "b2_hmm_smoother_from_filtered": (c_int32, [c_void_p, _PF, c_int64, _PF, c_int64, c_int32, c_int64, c_void_p,
                                                 c_int64, c_int32, c_int64, c_int64, c_int64, _PF, _PF, _PF]),
+    "b2_expected_state": (c_int32, [c_void_p, _PF, c_int64, _PF, c_int64, c_void_p, c_int64, _PF, c_int64, c_int64,
+                                    _P64, _P64, _P64, _P64, _P64, c_int64, _P64]),
+    "b2_multiaction_probabilities": (c_int32, [c_void_p, _PF, c_void_p, c_void_p, c_int64, c_int32, c_int64,
+                                               c_int64, c_int64, c_int64, _P64, _PF]),
+    "b2_sequence_infer": (c_int32, [c_void_p, c_int32, _PF, c_int64, c_int32, _P64, c_int64, c_void_p, _PF, c_int64,
+                                    _PF, c_int64, _PF, c_int64, _PF, c_int64, c_int64, c_int64, c_int64, _P64, _P64,
+                                    c_int64, _P64, _P64, c_int64, _P64, c_int32, ctypes.c_float]),
     "b2_rollout_setup": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int32]),
     "b2_rollout": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_uint64, c_int32,
                              c_int32, c_void_p]),

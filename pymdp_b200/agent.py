@@ -52,7 +52,7 @@ class Agent:
                  batch_size: int = 1, precision: str = "fp32", device="cuda", pA: Sequence | None = None,
                  pB: Sequence | None = None, H: Sequence | None = None, I: Sequence | None = None,
                  inductive_depth: int = 1, inductive_threshold: float = 0.1, inductive_epsilon=1e-3,
-                 learn_A: bool = False, learn_B: bool = False):
+                 learn_A: bool = False, learn_B: bool = False, efe_algorithm: str = "factored"):
         if inference_algo.lower() != "fpi":
             raise NotImplementedError("only inference_algo='fpi' is on the accelerated path")
         if use_param_info_gain and pA is None and pB is None:
@@ -67,6 +67,8 @@ class Agent:
             raise ValueError("action_selection must be 'deterministic' or 'stochastic'")
         if sampling_mode not in ("full", "marginal"):
             raise ValueError("sampling_mode must be 'full' or 'marginal'")
+        if efe_algorithm not in ("factored", "dense"):
+            raise ValueError("efe_algorithm must be 'factored' or 'dense'")
         dev = torch.device(device)
         self.device = dev
         self.batch_size = int(batch_size)
@@ -178,8 +180,12 @@ class Agent:
         self.inductive_depth, self.inductive_threshold = int(inductive_depth), float(inductive_threshold)
         # policies built here are construct_policies' full product set: let the
         # tensor-core paths share the evaluation of common policy prefixes
+        # and, with factor-local transitions, the factored contraction
+        # (efe_algorithm="factored"; the flag is ignored where it cannot apply)
+        self.efe_algorithm = efe_algorithm
         self._flags = ffi.efe_flags(use_utility, use_states_info_gain, use_param_info_gain, use_inductive,
-                                    precision=precision, policy_tree=policies is None)
+                                    precision=precision, policy_tree=policies is None,
+                                    factored=efe_algorithm == "factored")
         self.use_param_info_gain, self.use_inductive = use_param_info_gain, use_inductive
         # A, B (and pA, pB) are views of the flattened buffers the kernels read,
         # so learning updates them in place
@@ -250,7 +256,39 @@ class Agent:
         return ffi.sample_action(q_pi, self.policies, self.num_controls, self.sampling_mode, self.action_selection,
                                  self.alpha, rng_key)
 
-    def infer_parameters(self, beliefs_A, observations, actions, beliefs_B=None, lr_pA=1.0, lr_pB=1.0):
+    def update_empirical_prior(self, action, qs: Sequence[torch.Tensor]):
+        """``pymdp/agent.py:825-851`` for ``inference_algo="fpi"``: the prior of
+        the next ``infer_states``, ``compute_expected_state`` of the latest
+        posterior under the sampled ``action`` (``(batch, F)`` int), per agent
+        on the device (``b2_expected_state``). Returns ``pred[f]`` of shape
+        ``(batch, S_f)``."""
+        latest = [q[:, -1] if q.ndim == 3 else q for q in qs]
+        qs_flat, _ = ffi.flatten_ragged_f32(latest, 1, self.device)
+        act = torch.as_tensor(action, device=self.device).to(torch.int32).reshape(self.batch_size,
+                                                                                   self.num_factors)
+        pred = ffi.expected_state(qs_flat, self._B_flat, act, self._layout)
+        o = self._qs_offsets
+        return [pred[:, o[f]:o[f + 1]] for f in range(self.num_factors)]
+
+    @property
+    def unique_multiactions(self) -> torch.Tensor:
+        """``pymdp/agent.py:396-399``: the distinct first-step joint actions of the
+        policies (sorted), padded with -1 rows to ``prod(num_controls)``."""
+        if not hasattr(self, "_unique"):
+            self._unique = torch.as_tensor(ffi.unique_multiactions(self.policies.cpu().numpy(), self.num_controls),
+                                           device=self.device)
+        return self._unique
+
+    def multiaction_probabilities(self, q_pi: torch.Tensor) -> torch.Tensor:
+        """``pymdp/agent.py:908-937``: probabilities of the unique multi-actions,
+        ``(batch, prod(num_controls))``: q_pi summed over the policies that
+        start with each one ("full"), or the outer product of the per-factor
+        action marginals ("marginal"), on the device."""
+        return ffi.multiaction_probabilities(q_pi, self.policies, self.unique_multiactions, self.num_controls,
+                                             self.sampling_mode)
+
+    def infer_parameters(self, beliefs_A, observations, actions, beliefs_B=None, lr_pA=1.0, lr_pB=1.0,
+                         joint_beliefs=None):
         """``pymdp/agent.py:416-620`` for ``inference_algo="fpi"``: Dirichlet
         updates of pA -> A (``learn_A``) and pB -> B (``learn_B``), in place on
         the device buffers (``b2_update_obs_likelihood_dirichlet``,
@@ -263,7 +301,12 @@ class Agent:
         of the B belief sequence (``beliefs_B`` if given, else ``beliefs_A``).
         B learns only when some agent of the batch has a transition whose
         actions are all >= 0 (``agent.py:480-500``); with ``use_inductive``
-        and H, I is then regenerated from the new B (``agent.py:606-615``)."""
+        and H, I is then regenerated from the new B (``agent.py:606-615``).
+        ``joint_beliefs[f]``: ``(batch, T-1, S_f, *S[B_dependencies[f]])``
+        pairwise posteriors (e.g. from ``hmm.smoothing_exact``): B then learns
+        from them, as the smoothing algorithms' branch does
+        (``agent.py:530-567``), instead of from outer products of
+        ``beliefs_B``."""
         dev, nbat = self.device, self.batch_size
 
         def seq(beliefs):
@@ -287,7 +330,21 @@ class Agent:
                 o = torch.stack([x.reshape(nbat, T) for x in obs], dim=-1).to(torch.int32)
             self._layout.learn_A(self._pA_flat, self._A_flat, o.contiguous(), qa, rate(lr_pA), nbat, T,
                                  modality_mask=self._pA_mask, categorical=categorical)
-        if self.learn_B and actions is not None:
+        if self.learn_B and actions is not None and joint_beliefs is not None:
+            joint = torch.cat([_t(j, dev).reshape(nbat, -1) for j in joint_beliefs], dim=1).contiguous()
+            T = int(_t(joint_beliefs[0], dev).shape[1]) + 1
+            act = torch.as_tensor(actions, device=dev).to(torch.int32)
+            if act.ndim == 2:
+                act = act.unsqueeze(1)
+            act = act[:, :T - 1].contiguous()
+            if T > 1 and act.shape[1] == T - 1:
+                if not hasattr(self, "_learn_work"):
+                    self._learn_work = torch.zeros(1, dtype=torch.int32, device=dev)
+                self._layout.learn_B_joint(self._pB_flat, self._B_flat, joint, act, rate(lr_pB), self._learn_work,
+                                           nbat, T)
+                if self._H is not None and bool((act >= 0).all(dim=-1).any()):
+                    self._regenerate_I()
+        elif self.learn_B and actions is not None:
             qb = seq(beliefs_A if beliefs_B is None else beliefs_B)
             T = qb.shape[1]
             act = torch.as_tensor(actions, device=dev).to(torch.int32)

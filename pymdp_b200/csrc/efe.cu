@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(128)
   for (int i = 0; i < p.S_tot; ++i) qs[0][i] = __ldg(qs_init + b * p.S_tot + i);
   const int32_t* u_pol = pm + (pm_batched ? b * (int64_t)p.P * p.T * p.F : 0) + (int64_t)pol * p.T * p.F;
   const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
-  float g = 0.f;
+  double g = 0.0;  // G summed over steps and terms in FP64
   for (int t = 0; t < p.T; ++t) {
     // expected states
     const float* qc = qs[cur];
@@ -212,14 +212,14 @@ __global__ void __launch_bounds__(128)
         }
         qn[p.qs_off[f] + s] = acc;
         // pB term: qs_next_f[s] * factor_dot(wB_f[..., u], qs_prev[B_deps])[s] (control.py:555-602)
-        if (wBf) g -= acc * accw;
+        if (wBf) g -= (double)acc * accw;
       }
     }
     cur ^= 1;
     const float* q = qs[cur];
     // inductive value: linear in the predicted marginals (control.py:1021-1061)
     if (wI)
-      for (int i = 0; i < p.S_tot; ++i) g = fmaf(__ldg(wI + b * p.S_tot + i), q[i], g);
+      for (int i = 0; i < p.S_tot; ++i) g += (double)__ldg(wI + b * p.S_tot + i) * q[i];
     // expected observations, entropy and the linear row
     for (int m = 0; m < p.M; ++m) {
       const EfeModality& md = p.mod[m];
@@ -247,10 +247,10 @@ __global__ void __launch_bounds__(128)
       // pA term: qo_m . factor_dot(wA_m, qs) (control.py:511-553)
       if (wAm)
         for (int o = 0; o < md.O; ++o) h -= qo[o] * fd[o];
-      g += h + la;
+      g += (double)h + (double)la;
     }
   }
-  G[b * p.P + pol] = g;
+  G[b * p.P + pol] = (float)g;
 }
 
 // digamma(x) for x > 0 in FP64: the recurrence psi(x) = psi(x + 1) - 1/x up
@@ -571,6 +571,12 @@ int32_t neg_efe_impl(void* stream_, const int32_t* policy_matrix, int64_t pm_cou
     if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
     return rc;
   }
+  if ((flags & B2_FLAG_FACTORED) && (flags & B2_FLAG_POLICY_TREE) && !pm_batched) {
+    // factored contraction over the per-factor marginals of the policy tree
+    bool used = false;
+    B2_TRY(launch_efe_fact(p, Bn, qs_init, A, B, C, neg_efe_out, stream, &used));
+    if (used) return B2_OK;
+  }
   if (prec != B2_PRECISION_FP32) {
     // tensor-core path; models outside its limits take the SIMT FP32 path
     bool used = false;
@@ -652,7 +658,9 @@ extern "C" int32_t b2_neg_efe_pack_bytes(int64_t Bn, int64_t P, int64_t T, int64
                           I_depths, A_dep_flat, A_dep_flat_len, A_dep_offsets, B_dep_flat, B_dep_flat_len,
                           B_dep_offsets, flags));
   const bool simt_terms = (flags & (B2_FLAG_USE_PARAM_INFO_GAIN | B2_FLAG_USE_INDUCTIVE)) != 0;
-  *bytes = simt_terms ? 0 : efe_tc_pack_bytes(p, (flags >> B2_PRECISION_SHIFT) & 3, Bn);
+  // the factored path packs nothing
+  const bool factored = (flags & B2_FLAG_FACTORED) && (flags & B2_FLAG_POLICY_TREE) && efe_fact_applies(p, Bn);
+  *bytes = simt_terms || factored ? 0 : efe_tc_pack_bytes(p, (flags >> B2_PRECISION_SHIFT) & 3, Bn);
   return B2_OK;
 }
 

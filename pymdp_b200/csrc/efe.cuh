@@ -83,6 +83,13 @@ struct PackCache {
 int32_t launch_efe_tc(const EfeParams& p, int prec, int64_t Bn, const int32_t* pm, int pm_batched, const float* qs,
                       const float* A, const float* B, const float* C, float* G, cudaStream_t stream, bool* used,
                       const PackCache* cache = nullptr);
+// Factored path (efe_fact.cu): the contraction factor by factor over the
+// distinct per-factor marginals of the policy tree; *used = false when the
+// model is outside it (transitions not factor-local, a dependency tuple of
+// rank above 3, a factor above 64 states, ...) and nothing was launched.
+int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const float* A, const float* B,
+                        const float* C, float* G, cudaStream_t stream, bool* used);
+bool efe_fact_applies(const EfeParams& p, int64_t Bn);
 // Bytes of the tensor-core operand images for Bn agents at precision prec
 // (0 when the model takes the SIMT path).
 int64_t efe_tc_pack_bytes(const EfeParams& p, int prec, int64_t Bn);

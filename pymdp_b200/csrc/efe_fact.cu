@@ -1,0 +1,643 @@
+// Factored neg-EFE over the policy tree (B2_FLAG_FACTORED).
+//
+// With factor-local transitions (B_dependencies[f] == [f]) and the full
+// product policy set of construct_policies, the predicted marginal of factor
+// f after step t depends only on f's own actions u_{f,0..t}: there are
+// H_f(t) = U_f^(t+1) distinct ones, its "histories" (efe_tree_rollout_kernel
+// forms the joint prefixes instead: prod_f U_f^(t+1) of them). The expected
+// observation of a policy prefix c at depth t is then
+//   qo[c, n] = sum_{s_0..s_r-1} A[n, s] prod_i q_{f_i}^{h_{f_i}(c)}[s_i]
+// (compute_expected_obs, pymdp/control.py:420-447), a multilinear form that
+// is contracted one factor at a time over the distinct histories:
+//   V1[h0][n][s1, s2]  = sum_{s0} q_{f0}^{h0}[s0]  A[n, s]          (level 1)
+//   V2[h0,h1][n][s2]   = sum_{s1} q_{f1}^{h1}[s1]  V1[h0][n][s1, s2] (level 2)
+//   qo[h0,h1,h2][n]    = sum_{s2} q_{f2}^{h2}[s2]  V2[h0,h1][n][s2] (level 3)
+// The step's info gain + utility of the group's modalities (compute_info_gain
+// + compute_expected_utility, pymdp/control.py:449-509) is H(qo) over the
+// observation rows plus the linear row lin_t[k] = sum_o A[o,k] (log clip
+// A[o,k] + C_t[o]) contracted the same way (the same linear-term collapse as
+// efe_tc_pack_kernel). The per-group, per-depth tables T_g,t[h0,h1,h2] then
+// sum into G[p] = sum_t sum_g T_g,t[histories of p at t].
+//
+// Same arithmetic as the per-policy evaluation, in another summation order:
+// at the EFE benchmark model (S = [32,16,8], U = [4,4,1], T = 3, one group of
+// 52 observation rows) depth 2 costs 1.7 M + 3.5 M multiply-adds per agent
+// instead of 4096 x 55 x 4096 = 923 M, and the launch is bound by reading A
+// once per agent. FP32 products and short FP32 dot products (at most the
+// largest factor's size), entropies in FP32, G in FP64.
+//
+// Kernels: efe_fact_hist_kernel (history marginals), efe_fact_l1_kernel (one
+// pass over A: level 1 for the observation rows, and the linear row of each
+// depth through its information-gain and utility parts), efe_fact_tail_kernel
+// (levels 2 and 3 and the entropy epilogue into the tables),
+// efe_fact_combine_kernel (G per policy).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "efe.cuh"
+
+namespace b2 {
+namespace {
+
+constexpr int kFactMaxRank = 3;
+constexpr int kFactMaxT = 8;
+constexpr int kFactMaxG = 8;
+constexpr int kFactMaxS = 64;   // largest factor size on the factored path
+constexpr int kFactCombo = 8;   // (depth, history) combinations per level-1 pass over A
+constexpr int kFactTailThreads = 256;
+constexpr int kFactH1Tile = 8;  // level-2 histories per tail CTA
+constexpr int kFactTailSmem = 96 * 1024;  // tail shared memory: level-2 blocks of one h1 tile
+
+struct FactGroup {
+  int32_t rank;                         // 1..3
+  int32_t f[kFactMaxRank];              // factors in contraction order (f[0] first)
+  int32_t S[kFactMaxRank];              // their sizes (1 past rank)
+  int32_t stA[kFactMaxRank];            // stride of the factor's axis in the modalities' A (state axes only)
+  int32_t K, R;                         // prod of sizes; K / S[0] (one V1 row: s1 outer, s2 inner)
+  int32_t vec4;                         // level-1 axis contiguous and every row start 16-byte aligned
+  int32_t n_obs, m_begin, m_end;        // observation rows; modalities [m_begin, m_end) of mod_order
+  int32_t H[kFactMaxRank][kFactMaxT];   // histories of f[i] at depth t (1 past rank)
+  int64_t v1_off[kFactMaxT];            // per-agent float offset of V1 at depth t: [H0][n_obs + 1][R]
+  int64_t tab_off[kFactMaxT];           // per-agent double offset of the table at depth t: [H0][H1][H2]
+};
+
+struct FactParams {
+  int32_t G, T, F, nu;
+  int32_t ustride[kEfeMaxF];                // joint action a = sum_f u_f * ustride[f] (construct_policies order)
+  int64_t qh_off[kEfeMaxF][kFactMaxT];      // per-agent float offset of factor f's histories at depth t
+  int64_t qh_stride, v1_stride, tab_stride; // per-agent floats / floats / doubles
+  int32_t max_R, max_tiles;
+  int32_t smax;                             // largest size among the factors the tail contracts
+  int32_t tail_smem;                        // dynamic shared memory of the tail kernel (bytes)
+  int8_t mod_order[B2_MAX_MODALITIES];
+  FactGroup grp[kFactMaxG];
+};
+
+__host__ __device__ __forceinline__ int ipow(int b, int e) {
+  int r = 1;
+  for (int i = 0; i < e; ++i) r *= b;
+  return r;
+}
+
+// History marginals: Qh[f][t][h] = B_f[:, :, u] . Qh[f][t-1][h / U_f] with
+// u = h % U_f (qs_init at t = 0): compute_expected_state (pymdp/control.py:
+// 351-389) for a factor-local B, once per distinct action history.
+__global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constant__ EfeParams p,
+                                                            const __grid_constant__ FactParams fp,
+                                                            const float* __restrict__ qs_init,
+                                                            const float* __restrict__ B, float* __restrict__ Qh) {
+  const int64_t b = blockIdx.x;
+  float* Qb = Qh + b * fp.qh_stride;
+  const float* Bb = B + b * p.B_stride;
+  for (int t = 0; t < p.T; ++t) {
+    for (int f = 0; f < p.F; ++f) {
+      const int S = p.S[f], U = p.U[f];
+      const int H = ipow(U, t + 1);
+      const EfeFactor& fb = p.fac[f];
+      float* out = Qb + fp.qh_off[f][t];
+      for (int e = threadIdx.x; e < H * S; e += blockDim.x) {
+        const int h = e / S, s = e - h * S;
+        const int u = h % U;
+        const float* q = t == 0 ? qs_init + b * p.S_tot + p.qs_off[f] : Qb + fp.qh_off[f][t - 1] + (int64_t)(h / U) * S;
+        const float* Bs = Bb + fb.B_off + (int64_t)s * S * U + u;
+        float acc = 0.f;
+        for (int k = 0; k < S; ++k) acc = fmaf(__ldg(Bs + (int64_t)k * U), q[k], acc);
+        out[e] = acc;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Level 1: one thread per (group, rest index r = (s1, s2)). For each
+// observation row it streams the S0 entries A[row, s0, s1, s2] once and, for
+// up to kFactCombo (depth, h0) combinations at a time (their marginals staged
+// in shared memory), writes V1[h0][row][r] = sum_s0 q_{f0}^{h0}[s0] A and
+// accumulates the depth's linear row sum_row [sum_s0 q xlogx(A)] + C_t[o] V1
+// (information gain, utility).
+__global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant__ EfeParams p,
+                                                          const __grid_constant__ FactParams fp,
+                                                          const float* __restrict__ A, const float* __restrict__ C,
+                                                          const float* __restrict__ Qh, float* __restrict__ V1) {
+  __shared__ float qsm[kFactCombo * kFactMaxS];
+  const int64_t b = blockIdx.z;
+  const int g = blockIdx.y;
+  if (g >= fp.G) return;  // uniform over the CTA
+  const FactGroup& gr = fp.grp[g];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((int)(blockIdx.x * blockDim.x) >= gr.R) return;  // uniform over the CTA
+  const bool active = r < gr.R;
+  const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
+  const bool ut = (p.flags & B2_FLAG_USE_UTILITY) != 0;
+  const int S0 = gr.S[0];
+  const int s1 = gr.rank > 2 ? r / gr.S[2] : r;
+  const int s2 = gr.rank > 2 ? r - s1 * gr.S[2] : 0;
+  const int64_t base = active ? (int64_t)(gr.rank > 1 ? s1 : 0) * gr.stA[1] + (int64_t)s2 * gr.stA[2] : 0;
+  const int64_t st0 = gr.stA[0];
+  const float* Qb = Qh + b * fp.qh_stride;
+  float* Vb = V1 + b * fp.v1_stride;
+  // combinations of this group: depth-major, then h0
+  int ncomb = 0;
+  for (int t = 0; t < p.T; ++t) ncomb += gr.H[0][t];
+  int t0 = 0, h0 = 0;  // first combination of the current chunk
+  for (int c0 = 0; c0 < ncomb; c0 += kFactCombo) {
+    const int nc = ncomb - c0 < kFactCombo ? ncomb - c0 : kFactCombo;
+    int ct[kFactCombo], ch[kFactCombo];
+    {
+      int t = t0, h = h0;
+#pragma unroll
+      for (int i = 0; i < kFactCombo; ++i) {
+        ct[i] = t;
+        ch[i] = h;
+        if (i < nc && ++h == gr.H[0][t] && t + 1 < p.T) {
+          h = 0;
+          ++t;
+        }
+      }
+      t0 = t;
+      h0 = h;
+    }
+    __syncthreads();  // the previous chunk's readers are done with qsm
+    for (int e = threadIdx.x; e < nc * S0; e += blockDim.x) {
+      const int i = e / S0, s = e - i * S0;
+      int t = ct[0], h = ch[0];
+      for (int k = 0; k < i; ++k)
+        if (++h == gr.H[0][t]) {
+          h = 0;
+          ++t;
+        }
+      qsm[i * kFactMaxS + s] = Qb[fp.qh_off[gr.f[0]][t] + (int64_t)h * S0 + s];
+    }
+    __syncthreads();
+    if (!active) continue;
+    float lin[kFactCombo];
+#pragma unroll
+    for (int i = 0; i < kFactCombo; ++i) lin[i] = 0.f;
+    int row = 0;
+    for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
+      const EfeModality& md = p.mod[fp.mod_order[mi]];
+      const float* Am = A + b * p.A_stride + md.A_off + base;
+      const float* Cm = C + b * p.C_stride + md.C_off;
+      for (int o = 0; o < md.O; ++o, ++row) {
+        float v[kFactCombo], w[kFactCombo];
+#pragma unroll
+        for (int i = 0; i < kFactCombo; ++i) v[i] = w[i] = 0.f;
+        const float* Ar = Am + (int64_t)o * md.K;
+        auto take = [&](float a, int s) {
+          const float xl = ig ? a * log_stable(a) : 0.f;
+#pragma unroll
+          for (int i = 0; i < kFactCombo; ++i) {
+            const float q = qsm[i * kFactMaxS + s];
+            v[i] = fmaf(q, a, v[i]);
+            w[i] = fmaf(q, xl, w[i]);
+          }
+        };
+        if (gr.vec4) {
+          // contiguous, 16-byte aligned level-1 axis: four entries per load
+          for (int s = 0; s < S0; s += 4) {
+            const float4 a4 = __ldg(reinterpret_cast<const float4*>(Ar + s));
+            take(a4.x, s);
+            take(a4.y, s + 1);
+            take(a4.z, s + 2);
+            take(a4.w, s + 3);
+          }
+        } else {
+          for (int s = 0; s < S0; ++s) take(__ldg(Ar + s * st0), s);
+        }
+#pragma unroll
+        for (int i = 0; i < kFactCombo; ++i) {
+          if (i < nc) {
+            Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * (gr.n_obs + 1) + row) * gr.R + r] = v[i];
+            lin[i] += w[i] + (ut ? __ldg(Cm + (int64_t)ct[i] * md.O + o) * v[i] : 0.f);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kFactCombo; ++i)
+      if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * (gr.n_obs + 1) + gr.n_obs) * gr.R + r] = lin[i];
+  }
+}
+
+// Levels 2 and 3 and the epilogue. CTA (tile, b) covers one (group, depth t,
+// h0, tile of up to kFactH1Tile level-2 histories h1) of the tail work list.
+// rank 3: V2[n][s2] = sum_s1 q1^{h1}[s1] V1[h0][n][s1,s2] in shared memory,
+//         then qo[n] = sum_s2 q2^{h2}[s2] V2[n][s2] for every h2;
+// rank 2: qo[n] = sum_s1 q1^{h1}[s1] V1[h0][n][s1] for every h1 of the tile;
+// rank 1: qo[n] = V1[h0][n][0].
+// Four threads per output column share the rows; their entropy sums meet by
+// shuffles. Table entry = sum over observation rows of -qo log clip qo (when
+// the information gain is on) + the linear row.
+struct TailItem {
+  int32_t g, t, h0, h1_begin;
+};
+
+__device__ __forceinline__ void tail_item(const FactParams& fp, int idx, TailItem* it) {
+  for (int g = 0; g < fp.G; ++g) {
+    const FactGroup& gr = fp.grp[g];
+    for (int t = 0; t < fp.T; ++t) {
+      const int h1n = gr.rank >= 3 ? gr.H[1][t] : 1;
+      const int tiles = (h1n + kFactH1Tile - 1) / kFactH1Tile;
+      const int n = gr.H[0][t] * tiles;
+      if (idx < n) {
+        it->g = g;
+        it->t = t;
+        it->h0 = idx / tiles;
+        it->h1_begin = (idx - it->h0 * tiles) * kFactH1Tile;
+        return;
+      }
+      idx -= n;
+    }
+  }
+  it->g = -1;
+}
+
+// SMAX: a compile-time bound on the size of the factor of the last level (so
+// a thread's marginals stay in registers); HPT of them per thread share each
+// shared-memory load of the level's intermediate.
+template <int SMAX>
+struct TailShape {
+  static constexpr int kHpt = SMAX <= 16 ? 4 : (SMAX <= 32 ? 2 : 1);
+};
+
+// Epilogue terms of one qo column: -qo log clip qo over the observation rows
+// (information gain on) plus the linear row (its last row).
+__device__ __forceinline__ double tail_term(int n, int n_obs, bool ig, float d) {
+  if (n < n_obs) return ig ? -(double)d * (double)log_stable(d) : 0.0;
+  return (double)d;
+}
+
+// Final level for HPT columns per thread: qo[c][n] = sum_s qv[c][s] X[n][s]
+// over rows n = half, half + 2, ... of X (shared memory, row stride xs), the
+// two halves of a column meeting by one shuffle (lanes 2i, 2i + 1).
+template <int SMAX>
+__device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, int nrow, int n_obs, bool ig,
+                                           int S, const float (&qv)[TailShape<SMAX>::kHpt][SMAX], int half,
+                                           double (&out)[TailShape<SMAX>::kHpt]) {
+  constexpr int HPT = TailShape<SMAX>::kHpt;
+#pragma unroll
+  for (int c = 0; c < HPT; ++c) out[c] = 0.0;
+  for (int n = half; n < nrow; n += 2) {
+    const float* xr = X + n * xs;
+    float d[HPT];
+#pragma unroll
+    for (int c = 0; c < HPT; ++c) d[c] = 0.f;
+#pragma unroll
+    for (int s = 0; s < SMAX; ++s) {
+      if (s < S) {
+        const float x = xr[s];
+#pragma unroll
+        for (int c = 0; c < HPT; ++c) d[c] = fmaf(qv[c][s], x, d[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < HPT; ++c) out[c] += tail_term(n, n_obs, ig, d[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < HPT; ++c) out[c] += __shfl_xor_sync(0xffffffffu, out[c], 1);
+}
+
+template <int SMAX>
+__global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const __grid_constant__ EfeParams p,
+                                                                        const __grid_constant__ FactParams fp,
+                                                                        const float* __restrict__ Qh,
+                                                                        const float* __restrict__ V1,
+                                                                        double* __restrict__ tab) {
+  constexpr int HPT = TailShape<SMAX>::kHpt;
+  extern __shared__ float tsm[];  // rank 3: [kFactH1Tile][nrow][S2 + 1] level-2 blocks, then q1 tile
+  TailItem it;
+  tail_item(fp, blockIdx.x, &it);
+  if (it.g < 0) return;  // uniform over the CTA
+  const int64_t b = blockIdx.y;
+  const FactGroup& gr = fp.grp[it.g];
+  const int t = it.t, h0 = it.h0;
+  const int nrow = gr.n_obs + 1, n_obs = gr.n_obs;
+  const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
+  const float* Qb = Qh + b * fp.qh_stride;
+  const float* V1b = V1 + b * fp.v1_stride + gr.v1_off[t] + (int64_t)h0 * nrow * gr.R;
+  double* tb = tab + b * fp.tab_stride + gr.tab_off[t];
+  const int tid = threadIdx.x;
+
+  if (gr.rank == 1) {
+    if (tid < 32) {
+      double hs = 0.0;
+      for (int n = tid; n < nrow; n += 32) hs += tail_term(n, n_obs, ig, __ldg(V1b + (int64_t)n * gr.R));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) hs += __shfl_xor_sync(0xffffffffu, hs, o);
+      if (tid == 0) tb[h0] = hs;
+    }
+    return;
+  }
+  // the last level contracts factor fl (size SL, HL histories) against X
+  // ([nrow][SL] blocks in shared memory, row stride SL + 1)
+  const int rk = gr.rank;
+  const int fl = gr.f[rk - 1], SL = gr.S[rk - 1], HL = gr.H[rk - 1][t];
+  const int xs = SL + 1;
+  const float* ql = Qb + fp.qh_off[fl][t];
+  int nblk = 1, h1_begin = 0, H1 = 1;
+  if (rk == 2) {
+    // X = the V1 block itself
+    for (int e = tid; e < nrow * SL; e += kFactTailThreads) {
+      const int n = e / SL, s = e - n * SL;
+      tsm[n * xs + s] = __ldg(V1b + (int64_t)n * gr.R + s);
+    }
+  } else {
+    // level 2 for the tile's h1 values at once: each V1 element read once
+    const int S1 = gr.S[1];
+    H1 = gr.H[1][t];
+    h1_begin = it.h1_begin;
+    nblk = H1 - h1_begin < kFactH1Tile ? H1 - h1_begin : kFactH1Tile;
+    float* q1s = tsm + kFactH1Tile * nrow * xs;
+    const float* q1 = Qb + fp.qh_off[gr.f[1]][t] + (int64_t)h1_begin * S1;
+    for (int e = tid; e < nblk * S1; e += kFactTailThreads) q1s[(e / S1) * kFactMaxS + e % S1] = __ldg(q1 + e);
+    __syncthreads();
+    for (int e = tid; e < nrow * SL; e += kFactTailThreads) {
+      const int n = e / SL, s2 = e - n * SL;
+      const float* vr = V1b + (int64_t)n * gr.R + s2;
+      float acc[kFactH1Tile];
+#pragma unroll
+      for (int h = 0; h < kFactH1Tile; ++h) acc[h] = 0.f;
+      for (int s1 = 0; s1 < S1; ++s1) {
+        const float v = __ldg(vr + (int64_t)s1 * SL);
+#pragma unroll
+        for (int h = 0; h < kFactH1Tile; ++h) acc[h] = fmaf(q1s[h * kFactMaxS + s1], v, acc[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < kFactH1Tile; ++h)
+        if (h < nblk) tsm[(h * nrow + n) * xs + s2] = acc[h];
+    }
+  }
+  __syncthreads();
+  // final level: work items (block h, group of HPT histories of fl), two threads each
+  const int groups = (HL + HPT - 1) / HPT;
+  const int items = nblk * groups;
+  for (int w0 = 0; w0 < items; w0 += kFactTailThreads / 2) {
+    const int w = w0 + (tid >> 1), half = tid & 1;
+    const bool act = w < items;  // uniform per lane pair; every lane still takes part in the shuffle
+    const int hb = act ? w / groups : 0, hg = act ? w - hb * groups : 0;
+    float qv[HPT][SMAX];
+#pragma unroll
+    for (int c = 0; c < HPT; ++c) {
+      const int hl = hg * HPT + c;
+#pragma unroll
+      for (int s = 0; s < SMAX; ++s) qv[c][s] = (act && hl < HL && s < SL) ? __ldg(ql + (int64_t)hl * SL + s) : 0.f;
+    }
+    double out[HPT];
+    tail_final<SMAX>(tsm + hb * nrow * xs, xs, act ? nrow : 0, n_obs, ig, SL, qv, half, out);
+    if (act && half == 0) {
+#pragma unroll
+      for (int c = 0; c < HPT; ++c) {
+        const int hl = hg * HPT + c;
+        if (hl < HL) {
+          const int64_t base = rk == 2 ? (int64_t)h0 * HL : ((int64_t)h0 * H1 + h1_begin + hb) * HL;
+          tb[base + hl] = out[c];
+        }
+      }
+    }
+  }
+}
+
+// G[b, pol] = sum_t sum_g T_g,t[histories of pol's prefix at t]: the policy's
+// actions come from its index in construct_policies order (mixed radix: the
+// joint action of step t is digit T-1-t of pol in base nu).
+__global__ void efe_fact_combine_kernel(const __grid_constant__ EfeParams p, const __grid_constant__ FactParams fp,
+                                        const double* __restrict__ tab, float* __restrict__ G) {
+  const int64_t b = blockIdx.y;
+  const int pol = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pol >= p.P) return;
+  const double* tb = tab + b * fp.tab_stride;
+  int hist[kEfeMaxF];
+  for (int f = 0; f < p.F; ++f) hist[f] = 0;
+  int div = 1;
+  for (int t = 1; t < p.T; ++t) div *= fp.nu;
+  double g = 0.0;
+  for (int t = 0; t < p.T; ++t) {
+    const int a = (pol / div) % fp.nu;
+    div /= fp.nu > 0 ? fp.nu : 1;
+    for (int f = 0; f < p.F; ++f) hist[f] = hist[f] * p.U[f] + (a / fp.ustride[f]) % p.U[f];
+    for (int gi = 0; gi < fp.G; ++gi) {
+      const FactGroup& gr = fp.grp[gi];
+      int64_t idx = hist[gr.f[0]];
+      if (gr.rank > 1) idx = idx * gr.H[1][t] + hist[gr.f[1]];
+      if (gr.rank > 2) idx = idx * gr.H[2][t] + hist[gr.f[2]];
+      g += tb[gr.tab_off[t] + idx];
+    }
+  }
+  G[b * p.P + pol] = (float)g;
+}
+
+// Host plan; false when the model is outside the factored path.
+bool fact_plan(const EfeParams& p, FactParams* fp) {
+  std::memset(fp, 0, sizeof(*fp));
+  if (p.T < 1 || p.T > kFactMaxT) return false;
+  int64_t nu = 1, P = 1;
+  for (int f = 0; f < p.F; ++f) {
+    if (p.fac[f].rank != 1 || p.fac[f].dep[0] != f) return false;  // factor-local transitions only
+    if (p.S[f] > kFactMaxS) return false;
+    nu *= p.U[f];
+  }
+  for (int t = 0; t < p.T && P <= p.P; ++t) P *= nu;
+  if (P != p.P || nu > (1 << 20)) return false;
+  fp->T = p.T;
+  fp->F = p.F;
+  fp->nu = (int32_t)nu;
+  int us = 1;
+  for (int f = p.F - 1; f >= 0; --f) {
+    fp->ustride[f] = us;
+    us *= p.U[f];
+  }
+  // history marginals
+  int64_t off = 0;
+  for (int f = 0; f < p.F; ++f)
+    for (int t = 0; t < p.T; ++t) {
+      fp->qh_off[f][t] = off;
+      const double h = std::pow((double)p.U[f], t + 1);
+      if (h > (1 << 24)) return false;
+      off += (int64_t)h * p.S[f];
+    }
+  fp->qh_stride = (off + 63) / 64 * 64;
+  // groups: modalities sharing one dependency tuple
+  std::vector<std::vector<int>> tuples, members;
+  for (int m = 0; m < p.M; ++m) {
+    std::vector<int> tup(p.mod[m].dep, p.mod[m].dep + p.mod[m].rank);
+    size_t g = 0;
+    while (g < tuples.size() && tuples[g] != tup) ++g;
+    if (g == tuples.size()) {
+      tuples.push_back(tup);
+      members.emplace_back();
+    }
+    members[g].push_back(m);
+  }
+  if ((int)tuples.size() > kFactMaxG) return false;
+  fp->G = (int32_t)tuples.size();
+  int n_order = 0;
+  int64_t v1 = 0, tab = 0;
+  int max_R = 1;
+  for (int g = 0; g < fp->G; ++g) {
+    const std::vector<int>& tup = tuples[g];
+    const int r = (int)tup.size();
+    if (r < 1 || r > kFactMaxRank) return false;
+    FactGroup& gr = fp->grp[g];
+    gr.rank = r;
+    // A-axis strides of the tuple's factors (row-major over the state axes)
+    std::vector<int64_t> st(r);
+    int64_t s_ = 1;
+    for (int a = r - 1; a >= 0; --a) {
+      st[a] = s_;
+      s_ *= p.S[tup[a]];
+    }
+    int n_obs = 0;
+    for (int m : members[g]) n_obs += p.mod[m].O;
+    // contraction order: the cheapest permutation (summed over depths)
+    std::vector<int> perm(r);
+    for (int i = 0; i < r; ++i) perm[i] = i;
+    std::vector<int> best;
+    double best_cost = 0;
+    do {
+      double cost = 0;
+      for (int t = 0; t < p.T; ++t) {
+        double combos = 1, rest = (double)s_;
+        for (int i = 0; i < r; ++i) {
+          const int f = tup[perm[i]];
+          combos *= std::pow((double)p.U[f], t + 1);
+          cost += combos * (n_obs + 1) * rest;  // level i + 1: combos x rows x remaining size (incl. own axis)
+          rest /= p.S[f];
+        }
+      }
+      // level-1 intermediates live in global memory: prefer few level-1 histories
+      cost += 4.0 * std::pow((double)p.U[tup[perm[0]]], p.T) * (n_obs + 1) * (double)s_ / p.S[tup[perm[0]]];
+      if (best.empty() || cost < best_cost) {
+        best = perm;
+        best_cost = cost;
+      }
+    } while (std::next_permutation(perm.begin(), perm.end()));
+    for (int i = 0; i < kFactMaxRank; ++i) {
+      if (i < r) {
+        gr.f[i] = tup[best[i]];
+        gr.S[i] = p.S[gr.f[i]];
+        gr.stA[i] = (int32_t)st[best[i]];
+      } else {
+        gr.f[i] = gr.f[0];
+        gr.S[i] = 1;
+        gr.stA[i] = 0;
+      }
+    }
+    gr.K = (int32_t)s_;
+    gr.R = (int32_t)(s_ / gr.S[0]);
+    // float4 loads of the level-1 axis: stride 1, and every (agent, row, s1, s2)
+    // start a multiple of four floats
+    bool v4 = gr.stA[0] == 1 && gr.S[0] % 4 == 0 && p.A_stride % 4 == 0 && s_ % 4 == 0 &&
+              (r < 2 || gr.stA[1] % 4 == 0) && (r < 3 || gr.stA[2] % 4 == 0);
+    for (int m : members[g]) v4 = v4 && p.mod[m].A_off % 4 == 0;
+    gr.vec4 = v4 ? 1 : 0;
+    // the tail's shared memory: kFactH1Tile level-2 blocks (rank 3) or the V1 block (rank 2)
+    const int last = r == 3 ? gr.S[2] : (r == 2 ? gr.S[1] : 1);
+    const int64_t tail_words = (r == 3 ? (int64_t)kFactH1Tile * (n_obs + 1) * (last + 1) + kFactH1Tile * kFactMaxS
+                                       : (int64_t)(n_obs + 1) * (last + 1));
+    if (tail_words * 4 > kFactTailSmem) return false;
+    max_R = gr.R > max_R ? gr.R : max_R;
+    gr.n_obs = n_obs;
+    gr.m_begin = n_order;
+    for (int m : members[g]) fp->mod_order[n_order++] = (int8_t)m;
+    gr.m_end = n_order;
+    for (int t = 0; t < p.T; ++t) {
+      for (int i = 0; i < kFactMaxRank; ++i) gr.H[i][t] = i < r ? ipow(p.U[gr.f[i]], t + 1) : 1;
+      gr.v1_off[t] = v1;
+      v1 += (int64_t)gr.H[0][t] * (n_obs + 1) * gr.R;
+      gr.tab_off[t] = tab;
+      tab += (int64_t)gr.H[0][t] * gr.H[1][t] * gr.H[2][t];
+    }
+  }
+  fp->v1_stride = (v1 + 63) / 64 * 64;
+  fp->tab_stride = (tab + 31) / 32 * 32;
+  fp->max_R = max_R;
+  int smax = 1;
+  for (int g = 0; g < fp->G; ++g) {
+    const FactGroup& gr = fp->grp[g];
+    const int last = gr.rank == 3 ? gr.S[2] : (gr.rank == 2 ? gr.S[1] : 1);
+    smax = last > smax ? last : smax;
+  }
+  fp->smax = smax;
+  int64_t tsm = 0;
+  for (int g = 0; g < fp->G; ++g) {
+    const FactGroup& gr = fp->grp[g];
+    const int last = gr.rank == 3 ? gr.S[2] : (gr.rank == 2 ? gr.S[1] : 1);
+    const int64_t w = gr.rank == 3 ? (int64_t)kFactH1Tile * (gr.n_obs + 1) * (last + 1) + kFactH1Tile * kFactMaxS
+                                   : (int64_t)(gr.n_obs + 1) * (last + 1);
+    tsm = w > tsm ? w : tsm;
+  }
+  fp->tail_smem = (int32_t)(tsm * 4);
+  int items = 0;
+  for (int g = 0; g < fp->G; ++g)
+    for (int t = 0; t < p.T; ++t) {
+      const FactGroup& gr = fp->grp[g];
+      const int h1n = gr.rank >= 3 ? gr.H[1][t] : 1;
+      items += gr.H[0][t] * ((h1n + kFactH1Tile - 1) / kFactH1Tile);
+    }
+  fp->max_tiles = items;
+  return true;
+}
+
+}  // namespace
+
+bool efe_fact_applies(const EfeParams& p, int64_t Bn) {
+  FactParams fp;
+  return Bn <= 65535 && fact_plan(p, &fp);
+}
+
+int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const float* A, const float* B,
+                        const float* C, float* G, cudaStream_t stream, bool* used) {
+  *used = false;
+  FactParams fp;
+  if (Bn > 65535 || !fact_plan(p, &fp)) return B2_OK;
+  const size_t qh_bytes = (size_t)Bn * fp.qh_stride * sizeof(float);
+  const size_t v1_bytes = (size_t)Bn * fp.v1_stride * sizeof(float);
+  const size_t tab_bytes = (size_t)Bn * fp.tab_stride * sizeof(double);
+  if (v1_bytes > ((size_t)8 << 30)) return B2_OK;  // level-1 intermediates above 8 GB: take another path
+  uint8_t* ws = nullptr;
+  B2_TRY(ws_alloc((void**)&ws, tab_bytes + qh_bytes + v1_bytes, stream, kEfeName));
+  double* tab = reinterpret_cast<double*>(ws);
+  float* Qh = reinterpret_cast<float*>(ws + tab_bytes);
+  float* V1 = reinterpret_cast<float*>(ws + tab_bytes + qh_bytes);
+  efe_fact_hist_kernel<<<(unsigned)Bn, 256, 0, stream>>>(p, fp, qs, B, Qh);
+  int32_t rc = check_launch("efe_ffi factored histories");
+  if (rc == B2_OK) {
+    dim3 grid((unsigned)((fp.max_R + 127) / 128), (unsigned)fp.G, (unsigned)Bn);
+    efe_fact_l1_kernel<<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1);
+    rc = check_launch("efe_ffi factored level 1");
+  }
+  if (rc == B2_OK) {
+    const dim3 grid((unsigned)fp.max_tiles, (unsigned)Bn);
+    const int smem = fp.tail_smem;
+    const void* k = fp.smax <= 8    ? (const void*)efe_fact_tail_kernel<8>
+                    : fp.smax <= 16 ? (const void*)efe_fact_tail_kernel<16>
+                    : fp.smax <= 32 ? (const void*)efe_fact_tail_kernel<32>
+                                    : (const void*)efe_fact_tail_kernel<64>;
+    rc = ensure_smem_attr(k, smem, kEfeName);
+    if (rc == B2_OK) {
+      if (fp.smax <= 8)
+        efe_fact_tail_kernel<8><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+      else if (fp.smax <= 16)
+        efe_fact_tail_kernel<16><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+      else if (fp.smax <= 32)
+        efe_fact_tail_kernel<32><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+      else
+        efe_fact_tail_kernel<64><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+      rc = check_launch("efe_ffi factored tail");
+    }
+  }
+  if (rc == B2_OK) {
+    efe_fact_combine_kernel<<<dim3((unsigned)((p.P + 255) / 256), (unsigned)Bn), 256, 0, stream>>>(p, fp, tab, G);
+    rc = check_launch("efe_ffi factored combine");
+  }
+  cudaError_t fe = cudaFreeAsync(ws, stream);
+  if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
+  *used = rc == B2_OK;
+  return rc;
+}
+
+}  // namespace b2

@@ -28,11 +28,14 @@
 //    chunks per cp.async.bulk (no multicast) into a separate ring of large
 //    shared-memory slots: a bulk copy costs about the same few hundred cycles
 //    whether it moves 8 KB or 32 KB, so W arrives in big pieces.
-//  * One thread issues the UMMAs (kind::f16 BF16 operands, or kind::tf32 with
-//    the 3xTF32 hi/lo split for FP32-level accuracy, A from tensor memory and
-//    B from shared memory), accumulating in TMEM; consecutive stages rotate
-//    over `nacc` accumulators that the epilogue sums in FP64, which keeps the
-//    tensor core's FP32 accumulation chains short.
+//  * One thread issues the UMMAs (kind::f16 with a 3-pass BF16 hi/lo split,
+//    or kind::tf32 with the 3xTF32 hi/lo split, A from tensor memory and B
+//    from shared memory: hi*hi + hi*lo + lo*hi per K-step), accumulating in
+//    TMEM. Where the accumulators fit (N <= 64), each pipeline stage's hi*hi
+//    products go to a fresh accumulator that the producers fold into FP64
+//    before the slot is reused ("drain mode"); otherwise stages rotate over
+//    several accumulators. Either way the tensor core's FP32 accumulation
+//    chains stay short.
 //  * Epilogue: producer warp w reads TMEM lane quarter w % 4 (its 32
 //    policies) with tcgen05.ld, forms the entropy of the obs rows and adds the
 //    step's linear row, accumulating G in FP64 registers.
@@ -115,10 +118,10 @@ struct TcTraits;
 template <>
 struct TcTraits<B2_PRECISION_BF16> {
   static constexpr int kChunk = 64;
-  static constexpr int kPlanes = 1;
+  static constexpr int kPlanes = 2;  // hi, lo: the 3-pass BF16 split (hi*hi + hi*lo + lo*hi)
   static constexpr int kEsz = 2;
-  static constexpr int kCps = 4;
-  static constexpr int kMaxNst = 3;
+  static constexpr int kCps = 2;
+  static constexpr int kMaxNst = 2;
 };
 template <>
 struct TcTraits<B2_PRECISION_TF32X3> {
@@ -205,7 +208,9 @@ __global__ void efe_tc_pack_kernel(const __grid_constant__ EfeParams p, const __
   auto put = [&](int n, float v) {
     const uint32_t off = tc::sw128_offset((uint32_t)n, (uint32_t)(byte >> 4)) + (byte & 15);
     if (PREC == B2_PRECISION_BF16) {
+      const __nv_bfloat16 hi = __float2bfloat16_rn(v);
       *reinterpret_cast<uint16_t*>(img + off) = bf16_bits(v);
+      *reinterpret_cast<uint16_t*>(img + (int64_t)N * 128 + off) = bf16_bits(v - __bfloat162float(hi));
     } else {
       const float hi = tf32_round(v);
       *reinterpret_cast<float*>(img + off) = hi;
@@ -283,76 +288,92 @@ struct Ring {
 // dt = accumulator, a0 = A stage in tensor memory, wd = descriptor of the
 // stage's first W chunk, chunk16 / lo16 = descriptor steps to the next chunk
 // / the lo plane, first = accumulate flag of the stage's first MMA.
-__device__ __forceinline__ void issue_stage_bf16(uint32_t dt, uint32_t a0, uint64_t wd, uint32_t chunk16,
-                                                 uint32_t idesc, uint32_t first, uint32_t nx, uint32_t nxp,
-                                                 uint32_t nw, uint32_t nwp, uint32_t& rx, uint32_t& rw) {
+// 3-pass BF16 stage (kCps = 2 chunks, 4 K-steps of 16 each): per K-step
+// hi*hi into the accumulator dt (accumulate flag `first` on the stage's first
+// K-step), hi*lo (W lo plane) and lo*hi (A lo plane, 32 columns on) into dc
+// (`firstc` on the stage's first K-step).
+__device__ __forceinline__ void issue_stage_bf16(uint32_t dt, uint32_t dc, uint32_t a0, uint64_t wd,
+                                                 uint32_t chunk16, uint32_t idesc, uint32_t first, uint32_t firstc,
+                                                 uint32_t nx, uint32_t nxp, uint32_t nw, uint32_t nwp, uint32_t lo16,
+                                                 uint32_t& rx, uint32_t& rw) {
   asm volatile(
       "{\n\t"
-      ".reg .pred px, pw, pa, pt;\n\t"
+      ".reg .pred px, pw, pa, pc, pt;\n\t"
       ".reg .b32 at, atl;\n\t"
       ".reg .b64 bh, bd, bdl, c16, cl;\n\t"
       "mbarrier.test_wait.parity.shared::cta.b64 px, [%2], %3;\n\t"
       "mbarrier.test_wait.parity.shared::cta.b64 pw, [%4], %5;\n\t"
       "setp.ne.b32 pa, %6, 0;\n\t"
+      "setp.ne.b32 pc, %14, 0;\n\t"
       "setp.eq.b32 pt, 0, 0;\n\t"
       "cvt.u64.u32 c16, %10;\n\t"
+      "cvt.u64.u32 cl, %12;\n\t"
       "mov.b64 bh, %9;\n\t"
+      // chunk 0: K-steps at A columns 0, 8, 16, 24 (lo plane +32), W +0, +2, +4, +6
       "add.u32 at, %8, 0;\n\t"
       "add.u64 bd, bh, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pa;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pc;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 8;\n\t"
       "add.u64 bd, bh, 2;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 16;\n\t"
       "add.u64 bd, bh, 4;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 24;\n\t"
       "add.u64 bd, bh, 6;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u64 bh, bh, c16;\n\t"
-      "add.u32 at, %8, 32;\n\t"
-      "add.u64 bd, bh, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u32 at, %8, 40;\n\t"
-      "add.u64 bd, bh, 2;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u32 at, %8, 48;\n\t"
-      "add.u64 bd, bh, 4;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u32 at, %8, 56;\n\t"
-      "add.u64 bd, bh, 6;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
+      // chunk 1: A columns 64.. (a chunk is 64 columns: hi and lo planes), W one chunk on
       "add.u64 bh, bh, c16;\n\t"
       "add.u32 at, %8, 64;\n\t"
       "add.u64 bd, bh, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 72;\n\t"
       "add.u64 bd, bh, 2;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 80;\n\t"
       "add.u64 bd, bh, 4;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
       "add.u32 at, %8, 88;\n\t"
       "add.u64 bd, bh, 6;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u64 bh, bh, c16;\n\t"
-      "add.u32 at, %8, 96;\n\t"
-      "add.u64 bd, bh, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u32 at, %8, 104;\n\t"
-      "add.u64 bd, bh, 2;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u32 at, %8, 112;\n\t"
-      "add.u64 bd, bh, 4;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
-      "add.u32 at, %8, 120;\n\t"
-      "add.u64 bd, bh, 6;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%7], [at], bd, %11, pt;\n\t"
+      "add.u64 bdl, bd, cl;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [at], bdl, %11, pt;\n\t"
+      "add.u32 atl, at, 32;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%13], [atl], bd, %11, pt;\n\t"
       "selp.u32 %0, 1, 0, px;\n\t"
       "selp.u32 %1, 1, 0, pw;\n\t"
       "}"
       : "=r"(rx), "=r"(rw)
-      : "r"(nx), "r"(nxp), "r"(nw), "r"(nwp), "r"(first), "r"(dt), "r"(a0), "l"(wd), "r"(chunk16), "r"(idesc)
+      : "r"(nx), "r"(nxp), "r"(nw), "r"(nwp), "r"(first), "r"(dt), "r"(a0), "l"(wd), "r"(chunk16), "r"(idesc),
+        "r"(lo16), "r"(dc), "r"(firstc)
       : "memory");
 }
 
@@ -471,7 +492,7 @@ __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams&
   const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const int nstages = gr.nch / CPS;
   // drain mode: this warp's 16 accumulator columns (qt * 16 ..) exist when qt * 16 < N
-  const bool drain = PREC == B2_PRECISION_TF32X3 && tp.drain && qt * 16 < gr.N;
+  const bool drain = tp.drain && qt * 16 < gr.N;
   const uint32_t dcol = (uint32_t)(qt * 16);
   const int N = gr.N;
   for (int c = 0; c < nstages; ++c) {
@@ -516,10 +537,16 @@ __device__ __forceinline__ void produce_group(const TcGroup& gr, const TcParams&
       // this warp's 32 policy rows (TMEM lanes) x 8 columns of the A stage
       const uint32_t ta = ta_st + (uint32_t)(h * 32 * kPl);
       if (PREC == B2_PRECISION_BF16) {
-        uint32_t r[8];
+        // hi = bf16(v), lo = bf16(v - hi): the two planes of the 3-pass split
+        uint32_t r[8], rl[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) r[e] = bf16x2_bits(v[2 * e], v[2 * e + 1]);
+        for (int e = 0; e < 8; ++e) {
+          const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+          r[e] = *reinterpret_cast<const uint32_t*>(&h2);
+          rl[e] = bf16x2_bits(v[2 * e] - __low2float(h2), v[2 * e + 1] - __high2float(h2));
+        }
         tc::tmem_st8(ta, r);
+        tc::tmem_st8(ta + 32, rl);
       } else {
         uint32_t hi[8], lo[8];
 #pragma unroll
@@ -805,7 +832,7 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
       uint64_t* const acc_full = sm.acc_full;
       uint64_t* const acc_free = sm.acc_free;
       volatile int* const abort_flag = sm.abort_flag;
-      static_assert(PREC != B2_PRECISION_BF16 || CPS == 4, "issue_stage_bf16 covers 4 chunks");
+      static_assert(PREC != B2_PRECISION_BF16 || CPS == 2, "issue_stage_bf16 covers 2 chunks");
       static_assert(PREC != B2_PRECISION_TF32X3 || CPS == 1, "issue_stage_tf32x3 covers 1 chunk");
       Ring ar, wr;
       uint32_t j = 0;
@@ -845,15 +872,15 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
               const uint32_t first = drain ? 0u : (c < nacc ? 0u : 1u);
               const uint64_t wd = wdesc0 + (uint64_t)((uint32_t)wr.slot * ws16 + (uint32_t)wk * chunk16);
               const uint32_t a0 = acol0 + (uint32_t)(st * 32 * kPl * CPS);
-              if (PREC == B2_PRECISION_BF16) {
-                issue_stage_bf16(dt, a0, wd, chunk16, idesc, first, nx, nar.phase, nw, nwr.phase, rx, rw);
-              } else {
-                // correction products: their own accumulator (first use at stage 0), or dt's chain
-                const uint32_t dc = corr >= 0 ? tmem + (uint32_t)(corr * N) : dt;
-                const uint32_t firstc = corr >= 0 ? (c == 0 ? 0u : 1u) : 1u;
+              // correction products: their own accumulator (first use at stage 0), or dt's chain
+              const uint32_t dc = corr >= 0 ? tmem + (uint32_t)(corr * N) : dt;
+              const uint32_t firstc = corr >= 0 ? (c == 0 ? 0u : 1u) : 1u;
+              if (PREC == B2_PRECISION_BF16)
+                issue_stage_bf16(dt, dc, a0, wd, chunk16, idesc, first, firstc, nx, nar.phase, nw, nwr.phase, lo16,
+                                 rx, rw);
+              else
                 issue_stage_tf32x3(dt, dc, a0, wd, chunk16, idesc, first, firstc, nx, nar.phase, nw, nwr.phase,
                                    lo16, rx, rw);
-              }
             }
             x_ready = rx;
             w_ready = w_last ? rw : 1u;
@@ -937,7 +964,7 @@ __global__ void __launch_bounds__(kThreadsAll, 1)
               }
             }
           };
-          if (PREC == B2_PRECISION_TF32X3 && tp.drain) {
+          if (tp.drain) {
             if (qt * 16 < N) {
               // the stages still in their slots (the last nst), then the correction accumulator
               const int nst = tp.nst, nstages = gr.nch / CPS;
@@ -1180,9 +1207,8 @@ int32_t tc_plan_t(const EfeParams& p, TcParams* tp, int* smem_bytes) {
   tp->drain = 0;
   tp->corr = -1;
   tp->tmem_cols = 512;
-  if (PREC == B2_PRECISION_TF32X3 && Nmax <= 64 &&
-      (Tr::kMaxNst + 1) * Nmax + Tr::kMaxNst * stage_cols <= 512) {
-    // 3xTF32 drain mode: stage s's hi*hi products go to accumulator slot
+  if (Nmax <= 64 && (Tr::kMaxNst + 1) * Nmax + Tr::kMaxNst * stage_cols <= 512) {
+    // Drain mode (3xTF32 and 3-pass BF16): stage s's hi*hi products go to accumulator slot
     // (ring slot of s), fresh each stage, and the producers fold it into FP64
     // before the slot's next use; one more accumulator holds the correction
     // products (hi*lo + lo*hi, about 2^-11 of the result) of the whole GEMM.
@@ -1205,9 +1231,9 @@ int32_t tc_plan_t(const EfeParams& p, TcParams* tp, int* smem_bytes) {
     if (nacc < 1) return B2_ERR_UNSUPPORTED;
     tp->nst = nst;
     tp->a_col = (nacc * Nmax + 31) / 32 * 32;
-    // 3xTF32: the correction products share one accumulator of their own, so
-    // the main chains hold hi*hi products only (a third of the MMAs)
-    if (PREC == B2_PRECISION_TF32X3 && nacc >= 3) {
+    // the correction products share one accumulator of their own when there
+    // is room, so the main chains hold hi*hi products only (a third of the MMAs)
+    if (nacc >= 3) {
       tp->corr = nacc - 1;
       nacc -= 1;
     }

@@ -65,6 +65,7 @@ struct LearnSeg {
                     // start of m in categorical obs (sum_m O_m wide);
                     // transition model: column f of the action array
   FastDiv cols_div, u_div;          // cols; U (transition model)
+  int64_t joff;                     // transition model from given joints: offset of factor f's (T-1, S_f, K_f)
   int32_t dep_q[B2_MAX_DEP_RANK];   // qs offset of each dependency factor
   FastDiv dep_div[B2_MAX_DEP_RANK];  // its number of states
 };
@@ -74,6 +75,7 @@ struct LearnParams {
   int32_t nseg, T, S_tot, obs_stride, n_act;
   int32_t lanes;         // columns per work item: 1, or 4 on the float4 path
   int64_t agent_stride;  // parameter floats per agent
+  int64_t joint_stride;  // transition model from given joints: joint floats per agent
   LearnSeg seg[kLearnMaxSeg];
 };
 
@@ -434,6 +436,48 @@ learn_trans_kernel(const LearnParams p, float* __restrict__ pB, float* __restric
   }
 }
 
+// pB += lr * sum_t joint_t (x) onehot(a_t) with the pairwise posteriors given
+// (the smoothing algorithms' form: learning.py:119-157 fed by smoothing_ovf /
+// smoothing_exact, agent.py:530-567): joint [Bn][per factor (T-1, S_f, K_f)],
+// a transition counting only when it is valid (every action >= 0, the
+// reference's _apply_transition_mask) and takes action u for f; then
+// B = normalised pB as in learn_trans_kernel.
+__global__ void __launch_bounds__(kLearnThreads, kLearnMinBlocks)
+learn_trans_joint_kernel(const LearnParams p, float* __restrict__ pB, float* __restrict__ B,
+                         const float* __restrict__ joint, const int32_t* __restrict__ act,
+                         const float* __restrict__ lr, int lr_batched, int64_t update_mask,
+                         const int32_t* __restrict__ any_valid) {
+  const uint32_t g = blockIdx.x * kLearnThreads + threadIdx.x;
+  if (g >= p.total || *any_valid == 0) return;
+  const LearnSeg& sg = p.seg[find_seg(p, g)];
+  const uint32_t r = g - sg.first;
+  const uint32_t b = fdiv(r, sg.cols_div);
+  const uint32_t c = r - b * (uint32_t)sg.cols;
+  const uint32_t kq = fdiv(c, sg.u_div);
+  const int u = (int)(c - kq * sg.u_div.d);
+  const int K = sg.cols / (int)sg.u_div.d;
+  const float l = lr[lr_batched ? b : 0];
+  const int32_t* ab = act + (int64_t)b * (p.T - 1) * p.n_act;
+  const bool learn = (update_mask >> sg.obs_col) & 1;
+  const int64_t base = (int64_t)b * p.agent_stride + sg.off + c;
+  const float* jb = joint + (int64_t)b * p.joint_stride + sg.joff + kq;
+  const int n_tr = p.T - 1;
+  auto contrib = [&](int s, float& d) -> bool {
+    if (!learn) return false;
+    bool hit = false;
+    for (int t = 0; t < n_tr; ++t) {
+      const int32_t* at = ab + (int64_t)t * p.n_act;
+      bool ok = at[sg.obs_col] == u;
+      for (int f = 0; f < p.n_act && ok; ++f) ok = at[f] >= 0;
+      if (!ok) continue;
+      d += __ldg(jb + ((int64_t)t * sg.rows + s) * K);
+      hit = true;
+    }
+    return hit;
+  };
+  update_column(pB + base, B + base, sg.rows, sg.cols, l, contrib);
+}
+
 // Agents per launch so that every work index of the launch fits 31 bits;
 // 0 when a single agent's columns do not.
 int64_t agents_per_launch(const LearnParams& p) {
@@ -649,6 +693,70 @@ extern "C" int32_t b2_update_state_transition_dirichlet(
       default: B2_LEARN_TRANS(0); break;
     }
 #undef B2_LEARN_TRANS
+    B2_TRY(check_launch(op));
+  }
+  return B2_OK;
+}
+
+extern "C" int32_t b2_update_state_transition_from_joint(
+    void* stream, float* pB, float* B, int64_t B_count, const float* joint, int64_t joint_count,
+    const int32_t* actions, int64_t actions_count, const float* lr, int32_t lr_batched, int32_t* workspace, int64_t Bn,
+    int64_t T, int64_t F, const int64_t* S, const int64_t* U, const int64_t* qs_offsets, const int64_t* B_offsets,
+    const int64_t* B_dep_flat, int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int64_t factor_mask) {
+  const char* op = "update_state_transition_from_joint";
+  if (Bn < 0 || T < 1 || F < 1) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": invalid sizes");
+  if (F > B2_MAX_FACTORS) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": too many factors");
+  if (!S || !U || !qs_offsets || !B_offsets || !B_dep_offsets || (B_dep_flat_len > 0 && !B_dep_flat))
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null attribute");
+  int64_t S_tot = 0;
+  B2_TRY(check_states(op, F, S, qs_offsets, &S_tot));
+  LearnParams p{};
+  p.lanes = 1;
+  p.T = (int32_t)T;
+  p.S_tot = (int32_t)S_tot;
+  p.n_act = (int32_t)F;
+  p.agent_stride = B_offsets[F];
+  if (B_offsets[0] != 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": B_offsets[0] must be 0");
+  int64_t joff = 0;
+  for (int64_t f = 0; f < F; ++f) {
+    if (U[f] <= 0) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": num_controls must be positive");
+    LearnSeg sg{};
+    int64_t K = 0;
+    B2_TRY(fill_deps(op, sg, f, F, S, qs_offsets, B_dep_flat, B_dep_flat_len, B_dep_offsets, &K));
+    if (B_offsets[f + 1] - B_offsets[f] != S[f] * K * U[f])
+      return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": B_offsets inconsistent with S, U and dependencies");
+    if (K * U[f] > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": tensor too large");
+    sg.rows = (int32_t)S[f];
+    sg.cols = (int32_t)(K * U[f]);
+    sg.cols_div = make_fastdiv((uint32_t)sg.cols);
+    sg.u_div = make_fastdiv((uint32_t)U[f]);
+    sg.off = B_offsets[f];
+    sg.row_q = (int32_t)qs_offsets[f];
+    sg.obs_col = (int32_t)f;
+    sg.joff = joff;
+    joff += (T - 1) * S[f] * K;
+    p.seg[p.nseg++] = sg;
+  }
+  p.joint_stride = joff;
+  if (B_count != Bn * p.agent_stride) return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": B_count mismatch");
+  if (joint_count != Bn * joff)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": joint_count mismatch (expected Bn * sum_f (T-1) S_f K_f)");
+  if (actions_count != Bn * (T - 1) * F)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": actions_count mismatch (expected Bn * (T-1) * F)");
+  if (T < 2 || Bn == 0) return B2_OK;
+  if (!pB || !B || !joint || !lr || !actions || !workspace)
+    return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": null buffer");
+  const int64_t per = agents_per_launch(p);
+  if (per == 0) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": tensor too large");
+  cudaStream_t st = (cudaStream_t)stream;
+  learn_any_valid_kernel<<<1, 1024, 0, st>>>(actions, Bn * (T - 1), (int)F, workspace);
+  B2_TRY(check_launch(op));
+  for (int64_t b0 = 0; b0 < Bn; b0 += per) {
+    const int64_t nb = Bn - b0 < per ? Bn - b0 : per;
+    const unsigned blocks = plan_launch(p, nb);
+    learn_trans_joint_kernel<<<blocks, kLearnThreads, 0, st>>>(
+        p, pB + b0 * p.agent_stride, B + b0 * p.agent_stride, joint + b0 * joff, actions + b0 * (T - 1) * F,
+        lr + (lr_batched ? b0 : 0), lr_batched, factor_mask, workspace);
     B2_TRY(check_launch(op));
   }
   return B2_OK;

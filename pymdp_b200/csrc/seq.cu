@@ -1,0 +1,327 @@
+// Sequence inference over a window of T steps for a batch of agents:
+// run_mmp / run_vmp (pymdp/algos.py:392-430, :512-571), both through
+// update_marginals (:170-238). Per iteration, for every step t and factor f:
+//   ln q      = log clip q                               (log-marginals of the previous iterate)
+//   ln A      = all_marginal_log_likelihood (:30-51): the step's log-likelihood
+//               tensors contracted with every other dependency's marginal
+//   future    = ln prior at t = 0; for t >= 1 the forward message of the
+//               transition into t: MMP log(B_{t-1} . q_{t-1}[deps]), VMP
+//               (log B_{t-1}) . q_{t-1}[deps]; MMP halves it for t < T - 1
+//               (get_mmp_messages :432-510 / get_vmp_messages :312-390)
+//   past      = for t < T - 1, the backward messages of the transitions out of
+//               t into every factor i whose B depends on f: MMP 1/2 log(q_{t+1}^i
+//               . Bn) with Bn the contraction normalised over f's axis, VMP
+//               q_{t+1}^i . (log B) contracted
+//   q         = softmax(u - mean u), u = ln q + tau (ln A - ln q + past + future)
+//               (mirror_gradient_descent_step :157-168)
+// All of it in FP64 on chip: one CTA per agent; log-likelihoods of the whole
+// window and five [T][S_tot] planes in shared memory; B is read from global
+// memory (L1-resident across iterations).
+#include <string>
+
+#include "common.cuh"
+
+namespace b2 {
+namespace {
+
+constexpr int kSeqMaxF = B2_MAX_FACTORS;
+constexpr int kSeqMaxM = B2_MAX_MODALITIES;
+constexpr int kSeqMaxRank = B2_MAX_DEP_RANK;
+constexpr double kMinD = 2.220446049250313e-16;
+
+struct SeqParams {
+  int32_t F, M, T, num_iter, vmp, distr;
+  double tau;
+  int32_t S_tot;
+  int32_t S[kSeqMaxF];
+  int32_t qs_off[kSeqMaxF + 1];
+  // modalities
+  int32_t O[kSeqMaxM], K[kSeqMaxM], rank[kSeqMaxM];
+  int8_t dep[kSeqMaxM][kSeqMaxRank];
+  int64_t A_off[kSeqMaxM];  // per-agent offset of A_m
+  int32_t O_off[kSeqMaxM + 1];  // distribution observations: offset of modality m in one step's row
+  int32_t ll_off[kSeqMaxM + 1];  // per step: offset of modality m's log-likelihood in shared memory
+  int64_t A_stride;             // 0: A shared by the batch
+  // transitions, the action-conditioned sequence (T - 1, S_f, *S[B_deps f]) per factor
+  int32_t Kb[kSeqMaxF], brank[kSeqMaxF];
+  int8_t bdep[kSeqMaxF][kSeqMaxRank];
+  int64_t B_off[kSeqMaxF];
+  int64_t B_stride;
+  int32_t smem_words;  // doubles of shared memory per agent
+};
+
+// joint of the marginals q[dep_0] x ... x q[dep_{r-1}] at flattened index k
+// (row-major), skipping position `skip` (-1: none).
+__device__ __forceinline__ double joint_at(const double* __restrict__ q, const int32_t* qs_off, const int32_t* S,
+                                           const int8_t* dep, int rank, int k, int skip) {
+  double w = 1.0;
+  for (int i = rank - 1; i >= 0; --i) {
+    const int d = S[dep[i]];
+    const int dig = k % d;
+    k /= d;
+    if (i != skip) w *= q[qs_off[dep[i]] + dig];
+  }
+  return w;
+}
+
+__global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqParams p, const float* __restrict__ A,
+                                                  const int32_t* __restrict__ obs_idx,
+                                                  const float* __restrict__ obs_distr, const float* __restrict__ B,
+                                                  const float* __restrict__ prior, float* __restrict__ qs_out) {
+  extern __shared__ double sm[];
+  const int64_t b = blockIdx.x;
+  const int T = p.T, St = p.S_tot, nthr = blockDim.x, tid = threadIdx.x;
+  const int ll_step = p.ll_off[p.M];
+  double* ll = sm;                      // [T][ll_step]
+  double* q = ll + (int64_t)T * ll_step;  // [T][St]
+  double* lnq = q + T * St;
+  double* fut = lnq + T * St;
+  double* past = fut + T * St;
+  double* la = past + T * St;
+  double* lnp = la + T * St;  // [St]
+  const float* Ab = A + b * p.A_stride;
+  const float* Bb = B + b * p.B_stride;
+
+  // log-likelihoods of every step (compute_log_likelihood_single_modality, pymdp/maths.py:214-238)
+  for (int t = 0; t < T; ++t)
+    for (int m = 0; m < p.M; ++m) {
+      const float* Am = Ab + p.A_off[m];
+      for (int k = tid; k < p.K[m]; k += nthr) {
+        double v = 0.0;
+        if (p.distr) {
+          const float* o = obs_distr + (b * T + t) * p.O_off[p.M] + p.O_off[m];
+          for (int x = 0; x < p.O[m]; ++x) {
+            const double ov = (double)o[x];
+            if (ov != 0.0) v += ov * log(fmax((double)__ldg(Am + (int64_t)x * p.K[m] + k), kMinD));
+          }
+        } else {
+          const int o = obs_idx[(b * T + t) * p.M + m];
+          // an index outside [0, O) selects no row: jnp clamps it (A_m[o_m]), as here
+          const int oc = o < 0 ? (o + p.O[m] < 0 ? 0 : o + p.O[m]) : (o >= p.O[m] ? p.O[m] - 1 : o);
+          v = log(fmax((double)__ldg(Am + (int64_t)oc * p.K[m] + k), kMinD));
+        }
+        ll[t * ll_step + p.ll_off[m] + k] = v;
+      }
+    }
+  for (int j = tid; j < St; j += nthr) lnp[j] = log(fmax((double)__ldg(prior + b * St + j), kMinD));
+  for (int e = tid; e < T * St; e += nthr) {
+    const int j = e % St;
+    int f = 0;
+    while (f + 1 < p.F && j >= p.qs_off[f + 1]) ++f;
+    q[e] = 1.0 / p.S[f];
+  }
+  __syncthreads();
+
+  for (int it = 0; it < p.num_iter; ++it) {
+    for (int e = tid; e < T * St; e += nthr) lnq[e] = log(fmax(q[e], kMinD));
+    // messages and marginal log-likelihoods from the previous iterate
+    for (int e = tid; e < T * St; e += nthr) {
+      const int t = e / St, j = e - t * St;
+      int f = 0;
+      while (f + 1 < p.F && j >= p.qs_off[f + 1]) ++f;
+      const int s = j - p.qs_off[f];
+      // future message
+      double fv;
+      if (t == 0) {
+        fv = lnp[j];
+      } else {
+        const float* Bs = Bb + p.B_off[f] + ((int64_t)(t - 1) * p.S[f] + s) * p.Kb[f];
+        const double* qp = q + (t - 1) * St;
+        double acc = 0.0;
+        for (int k = 0; k < p.Kb[f]; ++k) {
+          const double w = joint_at(qp, p.qs_off, p.S, p.bdep[f], p.brank[f], k, -1);
+          const double bv = (double)__ldg(Bs + k);
+          acc += (p.vmp ? log(fmax(bv, kMinD)) : bv) * w;
+        }
+        fv = p.vmp ? acc : log(fmax(acc, kMinD));
+      }
+      if (!p.vmp && t < T - 1) fv *= 0.5;
+      fut[e] = fv;
+      // past message: transitions out of step t into every factor i whose B depends on f
+      double pv = 0.0;
+      if (t < T - 1) {
+        const double* qt = q + t * St;
+        const double* qn = q + (t + 1) * St;
+        for (int i = 0; i < p.F; ++i) {
+          int pos = -1;
+          for (int x = 0; x < p.brank[i]; ++x)
+            if (p.bdep[i][x] == f) pos = x;
+          if (pos < 0) continue;
+          const int Si = p.S[i], Kb = p.Kb[i];
+          // stride of f's axis inside B_i's parent index, and the number of other-parent combinations
+          int stf = 1;
+          for (int x = p.brank[i] - 1; x > pos; --x) stf *= p.S[p.bdep[i][x]];
+          const float* Bi = Bb + p.B_off[i] + (int64_t)t * Si * Kb;
+          double acc = 0.0;
+          for (int si = 0; si < Si; ++si) {
+            // bm[si][s] = sum over the other parents' states of M_i[si, k] prod q (k with digit_pos = s)
+            double bm_s = 0.0, bm_sum = 0.0;
+            for (int k = 0; k < Kb; ++k) {
+              const int dig = (k / stf) % p.S[f];
+              const double w = joint_at(qt, p.qs_off, p.S, p.bdep[i], p.brank[i], k, pos);
+              const double bv = (double)__ldg(Bi + (int64_t)si * Kb + k);
+              const double mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
+              if (dig == s) bm_s += mv * w;
+              if (!p.vmp) bm_sum += mv * w;
+            }
+            if (p.vmp)
+              acc += qn[p.qs_off[i] + si] * bm_s;
+            else
+              acc += qn[p.qs_off[i] + si] * (bm_s / fmax(bm_sum, kMinD));
+          }
+          pv += p.vmp ? acc : 0.5 * log(fmax(acc, kMinD));
+        }
+      }
+      past[e] = pv;
+      // marginal log-likelihood of factor f's state s at step t
+      double lv = 0.0;
+      const double* qt = q + t * St;
+      for (int m = 0; m < p.M; ++m) {
+        int pos = -1;
+        for (int x = 0; x < p.rank[m]; ++x)
+          if (p.dep[m][x] == f) pos = x;
+        if (pos < 0) continue;
+        int stf = 1;
+        for (int x = p.rank[m] - 1; x > pos; --x) stf *= p.S[p.dep[m][x]];
+        const double* L = ll + t * ll_step + p.ll_off[m];
+        const int Km = p.K[m], outer = Km / (stf * p.S[f]);
+        for (int a = 0; a < outer; ++a)
+          for (int c = 0; c < stf; ++c) {
+            const int k = (a * p.S[f] + s) * stf + c;
+            lv += L[k] * joint_at(qt, p.qs_off, p.S, p.dep[m], p.rank[m], k, pos);
+          }
+      }
+      la[e] = lv;
+    }
+    __syncthreads();
+    // mirror-descent step and softmax, one warp per (t, f)
+    const int warp = tid >> 5, lane = tid & 31, nw = nthr >> 5;
+    for (int tf = warp; tf < T * p.F; tf += nw) {
+      const int t = tf / p.F, f = tf - t * p.F;
+      const int o = t * St + p.qs_off[f], n = p.S[f];
+      double sum = 0.0;
+      for (int s = lane; s < n; s += 32) {
+        const double u = lnq[o + s] + p.tau * (la[o + s] - lnq[o + s] + past[o + s] + fut[o + s]);
+        lnq[o + s] = u;  // this warp alone owns (t, f): reuse the plane
+        sum += u;
+      }
+#pragma unroll
+      for (int x = 16; x > 0; x >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, x);
+      const double mean = sum / n;
+      double mx = -INFINITY;
+      for (int s = lane; s < n; s += 32) mx = fmax(mx, lnq[o + s] - mean);
+#pragma unroll
+      for (int x = 16; x > 0; x >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, x));
+      double z = 0.0;
+      for (int s = lane; s < n; s += 32) z += exp(lnq[o + s] - mean - mx);
+#pragma unroll
+      for (int x = 16; x > 0; x >>= 1) z += __shfl_xor_sync(0xffffffffu, z, x);
+      for (int s = lane; s < n; s += 32) q[o + s] = exp(lnq[o + s] - mean - mx) / z;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < T * St; e += nthr) qs_out[b * T * St + e] = (float)q[e];
+}
+
+}  // namespace
+}  // namespace b2
+
+using namespace b2;
+
+extern "C" int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, int64_t A_count, int32_t A_batched,
+                                     const int64_t* O, int64_t M, const int32_t* obs_idx, const float* obs_distr,
+                                     int64_t obs_count, const float* B_seq, int64_t B_count, const float* prior,
+                                     int64_t prior_count, float* qs_out, int64_t qs_count, int64_t Bn, int64_t T,
+                                     int64_t F, const int64_t* S, const int64_t* A_dep_flat, int64_t A_dep_flat_len,
+                                     const int64_t* A_dep_offsets, const int64_t* B_dep_flat,
+                                     int64_t B_dep_flat_len, const int64_t* B_dep_offsets, int32_t num_iter,
+                                     float tau) {
+  const char* op = vmp ? "run_vmp" : "run_mmp";
+  auto bad = [&](const std::string& m) { return fail(B2_ERR_INVALID_ARGUMENT, std::string(op) + ": " + m); };
+  if (F < 1 || F > kSeqMaxF || M < 1 || M > kSeqMaxM) return bad("F and M must lie in [1, 16] and [1, 32]");
+  if (T < 1 || T > 4096 || num_iter < 0 || Bn < 0) return bad("invalid T, num_iter or Bn");
+  if (!S || !O || !A_dep_offsets || !B_dep_offsets || (A_dep_flat_len && !A_dep_flat) ||
+      (B_dep_flat_len && !B_dep_flat))
+    return bad("null attribute array");
+  if ((obs_idx == nullptr) == (obs_distr == nullptr)) return bad("pass exactly one of obs_idx, obs_distr");
+  SeqParams p{};
+  p.F = (int32_t)F;
+  p.M = (int32_t)M;
+  p.T = (int32_t)T;
+  p.num_iter = num_iter;
+  p.vmp = vmp ? 1 : 0;
+  p.distr = obs_distr ? 1 : 0;
+  p.tau = (double)tau;
+  int St = 0;
+  for (int f = 0; f < F; ++f) {
+    if (S[f] < 1 || S[f] > 1024) return bad("S must lie in [1, 1024]");
+    p.S[f] = (int32_t)S[f];
+    p.qs_off[f] = St;
+    St += (int)S[f];
+  }
+  p.qs_off[F] = St;
+  p.S_tot = St;
+  if (A_dep_offsets[0] != 0 || B_dep_offsets[0] != 0) return bad("dependency offsets must start at 0");
+  int64_t aoff = 0, ll = 0, ooff = 0;
+  for (int m = 0; m < M; ++m) {
+    const int64_t r = A_dep_offsets[m + 1] - A_dep_offsets[m];
+    if (r < 1 || r > kSeqMaxRank || A_dep_offsets[m + 1] > A_dep_flat_len) return bad("A dependency ranks in [1, 8]");
+    if (O[m] < 1) return bad("O must be positive");
+    int64_t K = 1;
+    for (int64_t x = 0; x < r; ++x) {
+      const int64_t d = A_dep_flat[A_dep_offsets[m] + x];
+      if (d < 0 || d >= F) return bad("A dependency out of range");
+      for (int64_t y = 0; y < x; ++y)
+        if (A_dep_flat[A_dep_offsets[m] + y] == d) return bad("duplicate factor in A_dependencies");
+      p.dep[m][x] = (int8_t)d;
+      K *= S[d];
+    }
+    if (K > (1 << 20)) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": A modality too large");
+    p.O[m] = (int32_t)O[m];
+    p.K[m] = (int32_t)K;
+    p.rank[m] = (int32_t)r;
+    p.A_off[m] = aoff;
+    p.O_off[m] = (int32_t)ooff;
+    p.ll_off[m] = (int32_t)ll;
+    aoff += O[m] * K;
+    ooff += O[m];
+    ll += K;
+  }
+  p.O_off[M] = (int32_t)ooff;
+  p.ll_off[M] = (int32_t)ll;
+  p.A_stride = A_batched ? aoff : 0;
+  int64_t boff = 0;
+  for (int f = 0; f < F; ++f) {
+    const int64_t r = B_dep_offsets[f + 1] - B_dep_offsets[f];
+    if (r < 1 || r > kSeqMaxRank || B_dep_offsets[f + 1] > B_dep_flat_len) return bad("B dependency ranks in [1, 8]");
+    int64_t K = 1;
+    for (int64_t x = 0; x < r; ++x) {
+      const int64_t d = B_dep_flat[B_dep_offsets[f] + x];
+      if (d < 0 || d >= F) return bad("B dependency out of range");
+      p.bdep[f][x] = (int8_t)d;
+      K *= S[d];
+    }
+    if (K > (1 << 20)) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": B parent joint too large");
+    p.Kb[f] = (int32_t)K;
+    p.brank[f] = (int32_t)r;
+    p.B_off[f] = boff;
+    boff += (T - 1) * S[f] * K;
+  }
+  p.B_stride = boff;
+  const int64_t words = T * ll + 5 * T * St + St;
+  if (words * 8 > 200 * 1024)
+    return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": window of " + std::to_string(words * 8) +
+                                        " bytes of FP64 state exceeds 200 KB of shared memory");
+  p.smem_words = (int32_t)words;
+  if (A_count != (A_batched ? Bn : 1) * aoff) return bad("A element_count mismatch");
+  if (obs_count != Bn * T * (obs_distr ? ooff : M)) return bad("observation element_count mismatch");
+  if (B_count != Bn * boff) return bad("B element_count mismatch");
+  if (prior_count != Bn * St || qs_count != Bn * T * St) return bad("prior / qs element_count mismatch");
+  if (Bn == 0) return B2_OK;
+  if (!A || (boff > 0 && !B_seq) || !prior || !qs_out) return bad("null buffer");
+  if (Bn > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
+  const int bytes = (int)(words * 8);
+  B2_TRY(ensure_smem_attr((const void*)seq_kernel, bytes, op));
+  seq_kernel<<<(unsigned)Bn, 256, bytes, (cudaStream_t)stream>>>(p, A, obs_idx, obs_distr, B_seq, prior, qs_out);
+  return check_launch(op);
+}

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (FLAG_MODEL_PARAMS_STATIC, FLAG_POLICY_TREE, FLAG_USE_INDUCTIVE, FLAG_USE_PARAM_INFO_GAIN,  # noqa: F401
+from ._lib import (FLAG_FACTORED, FLAG_MODEL_PARAMS_STATIC, FLAG_POLICY_TREE, FLAG_USE_INDUCTIVE, FLAG_USE_PARAM_INFO_GAIN,  # noqa: F401
                    FLAG_USE_STATES_INFO_GAIN, FLAG_USE_UTILITY, MAX_DEP_RANK, PRECISIONS, PRECISION_SHIFT,
                    B2Error, InvalidArgumentError, UnsupportedError, check, i64, is_available)
 
@@ -241,11 +241,14 @@ def can_handle(A_dependencies, B_dependencies, use_param_info_gain: bool, *, num
 
 
 def efe_flags(use_utility=True, use_states_info_gain=True, use_param_info_gain=False, use_inductive=False,
-              ffi_cache_params_static=False, precision="fp32", policy_tree=False) -> int:
+              ffi_cache_params_static=False, precision="fp32", policy_tree=False, factored=False) -> int:
     """Flag word of ``b2_neg_efe``. ``policy_tree`` declares the policy matrix
     to be ``construct_policies``' full product set (``B2_FLAG_POLICY_TREE``):
-    the tensor-core paths then evaluate each distinct prefix once."""
+    the tensor-core paths then evaluate each distinct prefix once. With it,
+    ``factored`` (``B2_FLAG_FACTORED``) contracts A factor by factor over the
+    distinct per-factor marginals when the transitions are factor-local."""
     flags = FLAG_POLICY_TREE if policy_tree else 0
+    flags |= FLAG_FACTORED if (factored and policy_tree) else 0
     flags |= FLAG_USE_UTILITY if use_utility else 0
     flags |= FLAG_USE_STATES_INFO_GAIN if use_states_info_gain else 0
     flags |= FLAG_USE_INDUCTIVE if use_inductive else 0
@@ -342,11 +345,29 @@ class EfeLayout:
             c[0], c[2], c[3], c[5], c[11], len(self.B_dep_flat), c[12], mask))
 
 
+    def learn_B_joint(self, pB: torch.Tensor, B: torch.Tensor, joint: torch.Tensor, actions: torch.Tensor,
+                      lr: torch.Tensor, workspace: torch.Tensor, Bn: int, T: int, factor_mask: int | None = None):
+        """``b2_update_state_transition_from_joint`` in place on the flattened
+        ``pB`` / ``B``: ``joint`` ``[Bn, sum_f (T-1) S_f K_f]`` (per factor the
+        ``(T-1, S_f, *S_deps)`` pairwise posteriors), ``actions`` int32
+        ``[Bn, T-1, F]``, ``workspace`` one device int32."""
+        for t in (pB, B, joint, actions, lr, workspace):
+            _require_cuda(t, "learning buffer")
+        c = self._c
+        mask = (1 << self.F) - 1 if factor_mask is None else int(factor_mask)
+        check(_lib.load().b2_update_state_transition_from_joint(
+            _stream(pB), pB.data_ptr(), B.data_ptr(), B.numel(), joint.data_ptr(), joint.numel(), actions.data_ptr(),
+            actions.numel(), lr.data_ptr(), int(lr.numel() != 1), workspace.data_ptr(), int(Bn), int(T), self.F,
+            c[0], c[2], c[3], c[5], c[11], len(self.B_dep_flat), c[12], mask))
+
+
+
 def neg_efe_all_policies_ffi(policy_matrix, qs_init, A, B, C, I, A_dependencies, B_dependencies, *,
                              pA=None, pB=None, use_utility: bool = True, use_states_info_gain: bool = True,
                              use_param_info_gain: bool = False, use_inductive: bool = True,
                              inductive_epsilon: float = 1e-3, ffi_cache_params_static: bool = False,
-                             precision: str = "fp32", policy_tree: bool = False) -> torch.Tensor:
+                             precision: str = "fp32", policy_tree: bool = False,
+                             factored: bool = False) -> torch.Tensor:
     """``pymdp/ffi/_efe.py:491-711``: ``neg_efe`` (G) of every policy.
 
     ``qs_init[f]``: ``(*batch, S_f)``; ``A[m]``: ``(*batch, O_m, *S_deps)``;
@@ -419,7 +440,7 @@ def neg_efe_all_policies_ffi(policy_matrix, qs_init, A, B, C, I, A_dependencies,
     eps = _dev_f32(torch.as_tensor(inductive_epsilon, dtype=torch.float32), dev).reshape(-1).contiguous()
     out = torch.empty(lead + (P,), dtype=torch.float32, device=dev)
     flags = efe_flags(use_utility, use_states_info_gain, use_param_info_gain, use_inductive,
-                      ffi_cache_params_static, precision, policy_tree=policy_tree)
+                      ffi_cache_params_static, precision, policy_tree=policy_tree, factored=factored)
     lay.call(None, pm, 0, qs_flat, A_flat, B_flat, C_flat, I_flat, pA_flat, pB_flat, eps, out, Bn, P, flags)
     return out
 
@@ -477,3 +498,52 @@ def select_action(q_pi: torch.Tensor, policy_matrix: torch.Tensor) -> torch.Tens
     _require_cuda(q_pi, "q_pi")
     check(_lib.load().b2_select_action(_stream(act), q_pi.data_ptr(), pm.data_ptr(), act.data_ptr(), Bn, P, T, F))
     return act
+
+
+def expected_state(qs_flat: torch.Tensor, B_flat: torch.Tensor, action: torch.Tensor, lay: "EfeLayout",
+                   out: torch.Tensor | None = None) -> torch.Tensor:
+    """``b2_expected_state``: ``compute_expected_state`` (``pymdp/control.py:
+    351-389``) per agent on flattened beliefs ``[Bn, sum S]`` and transitions
+    ``[Bn, B_offsets[F]]`` with ``action`` int32 ``[Bn, F]``."""
+    for t in (qs_flat, B_flat, action):
+        _require_cuda(t, "expected-state buffer")
+    Bn = qs_flat.shape[0]
+    act = action.to(torch.int32).contiguous()
+    out = torch.empty_like(qs_flat) if out is None else out
+    c = lay._c
+    check(_lib.load().b2_expected_state(_stream(out), qs_flat.data_ptr(), qs_flat.numel(), B_flat.data_ptr(),
+                                        B_flat.numel(), act.data_ptr(), act.numel(), out.data_ptr(), int(Bn), lay.F,
+                                        c[0], c[2], c[3], c[5], c[11], len(lay.B_dep_flat), c[12]))
+    return out
+
+
+def unique_multiactions(policy_matrix, num_controls) -> np.ndarray:
+    """The reference's ``Agent.unique_multiactions`` (``pymdp/agent.py:396-399``):
+    the sorted distinct first-step joint actions, padded with -1 rows to
+    ``prod(num_controls)`` rows (``jnp.unique(..., size=, fill_value=-1)``)."""
+    first = np.unique(np.asarray(policy_matrix)[:, 0], axis=0)
+    size = int(np.prod(num_controls))
+    out = np.full((size, first.shape[1]), -1, dtype=np.int32)
+    out[:min(size, len(first))] = first[:size]
+    return out
+
+
+def multiaction_probabilities(q_pi: torch.Tensor, policy_matrix: torch.Tensor, unique: torch.Tensor,
+                              num_controls, sampling_mode: str = "full") -> torch.Tensor:
+    """``b2_multiaction_probabilities``: ``Agent.multiaction_probabilities``
+    (``pymdp/agent.py:908-937``) for a batch ``q_pi [Bn, P]``; returns
+    ``[Bn, prod(num_controls)]``."""
+    if sampling_mode not in ("full", "marginal"):
+        raise ValueError("sampling_mode must be 'full' or 'marginal'")
+    _require_cuda(q_pi, "q_pi")
+    q_pi = q_pi.contiguous()
+    pm = torch.as_tensor(policy_matrix, device=q_pi.device).to(torch.int32).contiguous()
+    uq = torch.as_tensor(unique, device=q_pi.device).to(torch.int32).contiguous()
+    P, T, F = pm.shape
+    Bn = q_pi.numel() // P
+    n = int(uq.shape[0])
+    out = torch.empty(q_pi.shape[:-1] + (n,), dtype=torch.float32, device=q_pi.device)
+    check(_lib.load().b2_multiaction_probabilities(_stream(out), q_pi.data_ptr(), pm.data_ptr(), uq.data_ptr(), n,
+                                                   int(sampling_mode == "marginal"), Bn, P, T, F,
+                                                   i64(list(num_controls)), out.data_ptr()))
+    return out

@@ -123,8 +123,8 @@ def test_transition_model_without_valid_transition_writes_nothing():
         np.testing.assert_allclose(got[f][1], ol.dirichlet_expected_value(pB[f][1]), rtol=E_RTOL, atol=E_ATOL)
 
 
-@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
-def test_agent_online_learning_loop_matches_oracle(precision):
+@pytest.mark.parametrize("precision,efe_algorithm", [("fp32", "dense"), ("tf32x3", "dense"), ("fp32", "factored")])
+def test_agent_online_learning_loop_matches_oracle(precision, efe_algorithm):
     """Agent.infer_parameters (pymdp/agent.py:416-620) in a closed loop:
     infer_states -> infer_policies -> sample_action -> infer_parameters, three
     steps; A, B, pA, pB and every step's G follow the FP64 oracle fed with the
@@ -146,7 +146,8 @@ def test_agent_online_learning_loop_matches_oracle(precision):
     pA = [rng.uniform(0.2, 2.0, size=a.shape).astype(np.float32) for a in A]
     pB = [rng.uniform(0.2, 2.0, size=b.shape).astype(np.float32) for b in B]
     agent = Agent(A, B, C=C, A_dependencies=A_deps, B_dependencies=B_deps, policy_len=T, gamma=16.0,
-                  batch_size=batch, pA=pA, pB=pB, learn_A=True, learn_B=True, precision=precision)
+                  batch_size=batch, pA=pA, pB=pB, learn_A=True, learn_B=True, precision=precision,
+                  efe_algorithm=efe_algorithm)
     ref = [[np.asarray(x, np.float64) for x in y] for y in (pA, A, pB, B)]
     pol = oefe.construct_policies(S, U, T)
     lrA = np.array([3.0, 1.0, 0.5], np.float32)
@@ -257,3 +258,85 @@ def test_obs_model_float4_path_matches_oracle(T, categorical):
             for m in range(len(O)):
                 np.testing.assert_allclose(got_p[m][b], qA[m], rtol=P_RTOL, atol=0)
                 np.testing.assert_allclose(got_e[m][b], EA[m], rtol=E_RTOL, atol=E_ATOL)
+
+
+def test_transition_learning_from_given_joints_matches_reference():
+    """b2_update_state_transition_from_joint on the fixture made by the
+    reference's own learning.py with pairwise joints (the smoothing
+    algorithms' branch of Agent.infer_parameters)."""
+    from pymdp_b200 import ffi
+    d = load_golden("learn_B_joint")
+    Bn, U = int(d["Bn"]), int(d["U"])
+    S = d["pB"].shape[1]
+    Tm1 = d["joint"].shape[1]
+    lay = ffi.EfeLayout([S], [1], [U], 1, [[0]], [[0]])
+    pB = torch.as_tensor(d["pB"].reshape(Bn, -1), device="cuda").float().contiguous()
+    B = torch.as_tensor(d["B"].reshape(Bn, -1), device="cuda").float().contiguous()
+    joint = torch.as_tensor(d["joint"].reshape(Bn, -1), device="cuda").float().contiguous()
+    act = torch.as_tensor(d["actions"], device="cuda").to(torch.int32).contiguous()
+    lr = torch.as_tensor(d["lr"], device="cuda").float()
+    work = torch.zeros(1, dtype=torch.int32, device="cuda")
+    lay.learn_B_joint(pB, B, joint, act, lr, work, Bn, Tm1 + 1)
+    np.testing.assert_allclose(pB.cpu().numpy().reshape(d["qB"].shape), d["qB"], rtol=2e-6, atol=1e-7)
+    np.testing.assert_allclose(B.cpu().numpy().reshape(d["EB"].shape), d["EB"], rtol=2e-6, atol=1e-7)
+
+
+def test_transition_learning_from_outer_product_joints_equals_the_filtering_form():
+    """Joints formed as q_{t+1} (x) q_t[deps] give the filtering form's update
+    (b2_update_state_transition_dirichlet) on a multi-factor model with
+    multi-parent transitions and one invalid step."""
+    from pymdp_b200 import ffi
+    rng = np.random.default_rng(41)
+    S, U, B_deps, T, Bn = [3, 4, 2], [2, 3, 1], [[0], [1, 0], [2, 1]], 4, 3
+    lay = ffi.EfeLayout(S, [1], U, 1, [[0]], B_deps)
+    nB = int(lay.B_offsets[-1])
+    pB = torch.as_tensor(rng.uniform(0.2, 2.0, size=(Bn, nB)), device="cuda").float()
+    B0 = torch.zeros_like(pB)
+    qs = [rng.dirichlet(np.ones(s), size=(Bn, T)).astype(np.float32) for s in S]
+    act = np.stack([rng.integers(0, u, size=(Bn, T - 1)) for u in U], -1).astype(np.int32)
+    act[1, 2, 0] = -1  # an invalid step: masked in both forms
+    joints = []
+    for f in range(len(S)):
+        parents = [qs[d][:, :-1] for d in B_deps[f]]
+        j = qs[f][:, 1:]
+        for p in parents:
+            j = j[..., None] * p.reshape(p.shape[:2] + (1,) * (j.ndim - 2) + (p.shape[-1],))
+        joints.append(j.reshape(Bn, -1))
+    joint = torch.as_tensor(np.concatenate(joints, 1), device="cuda").contiguous()
+    q_seq = torch.as_tensor(np.concatenate(qs, -1), device="cuda").contiguous()
+    act_d = torch.as_tensor(act, device="cuda").contiguous()
+    lr = torch.full((Bn,), 0.7, device="cuda")
+    w1, w2 = torch.zeros(1, dtype=torch.int32, device="cuda"), torch.zeros(1, dtype=torch.int32, device="cuda")
+    pB1, B1, pB2, B2 = pB.clone(), B0.clone(), pB.clone(), B0.clone()
+    lay.learn_B(pB1, B1, q_seq, act_d, lr, w1, Bn, T)
+    lay.learn_B_joint(pB2, B2, joint, act_d, lr, w2, Bn, T)
+    np.testing.assert_allclose(pB2.cpu().numpy(), pB1.cpu().numpy(), rtol=2e-6, atol=1e-7)
+    np.testing.assert_allclose(B2.cpu().numpy(), B1.cpu().numpy(), rtol=2e-6, atol=1e-7)
+
+
+def test_agent_learns_B_from_exact_smoothing_joints():
+    """The "exact" smoothing branch end to end on the device: filtered beliefs
+    -> hmm.smoothing_exact (pymdp/inference.py:595-634) -> pairwise joints ->
+    Agent.infer_parameters(joint_beliefs=...) (pymdp/agent.py:530-567), against
+    the FP64 oracle applied to the same joints."""
+    from pymdp_b200 import Agent, hmm
+    rng = np.random.default_rng(17)
+    S, U, O, T, Bn = 6, 3, 4, 5, 4
+    A = rng.dirichlet(np.ones(O), size=S).T.astype(np.float32)
+    B = np.moveaxis(rng.dirichlet(np.ones(S), size=(S, U)), -1, 0).astype(np.float32)
+    pB = rng.uniform(0.5, 2.0, size=(S, S, U)).astype(np.float32)
+    agent = Agent([A], [B], pB=[pB], learn_B=True, batch_size=Bn)
+    filt = torch.as_tensor(rng.dirichlet(np.ones(S), size=(Bn, T)).astype(np.float32), device="cuda")
+    acts = rng.integers(0, U, size=(Bn, T - 1)).astype(np.int32)
+    acts[2, 1] = -1  # no action taken at that step: the identity transition, and a masked learning step
+    B_dev = torch.as_tensor(np.broadcast_to(B, (Bn,) + B.shape).copy(), device="cuda")
+    _, joints = hmm.smoothing_exact([filt], [B_dev], torch.as_tensor(acts, device="cuda"))
+    agent.infer_parameters(None, None, torch.as_tensor(acts[..., None], device="cuda"), joint_beliefs=joints,
+                           lr_pB=0.5)
+    jn = joints[0].cpu().numpy().astype(np.float64)
+    for b in range(Bn):
+        a = acts[b].astype(np.int64)
+        jm = jn[b] * (a >= 0)[:, None, None]  # the reference masks invalid transitions
+        qb, eb = ol.update_state_transition_from_joint(pB, jm, np.where(a >= 0, a, 0), U, lr=0.5)
+        np.testing.assert_allclose(agent.pB[0][b].cpu().numpy(), qb, rtol=2e-6, atol=1e-7)
+        np.testing.assert_allclose(agent.B[0][b].cpu().numpy(), eb, rtol=2e-6, atol=1e-7)

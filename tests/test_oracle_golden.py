@@ -114,3 +114,18 @@ def test_efe_oracle_out_of_range_action_matches_reference():
                                              d["E"], A_deps, B_deps, gamma=float(d["gamma"]))
     np.testing.assert_allclose(G, d["G"], rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(q_pi, d["q_pi"], rtol=1e-10, atol=1e-300)
+
+
+def test_multiaction_oracle_marginal_and_full_agree_on_product_policies():
+    """For the full product policy set the "marginal" mode's outer product of
+    action marginals and the "full" mode's sums coincide when q_pi factorises
+    over the first-step actions; both sum to one."""
+    S, U, T = [3, 2, 2], [3, 2, 1], 2
+    pol = oefe.construct_policies(S, U, T)
+    rng = np.random.default_rng(0)
+    m = [rng.dirichlet(np.ones(u)) for u in U]
+    q = np.array([np.prod([m[f][p[0, f]] for f in range(len(U))]) for p in pol]) / (len(pol) // int(np.prod(U)))
+    full = oefe.multiaction_probabilities(q, pol, U, "full")
+    marg = oefe.multiaction_probabilities(q, pol, U, "marginal")
+    np.testing.assert_allclose(full, marg, rtol=1e-12)
+    np.testing.assert_allclose(full.sum(), 1.0, rtol=1e-12)
