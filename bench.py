@@ -253,6 +253,52 @@ def run_hmm_config(dev, steps: int, warmup: int, flush, agents: int = HMM_AGENTS
             "gbs": nbytes / (ms * 1e-3) / 1e9}
 
 
+SEQ_AGENTS, SEQ_T, SEQ_S, SEQ_O, SEQ_ITERS = 4096, 8, [16, 8], [16, 8], 16
+
+
+def run_seq_config(dev, steps: int, warmup: int, flush):
+    """Sequence inference (run_mmp, pymdp/algos.py:392-430) for 4096 agents:
+    a window of 8 steps, S=[16, 8], O=[16, 8] on both factors, factor-local
+    action-conditioned transitions, index observations, 16 iterations of
+    tau 0.25. Device time per launch (L2 flushed before each) and
+    agent-windows/s; algorithmic bytes = A, B sequence, observations, prior in
+    and the posteriors out."""
+    import torch
+
+    from pymdp_b200 import seq
+
+    g = torch.Generator(device=dev).manual_seed(13)
+    Bn, T, S, O = SEQ_AGENTS, SEQ_T, SEQ_S, SEQ_O
+    K = int(np.prod(S))
+    A = [torch.softmax(torch.randn((Bn, o) + tuple(S), device=dev, generator=g) * 2, dim=1) for o in O]
+    B = [torch.softmax(torch.randn((Bn, T - 1, s, s), device=dev, generator=g) * 2, dim=2) for s in S]
+    obs = [torch.randint(0, o, (Bn, T), device=dev, generator=g, dtype=torch.int32) for o in O]
+    prior = [torch.softmax(torch.randn((Bn, s), device=dev, generator=g), dim=1) for s in S]
+    deps = [[0, 1]] * len(O)
+
+    def launch():
+        return seq.run_mmp(A, B, obs, prior, deps, [[0], [1]], num_iter=SEQ_ITERS, tau=0.25, distr_obs=False)
+
+    for _ in range(max(1, warmup)):
+        launch()
+    torch.cuda.synchronize(dev)
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launch()
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    nbytes = 4.0 * Bn * (sum(O) * K + (T - 1) * sum(s * s for s in S) + T * len(O) + sum(S) + T * sum(S))
+    return {"workload": f"run_mmp, {Bn} agents, window T={T}, S={S}, O={O} on both factors, factor-local "
+                        f"transitions, index observations, {SEQ_ITERS} iterations (tau 0.25), L2 flushed",
+            "agent_windows_per_s": Bn / (ms * 1e-3), "ms_per_launch": ms, "bytes_per_launch": nbytes,
+            "gbs": nbytes / (ms * 1e-3) / 1e9}
+
+
 FIT_SUBJECTS, FIT_TRIALS = 1024, 64
 
 
@@ -779,6 +825,7 @@ def run_b200(args, rank, world, local_rank):
     ro_res = run_rollout_config(dev, min(args.steps, 5), args.warmup) if extras else None
     learn_res = run_learn_config(dev, args.steps, args.warmup, flush) if extras else None
     hmm_res = run_hmm_config(dev, args.steps, args.warmup, flush) if extras else None
+    seq_res = run_seq_config(dev, args.steps, args.warmup, flush) if extras else None
     c1_res = run_config1(dev, args.steps, args.warmup) if world == 1 and not main_only else None
     plain_res = run_plain_config(dev, model, min(args.steps, 3), 1, flush) if world == 1 and not main_only else None
     efe_ev = []
@@ -955,6 +1002,7 @@ def run_b200(args, rank, world, local_rank):
         "rollout": ro_res,
         "learn": learn_res,
         "hmm": hmm_res,
+        "seq": seq_res,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -979,7 +1027,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout", "learn", "hmm"],
+    ap.add_argument("--workload", default="step", choices=["step", "fpi", "fit", "rollout", "learn", "hmm", "seq"],
                     help="step: the agent step (default); fpi: only the 4096-agent FPI model; fit: only the "
                          "model-fitting gradient; rollout: only the uneven-size rollout (for profiling)")
     ap.add_argument("--legs", default="all", choices=["all", "step", "main"],
@@ -1025,6 +1073,8 @@ def main():
             res = run_rollout_config(dev, args.steps, args.warmup)
         elif args.workload == "hmm":
             res = run_hmm_config(dev, args.steps, args.warmup, flush, args.hmm_agents)
+        elif args.workload == "seq":
+            res = run_seq_config(dev, args.steps, args.warmup, flush)
         else:
             res = run_learn_config(dev, args.steps, args.warmup, flush)
         print(json.dumps(res), flush=True)

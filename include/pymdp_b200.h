@@ -56,10 +56,11 @@ enum {
  * the distinct predicted marginals of each factor (factor f has U_f^(t+1) of
  * them after step t, one per history of its own actions) instead of once per
  * policy prefix. Same G in another summation order, in FP32 with FP64
- * accumulation of G; the precision bits are not used. Ignored (the other
- * paths run) when the tree conditions do not hold, a dependency tuple has
- * rank above 3, a factor has more than 64 states, or the flag-gated terms
- * (bits 2 and 3) are on. */
+ * accumulation of G; the precision bits are not used. All four terms are
+ * supported (the pA weights ride along the contraction as extra rows; the pB
+ * and inductive terms are per factor history). Ignored (the other paths run)
+ * when the tree conditions do not hold, a dependency tuple has rank above 3,
+ * or a factor has more than 64 states. */
 #define B2_FLAG_FACTORED 64
 /* Precision selector, bits 8-9 of `flags` (unused by the reference ABI). */
 #define B2_PRECISION_SHIFT 8

@@ -535,7 +535,8 @@ int32_t neg_efe_impl(void* stream_, const int32_t* policy_matrix, int64_t pm_cou
   if ((use_pig && ((pA_count && !pA) || (pB_count && !pB))) || (use_ind && (!I || !inductive_epsilon)))
     return fail(B2_ERR_INVALID_ARGUMENT, std::string(kEfeName) + ": null buffer");
   if (use_pig || use_ind) {
-    // the flag-gated terms run on the SIMT FP32 kernel (any precision selector)
+    // the flag-gated terms: weights first (FP64 digamma / inductive paths),
+    // then the factored path where it applies, else the SIMT FP32 kernel
     const size_t lin_bytes = (size_t)Bn * p.T * p.K_tot * sizeof(float);
     const size_t wa_bytes = (use_pig && pA_count) ? (size_t)Bn * p.A_stride * sizeof(float) : 0;
     const size_t wb_bytes = (use_pig && pB_count) ? (size_t)Bn * p.B_stride * sizeof(float) : 0;
@@ -564,8 +565,11 @@ int32_t neg_efe_impl(void* stream_, const int32_t* policy_matrix, int64_t pm_cou
                                                                            eps_count == Bn && Bn > 1, wI, Bn);
       rc = check_launch("efe_ffi inductive weights");
     }
-    if (rc == B2_OK) rc = launch_linear_rows(p, Bn, A, C, lin, stream);
-    if (rc == B2_OK)
+    bool done = false;
+    if (rc == B2_OK && (flags & B2_FLAG_FACTORED) && (flags & B2_FLAG_POLICY_TREE) && !pm_batched)
+      rc = launch_efe_fact(p, Bn, qs_init, A, B, C, neg_efe_out, stream, &done, wA, wB, wI);
+    if (rc == B2_OK && !done) rc = launch_linear_rows(p, Bn, A, C, lin, stream);
+    if (rc == B2_OK && !done)
       rc = launch_efe_plain(p, Bn, policy_matrix, pm_batched, qs_init, A, B, lin, neg_efe_out, stream, wA, wB, wI);
     cudaError_t fe = cudaFreeAsync(ws, stream);
     if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);

@@ -87,8 +87,12 @@ int32_t launch_efe_tc(const EfeParams& p, int prec, int64_t Bn, const int32_t* p
 // distinct per-factor marginals of the policy tree; *used = false when the
 // model is outside it (transitions not factor-local, a dependency tuple of
 // rank above 3, a factor above 64 states, ...) and nothing was launched.
+// wA / wB / wI: the parameter-information-gain weights (laid out like A / B)
+// and the inductive weights per factor state (efe_wnorm_kernel,
+// efe_inductive_kernel), null when the term is off.
 int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const float* A, const float* B,
-                        const float* C, float* G, cudaStream_t stream, bool* used);
+                        const float* C, float* G, cudaStream_t stream, bool* used, const float* wA = nullptr,
+                        const float* wB = nullptr, const float* wI = nullptr);
 bool efe_fact_applies(const EfeParams& p, int64_t Bn);
 // Bytes of the tensor-core operand images for Bn agents at precision prec
 // (0 when the model takes the SIMT path).

@@ -60,8 +60,10 @@ struct FactGroup {
   int32_t K, R;                         // prod of sizes; K / S[0] (one V1 row: s1 outer, s2 inner)
   int32_t vec4;                         // level-1 axis contiguous and every row start 16-byte aligned
   int32_t n_obs, m_begin, m_end;        // observation rows; modalities [m_begin, m_end) of mod_order
+  int32_t n_w;                          // parameter-information-gain rows (wA, one per observation row) or 0;
+                                        // V1 rows: [n_obs A rows][n_w wA rows][1 linear row]
   int32_t H[kFactMaxRank][kFactMaxT];   // histories of f[i] at depth t (1 past rank)
-  int64_t v1_off[kFactMaxT];            // per-agent float offset of V1 at depth t: [H0][n_obs + 1][R]
+  int64_t v1_off[kFactMaxT];            // per-agent float offset of V1 at depth t: [H0][n_obs + n_w + 1][R]
   int64_t tab_off[kFactMaxT];           // per-agent double offset of the table at depth t: [H0][H1][H2]
 };
 
@@ -70,6 +72,9 @@ struct FactParams {
   int32_t ustride[kEfeMaxF];                // joint action a = sum_f u_f * ustride[f] (construct_policies order)
   int64_t qh_off[kEfeMaxF][kFactMaxT];      // per-agent float offset of factor f's histories at depth t
   int64_t qh_stride, v1_stride, tab_stride; // per-agent floats / floats / doubles
+  int32_t hterm;                            // 1: per-factor history terms (pB information gain, inductive value)
+  int64_t ht_off[kEfeMaxF][kFactMaxT];      // per-agent double offset of factor f's history terms at depth t
+  int64_t ht_stride;                        // doubles per agent
   int32_t max_R, max_tiles;
   int32_t smax;                             // largest size among the factors the tail contracts
   int32_t tail_smem;                        // dynamic shared memory of the tail kernel (bytes)
@@ -85,11 +90,17 @@ __host__ __device__ __forceinline__ int ipow(int b, int e) {
 
 // History marginals: Qh[f][t][h] = B_f[:, :, u] . Qh[f][t-1][h / U_f] with
 // u = h % U_f (qs_init at t = 0): compute_expected_state (pymdp/control.py:
-// 351-389) for a factor-local B, once per distinct action history.
+// 351-389) for a factor-local B, once per distinct action history. With the
+// flag-gated terms, also the per-history step terms Ht[f][t][h]: minus the
+// pB information gain q_next . (wB_f[..., u] . q_prev) (calc_negative_pB_info_gain,
+// pymdp/control.py:555-602) plus the inductive value wI_f . q_next
+// (calc_inductive_value_t, pymdp/control.py:1021-1061).
 __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constant__ EfeParams p,
                                                             const __grid_constant__ FactParams fp,
                                                             const float* __restrict__ qs_init,
-                                                            const float* __restrict__ B, float* __restrict__ Qh) {
+                                                            const float* __restrict__ B, float* __restrict__ Qh,
+                                                            const float* __restrict__ wB,
+                                                            const float* __restrict__ wI, double* __restrict__ Ht) {
   const int64_t b = blockIdx.x;
   float* Qb = Qh + b * fp.qh_stride;
   const float* Bb = B + b * p.B_stride;
@@ -110,6 +121,30 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
       }
     }
     __syncthreads();
+    if (fp.hterm) {
+      // one thread per history of each factor at this depth
+      for (int f = 0; f < p.F; ++f) {
+        const int S = p.S[f], U = p.U[f];
+        const int H = ipow(U, t + 1);
+        for (int h = threadIdx.x; h < H; h += blockDim.x) {
+          const int u = h % U;
+          const float* qn = Qb + fp.qh_off[f][t] + (int64_t)h * S;
+          const float* qp = t == 0 ? qs_init + b * p.S_tot + p.qs_off[f] : Qb + fp.qh_off[f][t - 1] + (int64_t)(h / U) * S;
+          double v = 0.0;
+          if (wB) {
+            const float* Ws = wB + b * p.B_stride + p.fac[f].B_off + u;
+            for (int s = 0; s < S; ++s) {
+              float fd = 0.f;
+              for (int k = 0; k < S; ++k) fd = fmaf(__ldg(Ws + ((int64_t)s * S + k) * U), qp[k], fd);
+              v -= (double)qn[s] * fd;
+            }
+          }
+          if (wI)
+            for (int s = 0; s < S; ++s) v += (double)__ldg(wI + b * p.S_tot + p.qs_off[f] + s) * qn[s];
+          Ht[b * fp.ht_stride + fp.ht_off[f][t] + h] = v;
+        }
+      }
+    }
   }
 }
 
@@ -122,12 +157,14 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
 __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant__ EfeParams p,
                                                           const __grid_constant__ FactParams fp,
                                                           const float* __restrict__ A, const float* __restrict__ C,
-                                                          const float* __restrict__ Qh, float* __restrict__ V1) {
+                                                          const float* __restrict__ Qh, float* __restrict__ V1,
+                                                          const float* __restrict__ wA) {
   __shared__ float qsm[kFactCombo * kFactMaxS];
   const int64_t b = blockIdx.z;
   const int g = blockIdx.y;
   if (g >= fp.G) return;  // uniform over the CTA
   const FactGroup& gr = fp.grp[g];
+  const int nrow = gr.n_obs + gr.n_w + 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if ((int)(blockIdx.x * blockDim.x) >= gr.R) return;  // uniform over the CTA
   const bool active = r < gr.R;
@@ -211,15 +248,37 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
 #pragma unroll
         for (int i = 0; i < kFactCombo; ++i) {
           if (i < nc) {
-            Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * (gr.n_obs + 1) + row) * gr.R + r] = v[i];
+            Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + row) * gr.R + r] = v[i];
             lin[i] += w[i] + (ut ? __ldg(Cm + (int64_t)ct[i] * md.O + o) * v[i] : 0.f);
           }
         }
       }
     }
+    if (gr.n_w) {
+      // parameter-information-gain weights: the same contraction, rows n_obs ..
+      int wrow = gr.n_obs;
+      for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
+        const EfeModality& md = p.mod[fp.mod_order[mi]];
+        const float* Wm = wA + b * p.A_stride + md.A_off + base;
+        for (int o = 0; o < md.O; ++o, ++wrow) {
+          float v[kFactCombo];
+#pragma unroll
+          for (int i = 0; i < kFactCombo; ++i) v[i] = 0.f;
+          const float* Wr = Wm + (int64_t)o * md.K;
+          for (int s = 0; s < S0; ++s) {
+            const float a = __ldg(Wr + s * st0);
+#pragma unroll
+            for (int i = 0; i < kFactCombo; ++i) v[i] = fmaf(qsm[i * kFactMaxS + s], a, v[i]);
+          }
+#pragma unroll
+          for (int i = 0; i < kFactCombo; ++i)
+            if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + wrow) * gr.R + r] = v[i];
+        }
+      }
+    }
 #pragma unroll
     for (int i = 0; i < kFactCombo; ++i)
-      if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * (gr.n_obs + 1) + gr.n_obs) * gr.R + r] = lin[i];
+      if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + nrow - 1) * gr.R + r] = lin[i];
   }
 }
 
@@ -264,26 +323,29 @@ struct TailShape {
   static constexpr int kHpt = SMAX <= 16 ? 4 : (SMAX <= 32 ? 2 : 1);
 };
 
-// Epilogue terms of one qo column: -qo log clip qo over the observation rows
-// (information gain on) plus the linear row (its last row).
-__device__ __forceinline__ double tail_term(int n, int n_obs, bool ig, float d) {
-  if (n < n_obs) return ig ? -(double)d * (double)log_stable(d) : 0.0;
-  return (double)d;
+// Step value of one prefix from its rows of the last level: for each
+// observation row o, -qo log clip qo (information gain on) and, with the
+// parameter-information-gain rows, -qo * (wA . x)[o] (calc_negative_pA_info_gain,
+// pymdp/control.py:511-553); plus the linear row (utility and the H_A part).
+__device__ __forceinline__ double obs_term(bool ig, float d, bool w, float dw) {
+  double v = ig ? -(double)d * (double)log_stable(d) : 0.0;
+  if (w) v -= (double)d * dw;
+  return v;
 }
 
-// Final level for HPT columns per thread: qo[c][n] = sum_s qv[c][s] X[n][s]
-// over rows n = half, half + 2, ... of X (shared memory, row stride xs), the
-// two halves of a column meeting by one shuffle (lanes 2i, 2i + 1).
+// Last level for HPT columns per thread: rows of X (shared memory, row stride
+// xs; [n_obs A rows][n_w wA rows][1 linear row]); observation rows o = half,
+// half + 2, ..., the linear row by half 0; the two halves of a column meet
+// by one shuffle (lanes 2i, 2i + 1). `act` false: the thread only joins the
+// shuffle.
 template <int SMAX>
-__device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, int nrow, int n_obs, bool ig,
+__device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, int n_obs, int n_w, bool ig,
                                            int S, const float (&qv)[TailShape<SMAX>::kHpt][SMAX], int half,
-                                           double (&out)[TailShape<SMAX>::kHpt]) {
+                                           bool act, double (&out)[TailShape<SMAX>::kHpt]) {
   constexpr int HPT = TailShape<SMAX>::kHpt;
 #pragma unroll
   for (int c = 0; c < HPT; ++c) out[c] = 0.0;
-  for (int n = half; n < nrow; n += 2) {
-    const float* xr = X + n * xs;
-    float d[HPT];
+  auto dot = [&](const float* xr, float (&d)[HPT]) {
 #pragma unroll
     for (int c = 0; c < HPT; ++c) d[c] = 0.f;
 #pragma unroll
@@ -294,8 +356,21 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
         for (int c = 0; c < HPT; ++c) d[c] = fmaf(qv[c][s], x, d[c]);
       }
     }
+  };
+  if (act) {
+    for (int o = half; o < n_obs; o += 2) {
+      float d[HPT], dw[HPT];
+      dot(X + o * xs, d);
+      if (n_w) dot(X + (n_obs + o) * xs, dw);
 #pragma unroll
-    for (int c = 0; c < HPT; ++c) out[c] += tail_term(n, n_obs, ig, d[c]);
+      for (int c = 0; c < HPT; ++c) out[c] += obs_term(ig, d[c], n_w != 0, n_w ? dw[c] : 0.f);
+    }
+    if (half == 0) {
+      float d[HPT];
+      dot(X + (n_obs + n_w) * xs, d);
+#pragma unroll
+      for (int c = 0; c < HPT; ++c) out[c] += (double)d[c];
+    }
   }
 #pragma unroll
   for (int c = 0; c < HPT; ++c) out[c] += __shfl_xor_sync(0xffffffffu, out[c], 1);
@@ -315,7 +390,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
   const int64_t b = blockIdx.y;
   const FactGroup& gr = fp.grp[it.g];
   const int t = it.t, h0 = it.h0;
-  const int nrow = gr.n_obs + 1, n_obs = gr.n_obs;
+  const int n_obs = gr.n_obs, n_w = gr.n_w, nrow = n_obs + n_w + 1;
   const bool ig = (p.flags & B2_FLAG_USE_STATES_INFO_GAIN) != 0;
   const float* Qb = Qh + b * fp.qh_stride;
   const float* V1b = V1 + b * fp.v1_stride + gr.v1_off[t] + (int64_t)h0 * nrow * gr.R;
@@ -325,7 +400,10 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
   if (gr.rank == 1) {
     if (tid < 32) {
       double hs = 0.0;
-      for (int n = tid; n < nrow; n += 32) hs += tail_term(n, n_obs, ig, __ldg(V1b + (int64_t)n * gr.R));
+      for (int o = tid; o < n_obs; o += 32)
+        hs += obs_term(ig, __ldg(V1b + (int64_t)o * gr.R), n_w != 0,
+                       n_w ? __ldg(V1b + (int64_t)(n_obs + o) * gr.R) : 0.f);
+      if (tid == 0) hs += (double)__ldg(V1b + (int64_t)(nrow - 1) * gr.R);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) hs += __shfl_xor_sync(0xffffffffu, hs, o);
       if (tid == 0) tb[h0] = hs;
@@ -387,7 +465,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
       for (int s = 0; s < SMAX; ++s) qv[c][s] = (act && hl < HL && s < SL) ? __ldg(ql + (int64_t)hl * SL + s) : 0.f;
     }
     double out[HPT];
-    tail_final<SMAX>(tsm + hb * nrow * xs, xs, act ? nrow : 0, n_obs, ig, SL, qv, half, out);
+    tail_final<SMAX>(tsm + hb * nrow * xs, xs, n_obs, n_w, ig, SL, qv, half, act, out);
     if (act && half == 0) {
 #pragma unroll
       for (int c = 0; c < HPT; ++c) {
@@ -405,7 +483,8 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
 // actions come from its index in construct_policies order (mixed radix: the
 // joint action of step t is digit T-1-t of pol in base nu).
 __global__ void efe_fact_combine_kernel(const __grid_constant__ EfeParams p, const __grid_constant__ FactParams fp,
-                                        const double* __restrict__ tab, float* __restrict__ G) {
+                                        const double* __restrict__ tab, const double* __restrict__ Ht,
+                                        float* __restrict__ G) {
   const int64_t b = blockIdx.y;
   const int pol = blockIdx.x * blockDim.x + threadIdx.x;
   if (pol >= p.P) return;
@@ -426,12 +505,14 @@ __global__ void efe_fact_combine_kernel(const __grid_constant__ EfeParams p, con
       if (gr.rank > 2) idx = idx * gr.H[2][t] + hist[gr.f[2]];
       g += tb[gr.tab_off[t] + idx];
     }
+    if (fp.hterm)
+      for (int f = 0; f < p.F; ++f) g += Ht[b * fp.ht_stride + fp.ht_off[f][t] + hist[f]];
   }
   G[b * p.P + pol] = (float)g;
 }
 
 // Host plan; false when the model is outside the factored path.
-bool fact_plan(const EfeParams& p, FactParams* fp) {
+bool fact_plan(const EfeParams& p, FactParams* fp, bool with_wA = false, bool with_hterm = false) {
   std::memset(fp, 0, sizeof(*fp));
   if (p.T < 1 || p.T > kFactMaxT) return false;
   int64_t nu = 1, P = 1;
@@ -460,6 +541,14 @@ bool fact_plan(const EfeParams& p, FactParams* fp) {
       off += (int64_t)h * p.S[f];
     }
   fp->qh_stride = (off + 63) / 64 * 64;
+  fp->hterm = with_hterm ? 1 : 0;
+  int64_t hoff = 0;
+  for (int f = 0; f < p.F; ++f)
+    for (int t = 0; t < p.T; ++t) {
+      fp->ht_off[f][t] = hoff;
+      hoff += ipow(p.U[f], t + 1);
+    }
+  fp->ht_stride = with_hterm ? (hoff + 31) / 32 * 32 : 0;
   // groups: modalities sharing one dependency tuple
   std::vector<std::vector<int>> tuples, members;
   for (int m = 0; m < p.M; ++m) {
@@ -492,6 +581,8 @@ bool fact_plan(const EfeParams& p, FactParams* fp) {
     }
     int n_obs = 0;
     for (int m : members[g]) n_obs += p.mod[m].O;
+    const int n_w = with_wA ? n_obs : 0;
+    const int nrow = n_obs + n_w + 1;
     // contraction order: the cheapest permutation (summed over depths)
     std::vector<int> perm(r);
     for (int i = 0; i < r; ++i) perm[i] = i;
@@ -504,12 +595,12 @@ bool fact_plan(const EfeParams& p, FactParams* fp) {
         for (int i = 0; i < r; ++i) {
           const int f = tup[perm[i]];
           combos *= std::pow((double)p.U[f], t + 1);
-          cost += combos * (n_obs + 1) * rest;  // level i + 1: combos x rows x remaining size (incl. own axis)
+          cost += combos * nrow * rest;  // level i + 1: combos x rows x remaining size (incl. own axis)
           rest /= p.S[f];
         }
       }
       // level-1 intermediates live in global memory: prefer few level-1 histories
-      cost += 4.0 * std::pow((double)p.U[tup[perm[0]]], p.T) * (n_obs + 1) * (double)s_ / p.S[tup[perm[0]]];
+      cost += 4.0 * std::pow((double)p.U[tup[perm[0]]], p.T) * nrow * (double)s_ / p.S[tup[perm[0]]];
       if (best.empty() || cost < best_cost) {
         best = perm;
         best_cost = cost;
@@ -536,18 +627,19 @@ bool fact_plan(const EfeParams& p, FactParams* fp) {
     gr.vec4 = v4 ? 1 : 0;
     // the tail's shared memory: kFactH1Tile level-2 blocks (rank 3) or the V1 block (rank 2)
     const int last = r == 3 ? gr.S[2] : (r == 2 ? gr.S[1] : 1);
-    const int64_t tail_words = (r == 3 ? (int64_t)kFactH1Tile * (n_obs + 1) * (last + 1) + kFactH1Tile * kFactMaxS
-                                       : (int64_t)(n_obs + 1) * (last + 1));
+    const int64_t tail_words = (r == 3 ? (int64_t)kFactH1Tile * nrow * (last + 1) + kFactH1Tile * kFactMaxS
+                                       : (int64_t)nrow * (last + 1));
     if (tail_words * 4 > kFactTailSmem) return false;
     max_R = gr.R > max_R ? gr.R : max_R;
     gr.n_obs = n_obs;
+    gr.n_w = n_w;
     gr.m_begin = n_order;
     for (int m : members[g]) fp->mod_order[n_order++] = (int8_t)m;
     gr.m_end = n_order;
     for (int t = 0; t < p.T; ++t) {
       for (int i = 0; i < kFactMaxRank; ++i) gr.H[i][t] = i < r ? ipow(p.U[gr.f[i]], t + 1) : 1;
       gr.v1_off[t] = v1;
-      v1 += (int64_t)gr.H[0][t] * (n_obs + 1) * gr.R;
+      v1 += (int64_t)gr.H[0][t] * nrow * gr.R;
       gr.tab_off[t] = tab;
       tab += (int64_t)gr.H[0][t] * gr.H[1][t] * gr.H[2][t];
     }
@@ -566,8 +658,9 @@ bool fact_plan(const EfeParams& p, FactParams* fp) {
   for (int g = 0; g < fp->G; ++g) {
     const FactGroup& gr = fp->grp[g];
     const int last = gr.rank == 3 ? gr.S[2] : (gr.rank == 2 ? gr.S[1] : 1);
-    const int64_t w = gr.rank == 3 ? (int64_t)kFactH1Tile * (gr.n_obs + 1) * (last + 1) + kFactH1Tile * kFactMaxS
-                                   : (int64_t)(gr.n_obs + 1) * (last + 1);
+    const int nr = gr.n_obs + gr.n_w + 1;
+    const int64_t w = gr.rank == 3 ? (int64_t)kFactH1Tile * nr * (last + 1) + kFactH1Tile * kFactMaxS
+                                   : (int64_t)nr * (last + 1);
     tsm = w > tsm ? w : tsm;
   }
   fp->tail_smem = (int32_t)(tsm * 4);
@@ -590,24 +683,28 @@ bool efe_fact_applies(const EfeParams& p, int64_t Bn) {
 }
 
 int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const float* A, const float* B,
-                        const float* C, float* G, cudaStream_t stream, bool* used) {
+                        const float* C, float* G, cudaStream_t stream, bool* used, const float* wA,
+                        const float* wB, const float* wI) {
   *used = false;
   FactParams fp;
-  if (Bn > 65535 || !fact_plan(p, &fp)) return B2_OK;
+  const bool hterm = wB != nullptr || wI != nullptr;
+  if (Bn > 65535 || !fact_plan(p, &fp, wA != nullptr, hterm)) return B2_OK;
   const size_t qh_bytes = (size_t)Bn * fp.qh_stride * sizeof(float);
   const size_t v1_bytes = (size_t)Bn * fp.v1_stride * sizeof(float);
   const size_t tab_bytes = (size_t)Bn * fp.tab_stride * sizeof(double);
+  const size_t ht_bytes = (size_t)Bn * fp.ht_stride * sizeof(double);
   if (v1_bytes > ((size_t)8 << 30)) return B2_OK;  // level-1 intermediates above 8 GB: take another path
   uint8_t* ws = nullptr;
-  B2_TRY(ws_alloc((void**)&ws, tab_bytes + qh_bytes + v1_bytes, stream, kEfeName));
+  B2_TRY(ws_alloc((void**)&ws, tab_bytes + ht_bytes + qh_bytes + v1_bytes, stream, kEfeName));
   double* tab = reinterpret_cast<double*>(ws);
-  float* Qh = reinterpret_cast<float*>(ws + tab_bytes);
-  float* V1 = reinterpret_cast<float*>(ws + tab_bytes + qh_bytes);
-  efe_fact_hist_kernel<<<(unsigned)Bn, 256, 0, stream>>>(p, fp, qs, B, Qh);
+  double* Ht = hterm ? reinterpret_cast<double*>(ws + tab_bytes) : nullptr;
+  float* Qh = reinterpret_cast<float*>(ws + tab_bytes + ht_bytes);
+  float* V1 = reinterpret_cast<float*>(ws + tab_bytes + ht_bytes + qh_bytes);
+  efe_fact_hist_kernel<<<(unsigned)Bn, 256, 0, stream>>>(p, fp, qs, B, Qh, wB, wI, Ht);
   int32_t rc = check_launch("efe_ffi factored histories");
   if (rc == B2_OK) {
     dim3 grid((unsigned)((fp.max_R + 127) / 128), (unsigned)fp.G, (unsigned)Bn);
-    efe_fact_l1_kernel<<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1);
+    efe_fact_l1_kernel<<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
     rc = check_launch("efe_ffi factored level 1");
   }
   if (rc == B2_OK) {
@@ -631,7 +728,8 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
     }
   }
   if (rc == B2_OK) {
-    efe_fact_combine_kernel<<<dim3((unsigned)((p.P + 255) / 256), (unsigned)Bn), 256, 0, stream>>>(p, fp, tab, G);
+    efe_fact_combine_kernel<<<dim3((unsigned)((p.P + 255) / 256), (unsigned)Bn), 256, 0, stream>>>(p, fp, tab, Ht,
+                                                                                                  G);
     rc = check_launch("efe_ffi factored combine");
   }
   cudaError_t fe = cudaFreeAsync(ws, stream);

@@ -113,18 +113,23 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-// softmax(logq) of n values by one warp, in FP64 throughout.
-template <typename OutT>
+// softmax(logq) of n values by one warp: max, shift and sum in FP64; the
+// exponential of the shifted value in FP64, or (F32EXP) in FP32 (expf, within
+// 2 ulp): the argument is reduced in FP64 first, so the posteriors move by
+// at most a few 1e-7 relative (checked against the FP64 oracle on every FPI
+// fixture), while log q itself stays FP64.
+template <bool F32EXP = false, typename OutT>
 __device__ __forceinline__ void softmax_warp(const double* __restrict__ logq, OutT* __restrict__ out, int n,
                                              int lane) {
   double mx = -INFINITY;
   for (int i = lane; i < n; i += 32) mx = fmax(mx, logq[i]);
   mx = warp_max_d(mx);
+  auto ex = [&](double x) { return F32EXP ? (double)expf((float)(x - mx)) : exp(x - mx); };
   double sum = 0.0;
-  for (int i = lane; i < n; i += 32) sum += exp(logq[i] - mx);
+  for (int i = lane; i < n; i += 32) sum += ex(logq[i]);
   sum = warp_sum_d(sum);
   const double inv = 1.0 / sum;
-  for (int i = lane; i < n; i += 32) out[i] = (OutT)(exp(logq[i] - mx) * inv);
+  for (int i = lane; i < n; i += 32) out[i] = (OutT)(ex(logq[i]) * inv);
 }
 
 // rank >= 4: mixed-radix counter over the other axes (innermost last).
@@ -270,7 +275,7 @@ __global__ void __launch_bounds__(TEAM * APC)
         const int m = p.src_order[si];
         if (!((obs_ok >> m) & 1u)) continue;
         const float a = __ldg(io.src + rowoff[m] + k);
-        v += FUSED ? log((double)fmaxf(a, kMinVal)) : (double)a;
+        v += FUSED ? (double)logf(fmaxf(a, kMinVal)) : (double)a;
       }
       int rem = k, addr = 0;
       for (int x = gr.rank - 1; x > 0; --x) {
@@ -285,14 +290,14 @@ __global__ void __launch_bounds__(TEAM * APC)
   }
   for (int i = t; i < p.S_tot; i += TEAM) {
     const float v = __ldg(io.prior + b * p.S_tot + i);
-    lp[i] = FUSED ? log((double)fmaxf(v, kMinVal)) : (double)v;
+    lp[i] = FUSED ? (double)logf(fmaxf(v, kMinVal)) : (double)v;
     logq[i] = 0.0;
   }
   team_sync<TEAM>();
 
   // ---- fixed-point iterations (Jacobi: every factor uses the previous q)
   for (int it = 0; it < p.num_iter; ++it) {
-    for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp(logq + p.lp_off[f], q + p.lp_off[f], p.S[f], lane);
+    for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp<true>(logq + p.lp_off[f], q + p.lp_off[f], p.S[f], lane);
     team_sync<TEAM>();
     for (int f = 0; f < p.F; ++f) {
       const int Sf = p.S[f];
@@ -316,7 +321,7 @@ __global__ void __launch_bounds__(TEAM * APC)
 
   // ---- posterior marginals
   float* out = io.q_out + b * p.S_tot;
-  for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp(logq + p.lp_off[f], out + p.lp_off[f], p.S[f], lane);
+  for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp<true>(logq + p.lp_off[f], out + p.lp_off[f], p.S[f], lane);
 }
 
 // --------------------------------------------------------------- host side
@@ -624,7 +629,7 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
     double v = 0.0;
     if (s < p.S[f]) {
       const float x = __ldg(io.prior + b * p.S_tot + p.lp_off[f] + s);
-      v = FUSED ? log((double)fmaxf(x, kMinVal)) : (double)x;
+      v = FUSED ? (double)logf(fmaxf(x, kMinVal)) : (double)x;
     }
     lpp[i] = v;
     logq[i] = 0.0;  // log q starts at 0 (pymdp/algos.py:121-133)
@@ -684,8 +689,8 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
           const float a1[4] = {va[x][1].x, va[x][1].y, va[x][1].z, va[x][1].w};
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
-            double v = FUSED ? log((double)fmaxf(a0[e], kMinVal)) : (double)a0[e];
-            if (two) v += FUSED ? log((double)fmaxf(a1[e], kMinVal)) : (double)a1[e];
+            double v = FUSED ? (double)logf(fmaxf(a0[e], kMinVal)) : (double)a0[e];
+            if (two) v += FUSED ? (double)logf(fmaxf(a1[e], kMinVal)) : (double)a1[e];
             store(gi[x], 4 * ki[x] + e, v);
           }
         }
@@ -700,7 +705,7 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
           const int m = p.src_order[si];
           if (!((obs_ok >> m) & 1u)) continue;
           const float a = __ldg(io.src + rowoff[m] + k);
-          v += FUSED ? log((double)fmaxf(a, kMinVal)) : (double)a;
+          v += FUSED ? (double)logf(fmaxf(a, kMinVal)) : (double)a;
         }
         store(g, k, v);
       }
@@ -727,7 +732,7 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
       double mx = x;
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      const double e = valid ? exp(x - mx) : 0.0;
+      const double e = valid ? (double)expf((float)(x - mx)) : 0.0;
       double sum = e;
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);

@@ -517,3 +517,66 @@ def test_factored_neg_efe_matches_reference(name):
     np.testing.assert_allclose(G.cpu().numpy(), d["G"], rtol=G_RTOL, atol=G_ATOL)
     np.testing.assert_allclose(q_pi.cpu().numpy(), d["q_pi"], rtol=Q_RTOL, atol=Q_ATOL)
     np.testing.assert_array_equal(act.cpu().numpy(), d["action"])
+
+
+@pytest.mark.parametrize("name", ["efe_pigA", "efe_ind", "efe_all"])
+def test_factored_flag_gated_terms_match_reference(name):
+    """Parameter information gain (pA rows carried through the factored
+    contraction, pB per factor history) and the inductive value on the
+    factored path, against the reference's update_posterior_policies_inductive
+    fixtures (factor-local transitions)."""
+    from pymdp_b200 import _lib, ffi
+    d = load_golden(name)
+    A_deps = deps_from(d["A_dep_flat"], d["A_dep_offsets"])
+    B_deps = deps_from(d["B_dep_flat"], d["B_dep_offsets"])
+    assert all(b == [f] for f, b in enumerate(B_deps))
+    qs = [cuda(q) for q in unpack(d, "qs")]
+    pA = [cuda(a) for a in unpack(d, "pA")] if int(d["has_pA"]) else None
+    pB = [cuda(b) for b in unpack(d, "pB")] if int(d["has_pB"]) else None
+    n0 = _lib.launch_count()
+    G = ffi.neg_efe_all_policies_ffi(d["policies"], qs, [cuda(a) for a in unpack(d, "A")],
+                                     [cuda(b) for b in unpack(d, "B")], [cuda(c) for c in unpack(d, "C")],
+                                     [cuda(i) for i in unpack(d, "I")], A_deps, B_deps, pA=pA, pB=pB,
+                                     use_param_info_gain=bool(int(d["use_param_info_gain"])),
+                                     use_inductive=bool(int(d["use_inductive"])),
+                                     inductive_epsilon=float(d["eps"]), policy_tree=True, factored=True)
+    launches = _lib.launch_count() - n0
+    q_pi = ffi.policy_posterior(G, cuda(d["E"]), float(d["gamma"]))
+    act = ffi.select_action(q_pi, d["policies"])
+    weights = int(pA is not None) + int(pB is not None) + int(bool(int(d["use_inductive"])))
+    assert launches == 4 + weights  # the weight kernels, then the factored path's four
+    np.testing.assert_allclose(G.cpu().numpy(), d["G"], rtol=G_RTOL, atol=G_ATOL)
+    np.testing.assert_allclose(q_pi.cpu().numpy(), d["q_pi"], rtol=Q_RTOL, atol=Q_ATOL)
+    np.testing.assert_array_equal(act.cpu().numpy(), d["action"])
+
+
+@pytest.mark.parametrize("terms", ["pA", "pB", "pApB", "ind", "all"])
+def test_factored_flag_gated_terms_random_models_match_oracle(terms):
+    from pymdp_b200 import ffi
+    S, O, U, T = [4, 3, 2], [5, 3, 2], [3, 2, 2], 2
+    A_deps, B_deps = [[0, 2], [1, 0], [2, 1, 0]], [[0], [1], [2]]
+    rng = np.random.default_rng(len(terms) + 61)
+    batch = 3
+    A, B, C, qs = random_efe(rng, S, O, U, T, A_deps, B_deps, batch)
+    counts = lambda shape: (rng.gamma(1.5, size=shape) * 2 * (rng.random(size=shape) > 0.1)).astype(np.float32)
+    pA = [counts(a.shape) for a in A] if "pA" in terms or terms == "all" else None
+    pB = [counts(b.shape) for b in B] if "pB" in terms or terms == "all" else None
+    use_ind = terms in ("ind", "all")
+    I = [(rng.random(size=(batch, 3, s)) > 0.5).astype(np.float32) for s in S]
+    eps = np.array([1e-3, 1e-2, 0.2], np.float32)
+    pol = oefe.construct_policies(S, U, T)
+    G = ffi.neg_efe_all_policies_ffi(pol, [cuda(q) for q in qs], [cuda(a) for a in A], [cuda(b) for b in B],
+                                     [cuda(c) for c in C], [cuda(i) for i in I], A_deps, B_deps,
+                                     pA=[cuda(x) for x in pA] if pA else None,
+                                     pB=[cuda(x) for x in pB] if pB else None,
+                                     use_param_info_gain=pA is not None or pB is not None, use_inductive=use_ind,
+                                     inductive_epsilon=cuda(eps), policy_tree=True, factored=True).cpu().numpy()
+    for b in range(batch):
+        ref = oefe.neg_efe_all_policies(pol, [q[b] for q in qs], [a[b] for a in A], [x[b] for x in B],
+                                        [c[b] for c in C], A_deps, B_deps,
+                                        pA=[x[b] for x in pA] if pA else None,
+                                        pB=[x[b] for x in pB] if pB else None,
+                                        use_param_info_gain=pA is not None or pB is not None,
+                                        I=[i[b] for i in I], use_inductive=use_ind,
+                                        inductive_epsilon=float(eps[b]))
+        np.testing.assert_allclose(G[b], ref, rtol=G_RTOL, atol=G_ATOL * max(1.0, np.abs(ref).max()))
