@@ -12,16 +12,21 @@ infer_policies (neg-EFE of all policies + q_pi) -> sample_action
 (deterministic). Synthetic seeded inputs with those shapes/distributions.
 
 * ``value``: device time (CUDA events, max over ranks) with every input
-  resident in HBM; L2 is flushed (a 256 MiB write) between timed steps,
-  outside the per-step event pairs.
-* ``e2e``: the same step through the public ``Agent`` API with host
-  buffers: pinned observations + priors copied in, actions copied out,
-  inside the timed region.
-* ``roofline``: the dominant kernel (neg-EFE), its algorithmic FLOPs
-  2*T*P*sum_m(O_m*K_m) per agent over its measured launch time.
-* ``cpu_baseline``: the FP64 oracle on all host cores (one spawned worker
-  process per core) for a bounded sample of the same agents; the same sample
+  resident in HBM, the step replayed as CUDA graphs (belief update, then
+  policies + action; ``Agent.capture_step``); L2 is flushed (a 256 MiB
+  write) between timed steps, outside the per-step event pairs.
+* ``e2e``: the same step through the public API
+  (``Agent.capture_step().step``) with host buffers: pinned observations +
+  priors copied in, actions copied out, inside the timed region.
+* ``roofline``: the dominant launch (the factored neg-EFE + q_pi), its
+  algorithmic HBM bytes per agent over its event-timed duration inside the
+  timed steps (tensor-pipe FLOPs for ``--efe dense``).
+* ``cpu_baseline``: the reference's own CPU kernels (NegEfeCpu + FpiCpu,
+  compiled from its sources into ``oracle/_ref``) on the host cores for a
+  bounded sample of the same agents; the FP64 oracle on another sample
   gives ``error_vs_fp64``, the GPU outputs' max error against FP64.
+* ``--impl reference``: the same reference CPU step alone, as the
+  reference arm.
 
 Multi-GPU: agents are independent, so each rank runs its own 256 agents
 (weak scaling, no data-path collective); the only collective is the
@@ -828,17 +833,10 @@ def run_b200(args, rank, world, local_rank):
     seq_res = run_seq_config(dev, args.steps, args.warmup, flush) if extras else None
     c1_res = run_config1(dev, args.steps, args.warmup) if world == 1 and not main_only else None
     plain_res = run_plain_config(dev, model, min(args.steps, 3), 1, flush) if world == 1 and not main_only else None
-    efe_ev = []
 
-    def step(timed_efe=False):
+    def step():
         qs = agent.infer_states(obs_d, prior_d)
-        if timed_efe:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
         q_pi, G = agent.infer_policies(qs)
-        if timed_efe:
-            e1.record(stream)
-            efe_ev.append((e0, e1))
         return agent.sample_action(q_pi)
 
     def barrier():
@@ -856,32 +854,54 @@ def run_b200(args, rank, world, local_rank):
     chk = ([q[:, -1].cpu().numpy() for q in qs_chk], G_chk.cpu().numpy(), q_pi_chk.cpu().numpy(),
            act_chk.cpu().numpy())
     barrier()
-    evs = []
+    # eager steps (one Python call per kernel), for the record
     n0 = _lib.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    barrier()
+    per_step_launches = (_lib.launch_count() - n0) // args.steps
+    eager_ms = ev0.elapsed_time(ev1) / args.steps
+    # the timed step: the agent step captured as CUDA graphs (belief update |
+    # policies + action) and replayed, inputs resident; events between the two
+    # graphs time the neg-EFE launch for the roofline
+    gstep = agent.capture_step(warmup=args.warmup, split=True)
+    gstep.obs.copy_(obs_d)
+    gstep.prior.copy_(torch.cat([p.reshape(n_agents, -1) for p in prior_d], dim=1))
+    g_states, g_policies = gstep.graphs
+    for _ in range(args.warmup):
+        gstep.step()
+    barrier()
+    graph_same = int((gstep.action.cpu().numpy() == chk[3]).all(axis=1).sum())
+    evs, efe_ev = [], []
     with ClockSampler(local_rank) as clocks:
         barrier()
         for _ in range(args.steps):
             flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             e0.record(stream)
-            step(timed_efe=True)
+            g_states.replay()
+            em.record(stream)
+            g_policies.replay()
             e1.record(stream)
             evs.append((e0, e1))
+            efe_ev.append((em, e1))
         barrier()
-    launches = _lib.launch_count() - n0
+    launches = args.steps * per_step_launches
     ms = sum(a.elapsed_time(b) for a, b in evs)
     efe_ms = sum(a.elapsed_time(b) for a, b in efe_ev) / len(efe_ev)
-    # e2e through the public API with host buffers
+    # e2e through the public API (Agent.capture_step -> GraphedAgentStep.step)
+    # with host buffers: pinned observations and prior in, the action out
+    estep = agent.capture_step(warmup=1)
     obs_h = torch.as_tensor(obs).pin_memory()
-    prior_h = [torch.as_tensor(d).pin_memory() for d in D]
+    prior_h = torch.cat([torch.as_tensor(d).reshape(n_agents, -1) for d in D], dim=1).pin_memory()
     act_h = torch.empty((n_agents, len(S)), dtype=torch.int32).pin_memory()
 
     def e2e_step():
-        o = obs_h.to(dev, non_blocking=True)
-        p = [x.to(dev, non_blocking=True) for x in prior_h]
-        qs = agent.infer_states(o, p)
-        q_pi, _ = agent.infer_policies(qs)
-        act_h.copy_(agent.sample_action(q_pi), non_blocking=True)
+        _, _, _, act = estep.step(obs_h, prior_h)
+        act_h.copy_(act, non_blocking=True)
 
     for _ in range(args.warmup):
         e2e_step()
@@ -893,7 +913,8 @@ def run_b200(args, rank, world, local_rank):
     ev1.record(stream)
     barrier()
     e2e_ms = ev0.elapsed_time(ev1)
-    h2d = obs_h.numel() * 4 + sum(x.numel() * 4 for x in prior_h)
+    e2e_same = int((act_h.numpy() == chk[3]).all(axis=1).sum())
+    h2d = obs_h.numel() * 4 + prior_h.numel() * 4
     d2h = act_h.numel() * 4
     ms, e2e_ms, efe_ms = reduce_max_over_ranks([ms, e2e_ms, efe_ms], world, dev)
     if rank != 0:
@@ -964,6 +985,9 @@ def run_b200(args, rank, world, local_rank):
         "e2e": {"value": total_agents * args.steps / (e2e_ms * 1e-3), "unit": "agent-steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
+        "step_form": {"timed": "CUDA graph replay (belief update | policies + action)",
+                      "kernels_per_step": per_step_launches, "eager_ms_per_step": eager_ms,
+                      "graph_actions_equal_eager": graph_same, "e2e_actions_equal_eager": e2e_same},
         "fused_over_plain": fused_over_plain,
         "plain": plain_res,
         "config1": c1_res,

@@ -228,23 +228,31 @@ class Agent:
         prior_flat, _ = ffi.flatten_ragged_f32(
             [torch.broadcast_to(_t(p, dev), (self.batch_size, self.num_states[f]))
              for f, p in enumerate(empirical_prior)], 1, dev)
-        q = ffi.fpi_obs_flat(self._A_flat, int(self._A_offsets[-1]), self._A_offsets, self.num_obs, obs,
-                             prior_flat, self.num_states, self.A_dependencies, self.num_iter)
+        q = self._fpi_flat(obs, prior_flat)
         o = self._qs_offsets
         return [q[:, o[f]:o[f + 1]].unsqueeze(1) for f in range(self.num_factors)]
 
-    def infer_policies(self, qs: Sequence[torch.Tensor]):
-        """``pymdp/agent.py:853-906``: returns ``(q_pi, neg_efe)``, each ``(batch, P)``."""
-        latest = [q[:, -1] if q.ndim == 3 else q for q in qs]
-        qs_flat, _ = ffi.flatten_ragged_f32(latest, 1, self.device)
+    def _fpi_flat(self, obs: torch.Tensor, prior_flat: torch.Tensor, out=None) -> torch.Tensor:
+        """Fused FPI on flat ``(batch, M)`` int32 observations and a flat
+        ``(batch, sum S)`` prior: the flat posterior ``(batch, sum S)``."""
+        return ffi.fpi_obs_flat(self._A_flat, int(self._A_offsets[-1]), self._A_offsets, self.num_obs, obs,
+                                prior_flat, self.num_states, self.A_dependencies, self.num_iter, out=out)
+
+    def _policies_flat(self, qs_flat: torch.Tensor):
+        """neg-EFE of every policy and q_pi from the flat ``(batch, sum S)`` posterior."""
         P = self.policies.shape[0]
         G = torch.empty((self.batch_size, P), device=self.device)
         pig = self.use_param_info_gain
         self._layout.call(None, self.policies, 0, qs_flat, self._A_flat, self._B_flat, self._C_flat,
                           self._I_flat, self._pA_flat if pig else None, self._pB_flat if pig else None, self._eps, G,
                           self.batch_size, P, self._flags, cache=self._pack_cache(P))
-        q_pi = ffi.policy_posterior(G, self.E, self.gamma)
-        return q_pi, G
+        return ffi.policy_posterior(G, self.E, self.gamma), G
+
+    def infer_policies(self, qs: Sequence[torch.Tensor]):
+        """``pymdp/agent.py:853-906``: returns ``(q_pi, neg_efe)``, each ``(batch, P)``."""
+        latest = [q[:, -1] if q.ndim == 3 else q for q in qs]
+        qs_flat, _ = ffi.flatten_ragged_f32(latest, 1, self.device)
+        return self._policies_flat(qs_flat)
 
     def sample_action(self, q_pi: torch.Tensor, rng_key=None) -> torch.Tensor:
         """``pymdp/agent.py:939-967``: ``(batch, F)`` int32 actions by this
@@ -255,6 +263,13 @@ class Agent:
             return ffi.select_action(q_pi, self.policies)
         return ffi.sample_action(q_pi, self.policies, self.num_controls, self.sampling_mode, self.action_selection,
                                  self.alpha, rng_key)
+
+    def capture_step(self, warmup: int = 2, split: bool = False) -> "GraphedAgentStep":
+        """The agent step ``infer_states`` -> ``infer_policies`` ->
+        ``sample_action`` as one CUDA graph over static buffers
+        (``GraphedAgentStep``): a replay is one host call for the whole step
+        (two with ``split``: the belief update, then policies and action)."""
+        return GraphedAgentStep(self, warmup, split)
 
     def update_empirical_prior(self, action, qs: Sequence[torch.Tensor]):
         """``pymdp/agent.py:825-851`` for ``inference_algo="fpi"``: the prior of
@@ -376,3 +391,89 @@ class Agent:
             raise NotImplementedError("the learned B changed the inductive depth of I")
         self.I = I
         self._I_flat, _ = ffi.flatten_ragged_f32(I, 1, self.device)
+
+
+class GraphedAgentStep:
+    """One agent step of ``agent`` — fused FPI, neg-EFE of every policy, q_pi
+    and the action — captured once in a CUDA graph and replayed.
+
+    The graph reads two static input buffers, ``obs`` (``(batch, M)`` int32)
+    and ``prior`` (``(batch, sum S)`` float32, factor-major like the flat
+    posterior), and writes four static outputs, ``qs`` (per-factor views of
+    ``(batch, 1, S_f)``), ``q_pi``, ``G`` (``(batch, P)``) and ``action``
+    (``(batch, F)`` int32). ``step`` copies new inputs into the buffers (on
+    the current stream), replays the graph and returns the outputs, which
+    the next replay overwrites. The model buffers (A, B, C, ...) are read in
+    place, so in-place learning between replays is seen by the next one.
+    Deterministic action selection only: a stochastic draw would replay the
+    key it was captured with. ``split=True`` captures two graphs, the belief
+    update and then policies + action (``graphs``), so that a caller can
+    time or interleave them; ``step`` replays both.
+    """
+
+    def __init__(self, agent: Agent, warmup: int = 2, split: bool = False):
+        if agent.action_selection != "deterministic":
+            raise ValueError("capture_step needs action_selection='deterministic' (a replay reuses its captured key)")
+        dev = agent.device
+        self.agent = agent
+        B, S = agent.batch_size, agent.num_states
+        self.obs = torch.zeros((B, agent.num_modalities), dtype=torch.int32, device=dev)
+        self.prior = torch.cat([torch.full((B, s), 1.0 / s, device=dev) for s in S], dim=1).contiguous()
+        self._post = torch.empty_like(self.prior)
+        self.stream = torch.cuda.Stream(dev)
+
+        def states():
+            agent._fpi_flat(self.obs, self.prior, out=self._post)
+
+        def policies():
+            q_pi, G = agent._policies_flat(self._post)
+            return q_pi, G, agent.sample_action(q_pi)
+
+        self.stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(self.stream):
+            for _ in range(max(int(warmup), 1)):  # first calls build the per-model caches outside the capture
+                states()
+                policies()
+        self.stream.synchronize()
+        if split:
+            g_states, g_policies = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g_states, stream=self.stream):
+                states()
+            with torch.cuda.graph(g_policies, stream=self.stream):
+                self.q_pi, self.G, self.action = policies()
+            self.graphs = (g_states, g_policies)
+        else:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=self.stream):
+                states()
+                self.q_pi, self.G, self.action = policies()
+            self.graphs = (g,)
+        o = agent._qs_offsets
+        self.qs = [self._post[:, o[f]:o[f + 1]].unsqueeze(1) for f in range(agent.num_factors)]
+
+    def step(self, observations=None, empirical_prior=None):
+        """Replay the step; returns ``(qs, q_pi, G, action)`` (static buffers).
+
+        ``observations``: ``(batch, M)`` indices or a list of M ``(batch,)``
+        arrays; ``empirical_prior``: a list of F ``(batch, S_f)`` arrays or
+        one flat ``(batch, sum S)`` tensor. Omitted inputs keep the buffers'
+        contents."""
+        # tensors (host or device) are copied straight into the buffers, on the
+        # current stream; a pinned host tensor makes that an asynchronous copy
+        if observations is not None:
+            if isinstance(observations, (list, tuple)):
+                obs = torch.stack([torch.as_tensor(x).reshape(-1) for x in observations], dim=-1)
+            else:
+                obs = torch.as_tensor(observations)
+            self.obs.copy_(obs.reshape(self.obs.shape), non_blocking=True)
+        if empirical_prior is not None:
+            if isinstance(empirical_prior, (list, tuple)):
+                o = self.agent._qs_offsets
+                for f, p in enumerate(empirical_prior):
+                    self.prior[:, o[f]:o[f + 1]].copy_(torch.as_tensor(p).reshape(-1, o[f + 1] - o[f]),
+                                                       non_blocking=True)
+            else:
+                self.prior.copy_(torch.as_tensor(empirical_prior).reshape(self.prior.shape), non_blocking=True)
+        for g in self.graphs:
+            g.replay()
+        return self.qs, self.q_pi, self.G, self.action

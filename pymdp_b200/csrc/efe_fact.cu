@@ -78,6 +78,9 @@ struct FactParams {
   int32_t max_R, max_tiles;
   int32_t smax;                             // largest size among the factors the tail contracts
   int32_t tail_smem;                        // dynamic shared memory of the tail kernel (bytes)
+  int32_t hist_smem;                        // dynamic shared memory of the history kernel (bytes; 0: global path)
+  int32_t bt_off[kEfeMaxF], bt_plane[kEfeMaxF];  // staged B_f^T: plane u at bt_off + u * bt_plane, [k][s]
+  int32_t qi_sm, qh_sm, qh_words;           // staged qs_init and histories (float offsets); histories per agent
   int8_t mod_order[B2_MAX_MODALITIES];
   FactGroup grp[kFactMaxG];
 };
@@ -101,23 +104,63 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
                                                             const float* __restrict__ B, float* __restrict__ Qh,
                                                             const float* __restrict__ wB,
                                                             const float* __restrict__ wI, double* __restrict__ Ht) {
+  extern __shared__ float hsm[];
   const int64_t b = blockIdx.x;
   float* Qb = Qh + b * fp.qh_stride;
   const float* Bb = B + b * p.B_stride;
+  const float* qi = qs_init + b * p.S_tot;
+  const bool staged = fp.hist_smem > 0;  // uniform over the grid
+  if (staged) {
+    // B_f transposed to [u][k][s] (planes padded so that the half-warps of
+    // small factors fall on different banks) and qs_init, in shared memory
+    for (int f = 0; f < p.F; ++f) {
+      const int S = p.S[f], U = p.U[f], n = S * S * U;
+      const float* src = Bb + p.fac[f].B_off;
+      float* dst = hsm + fp.bt_off[f];
+#pragma unroll 4
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int s = i / (S * U), rem = i - s * S * U, k = rem / U, u = rem - k * U;
+        dst[u * fp.bt_plane[f] + k * S + s] = __ldg(src + i);
+      }
+    }
+    for (int i = threadIdx.x; i < p.S_tot; i += blockDim.x) hsm[fp.qi_sm + i] = __ldg(qi + i);
+    __syncthreads();
+  }
+  float* Qw = staged ? hsm + fp.qh_sm : Qb;  // where this CTA writes (and reads back) the histories
+  const float* q0 = staged ? hsm + fp.qi_sm : qi;
   for (int t = 0; t < p.T; ++t) {
     for (int f = 0; f < p.F; ++f) {
       const int S = p.S[f], U = p.U[f];
       const int H = ipow(U, t + 1);
-      const EfeFactor& fb = p.fac[f];
-      float* out = Qb + fp.qh_off[f][t];
-      for (int e = threadIdx.x; e < H * S; e += blockDim.x) {
-        const int h = e / S, s = e - h * S;
-        const int u = h % U;
-        const float* q = t == 0 ? qs_init + b * p.S_tot + p.qs_off[f] : Qb + fp.qh_off[f][t - 1] + (int64_t)(h / U) * S;
-        const float* Bs = Bb + fb.B_off + (int64_t)s * S * U + u;
-        float acc = 0.f;
-        for (int k = 0; k < S; ++k) acc = fmaf(__ldg(Bs + (int64_t)k * U), q[k], acc);
-        out[e] = acc;
+      float* out = Qw + fp.qh_off[f][t];
+      if (staged) {
+        for (int e = threadIdx.x; e < H * S; e += blockDim.x) {
+          const int h = e / S, s = e - h * S;
+          const int u = h % U;
+          const float* q = t == 0 ? q0 + p.qs_off[f] : Qw + fp.qh_off[f][t - 1] + (h / U) * S;
+          const float* Bt = hsm + fp.bt_off[f] + u * fp.bt_plane[f] + s;
+          float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+          int k = 0;
+          for (; k + 4 <= S; k += 4) {
+            a0 = fmaf(Bt[k * S], q[k], a0);
+            a1 = fmaf(Bt[(k + 1) * S], q[k + 1], a1);
+            a2 = fmaf(Bt[(k + 2) * S], q[k + 2], a2);
+            a3 = fmaf(Bt[(k + 3) * S], q[k + 3], a3);
+          }
+          for (; k < S; ++k) a0 = fmaf(Bt[k * S], q[k], a0);
+          out[e] = (a0 + a1) + (a2 + a3);
+        }
+      } else {
+        const EfeFactor& fb = p.fac[f];
+        for (int e = threadIdx.x; e < H * S; e += blockDim.x) {
+          const int h = e / S, s = e - h * S;
+          const int u = h % U;
+          const float* q = t == 0 ? qi + p.qs_off[f] : Qb + fp.qh_off[f][t - 1] + (int64_t)(h / U) * S;
+          const float* Bs = Bb + fb.B_off + (int64_t)s * S * U + u;
+          float acc = 0.f;
+          for (int k = 0; k < S; ++k) acc = fmaf(__ldg(Bs + (int64_t)k * U), q[k], acc);
+          out[e] = acc;
+        }
       }
     }
     __syncthreads();
@@ -128,8 +171,8 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
         const int H = ipow(U, t + 1);
         for (int h = threadIdx.x; h < H; h += blockDim.x) {
           const int u = h % U;
-          const float* qn = Qb + fp.qh_off[f][t] + (int64_t)h * S;
-          const float* qp = t == 0 ? qs_init + b * p.S_tot + p.qs_off[f] : Qb + fp.qh_off[f][t - 1] + (int64_t)(h / U) * S;
+          const float* qn = Qw + fp.qh_off[f][t] + (int64_t)h * S;
+          const float* qp = t == 0 ? q0 + p.qs_off[f] : Qw + fp.qh_off[f][t - 1] + (int64_t)(h / U) * S;
           double v = 0.0;
           if (wB) {
             const float* Ws = wB + b * p.B_stride + p.fac[f].B_off + u;
@@ -146,20 +189,23 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
       }
     }
   }
+  if (staged)  // the last depth's barrier above orders every history write before this copy
+    for (int i = threadIdx.x; i < fp.qh_words; i += blockDim.x) Qb[i] = hsm[fp.qh_sm + i];
 }
 
 // Level 1: one thread per (group, rest index r = (s1, s2)). For each
 // observation row it streams the S0 entries A[row, s0, s1, s2] once and, for
-// up to kFactCombo (depth, h0) combinations at a time (their marginals staged
+// up to KC <= kFactCombo (depth, h0) combinations at a time (their marginals staged
 // in shared memory), writes V1[h0][row][r] = sum_s0 q_{f0}^{h0}[s0] A and
 // accumulates the depth's linear row sum_row [sum_s0 q xlogx(A)] + C_t[o] V1
 // (information gain, utility).
+template <int KC>
 __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant__ EfeParams p,
                                                           const __grid_constant__ FactParams fp,
                                                           const float* __restrict__ A, const float* __restrict__ C,
                                                           const float* __restrict__ Qh, float* __restrict__ V1,
                                                           const float* __restrict__ wA) {
-  __shared__ float qsm[kFactCombo * kFactMaxS];
+  __shared__ float qsm[KC * kFactMaxS];
   const int64_t b = blockIdx.z;
   const int g = blockIdx.y;
   if (g >= fp.G) return;  // uniform over the CTA
@@ -181,13 +227,13 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
   int ncomb = 0;
   for (int t = 0; t < p.T; ++t) ncomb += gr.H[0][t];
   int t0 = 0, h0 = 0;  // first combination of the current chunk
-  for (int c0 = 0; c0 < ncomb; c0 += kFactCombo) {
-    const int nc = ncomb - c0 < kFactCombo ? ncomb - c0 : kFactCombo;
-    int ct[kFactCombo], ch[kFactCombo];
+  for (int c0 = 0; c0 < ncomb; c0 += KC) {
+    const int nc = ncomb - c0 < KC ? ncomb - c0 : KC;
+    int ct[KC], ch[KC];
     {
       int t = t0, h = h0;
 #pragma unroll
-      for (int i = 0; i < kFactCombo; ++i) {
+      for (int i = 0; i < KC; ++i) {
         ct[i] = t;
         ch[i] = h;
         if (i < nc && ++h == gr.H[0][t] && t + 1 < p.T) {
@@ -211,29 +257,58 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
     }
     __syncthreads();
     if (!active) continue;
-    float lin[kFactCombo];
+    float lin[KC];
 #pragma unroll
-    for (int i = 0; i < kFactCombo; ++i) lin[i] = 0.f;
+    for (int i = 0; i < KC; ++i) lin[i] = 0.f;
     int row = 0;
     for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
       const EfeModality& md = p.mod[fp.mod_order[mi]];
       const float* Am = A + b * p.A_stride + md.A_off + base;
       const float* Cm = C + b * p.C_stride + md.C_off;
-      for (int o = 0; o < md.O; ++o, ++row) {
-        float v[kFactCombo], w[kFactCombo];
+      // short contiguous level-1 axis (<= 16 entries): the next row's loads are
+      // issued before this row's arithmetic, two rows in flight per thread
+      const bool pipe = gr.vec4 && S0 <= 16;
+      float4 nx[4];
+      if (pipe) {
+        const float4* A4 = reinterpret_cast<const float4*>(Am);
 #pragma unroll
-        for (int i = 0; i < kFactCombo; ++i) v[i] = w[i] = 0.f;
+        for (int j = 0; j < 4; ++j)
+          if (4 * j < S0) nx[j] = __ldg(A4 + j);
+      }
+      for (int o = 0; o < md.O; ++o, ++row) {
+        float v[KC], w[KC];
+#pragma unroll
+        for (int i = 0; i < KC; ++i) v[i] = w[i] = 0.f;
         const float* Ar = Am + (int64_t)o * md.K;
         auto take = [&](float a, int s) {
           const float xl = ig ? a * log_stable(a) : 0.f;
 #pragma unroll
-          for (int i = 0; i < kFactCombo; ++i) {
+          for (int i = 0; i < KC; ++i) {
             const float q = qsm[i * kFactMaxS + s];
             v[i] = fmaf(q, a, v[i]);
             w[i] = fmaf(q, xl, w[i]);
           }
         };
-        if (gr.vec4) {
+        if (pipe) {
+          float4 cu[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) cu[j] = nx[j];
+          if (o + 1 < md.O) {
+            const float4* A4 = reinterpret_cast<const float4*>(Ar + md.K);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (4 * j < S0) nx[j] = __ldg(A4 + j);
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (4 * j < S0) {
+              take(cu[j].x, 4 * j);
+              take(cu[j].y, 4 * j + 1);
+              take(cu[j].z, 4 * j + 2);
+              take(cu[j].w, 4 * j + 3);
+            }
+          }
+        } else if (gr.vec4) {
           // contiguous, 16-byte aligned level-1 axis: four entries per load
           for (int s = 0; s < S0; s += 4) {
             const float4 a4 = __ldg(reinterpret_cast<const float4*>(Ar + s));
@@ -246,7 +321,7 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
           for (int s = 0; s < S0; ++s) take(__ldg(Ar + s * st0), s);
         }
 #pragma unroll
-        for (int i = 0; i < kFactCombo; ++i) {
+        for (int i = 0; i < KC; ++i) {
           if (i < nc) {
             Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + row) * gr.R + r] = v[i];
             lin[i] += w[i] + (ut ? __ldg(Cm + (int64_t)ct[i] * md.O + o) * v[i] : 0.f);
@@ -261,23 +336,23 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
         const EfeModality& md = p.mod[fp.mod_order[mi]];
         const float* Wm = wA + b * p.A_stride + md.A_off + base;
         for (int o = 0; o < md.O; ++o, ++wrow) {
-          float v[kFactCombo];
+          float v[KC];
 #pragma unroll
-          for (int i = 0; i < kFactCombo; ++i) v[i] = 0.f;
+          for (int i = 0; i < KC; ++i) v[i] = 0.f;
           const float* Wr = Wm + (int64_t)o * md.K;
           for (int s = 0; s < S0; ++s) {
             const float a = __ldg(Wr + s * st0);
 #pragma unroll
-            for (int i = 0; i < kFactCombo; ++i) v[i] = fmaf(qsm[i * kFactMaxS + s], a, v[i]);
+            for (int i = 0; i < KC; ++i) v[i] = fmaf(qsm[i * kFactMaxS + s], a, v[i]);
           }
 #pragma unroll
-          for (int i = 0; i < kFactCombo; ++i)
+          for (int i = 0; i < KC; ++i)
             if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + wrow) * gr.R + r] = v[i];
         }
       }
     }
 #pragma unroll
-    for (int i = 0; i < kFactCombo; ++i)
+    for (int i = 0; i < KC; ++i)
       if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + nrow - 1) * gr.R + r] = lin[i];
   }
 }
@@ -334,7 +409,8 @@ __device__ __forceinline__ double obs_term(bool ig, float d, bool w, float dw) {
 }
 
 // Last level for HPT columns per thread: rows of X (shared memory, row stride
-// xs; [n_obs A rows][n_w wA rows][1 linear row]); observation rows o = half,
+// xs, a multiple of 4 floats read as float4, zero past S; [n_obs A rows]
+// [n_w wA rows][1 linear row]); observation rows o = half,
 // half + 2, ..., the linear row by half 0; the two halves of a column meet
 // by one shuffle (lanes 2i, 2i + 1). `act` false: the thread only joins the
 // shuffle.
@@ -349,11 +425,16 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
 #pragma unroll
     for (int c = 0; c < HPT; ++c) d[c] = 0.f;
 #pragma unroll
-    for (int s = 0; s < SMAX; ++s) {
-      if (s < S) {
-        const float x = xr[s];
+    for (int s4 = 0; s4 < SMAX / 4; ++s4) {
+      if (4 * s4 < S) {
+        const float4 x = *reinterpret_cast<const float4*>(xr + 4 * s4);
 #pragma unroll
-        for (int c = 0; c < HPT; ++c) d[c] = fmaf(qv[c][s], x, d[c]);
+        for (int c = 0; c < HPT; ++c) {
+          d[c] = fmaf(qv[c][4 * s4], x.x, d[c]);
+          d[c] = fmaf(qv[c][4 * s4 + 1], x.y, d[c]);
+          d[c] = fmaf(qv[c][4 * s4 + 2], x.z, d[c]);
+          d[c] = fmaf(qv[c][4 * s4 + 3], x.w, d[c]);
+        }
       }
     }
   };
@@ -383,7 +464,9 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
                                                                         const float* __restrict__ V1,
                                                                         double* __restrict__ tab) {
   constexpr int HPT = TailShape<SMAX>::kHpt;
-  extern __shared__ float tsm[];  // rank 3: [kFactH1Tile][nrow][S2 + 1] level-2 blocks, then q1 tile
+  static_assert(kFactH1Tile == 8, "level 2 reads the tile's marginals as two float4");
+  extern __shared__ float4 tsm4[];  // rank 3: [kFactH1Tile][nrow][xs] level-2 blocks, then q1 tile [S1][8]
+  float* tsm = reinterpret_cast<float*>(tsm4);
   TailItem it;
   tail_item(fp, blockIdx.x, &it);
   if (it.g < 0) return;  // uniform over the CTA
@@ -411,17 +494,18 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
     return;
   }
   // the last level contracts factor fl (size SL, HL histories) against X
-  // ([nrow][SL] blocks in shared memory, row stride SL + 1)
+  // ([nrow][SL] blocks in shared memory, row stride xs = SL rounded up to 4,
+  // zero-filled past SL)
   const int rk = gr.rank;
   const int fl = gr.f[rk - 1], SL = gr.S[rk - 1], HL = gr.H[rk - 1][t];
-  const int xs = SL + 1;
+  const int xs = (SL + 3) & ~3;
   const float* ql = Qb + fp.qh_off[fl][t];
   int nblk = 1, h1_begin = 0, H1 = 1;
   if (rk == 2) {
     // X = the V1 block itself
-    for (int e = tid; e < nrow * SL; e += kFactTailThreads) {
-      const int n = e / SL, s = e - n * SL;
-      tsm[n * xs + s] = __ldg(V1b + (int64_t)n * gr.R + s);
+    for (int e = tid; e < nrow * xs; e += kFactTailThreads) {
+      const int n = e / xs, s = e - n * xs;
+      tsm[e] = s < SL ? __ldg(V1b + (int64_t)n * gr.R + s) : 0.f;
     }
   } else {
     // level 2 for the tile's h1 values at once: each V1 element read once
@@ -429,20 +513,33 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
     H1 = gr.H[1][t];
     h1_begin = it.h1_begin;
     nblk = H1 - h1_begin < kFactH1Tile ? H1 - h1_begin : kFactH1Tile;
-    float* q1s = tsm + kFactH1Tile * nrow * xs;
+    float* q1s = tsm + kFactH1Tile * nrow * xs;  // [s1][h], h innermost
     const float* q1 = Qb + fp.qh_off[gr.f[1]][t] + (int64_t)h1_begin * S1;
-    for (int e = tid; e < nblk * S1; e += kFactTailThreads) q1s[(e / S1) * kFactMaxS + e % S1] = __ldg(q1 + e);
+    for (int e = tid; e < kFactH1Tile * S1; e += kFactTailThreads) {
+      const int h = e / S1, s1 = e - h * S1;
+      q1s[s1 * kFactH1Tile + h] = h < nblk ? __ldg(q1 + e) : 0.f;
+    }
     __syncthreads();
-    for (int e = tid; e < nrow * SL; e += kFactTailThreads) {
-      const int n = e / SL, s2 = e - n * SL;
-      const float* vr = V1b + (int64_t)n * gr.R + s2;
+    const float4* q1s4 = reinterpret_cast<const float4*>(q1s);
+    for (int e = tid; e < nrow * xs; e += kFactTailThreads) {
+      const int n = e / xs, s2 = e - n * xs;
       float acc[kFactH1Tile];
 #pragma unroll
       for (int h = 0; h < kFactH1Tile; ++h) acc[h] = 0.f;
-      for (int s1 = 0; s1 < S1; ++s1) {
-        const float v = __ldg(vr + (int64_t)s1 * SL);
-#pragma unroll
-        for (int h = 0; h < kFactH1Tile; ++h) acc[h] = fmaf(q1s[h * kFactMaxS + s1], v, acc[h]);
+      if (s2 < SL) {
+        const float* vr = V1b + (int64_t)n * gr.R + s2;
+        for (int s1 = 0; s1 < S1; ++s1) {
+          const float v = __ldg(vr + (int64_t)s1 * SL);
+          const float4 qa = q1s4[2 * s1], qb = q1s4[2 * s1 + 1];
+          acc[0] = fmaf(qa.x, v, acc[0]);
+          acc[1] = fmaf(qa.y, v, acc[1]);
+          acc[2] = fmaf(qa.z, v, acc[2]);
+          acc[3] = fmaf(qa.w, v, acc[3]);
+          acc[4] = fmaf(qb.x, v, acc[4]);
+          acc[5] = fmaf(qb.y, v, acc[5]);
+          acc[6] = fmaf(qb.z, v, acc[6]);
+          acc[7] = fmaf(qb.w, v, acc[7]);
+        }
       }
 #pragma unroll
       for (int h = 0; h < kFactH1Tile; ++h)
@@ -541,6 +638,19 @@ bool fact_plan(const EfeParams& p, FactParams* fp, bool with_wA = false, bool wi
       off += (int64_t)h * p.S[f];
     }
   fp->qh_stride = (off + 63) / 64 * 64;
+  fp->qh_words = (int32_t)off;
+  // the history kernel's staging: B_f^T planes, qs_init, every history
+  int64_t hw = 0;
+  for (int f = 0; f < p.F; ++f) {
+    fp->bt_plane[f] = p.S[f] * p.S[f] + (p.S[f] < 32 ? p.S[f] : 0);
+    fp->bt_off[f] = (int32_t)hw;
+    hw += (int64_t)p.U[f] * fp->bt_plane[f];
+  }
+  fp->qi_sm = (int32_t)hw;
+  hw += p.S_tot;
+  fp->qh_sm = (int32_t)hw;
+  hw += off;
+  fp->hist_smem = hw * 4 <= 160 * 1024 ? (int32_t)(hw * 4) : 0;
   fp->hterm = with_hterm ? 1 : 0;
   int64_t hoff = 0;
   for (int f = 0; f < p.F; ++f)
@@ -627,8 +737,9 @@ bool fact_plan(const EfeParams& p, FactParams* fp, bool with_wA = false, bool wi
     gr.vec4 = v4 ? 1 : 0;
     // the tail's shared memory: kFactH1Tile level-2 blocks (rank 3) or the V1 block (rank 2)
     const int last = r == 3 ? gr.S[2] : (r == 2 ? gr.S[1] : 1);
-    const int64_t tail_words = (r == 3 ? (int64_t)kFactH1Tile * nrow * (last + 1) + kFactH1Tile * kFactMaxS
-                                       : (int64_t)nrow * (last + 1));
+    const int64_t xs = (last + 3) / 4 * 4;
+    const int64_t tail_words = (r == 3 ? (int64_t)kFactH1Tile * nrow * xs + kFactH1Tile * kFactMaxS
+                                       : (int64_t)nrow * xs);
     if (tail_words * 4 > kFactTailSmem) return false;
     max_R = gr.R > max_R ? gr.R : max_R;
     gr.n_obs = n_obs;
@@ -659,8 +770,9 @@ bool fact_plan(const EfeParams& p, FactParams* fp, bool with_wA = false, bool wi
     const FactGroup& gr = fp->grp[g];
     const int last = gr.rank == 3 ? gr.S[2] : (gr.rank == 2 ? gr.S[1] : 1);
     const int nr = gr.n_obs + gr.n_w + 1;
-    const int64_t w = gr.rank == 3 ? (int64_t)kFactH1Tile * nr * (last + 1) + kFactH1Tile * kFactMaxS
-                                   : (int64_t)nr * (last + 1);
+    const int64_t xs = (last + 3) / 4 * 4;
+    const int64_t w = gr.rank == 3 ? (int64_t)kFactH1Tile * nr * xs + kFactH1Tile * kFactMaxS
+                                   : (int64_t)nr * xs;
     tsm = w > tsm ? w : tsm;
   }
   fp->tail_smem = (int32_t)(tsm * 4);
@@ -700,11 +812,29 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
   double* Ht = hterm ? reinterpret_cast<double*>(ws + tab_bytes) : nullptr;
   float* Qh = reinterpret_cast<float*>(ws + tab_bytes + ht_bytes);
   float* V1 = reinterpret_cast<float*>(ws + tab_bytes + ht_bytes + qh_bytes);
-  efe_fact_hist_kernel<<<(unsigned)Bn, 256, 0, stream>>>(p, fp, qs, B, Qh, wB, wI, Ht);
-  int32_t rc = check_launch("efe_ffi factored histories");
+  int32_t rc = ensure_smem_attr((const void*)efe_fact_hist_kernel, fp.hist_smem, kEfeName);
+  if (rc == B2_OK) {
+    efe_fact_hist_kernel<<<(unsigned)Bn, 256, fp.hist_smem, stream>>>(p, fp, qs, B, Qh, wB, wI, Ht);
+    rc = check_launch("efe_ffi factored histories");
+  }
   if (rc == B2_OK) {
     dim3 grid((unsigned)((fp.max_R + 127) / 128), (unsigned)fp.G, (unsigned)Bn);
-    efe_fact_l1_kernel<<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+    // combinations per pass: enough for the group with the most, at most
+    // kFactCombo (fewer live accumulators, more resident CTAs)
+    int nc = 1;
+    for (int g = 0; g < fp.G; ++g) {
+      int n = 0;
+      for (int t = 0; t < p.T; ++t) n += fp.grp[g].H[0][t];
+      nc = n > nc ? n : nc;
+    }
+    if (nc <= 1)
+      efe_fact_l1_kernel<1><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+    else if (nc <= 2)
+      efe_fact_l1_kernel<2><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+    else if (nc <= 4)
+      efe_fact_l1_kernel<4><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+    else
+      efe_fact_l1_kernel<kFactCombo><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
     rc = check_launch("efe_ffi factored level 1");
   }
   if (rc == B2_OK) {

@@ -23,9 +23,12 @@
 //    FP64, so the marginal dot products and the per-factor sums carry FP64
 //    accumulation error only (FP32 accumulation misses the 1e-5-relative
 //    posterior target vs the FP64 reference on ill-conditioned Dirichlet(0.5)
-//    models). The log of each gathered A entry and prior and the softmax
-//    are FP64 as well: on models with many coupled factors the Jacobi sweeps
-//    amplify per-iteration rounding, and FP32 logf/expf alone move some
+//    models). The softmax is FP64. The log of each gathered A entry and
+//    prior is taken as e ln 2 (FP64) + logf(m) for x = m 2^e, m in
+//    [sqrt(1/2), sqrt(2)): absolute error about 4e-8 whatever the magnitude
+//    of log x. On models with many coupled factors the Jacobi sweeps amplify
+//    per-iteration rounding, and a plain FP32 logf/expf (absolute error
+//    proportional to |log x|, up to ~1.4e-6 at the clip) moves some
 //    posteriors by up to ~2e-5 relative after 16 iterations.
 //  * Modalities with identical dependency tuples are merged at plan time
 //    (their ll blocks are summed once at load), removing duplicate
@@ -113,18 +116,27 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-// softmax(logq) of n values by one warp: max, shift and sum in FP64; the
-// exponential of the shifted value in FP64, or (F32EXP) in FP32 (expf, within
-// 2 ulp): the argument is reduced in FP64 first, so the posteriors move by
-// at most a few 1e-7 relative (checked against the FP64 oracle on every FPI
-// fixture), while log q itself stays FP64.
-template <bool F32EXP = false, typename OutT>
+// log of a positive normal float to about 4e-8 absolute: x = m 2^e with m in
+// [sqrt(1/2), sqrt(2)), log x = e ln 2 in FP64 plus logf(m) in FP32, where
+// |log m| <= 0.35 keeps logf's relative error an absolute one that small.
+__device__ __forceinline__ double log_split(float x) {
+  int e;
+  float m = frexpf(x, &e);  // x = m 2^e, m in [0.5, 1)
+  if (m < 0.70710678f) {
+    m *= 2.f;
+    --e;
+  }
+  return (double)e * 0.69314718055994530942 + (double)logf(m);
+}
+
+// softmax(logq) of n values by one warp, in FP64 (max, shifted exponential, sum).
+template <typename OutT>
 __device__ __forceinline__ void softmax_warp(const double* __restrict__ logq, OutT* __restrict__ out, int n,
                                              int lane) {
   double mx = -INFINITY;
   for (int i = lane; i < n; i += 32) mx = fmax(mx, logq[i]);
   mx = warp_max_d(mx);
-  auto ex = [&](double x) { return F32EXP ? (double)expf((float)(x - mx)) : exp(x - mx); };
+  auto ex = [&](double x) { return exp(x - mx); };
   double sum = 0.0;
   for (int i = lane; i < n; i += 32) sum += ex(logq[i]);
   sum = warp_sum_d(sum);
@@ -275,7 +287,7 @@ __global__ void __launch_bounds__(TEAM * APC)
         const int m = p.src_order[si];
         if (!((obs_ok >> m) & 1u)) continue;
         const float a = __ldg(io.src + rowoff[m] + k);
-        v += FUSED ? (double)logf(fmaxf(a, kMinVal)) : (double)a;
+        v += FUSED ? log_split(fmaxf(a, kMinVal)) : (double)a;
       }
       int rem = k, addr = 0;
       for (int x = gr.rank - 1; x > 0; --x) {
@@ -290,14 +302,14 @@ __global__ void __launch_bounds__(TEAM * APC)
   }
   for (int i = t; i < p.S_tot; i += TEAM) {
     const float v = __ldg(io.prior + b * p.S_tot + i);
-    lp[i] = FUSED ? (double)logf(fmaxf(v, kMinVal)) : (double)v;
+    lp[i] = FUSED ? log_split(fmaxf(v, kMinVal)) : (double)v;
     logq[i] = 0.0;
   }
   team_sync<TEAM>();
 
   // ---- fixed-point iterations (Jacobi: every factor uses the previous q)
   for (int it = 0; it < p.num_iter; ++it) {
-    for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp<true>(logq + p.lp_off[f], q + p.lp_off[f], p.S[f], lane);
+    for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp(logq + p.lp_off[f], q + p.lp_off[f], p.S[f], lane);
     team_sync<TEAM>();
     for (int f = 0; f < p.F; ++f) {
       const int Sf = p.S[f];
@@ -321,7 +333,7 @@ __global__ void __launch_bounds__(TEAM * APC)
 
   // ---- posterior marginals
   float* out = io.q_out + b * p.S_tot;
-  for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp<true>(logq + p.lp_off[f], out + p.lp_off[f], p.S[f], lane);
+  for (int f = wid; f < p.F; f += TEAM / 32) softmax_warp(logq + p.lp_off[f], out + p.lp_off[f], p.S[f], lane);
 }
 
 // --------------------------------------------------------------- host side
@@ -629,7 +641,7 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
     double v = 0.0;
     if (s < p.S[f]) {
       const float x = __ldg(io.prior + b * p.S_tot + p.lp_off[f] + s);
-      v = FUSED ? (double)logf(fmaxf(x, kMinVal)) : (double)x;
+      v = FUSED ? log_split(fmaxf(x, kMinVal)) : (double)x;
     }
     lpp[i] = v;
     logq[i] = 0.0;  // log q starts at 0 (pymdp/algos.py:121-133)
@@ -689,8 +701,8 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
           const float a1[4] = {va[x][1].x, va[x][1].y, va[x][1].z, va[x][1].w};
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
-            double v = FUSED ? (double)logf(fmaxf(a0[e], kMinVal)) : (double)a0[e];
-            if (two) v += FUSED ? (double)logf(fmaxf(a1[e], kMinVal)) : (double)a1[e];
+            double v = FUSED ? log_split(fmaxf(a0[e], kMinVal)) : (double)a0[e];
+            if (two) v += FUSED ? log_split(fmaxf(a1[e], kMinVal)) : (double)a1[e];
             store(gi[x], 4 * ki[x] + e, v);
           }
         }
@@ -705,7 +717,7 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
           const int m = p.src_order[si];
           if (!((obs_ok >> m) & 1u)) continue;
           const float a = __ldg(io.src + rowoff[m] + k);
-          v += FUSED ? (double)logf(fmaxf(a, kMinVal)) : (double)a;
+          v += FUSED ? log_split(fmaxf(a, kMinVal)) : (double)a;
         }
         store(g, k, v);
       }
@@ -732,7 +744,7 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
       double mx = x;
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      const double e = valid ? (double)expf((float)(x - mx)) : 0.0;
+      const double e = valid ? exp(x - mx) : 0.0;
       double sum = e;
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
