@@ -408,6 +408,14 @@ __device__ __forceinline__ double obs_term(bool ig, float d, bool w, float dw) {
   return v;
 }
 
+// The same in FP32, for the per-thread sums of the last level (at most a few
+// dozen terms in [0, 0.37] each, FP64 from the pair sum on).
+__device__ __forceinline__ float obs_term_f(bool ig, float d, bool w, float dw) {
+  float v = ig ? -d * log_stable(d) : 0.f;
+  if (w) v = fmaf(-d, dw, v);
+  return v;
+}
+
 // Last level for HPT columns per thread: rows of X (shared memory, row stride
 // xs, a multiple of 4 floats read as float4, zero past S; [n_obs A rows]
 // [n_w wA rows][1 linear row]); observation rows o = half,
@@ -438,23 +446,29 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
       }
     }
   };
+  float acc[HPT];
+#pragma unroll
+  for (int c = 0; c < HPT; ++c) acc[c] = 0.f;
   if (act) {
     for (int o = half; o < n_obs; o += 2) {
       float d[HPT], dw[HPT];
       dot(X + o * xs, d);
       if (n_w) dot(X + (n_obs + o) * xs, dw);
 #pragma unroll
-      for (int c = 0; c < HPT; ++c) out[c] += obs_term(ig, d[c], n_w != 0, n_w ? dw[c] : 0.f);
+      for (int c = 0; c < HPT; ++c) acc[c] += obs_term_f(ig, d[c], n_w != 0, n_w ? dw[c] : 0.f);
     }
     if (half == 0) {
       float d[HPT];
       dot(X + (n_obs + n_w) * xs, d);
 #pragma unroll
-      for (int c = 0; c < HPT; ++c) out[c] += (double)d[c];
+      for (int c = 0; c < HPT; ++c) out[c] = (double)d[c];
     }
   }
 #pragma unroll
-  for (int c = 0; c < HPT; ++c) out[c] += __shfl_xor_sync(0xffffffffu, out[c], 1);
+  for (int c = 0; c < HPT; ++c) {
+    out[c] += (double)acc[c];
+    out[c] += __shfl_xor_sync(0xffffffffu, out[c], 1);
+  }
 }
 
 template <int SMAX>
@@ -528,6 +542,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
       for (int h = 0; h < kFactH1Tile; ++h) acc[h] = 0.f;
       if (s2 < SL) {
         const float* vr = V1b + (int64_t)n * gr.R + s2;
+#pragma unroll 8
         for (int s1 = 0; s1 < S1; ++s1) {
           const float v = __ldg(vr + (int64_t)s1 * SL);
           const float4 qa = q1s4[2 * s1], qb = q1s4[2 * s1 + 1];
@@ -549,17 +564,36 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
   __syncthreads();
   // final level: work items (block h, group of HPT histories of fl), two threads each
   const int groups = (HL + HPT - 1) / HPT;
+  // histories as float4: SL a multiple of 4 and the depth's block 16-byte aligned
+  const bool q4 = (SL & 3) == 0 && (fp.qh_off[fl][t] & 3) == 0;
   const int items = nblk * groups;
   for (int w0 = 0; w0 < items; w0 += kFactTailThreads / 2) {
     const int w = w0 + (tid >> 1), half = tid & 1;
     const bool act = w < items;  // uniform per lane pair; every lane still takes part in the shuffle
     const int hb = act ? w / groups : 0, hg = act ? w - hb * groups : 0;
     float qv[HPT][SMAX];
+    if (q4) {
 #pragma unroll
-    for (int c = 0; c < HPT; ++c) {
-      const int hl = hg * HPT + c;
+      for (int c = 0; c < HPT; ++c) {
+        const int hl = hg * HPT + c;
+        const float4* q4p = reinterpret_cast<const float4*>(ql + (int64_t)hl * SL);
 #pragma unroll
-      for (int s = 0; s < SMAX; ++s) qv[c][s] = (act && hl < HL && s < SL) ? __ldg(ql + (int64_t)hl * SL + s) : 0.f;
+        for (int s4 = 0; s4 < SMAX / 4; ++s4) {
+          const float4 v = (act && hl < HL && 4 * s4 < SL) ? __ldg(q4p + s4) : make_float4(0.f, 0.f, 0.f, 0.f);
+          qv[c][4 * s4] = v.x;
+          qv[c][4 * s4 + 1] = v.y;
+          qv[c][4 * s4 + 2] = v.z;
+          qv[c][4 * s4 + 3] = v.w;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < HPT; ++c) {
+        const int hl = hg * HPT + c;
+#pragma unroll
+        for (int s = 0; s < SMAX; ++s)
+          qv[c][s] = (act && hl < HL && s < SL) ? __ldg(ql + (int64_t)hl * SL + s) : 0.f;
+      }
     }
     double out[HPT];
     tail_final<SMAX>(tsm + hb * nrow * xs, xs, n_obs, n_w, ig, SL, qv, half, act, out);

@@ -792,6 +792,393 @@ __global__ void __launch_bounds__(32 * kR2MaxWarps) fpi_r2_kernel(const __grid_c
 }
 
 
+// ---------------------------------------------- rank <= 3 two-step path
+// Models with a modality on three factors, no modality on more than three
+// and no factor above 64 states (the agent-step model: S = [32, 16, 8], five
+// modalities on all three factors, merged into one group) run one agent per
+// CTA with each rank-3 contraction taken in two steps:
+//   X_g[a][b] = sum_c L_g[a][b][c] q_c[c],   Y_g[a][c] = sum_b L_g[a][b][c] q_b[b]
+// (2 K multiply-adds per group, spread over every thread of the CTA), then
+//   m_a = X_g q_b,   m_b = X_g^T q_a,   m_c = Y_g^T q_a
+// and the rank-2 groups' L q_b / L^T q_a, one warp per output factor, which
+// goes on to that factor's softmax. The direct form takes 3 K three-term
+// products per group and sweep. The same sums in another order, FP64 on
+// chip like the generic kernel; two barriers per sweep.
+//  * Load phase: each thread issues float4 loads of its columns of up to four
+//    observed rows at a time, all in flight before the logs are taken.
+//  * rank-1 groups are constant in the iteration and fold into the log prior.
+constexpr int kR3MaxS = 64;
+constexpr int kR3MaxTerm = 3 * kMaxM;
+
+// One message term of output factor f: m_f[s] += sum_{k < n} M[s * rs + k * cs] q[q_off + k].
+struct FpiR3Term {
+  int16_t m_off;  // the matrix (an ll block, or a group's X or Y): double offset in the agent's shared memory
+  int16_t rs, cs;
+  int16_t n;
+  int16_t q_off;
+  int16_t pad;
+};
+
+struct FpiR3 {
+  int32_t n_items;                // X and Y entries of every rank-3 group (one dot product each)
+  int32_t n3;                     // rank-3 groups
+  int32_t item_begin[kMaxM + 1];  // entries of the i-th rank-3 group: [item_begin[i], item_begin[i + 1])
+  int16_t g3[kMaxM];              // its group index
+  int16_t x_off[kMaxM], y_off[kMaxM];  // X_i [S_a][xs], Y_i [S_a][ys] (odd row strides)
+  int16_t xs[kMaxM], ys[kMaxM];
+  int32_t lp_sm, q_sm, row_sm;    // log prior (+ rank-1 terms) | q, two buffers | source row offsets (int64)
+  int32_t agent_words;
+  int32_t vec4;                   // float4 loads of the observed rows
+  int16_t term_begin[kMaxF + 1];
+  int8_t f_lg[kMaxF];             // S_f <= 32: log2 of the lanes that split each of its message sums
+  FpiR3Term term[kR3MaxTerm];
+};
+
+// The two-step plan; false when the model is outside it.
+bool build_r3(const FpiParams& p, FpiR3* r) {
+  std::memset(r, 0, sizeof(*r));
+  bool any3 = false;
+  for (int g = 0; g < p.G; ++g) {
+    if (p.grp[g].rank > 3) return false;
+    any3 |= p.grp[g].rank == 3;
+  }
+  if (!any3) return false;
+  for (int f = 0; f < p.F; ++f)
+    if (p.S[f] > kR3MaxS) return false;
+  int64_t sm = p.ll_sm_total;
+  std::vector<std::vector<FpiR3Term>> terms(p.F);
+  int items = 0;
+  auto odd = [](int s) { return s % 2 ? s : s + 1; };
+  for (int g = 0; g < p.G; ++g) {
+    const FpiGroup& gr = p.grp[g];
+    if (gr.rank == 2) {
+      const int a = gr.dep[0], b = gr.dep[1];
+      terms[a].push_back({(int16_t)gr.sm_off, gr.sst[0], gr.sst[1], (int16_t)p.S[b], (int16_t)p.lp_off[b], 0});
+      terms[b].push_back({(int16_t)gr.sm_off, gr.sst[1], gr.sst[0], (int16_t)p.S[a], (int16_t)p.lp_off[a], 0});
+    } else if (gr.rank == 3) {
+      const int a = gr.dep[0], b = gr.dep[1], c = gr.dep[2];
+      const int i = r->n3++;
+      r->g3[i] = (int16_t)g;
+      r->xs[i] = (int16_t)odd(p.S[b]);
+      r->ys[i] = (int16_t)odd(p.S[c]);
+      r->x_off[i] = (int16_t)sm;
+      sm += (int64_t)p.S[a] * r->xs[i];
+      r->y_off[i] = (int16_t)sm;
+      sm += (int64_t)p.S[a] * r->ys[i];
+      if (sm > 32767) return false;
+      r->item_begin[i] = items;
+      items += p.S[a] * (p.S[b] + p.S[c]);
+      terms[a].push_back({r->x_off[i], r->xs[i], 1, (int16_t)p.S[b], (int16_t)p.lp_off[b], 0});
+      terms[b].push_back({r->x_off[i], 1, r->xs[i], (int16_t)p.S[a], (int16_t)p.lp_off[a], 0});
+      terms[c].push_back({r->y_off[i], 1, r->ys[i], (int16_t)p.S[a], (int16_t)p.lp_off[a], 0});
+    }
+  }
+  r->item_begin[r->n3] = items;
+  r->n_items = items;
+  int n = 0;
+  for (int f = 0; f < p.F; ++f) {
+    r->term_begin[f] = (int16_t)n;
+    for (const FpiR3Term& t : terms[f]) {
+      if (n >= kR3MaxTerm) return false;
+      r->term[n++] = t;
+    }
+  }
+  r->term_begin[p.F] = (int16_t)n;
+  for (int f = 0; f < p.F; ++f) {
+    int lg = 5;  // 32 lanes per state, halved until every state has its lanes
+    while (lg > 0 && (p.S[f] << lg) > 32) --lg;
+    r->f_lg[f] = (int8_t)lg;
+  }
+  sm = (sm + 1) / 2 * 2;
+  r->lp_sm = (int32_t)sm;
+  sm += p.S_tot;
+  r->q_sm = (int32_t)sm;
+  sm += 2 * p.S_tot;
+  r->row_sm = (int32_t)sm;
+  sm += p.M;
+  r->agent_words = (int32_t)((sm + 1) / 2 * 2);
+  return (int64_t)r->agent_words * 8 <= kMaxSmemPerCta;
+}
+
+// One X or Y entry of a rank-3 group: a dot product of n shared-memory
+// doubles at stride st from L (the group's block) with n consecutive q's.
+struct R3Item {
+  int32_t L, st, n, q, out;
+};
+
+__device__ __forceinline__ R3Item r3_item(const FpiParams& p, const FpiR3& r, int i) {
+  int j = 0;
+  while (i >= r.item_begin[j + 1]) ++j;
+  const FpiGroup& gr = p.grp[r.g3[j]];
+  const int Sa = p.S[gr.dep[0]], Sb = p.S[gr.dep[1]], Sc = p.S[gr.dep[2]];
+  int li = i - r.item_begin[j];
+  R3Item it;
+  if (li < Sa * Sb) {  // X[a][b] = sum_c L[a][b][c] q_c[c]
+    const int a = li / Sb, bb = li - a * Sb;
+    it = {gr.sm_off + a * gr.sst[0] + bb * gr.sst[1], gr.sst[2], Sc, p.lp_off[gr.dep[2]], r.x_off[j] + a * r.xs[j] + bb};
+  } else {  // Y[a][c] = sum_b L[a][b][c] q_b[b]
+    li -= Sa * Sb;
+    const int a = li / Sc, c = li - a * Sc;
+    it = {gr.sm_off + a * gr.sst[0] + c * gr.sst[2], gr.sst[1], Sb, p.lp_off[gr.dep[1]], r.y_off[j] + a * r.ys[j] + c};
+  }
+  return it;
+}
+
+__device__ __forceinline__ double r3_dot(const double* __restrict__ L, int st, int n, const double* __restrict__ q) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    a0 = fma(L[k * st], q[k], a0);
+    a1 = fma(L[(k + 1) * st], q[k + 1], a1);
+    a2 = fma(L[(k + 2) * st], q[k + 2], a2);
+    a3 = fma(L[(k + 3) * st], q[k + 3], a3);
+  }
+  for (; k < n; ++k) a0 = fma(L[k * st], q[k], a0);
+  return (a0 + a1) + (a2 + a3);
+}
+
+// Per-factor data of the message step, copied to shared memory once.
+struct R3Factor {
+  int32_t S, off, lg, t0, t1;
+};
+
+template <int TEAM, bool FUSED>
+__global__ void __launch_bounds__(TEAM, TEAM >= 256 ? 2 : 4) fpi_r3_kernel(const __grid_constant__ FpiParams p,
+                                                                         const __grid_constant__ FpiR3 r,
+                                                                         const FpiIO io) {
+  extern __shared__ double smem_d[];
+  __shared__ uint32_t s_ok;
+  __shared__ R3Factor s_fac[kMaxF];
+  __shared__ FpiR3Term s_term[kR3MaxTerm];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  constexpr int kWarps = TEAM / 32;
+  const int64_t b = blockIdx.x;
+  if (b >= io.batch) return;  // uniform over the CTA (one agent per CTA)
+  double* sm = smem_d;
+  double* lpp = sm + r.lp_sm;
+  double* qbuf = sm + r.q_sm;
+  int64_t* rowoff = reinterpret_cast<int64_t*>(sm + r.row_sm);
+
+  // ---- load phase: observations (one lane per modality; M <= 32) and the
+  // prior are read side by side; an out-of-range observation adds nothing
+  // (see fpi_kernel)
+  if (wid == 0) {
+    bool ok = false;
+    if (lane < p.M) {
+      int64_t ro = b * io.src_stride + p.src[lane].src_off;
+      ok = true;
+      if (FUSED) {
+        const int o = io.obs[b * p.M + lane];
+        ok = o >= 0 && o < p.src[lane].O;
+        ro += (int64_t)(ok ? o : 0) * p.src[lane].K;
+      }
+      rowoff[lane] = ro;
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+    if (lane == 0) s_ok = bal;
+  }
+  for (int i = tid; i < p.S_tot; i += TEAM) {
+    const float x = __ldg(io.prior + b * p.S_tot + i);
+    lpp[i] = FUSED ? log_split(fmaxf(x, kMinVal)) : (double)x;
+  }
+  for (int f = wid; f < p.F; f += kWarps)  // q of the first sweep: softmax(log q = 0), uniform
+    for (int s = lane; s < p.S[f]; s += 32) qbuf[p.lp_off[f] + s] = 1.0 / p.S[f];
+  for (int f = tid; f < p.F; f += TEAM) s_fac[f] = {p.S[f], p.lp_off[f], r.f_lg[f], r.term_begin[f], r.term_begin[f + 1]};
+  for (int i = tid; i < r.term_begin[p.F]; i += TEAM) s_term[i] = r.term[i];
+  __syncthreads();
+  const uint32_t obs_ok = s_ok;
+  auto term_of = [&](float a) { return FUSED ? log_split(fmaxf(a, kMinVal)) : (double)a; };
+  // shared-memory address of ll element k of a rank >= 2 group
+  auto addr_of = [&](const FpiGroup& gr, int k) {
+    int rem = k, addr = 0;
+    for (int x = gr.rank - 1; x > 0; --x) {
+      const int d = p.S[gr.dep[x]];
+      const int qd = rem / d;
+      addr += (rem - qd * d) * gr.sst[x];
+      rem = qd;
+    }
+    return gr.sm_off + addr + rem * gr.sst[0];
+  };
+  // ll element k of group g into its padded block (rank >= 2) or the log prior (rank 1)
+  auto put = [&](const FpiGroup& gr, int k, double v) {
+    if (gr.rank == 1)
+      lpp[p.lp_off[gr.dep[0]] + k] += v;  // one group per rank-1 tuple, one thread per state: no race
+    else
+      sm[addr_of(gr, k)] = v;
+  };
+  for (int g = 0; g < p.G; ++g) {
+    const FpiGroup& gr = p.grp[g];
+    if (r.vec4) {
+      // two float4 columns per thread and up to four sources per batch of loads
+      const int K4 = gr.K >> 2;
+      const bool inner4 = gr.rank >= 2 && p.S[gr.dep[gr.rank - 1]] % 4 == 0;  // 4 columns share all outer digits
+      for (int e0 = tid; e0 < K4; e0 += 2 * TEAM) {
+        double v[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+        for (int s0 = gr.src_begin; s0 < gr.src_end; s0 += 4) {
+          float4 a[4][2];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int si = s0 + j;
+            const int m = si < gr.src_end ? p.src_order[si] : 0;
+            const bool use = si < gr.src_end && ((obs_ok >> m) & 1u);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int e4 = e0 + h * TEAM;
+              a[j][h] = use && e4 < K4 ? __ldg(reinterpret_cast<const float4*>(io.src + rowoff[m]) + e4)
+                                       : make_float4(1.f, 1.f, 1.f, 1.f);
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int si = s0 + j;
+            if (si < gr.src_end && ((obs_ok >> p.src_order[si]) & 1u)) {
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                v[h][0] += term_of(a[j][h].x);
+                v[h][1] += term_of(a[j][h].y);
+                v[h][2] += term_of(a[j][h].z);
+                v[h][3] += term_of(a[j][h].w);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int e4 = e0 + h * TEAM;
+          if (e4 < K4) {
+            if (inner4) {
+              const int a0 = addr_of(gr, 4 * e4);
+#pragma unroll
+              for (int x = 0; x < 4; ++x) sm[a0 + x] = v[h][x];
+            } else {
+#pragma unroll
+              for (int x = 0; x < 4; ++x) put(gr, 4 * e4 + x, v[h][x]);
+            }
+          }
+        }
+      }
+    } else {
+      for (int k = tid; k < gr.K; k += TEAM) {
+        double v = 0.0;
+        for (int si = gr.src_begin; si < gr.src_end; ++si) {
+          const int m = p.src_order[si];
+          if ((obs_ok >> m) & 1u) v += term_of(__ldg(io.src + rowoff[m] + k));
+        }
+        put(gr, k, v);
+      }
+    }
+  }
+  // this thread's first two X / Y entries, fixed for every sweep
+  R3Item mine[2];
+  int n_mine = 0;
+#pragma unroll
+  for (int c = 0; c < 2; ++c)
+    if (tid + c * TEAM < r.n_items) {
+      mine[c] = r3_item(p, r, tid + c * TEAM);
+      n_mine = c + 1;
+    }
+  __syncthreads();
+
+  // ---- sweeps (Jacobi: every factor uses the previous q)
+  for (int it = 0; it < p.num_iter; ++it) {
+    const double* q = qbuf + (it & 1) * p.S_tot;
+    double* qn = qbuf + ((it + 1) & 1) * p.S_tot;
+    // step 1: X and Y of every rank-3 group, one entry per thread
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+      if (c < n_mine) sm[mine[c].out] = r3_dot(sm + mine[c].L, mine[c].st, mine[c].n, q + mine[c].q);
+    for (int i = tid + 2 * TEAM; i < r.n_items; i += TEAM) {
+      const R3Item e = r3_item(p, r, i);
+      sm[e.out] = r3_dot(sm + e.L, e.st, e.n, q + e.q);
+    }
+    __syncthreads();
+    // step 2: one warp per output factor: log q = log prior + its messages,
+    // then the softmax (the posterior itself after the last sweep). S <= 32:
+    // 2^lg lanes per state split each message sum; S > 32: every lane takes
+    // states lane and lane + 32.
+    for (int f = wid; f < p.F; f += kWarps) {
+      const R3Factor fc = s_fac[f];
+      const int S = fc.S, off = fc.off;
+      double x0, x1 = 0.0;
+      bool v0, v1 = false, w0;
+      if (S <= 32) {
+        const int G = 1 << fc.lg;
+        const int s = lane >> fc.lg, j = lane & (G - 1);
+        v0 = s < S;
+        w0 = v0 && j == 0;  // the lane that writes state s
+        double acc = 0.0;
+        if (v0) {
+          for (int ti = fc.t0; ti < fc.t1; ++ti) {
+            const FpiR3Term tm = s_term[ti];
+            const double* Ms = sm + tm.m_off + s * tm.rs;
+            const double* qo = q + tm.q_off;
+            double a0 = 0.0, a1 = 0.0;
+            int k = j;
+            for (; k + G < tm.n; k += 2 * G) {
+              a0 = fma(Ms[k * tm.cs], qo[k], a0);
+              a1 = fma(Ms[(k + G) * tm.cs], qo[k + G], a1);
+            }
+            if (k < tm.n) a0 = fma(Ms[k * tm.cs], qo[k], a0);
+            acc += a0 + a1;
+          }
+        }
+        for (int o = 1; o < G; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        x0 = v0 ? acc + lpp[off + s] : 0.0;
+      } else {
+        v0 = true;  // S > 32: lane < S always
+        w0 = true;
+        v1 = lane + 32 < S;
+        x0 = lpp[off + lane];
+        x1 = v1 ? lpp[off + lane + 32] : 0.0;
+        for (int ti = fc.t0; ti < fc.t1; ++ti) {
+          const FpiR3Term tm = s_term[ti];
+          const double* M0 = sm + tm.m_off + lane * tm.rs;
+          const double* M1 = M0 + 32 * tm.rs;
+          const double* qo = q + tm.q_off;
+          double a0 = 0.0, a1 = 0.0, c0 = 0.0, c1 = 0.0;
+          int k = 0;
+          for (; k + 2 <= tm.n; k += 2) {
+            const double qa = qo[k], qb = qo[k + 1];
+            a0 = fma(M0[k * tm.cs], qa, a0);
+            a1 = fma(M0[(k + 1) * tm.cs], qb, a1);
+            if (v1) {
+              c0 = fma(M1[k * tm.cs], qa, c0);
+              c1 = fma(M1[(k + 1) * tm.cs], qb, c1);
+            }
+          }
+          if (k < tm.n) {
+            a0 = fma(M0[k * tm.cs], qo[k], a0);
+            if (v1) c0 = fma(M1[k * tm.cs], qo[k], c0);
+          }
+          x0 += a0 + a1;
+          x1 += c0 + c1;
+        }
+      }
+      // softmax: any shift near the maximum cancels, so the maximum is taken
+      // in FP32; exponentials and their sum in FP64, the reciprocal as FP32
+      // plus one Newton step
+      float mf = fmaxf(v0 ? (float)x0 : -INFINITY, v1 ? (float)x1 : -INFINITY);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mf = fmaxf(mf, __shfl_xor_sync(0xffffffffu, mf, o));
+      const double mx = (double)mf;
+      const double e0 = v0 ? exp(x0 - mx) : 0.0, e1 = v1 ? exp(x1 - mx) : 0.0;
+      const double sum = warp_sum_d((w0 ? e0 : 0.0) + e1);
+      double inv = (double)__frcp_rn((float)sum);
+      inv = inv * fma(-sum, inv, 2.0);
+      const int s_out = S <= 32 ? lane >> fc.lg : lane;
+      if (it + 1 == p.num_iter) {
+        float* out = io.q_out + b * p.S_tot + off;
+        if (w0) out[s_out] = (float)(e0 * inv);
+        if (v1) out[lane + 32] = (float)(e1 * inv);
+      } else {
+        if (w0) qn[off + s_out] = e0 * inv;
+        if (v1) qn[off + lane + 32] = e1 * inv;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------ adjoint
 // Reverse pass of the fused-observation FPI for gradients of a loss on the
 // posteriors with respect to the observed A rows and the prior. The reference
@@ -976,6 +1363,14 @@ int32_t launch_one(const FpiParams& p, const FpiIO& io, cudaStream_t stream, con
   return check_launch(op);
 }
 
+template <int TEAM, bool FUSED>
+int32_t launch_r3(const FpiParams& p, const FpiR3& r, const FpiIO& io, cudaStream_t stream, const char* op) {
+  const int bytes = r.agent_words * 8;
+  B2_TRY(ensure_smem_attr((const void*)fpi_r3_kernel<TEAM, FUSED>, bytes, op));
+  fpi_r3_kernel<TEAM, FUSED><<<(unsigned)io.batch, TEAM, bytes, stream>>>(p, r, io);
+  return check_launch(op);
+}
+
 template <bool FUSED>
 int32_t launch(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const char* op) {
   if (io.batch <= 0) return B2_OK;
@@ -990,6 +1385,17 @@ int32_t launch(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const c
     B2_TRY(ensure_smem_attr((const void*)fpi_r2_kernel<FUSED>, bytes, op));
     fpi_r2_kernel<FUSED><<<(unsigned)io.batch, 32 * r2.warps, bytes, stream>>>(p, r2, io);
     return check_launch(op);
+  }
+  FpiR3 r3;
+  if (build_r3(p, &r3)) {
+    if (io.batch > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
+    bool v4 = (reinterpret_cast<uintptr_t>(io.src) % 16 == 0) && io.src_stride % 4 == 0;
+    for (int m = 0; m < p.M; ++m) v4 = v4 && p.src[m].src_off % 4 == 0 && p.src[m].K % 4 == 0;
+    r3.vec4 = v4 ? 1 : 0;
+    // threads: about two X / Y entries per thread and sweep
+    if (r3.n_items > 512) return launch_r3<512, FUSED>(p, r3, io, stream, op);
+    if (r3.n_items > 256) return launch_r3<256, FUSED>(p, r3, io, stream, op);
+    return launch_r3<128, FUSED>(p, r3, io, stream, op);
   }
   const int64_t work = work_per_iter(p);
   const int bytes_agent = p.agent_words * 8;

@@ -69,10 +69,15 @@ SHAPES = [
     ([2, 2, 2, 2, 2, 2, 2, 2], [3], [[7, 6, 5, 4, 3, 2, 1, 0]]),  # rank 8 (ABI cap)
     ([16, 16, 16, 16], [32] * 6, [[0, 1], [2, 3], [1, 3], [0, 2], [3, 0], [2, 1]]),
     ([3] * 16, [2] * 32, [[m % 16, (m + 5) % 16] for m in range(32)]),  # F = 16, M = 32 limits
+    # two-step rank-3 kernel: the agent-step model (float4 loads), S = 64 (two states a lane)
+    # with rank-1/2 groups beside, and two rank-3 groups with K % 4 != 0 (scalar loads)
+    ([32, 16, 8], [16, 16, 8, 8, 4], [[0, 1, 2]] * 5),
+    ([64, 5, 3], [3, 4, 5], [[0, 1, 2], [2, 0], [1]]),
+    ([7, 5, 3, 6], [3, 2, 4, 5], [[0, 1, 2], [1, 3], [3, 2, 0], [2]]),
 ]
 
 
-@pytest.mark.parametrize("shape", SHAPES, ids=[f"S{len(s[0])}M{len(s[1])}" for s in SHAPES])
+@pytest.mark.parametrize("shape", SHAPES, ids=[f"S{len(s[0])}M{len(s[1])}-{i}" for i, s in enumerate(SHAPES)])
 @pytest.mark.parametrize("shared", [False, True])
 def test_fpi_random_shapes_match_oracle(shape, shared):
     from pymdp_b200 import ffi
@@ -151,6 +156,20 @@ def test_fpi_out_of_range_observation_on_the_rank2_fast_path():
         np.testing.assert_allclose(qs[f].cpu().numpy(), ref[f], rtol=RTOL, atol=ATOL)
     # all observations out of range: the posterior is the FPI of the prior alone
     np.testing.assert_allclose(qs[0].cpu().numpy()[3], prior[0][3], rtol=1e-5, atol=1e-7)
+
+
+def test_fpi_out_of_range_observation_on_the_rank3_two_step_path():
+    """The agent-step model (the two-step rank-3 kernel): out-of-range
+    observations add nothing, as the oracle's zero one-hots."""
+    from pymdp_b200 import ffi
+    rng = np.random.default_rng(13)
+    S, O, deps = [32, 16, 8], [16, 16, 8, 8, 4], [[0, 1, 2]] * 5
+    A, prior, obs = random_model(rng, S, O, deps, 4)
+    obs[0, 1], obs[1, :], obs[2, 4] = -1, 99, 4
+    qs = ffi.fpi_obs([cuda(a) for a in A], cuda(obs, torch.int32), [cuda(p) for p in prior], deps, 16)
+    ref = ofpi.run_fpi_batch([a.astype(np.float64) for a in A], obs, [p.astype(np.float64) for p in prior], deps, 16)
+    for f in range(3):
+        np.testing.assert_allclose(qs[f].cpu().numpy(), ref[f], rtol=RTOL, atol=ATOL)
 
 
 def test_fpi_empty_batch_and_errors():
