@@ -49,7 +49,7 @@ constexpr int kFactMaxG = 8;
 constexpr int kFactMaxS = 64;   // largest factor size on the factored path
 constexpr int kFactCombo = 8;   // (depth, history) combinations per level-1 pass over A
 constexpr int kFactTailThreads = 256;
-constexpr int kFactH1Tile = 8;  // level-2 histories per tail CTA
+constexpr int kFactH1Tile = 8;  // level-2 histories per tail CTA (at least; 16 where shared memory allows)
 constexpr int kFactTailSmem = 96 * 1024;  // tail shared memory: level-2 blocks of one h1 tile
 
 struct FactGroup {
@@ -78,6 +78,7 @@ struct FactParams {
   int32_t max_R, max_tiles;
   int32_t smax;                             // largest size among the factors the tail contracts
   int32_t tail_smem;                        // dynamic shared memory of the tail kernel (bytes)
+  int32_t h1_tile;                          // level-2 histories per tail CTA: 8 or 16
   int32_t hist_smem;                        // dynamic shared memory of the history kernel (bytes; 0: global path)
   int32_t bt_off[kEfeMaxF], bt_plane[kEfeMaxF];  // staged B_f^T: plane u at bt_off + u * bt_plane, [k][s]
   int32_t qi_sm, qh_sm, qh_words;           // staged qs_init and histories (float offsets); histories per agent
@@ -199,13 +200,13 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
 // in shared memory), writes V1[h0][row][r] = sum_s0 q_{f0}^{h0}[s0] A and
 // accumulates the depth's linear row sum_row [sum_s0 q xlogx(A)] + C_t[o] V1
 // (information gain, utility).
-template <int KC>
+template <int KC, int NJ>
 __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant__ EfeParams p,
                                                           const __grid_constant__ FactParams fp,
                                                           const float* __restrict__ A, const float* __restrict__ C,
                                                           const float* __restrict__ Qh, float* __restrict__ V1,
                                                           const float* __restrict__ wA) {
-  __shared__ float qsm[KC * kFactMaxS];
+  __shared__ __align__(16) float qsm[KC * kFactMaxS];  // [s][combination]
   const int64_t b = blockIdx.z;
   const int g = blockIdx.y;
   if (g >= fp.G) return;  // uniform over the CTA
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
           h = 0;
           ++t;
         }
-      qsm[i * kFactMaxS + s] = Qb[fp.qh_off[gr.f[0]][t] + (int64_t)h * S0 + s];
+      qsm[s * KC + i] = Qb[fp.qh_off[gr.f[0]][t] + (int64_t)h * S0 + s];
     }
     __syncthreads();
     if (!active) continue;
@@ -265,48 +266,68 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
       const EfeModality& md = p.mod[fp.mod_order[mi]];
       const float* Am = A + b * p.A_stride + md.A_off + base;
       const float* Cm = C + b * p.C_stride + md.C_off;
-      // short contiguous level-1 axis (<= 16 entries): the next row's loads are
-      // issued before this row's arithmetic, two rows in flight per thread
-      const bool pipe = gr.vec4 && S0 <= 16;
-      float4 nx[4];
+      // NJ > 0: every group's level-1 axis is 4 NJ contiguous, 16-byte aligned
+      // entries; the next row's loads are issued before this row's
+      // arithmetic, two rows in flight per thread
+      constexpr bool pipe = NJ > 0;
+      constexpr int NJ1 = NJ > 0 ? NJ : 1;
+      float4 nx[NJ1];
       if (pipe) {
         const float4* A4 = reinterpret_cast<const float4*>(Am);
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (4 * j < S0) nx[j] = __ldg(A4 + j);
+        for (int j = 0; j < NJ1; ++j) nx[j] = __ldg(A4 + j);
       }
       for (int o = 0; o < md.O; ++o, ++row) {
-        float v[KC], w[KC];
+        // combinations (2i, 2i + 1) in the halves of packed accumulators
+        constexpr int KP = (KC + 1) / 2;
+        float2 v2[KP], w2[KP];
 #pragma unroll
-        for (int i = 0; i < KC; ++i) v[i] = w[i] = 0.f;
+        for (int i = 0; i < KP; ++i) v2[i] = w2[i] = make_float2(0.f, 0.f);
         const float* Ar = Am + (int64_t)o * md.K;
         auto take = [&](float a, int s) {
-          const float xl = ig ? a * log_stable(a) : 0.f;
+          const float xl = ig ? a * log_fast(a) : 0.f;
+          const float2 aa = make_float2(a, a), xx = make_float2(xl, xl);
+          if (KC % 4 == 0) {
 #pragma unroll
-          for (int i = 0; i < KC; ++i) {
-            const float q = qsm[i * kFactMaxS + s];
-            v[i] = fmaf(q, a, v[i]);
-            w[i] = fmaf(q, xl, w[i]);
+            for (int i = 0; i < KC / 4; ++i) {
+              const float4 q4 = *reinterpret_cast<const float4*>(qsm + s * KC + 4 * i);
+              const float2 qa = make_float2(q4.x, q4.y), qb = make_float2(q4.z, q4.w);
+              v2[2 * i] = fma2(qa, aa, v2[2 * i]);
+              w2[2 * i] = fma2(qa, xx, w2[2 * i]);
+              v2[2 * i + 1] = fma2(qb, aa, v2[2 * i + 1]);
+              w2[2 * i + 1] = fma2(qb, xx, w2[2 * i + 1]);
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < KC; ++i) {
+              const float q = qsm[s * KC + i];
+              float2& vv = v2[i >> 1];
+              float2& ww = w2[i >> 1];
+              if (i & 1) {
+                vv.y = fmaf(q, a, vv.y);
+                ww.y = fmaf(q, xl, ww.y);
+              } else {
+                vv.x = fmaf(q, a, vv.x);
+                ww.x = fmaf(q, xl, ww.x);
+              }
+            }
           }
         };
         if (pipe) {
-          float4 cu[4];
+          float4 cu[NJ1];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) cu[j] = nx[j];
+          for (int j = 0; j < NJ1; ++j) cu[j] = nx[j];
           if (o + 1 < md.O) {
             const float4* A4 = reinterpret_cast<const float4*>(Ar + md.K);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-              if (4 * j < S0) nx[j] = __ldg(A4 + j);
+            for (int j = 0; j < NJ1; ++j) nx[j] = __ldg(A4 + j);
           }
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if (4 * j < S0) {
-              take(cu[j].x, 4 * j);
-              take(cu[j].y, 4 * j + 1);
-              take(cu[j].z, 4 * j + 2);
-              take(cu[j].w, 4 * j + 3);
-            }
+          for (int j = 0; j < NJ1; ++j) {
+            take(cu[j].x, 4 * j);
+            take(cu[j].y, 4 * j + 1);
+            take(cu[j].z, 4 * j + 2);
+            take(cu[j].w, 4 * j + 3);
           }
         } else if (gr.vec4) {
           // contiguous, 16-byte aligned level-1 axis: four entries per load
@@ -323,8 +344,10 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
 #pragma unroll
         for (int i = 0; i < KC; ++i) {
           if (i < nc) {
-            Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + row) * gr.R + r] = v[i];
-            lin[i] += w[i] + (ut ? __ldg(Cm + (int64_t)ct[i] * md.O + o) * v[i] : 0.f);
+            const float vi = i & 1 ? v2[i >> 1].y : v2[i >> 1].x;
+            const float wi = i & 1 ? w2[i >> 1].y : w2[i >> 1].x;
+            Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + row) * gr.R + r] = vi;
+            lin[i] += wi + (ut ? __ldg(Cm + (int64_t)ct[i] * md.O + o) * vi : 0.f);
           }
         }
       }
@@ -343,7 +366,7 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
           for (int s = 0; s < S0; ++s) {
             const float a = __ldg(Wr + s * st0);
 #pragma unroll
-            for (int i = 0; i < KC; ++i) v[i] = fmaf(qsm[i * kFactMaxS + s], a, v[i]);
+            for (int i = 0; i < KC; ++i) v[i] = fmaf(qsm[s * KC + i], a, v[i]);
           }
 #pragma unroll
           for (int i = 0; i < KC; ++i)
@@ -358,7 +381,7 @@ __global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant_
 }
 
 // Levels 2 and 3 and the epilogue. CTA (tile, b) covers one (group, depth t,
-// h0, tile of up to kFactH1Tile level-2 histories h1) of the tail work list.
+// h0, tile of up to TILE level-2 histories h1) of the tail work list.
 // rank 3: V2[n][s2] = sum_s1 q1^{h1}[s1] V1[h0][n][s1,s2] in shared memory,
 //         then qo[n] = sum_s2 q2^{h2}[s2] V2[n][s2] for every h2;
 // rank 2: qo[n] = sum_s1 q1^{h1}[s1] V1[h0][n][s1] for every h1 of the tile;
@@ -375,13 +398,13 @@ __device__ __forceinline__ void tail_item(const FactParams& fp, int idx, TailIte
     const FactGroup& gr = fp.grp[g];
     for (int t = 0; t < fp.T; ++t) {
       const int h1n = gr.rank >= 3 ? gr.H[1][t] : 1;
-      const int tiles = (h1n + kFactH1Tile - 1) / kFactH1Tile;
+      const int tiles = (h1n + fp.h1_tile - 1) / fp.h1_tile;
       const int n = gr.H[0][t] * tiles;
       if (idx < n) {
         it->g = g;
         it->t = t;
         it->h0 = idx / tiles;
-        it->h1_begin = (idx - it->h0 * tiles) * kFactH1Tile;
+        it->h1_begin = (idx - it->h0 * tiles) * fp.h1_tile;
         return;
       }
       idx -= n;
@@ -411,7 +434,7 @@ __device__ __forceinline__ double obs_term(bool ig, float d, bool w, float dw) {
 // The same in FP32, for the per-thread sums of the last level (at most a few
 // dozen terms in [0, 0.37] each, FP64 from the pair sum on).
 __device__ __forceinline__ float obs_term_f(bool ig, float d, bool w, float dw) {
-  float v = ig ? -d * log_stable(d) : 0.f;
+  float v = ig ? -d * log_fast(d) : 0.f;
   if (w) v = fmaf(-d, dw, v);
   return v;
 }
@@ -424,27 +447,30 @@ __device__ __forceinline__ float obs_term_f(bool ig, float d, bool w, float dw) 
 // shuffle.
 template <int SMAX>
 __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, int n_obs, int n_w, bool ig,
-                                           int S, const float (&qv)[TailShape<SMAX>::kHpt][SMAX], int half,
-                                           bool act, double (&out)[TailShape<SMAX>::kHpt]) {
+                                           int S, const float2 (&qv)[TailShape<SMAX>::kHpt][SMAX / 2],
+                                           int half, bool act, double (&out)[TailShape<SMAX>::kHpt]) {
   constexpr int HPT = TailShape<SMAX>::kHpt;
 #pragma unroll
   for (int c = 0; c < HPT; ++c) out[c] = 0.0;
+  // even and odd states in the two halves of a packed accumulator
   auto dot = [&](const float* xr, float (&d)[HPT]) {
+    float2 a2[HPT];
 #pragma unroll
-    for (int c = 0; c < HPT; ++c) d[c] = 0.f;
+    for (int c = 0; c < HPT; ++c) a2[c] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int s4 = 0; s4 < SMAX / 4; ++s4) {
       if (4 * s4 < S) {
         const float4 x = *reinterpret_cast<const float4*>(xr + 4 * s4);
+        const float2 x01 = make_float2(x.x, x.y), x23 = make_float2(x.z, x.w);
 #pragma unroll
         for (int c = 0; c < HPT; ++c) {
-          d[c] = fmaf(qv[c][4 * s4], x.x, d[c]);
-          d[c] = fmaf(qv[c][4 * s4 + 1], x.y, d[c]);
-          d[c] = fmaf(qv[c][4 * s4 + 2], x.z, d[c]);
-          d[c] = fmaf(qv[c][4 * s4 + 3], x.w, d[c]);
+          a2[c] = fma2(qv[c][2 * s4], x01, a2[c]);
+          a2[c] = fma2(qv[c][2 * s4 + 1], x23, a2[c]);
         }
       }
     }
+#pragma unroll
+    for (int c = 0; c < HPT; ++c) d[c] = a2[c].x + a2[c].y;
   };
   float acc[HPT];
 #pragma unroll
@@ -471,15 +497,15 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
   }
 }
 
-template <int SMAX>
+template <int SMAX, int TILE>
 __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const __grid_constant__ EfeParams p,
                                                                         const __grid_constant__ FactParams fp,
                                                                         const float* __restrict__ Qh,
                                                                         const float* __restrict__ V1,
                                                                         double* __restrict__ tab) {
   constexpr int HPT = TailShape<SMAX>::kHpt;
-  static_assert(kFactH1Tile == 8, "level 2 reads the tile's marginals as two float4");
-  extern __shared__ float4 tsm4[];  // rank 3: [kFactH1Tile][nrow][xs] level-2 blocks, then q1 tile [S1][8]
+  static_assert(TILE % 4 == 0, "level 2 reads the tile's marginals as float4");
+  extern __shared__ float4 tsm4[];  // rank 3: [TILE][nrow][xs] level-2 blocks, then q1 tile [S1][TILE]
   float* tsm = reinterpret_cast<float*>(tsm4);
   TailItem it;
   tail_item(fp, blockIdx.x, &it);
@@ -526,39 +552,37 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
     const int S1 = gr.S[1];
     H1 = gr.H[1][t];
     h1_begin = it.h1_begin;
-    nblk = H1 - h1_begin < kFactH1Tile ? H1 - h1_begin : kFactH1Tile;
-    float* q1s = tsm + kFactH1Tile * nrow * xs;  // [s1][h], h innermost
+    nblk = H1 - h1_begin < TILE ? H1 - h1_begin : TILE;
+    float* q1s = tsm + TILE * nrow * xs;  // [s1][h], h innermost
     const float* q1 = Qb + fp.qh_off[gr.f[1]][t] + (int64_t)h1_begin * S1;
-    for (int e = tid; e < kFactH1Tile * S1; e += kFactTailThreads) {
+    for (int e = tid; e < TILE * S1; e += kFactTailThreads) {
       const int h = e / S1, s1 = e - h * S1;
-      q1s[s1 * kFactH1Tile + h] = h < nblk ? __ldg(q1 + e) : 0.f;
+      q1s[s1 * TILE + h] = h < nblk ? __ldg(q1 + e) : 0.f;
     }
     __syncthreads();
     const float4* q1s4 = reinterpret_cast<const float4*>(q1s);
     for (int e = tid; e < nrow * xs; e += kFactTailThreads) {
       const int n = e / xs, s2 = e - n * xs;
-      float acc[kFactH1Tile];
+      float2 acc2[TILE / 2];  // histories (2i, 2i + 1)
 #pragma unroll
-      for (int h = 0; h < kFactH1Tile; ++h) acc[h] = 0.f;
+      for (int h = 0; h < TILE / 2; ++h) acc2[h] = make_float2(0.f, 0.f);
       if (s2 < SL) {
         const float* vr = V1b + (int64_t)n * gr.R + s2;
 #pragma unroll 8
         for (int s1 = 0; s1 < S1; ++s1) {
           const float v = __ldg(vr + (int64_t)s1 * SL);
-          const float4 qa = q1s4[2 * s1], qb = q1s4[2 * s1 + 1];
-          acc[0] = fmaf(qa.x, v, acc[0]);
-          acc[1] = fmaf(qa.y, v, acc[1]);
-          acc[2] = fmaf(qa.z, v, acc[2]);
-          acc[3] = fmaf(qa.w, v, acc[3]);
-          acc[4] = fmaf(qb.x, v, acc[4]);
-          acc[5] = fmaf(qb.y, v, acc[5]);
-          acc[6] = fmaf(qb.z, v, acc[6]);
-          acc[7] = fmaf(qb.w, v, acc[7]);
+          const float2 vv = make_float2(v, v);
+#pragma unroll
+          for (int h4 = 0; h4 < TILE / 4; ++h4) {
+            const float4 qa = q1s4[(TILE / 4) * s1 + h4];
+            acc2[2 * h4] = fma2(make_float2(qa.x, qa.y), vv, acc2[2 * h4]);
+            acc2[2 * h4 + 1] = fma2(make_float2(qa.z, qa.w), vv, acc2[2 * h4 + 1]);
+          }
         }
       }
 #pragma unroll
-      for (int h = 0; h < kFactH1Tile; ++h)
-        if (h < nblk) tsm[(h * nrow + n) * xs + s2] = acc[h];
+      for (int h = 0; h < TILE; ++h)
+        if (h < nblk) tsm[(h * nrow + n) * xs + s2] = h & 1 ? acc2[h >> 1].y : acc2[h >> 1].x;
     }
   }
   __syncthreads();
@@ -571,7 +595,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
     const int w = w0 + (tid >> 1), half = tid & 1;
     const bool act = w < items;  // uniform per lane pair; every lane still takes part in the shuffle
     const int hb = act ? w / groups : 0, hg = act ? w - hb * groups : 0;
-    float qv[HPT][SMAX];
+    float2 qv[HPT][SMAX / 2];  // marginals of this thread's histories, zero past SL
     if (q4) {
 #pragma unroll
       for (int c = 0; c < HPT; ++c) {
@@ -580,19 +604,21 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
 #pragma unroll
         for (int s4 = 0; s4 < SMAX / 4; ++s4) {
           const float4 v = (act && hl < HL && 4 * s4 < SL) ? __ldg(q4p + s4) : make_float4(0.f, 0.f, 0.f, 0.f);
-          qv[c][4 * s4] = v.x;
-          qv[c][4 * s4 + 1] = v.y;
-          qv[c][4 * s4 + 2] = v.z;
-          qv[c][4 * s4 + 3] = v.w;
+          qv[c][2 * s4] = make_float2(v.x, v.y);
+          qv[c][2 * s4 + 1] = make_float2(v.z, v.w);
         }
       }
     } else {
 #pragma unroll
       for (int c = 0; c < HPT; ++c) {
         const int hl = hg * HPT + c;
+        const bool ok = act && hl < HL;
 #pragma unroll
-        for (int s = 0; s < SMAX; ++s)
-          qv[c][s] = (act && hl < HL && s < SL) ? __ldg(ql + (int64_t)hl * SL + s) : 0.f;
+        for (int s2 = 0; s2 < SMAX / 2; ++s2) {
+          const int s = 2 * s2;
+          qv[c][s2] = make_float2(ok && s < SL ? __ldg(ql + (int64_t)hl * SL + s) : 0.f,
+                                  ok && s + 1 < SL ? __ldg(ql + (int64_t)hl * SL + s + 1) : 0.f);
+        }
       }
     }
     double out[HPT];
@@ -640,6 +666,35 @@ __global__ void efe_fact_combine_kernel(const __grid_constant__ EfeParams p, con
       for (int f = 0; f < p.F; ++f) g += Ht[b * fp.ht_stride + fp.ht_off[f][t] + hist[f]];
   }
   G[b * p.P + pol] = (float)g;
+}
+
+template <int SMAX, int TILE>
+int32_t launch_tail_s(dim3 grid, int smem, cudaStream_t stream, const EfeParams& p, const FactParams& fp,
+                      const float* Qh, const float* V1, double* tab) {
+  B2_TRY(ensure_smem_attr((const void*)efe_fact_tail_kernel<SMAX, TILE>, smem, kEfeName));
+  efe_fact_tail_kernel<SMAX, TILE><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+  return check_launch("efe_ffi factored tail");
+}
+
+template <int TILE>
+int32_t launch_tail(dim3 grid, int smem, cudaStream_t stream, const EfeParams& p, const FactParams& fp,
+                    const float* Qh, const float* V1, double* tab) {
+  if (fp.smax <= 8) return launch_tail_s<8, TILE>(grid, smem, stream, p, fp, Qh, V1, tab);
+  if (fp.smax <= 16) return launch_tail_s<16, TILE>(grid, smem, stream, p, fp, Qh, V1, tab);
+  if (fp.smax <= 32) return launch_tail_s<32, TILE>(grid, smem, stream, p, fp, Qh, V1, tab);
+  return launch_tail_s<64, TILE>(grid, smem, stream, p, fp, Qh, V1, tab);
+}
+
+template <int KC>
+void launch_l1(int nj, dim3 grid, cudaStream_t stream, const EfeParams& p, const FactParams& fp, const float* A,
+               const float* C, const float* Qh, float* V1, const float* wA) {
+  switch (nj) {
+    case 1: efe_fact_l1_kernel<KC, 1><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
+    case 2: efe_fact_l1_kernel<KC, 2><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
+    case 3: efe_fact_l1_kernel<KC, 3><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
+    case 4: efe_fact_l1_kernel<KC, 4><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
+    default: efe_fact_l1_kernel<KC, 0><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
+  }
 }
 
 // Host plan; false when the model is outside the factored path.
@@ -773,7 +828,7 @@ bool fact_plan(const EfeParams& p, FactParams* fp, bool with_wA = false, bool wi
     const int last = r == 3 ? gr.S[2] : (r == 2 ? gr.S[1] : 1);
     const int64_t xs = (last + 3) / 4 * 4;
     const int64_t tail_words = (r == 3 ? (int64_t)kFactH1Tile * nrow * xs + kFactH1Tile * kFactMaxS
-                                       : (int64_t)nrow * xs);
+                                       : (int64_t)nrow * xs);  // with the smallest tile
     if (tail_words * 4 > kFactTailSmem) return false;
     max_R = gr.R > max_R ? gr.R : max_R;
     gr.n_obs = n_obs;
@@ -799,23 +854,27 @@ bool fact_plan(const EfeParams& p, FactParams* fp, bool with_wA = false, bool wi
     smax = last > smax ? last : smax;
   }
   fp->smax = smax;
-  int64_t tsm = 0;
-  for (int g = 0; g < fp->G; ++g) {
-    const FactGroup& gr = fp->grp[g];
-    const int last = gr.rank == 3 ? gr.S[2] : (gr.rank == 2 ? gr.S[1] : 1);
-    const int nr = gr.n_obs + gr.n_w + 1;
-    const int64_t xs = (last + 3) / 4 * 4;
-    const int64_t w = gr.rank == 3 ? (int64_t)kFactH1Tile * nr * xs + kFactH1Tile * kFactMaxS
-                                   : (int64_t)nr * xs;
-    tsm = w > tsm ? w : tsm;
-  }
-  fp->tail_smem = (int32_t)(tsm * 4);
+  // level-2 tile: 16 histories when their blocks fit, else 8
+  auto tail_bytes = [&](int tile) {
+    int64_t tsm = 0;
+    for (int g = 0; g < fp->G; ++g) {
+      const FactGroup& gr = fp->grp[g];
+      const int last = gr.rank == 3 ? gr.S[2] : (gr.rank == 2 ? gr.S[1] : 1);
+      const int nr = gr.n_obs + gr.n_w + 1;
+      const int64_t xs = (last + 3) / 4 * 4;
+      const int64_t w = gr.rank == 3 ? (int64_t)tile * nr * xs + (int64_t)tile * kFactMaxS : (int64_t)nr * xs;
+      tsm = w > tsm ? w : tsm;
+    }
+    return tsm * 4;
+  };
+  fp->h1_tile = tail_bytes(2 * kFactH1Tile) <= kFactTailSmem ? 2 * kFactH1Tile : kFactH1Tile;
+  fp->tail_smem = (int32_t)tail_bytes(fp->h1_tile);
   int items = 0;
   for (int g = 0; g < fp->G; ++g)
     for (int t = 0; t < p.T; ++t) {
       const FactGroup& gr = fp->grp[g];
       const int h1n = gr.rank >= 3 ? gr.H[1][t] : 1;
-      items += gr.H[0][t] * ((h1n + kFactH1Tile - 1) / kFactH1Tile);
+      items += gr.H[0][t] * ((h1n + fp->h1_tile - 1) / fp->h1_tile);
     }
   fp->max_tiles = items;
   return true;
@@ -861,35 +920,25 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
       for (int t = 0; t < p.T; ++t) n += fp.grp[g].H[0][t];
       nc = n > nc ? n : nc;
     }
+    // the pipelined form: every group's level-1 axis vec4 with one size <= 16
+    int nj = fp.grp[0].vec4 && fp.grp[0].S[0] <= 16 ? fp.grp[0].S[0] / 4 : 0;
+    for (int g = 1; g < fp.G; ++g)
+      if (!fp.grp[g].vec4 || fp.grp[g].S[0] != fp.grp[0].S[0]) nj = 0;
     if (nc <= 1)
-      efe_fact_l1_kernel<1><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+      launch_l1<1>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
     else if (nc <= 2)
-      efe_fact_l1_kernel<2><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+      launch_l1<2>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
     else if (nc <= 4)
-      efe_fact_l1_kernel<4><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+      launch_l1<4>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
     else
-      efe_fact_l1_kernel<kFactCombo><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA);
+      launch_l1<kFactCombo>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
     rc = check_launch("efe_ffi factored level 1");
   }
   if (rc == B2_OK) {
     const dim3 grid((unsigned)fp.max_tiles, (unsigned)Bn);
     const int smem = fp.tail_smem;
-    const void* k = fp.smax <= 8    ? (const void*)efe_fact_tail_kernel<8>
-                    : fp.smax <= 16 ? (const void*)efe_fact_tail_kernel<16>
-                    : fp.smax <= 32 ? (const void*)efe_fact_tail_kernel<32>
-                                    : (const void*)efe_fact_tail_kernel<64>;
-    rc = ensure_smem_attr(k, smem, kEfeName);
-    if (rc == B2_OK) {
-      if (fp.smax <= 8)
-        efe_fact_tail_kernel<8><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
-      else if (fp.smax <= 16)
-        efe_fact_tail_kernel<16><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
-      else if (fp.smax <= 32)
-        efe_fact_tail_kernel<32><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
-      else
-        efe_fact_tail_kernel<64><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
-      rc = check_launch("efe_ffi factored tail");
-    }
+    rc = fp.h1_tile == 2 * kFactH1Tile ? launch_tail<2 * kFactH1Tile>(grid, smem, stream, p, fp, Qh, V1, tab)
+                                       : launch_tail<kFactH1Tile>(grid, smem, stream, p, fp, Qh, V1, tab);
   }
   if (rc == B2_OK) {
     efe_fact_combine_kernel<<<dim3((unsigned)((p.P + 255) / 256), (unsigned)Bn), 256, 0, stream>>>(p, fp, tab, Ht,
