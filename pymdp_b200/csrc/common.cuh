@@ -51,17 +51,9 @@ __device__ __forceinline__ float log_stable(float x) { return logf(fmaxf(x, kMin
 // terms whose products with x leave that error far below the FP32 sums they feed.
 __device__ __forceinline__ float log_fast(float x) { return __logf(fmaxf(x, kMinVal)); }
 
-// Two FP32 fused multiply-adds in one instruction (fma.rn.f32x2, sm_100):
+// Two FP32 fused multiply-adds in one instruction (fma.rn.f32x2 on sm_100):
 // d = a * b + c lane by lane, each rounded as fmaf rounds it.
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-  float2 d;
-  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
-      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return d;
-}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll

@@ -386,6 +386,60 @@ __global__ void __launch_bounds__(256)
   for (int i = threadIdx.x; i < P; i += blockDim.x) q_pi[b * P + i] = expf(gm * g[i] + log_stable(e[i]) - mx) / sum;
 }
 
+// The same with every policy of the agent in registers (P <= 256 EPT): one
+// pass over G and E; the same per-thread and block summation order, so the
+// results equal the kernel above bit for bit.
+template <int EPT>
+__global__ void __launch_bounds__(256)
+    policy_posterior_reg_kernel(const float* __restrict__ G, const float* __restrict__ E, int E_batched,
+                                const float* __restrict__ gamma, int gamma_batched, float* __restrict__ q_pi, int P) {
+  __shared__ float red[32];
+  const int64_t b = blockIdx.x;
+  const float gm = gamma[gamma_batched ? b : 0];
+  const float* g = G + b * P;
+  const float* e = E + (E_batched ? b * P : 0);
+  float z[EPT];
+  float mx = -INFINITY;
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) {
+    const int i = threadIdx.x + k * 256;
+    z[k] = i < P ? gm * g[i] + log_stable(e[i]) : -INFINITY;
+    mx = fmaxf(mx, z[k]);
+  }
+  mx = warp_max(mx);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
+    v = warp_max(v);
+    if (threadIdx.x == 0) red[0] = v;
+  }
+  __syncthreads();
+  mx = red[0];
+  __syncthreads();
+  float sum = 0.f;
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) {
+    z[k] = threadIdx.x + k * 256 < P ? expf(z[k] - mx) : 0.f;
+    sum += z[k];
+  }
+  sum = warp_sum(sum);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) red[0] = v;
+  }
+  __syncthreads();
+  sum = red[0];
+#pragma unroll
+  for (int k = 0; k < EPT; ++k) {
+    const int i = threadIdx.x + k * 256;
+    if (i < P) q_pi[b * P + i] = z[k] / sum;
+  }
+}
+
 // action[b, :] = policy_matrix[first argmax q_pi[b], 0, :] — one CTA per agent.
 __global__ void __launch_bounds__(256)
     select_action_kernel(const float* __restrict__ q_pi, const int32_t* __restrict__ pm, int32_t* __restrict__ action,
@@ -395,11 +449,22 @@ __global__ void __launch_bounds__(256)
   const int64_t b = blockIdx.x;
   float best = -INFINITY;
   int bi = 0x7fffffff;
-  for (int i = threadIdx.x; i < P; i += blockDim.x) {
-    const float v = q_pi[b * P + i];
-    if (v > best || (v == best && i < bi) || (bi == 0x7fffffff && v != v)) {
-      best = v;
-      bi = i;
+  // eight loads in flight, then the scan in index order
+  for (int i0 = threadIdx.x; i0 < P; i0 += 8 * blockDim.x) {
+    float v8[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = i0 + k * blockDim.x;
+      v8[k] = i < P ? q_pi[b * P + i] : -INFINITY;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = i0 + k * blockDim.x;
+      const float v = v8[k];
+      if (i < P && (v > best || (v == best && i < bi) || (bi == 0x7fffffff && v != v))) {
+        best = v;
+        bi = i;
+      }
     }
   }
 #pragma unroll
@@ -676,8 +741,18 @@ extern "C" int32_t b2_policy_posterior(void* stream, const float* neg_efe, const
   if (Bn == 0) return B2_OK;
   if (!neg_efe || !E || !gamma || !q_pi) return fail(B2_ERR_INVALID_ARGUMENT, "policy_posterior: null buffer");
   if (Bn > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, "policy_posterior: Bn too large");
-  policy_posterior_kernel<<<(unsigned)Bn, 256, 0, (cudaStream_t)stream>>>(neg_efe, E, E_batched, gamma,
-                                                                           gamma_batched, q_pi, (int)P);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (P <= 256 * 4)
+    policy_posterior_reg_kernel<4><<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi,
+                                                                 (int)P);
+  else if (P <= 256 * 16)
+    policy_posterior_reg_kernel<16><<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi,
+                                                                  (int)P);
+  else if (P <= 256 * 64)
+    policy_posterior_reg_kernel<64><<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi,
+                                                                  (int)P);
+  else
+    policy_posterior_kernel<<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi, (int)P);
   return check_launch("policy_posterior");
 }
 

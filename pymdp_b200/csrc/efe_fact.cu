@@ -115,13 +115,25 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
     // B_f transposed to [u][k][s] (planes padded so that the half-warps of
     // small factors fall on different banks) and qs_init, in shared memory
     for (int f = 0; f < p.F; ++f) {
-      const int S = p.S[f], U = p.U[f], n = S * S * U;
+      // one thread per (s, k): its U contiguous actions go to the U planes
+      const int S = p.S[f], U = p.U[f];
       const float* src = Bb + p.fac[f].B_off;
       float* dst = hsm + fp.bt_off[f];
-#pragma unroll 4
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int s = i / (S * U), rem = i - s * S * U, k = rem / U, u = rem - k * U;
-        dst[u * fp.bt_plane[f] + k * S + s] = __ldg(src + i);
+      const int plane = fp.bt_plane[f];
+#pragma unroll 2
+      for (int pr = threadIdx.x; pr < S * S; pr += blockDim.x) {
+        const int s = pr / S, k = pr - s * S;
+        const float* sp = src + (int64_t)pr * U;
+        float* dp = dst + k * S + s;
+        if (U == 4 && (reinterpret_cast<uintptr_t>(sp) & 15) == 0) {
+          const float4 v = __ldg(reinterpret_cast<const float4*>(sp));
+          dp[0] = v.x;
+          dp[plane] = v.y;
+          dp[2 * plane] = v.z;
+          dp[3 * plane] = v.w;
+        } else {
+          for (int u = 0; u < U; ++u) dp[u * plane] = __ldg(sp + u);
+        }
       }
     }
     for (int i = threadIdx.x; i < p.S_tot; i += blockDim.x) hsm[fp.qi_sm + i] = __ldg(qi + i);
@@ -445,7 +457,7 @@ __device__ __forceinline__ float obs_term_f(bool ig, float d, bool w, float dw) 
 // half + 2, ..., the linear row by half 0; the two halves of a column meet
 // by one shuffle (lanes 2i, 2i + 1). `act` false: the thread only joins the
 // shuffle.
-template <int SMAX>
+template <int SMAX, bool FULL>
 __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, int n_obs, int n_w, bool ig,
                                            int S, const float2 (&qv)[TailShape<SMAX>::kHpt][SMAX / 2],
                                            int half, bool act, double (&out)[TailShape<SMAX>::kHpt]) {
@@ -459,7 +471,7 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
     for (int c = 0; c < HPT; ++c) a2[c] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int s4 = 0; s4 < SMAX / 4; ++s4) {
-      if (4 * s4 < S) {
+      if (FULL || 4 * s4 < S) {  // FULL: S == SMAX, no guard
         const float4 x = *reinterpret_cast<const float4*>(xr + 4 * s4);
         const float2 x01 = make_float2(x.x, x.y), x23 = make_float2(x.z, x.w);
 #pragma unroll
@@ -476,6 +488,7 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
 #pragma unroll
   for (int c = 0; c < HPT; ++c) acc[c] = 0.f;
   if (act) {
+#pragma unroll 2
     for (int o = half; o < n_obs; o += 2) {
       float d[HPT], dw[HPT];
       dot(X + o * xs, d);
@@ -497,7 +510,7 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
   }
 }
 
-template <int SMAX, int TILE>
+template <int SMAX, int TILE, bool FULL>
 __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const __grid_constant__ EfeParams p,
                                                                         const __grid_constant__ FactParams fp,
                                                                         const float* __restrict__ Qh,
@@ -622,7 +635,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
       }
     }
     double out[HPT];
-    tail_final<SMAX>(tsm + hb * nrow * xs, xs, n_obs, n_w, ig, SL, qv, half, act, out);
+    tail_final<SMAX, FULL>(tsm + hb * nrow * xs, xs, n_obs, n_w, ig, SL, qv, half, act, out);
     if (act && half == 0) {
 #pragma unroll
       for (int c = 0; c < HPT; ++c) {
@@ -636,25 +649,38 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
   }
 }
 
-// G[b, pol] = sum_t sum_g T_g,t[histories of pol's prefix at t]: the policy's
-// actions come from its index in construct_policies order (mixed radix: the
-// joint action of step t is digit T-1-t of pol in base nu).
-__global__ void efe_fact_combine_kernel(const __grid_constant__ EfeParams p, const __grid_constant__ FactParams fp,
-                                        const double* __restrict__ tab, const double* __restrict__ Ht,
-                                        float* __restrict__ G) {
-  const int64_t b = blockIdx.y;
-  const int pol = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pol >= p.P) return;
+// G[b, pol] = sum_t sum_g T_g,t[histories of pol's prefix at t] (+ the
+// per-factor history terms): the policy's actions come from its index in
+// construct_policies order (mixed radix: the joint action of step t is digit
+// T-1-t of pol in base nu). One CTA per agent with its tables staged in shared
+// memory (when they fit); a work item is one prefix of the first T-1 steps
+// and a run of up to kCombRun consecutive last actions, whose factor digits
+// advance as a mixed-radix counter (no division per policy).
+constexpr int kCombRun = 16;
+
+__global__ void __launch_bounds__(256) efe_fact_combine_kernel(const __grid_constant__ EfeParams p,
+                                                               const __grid_constant__ FactParams fp,
+                                                               const double* __restrict__ tab,
+                                                               const double* __restrict__ Ht, float* __restrict__ G,
+                                                               int staged) {
+  extern __shared__ double ctab[];  // staged: tables [tab_stride], then history terms [ht_stride]
+  const int64_t b = blockIdx.x;
   const double* tb = tab + b * fp.tab_stride;
-  int hist[kEfeMaxF];
-  for (int f = 0; f < p.F; ++f) hist[f] = 0;
-  int div = 1;
-  for (int t = 1; t < p.T; ++t) div *= fp.nu;
-  double g = 0.0;
-  for (int t = 0; t < p.T; ++t) {
-    const int a = (pol / div) % fp.nu;
-    div /= fp.nu > 0 ? fp.nu : 1;
-    for (int f = 0; f < p.F; ++f) hist[f] = hist[f] * p.U[f] + (a / fp.ustride[f]) % p.U[f];
+  const double* hb = fp.hterm ? Ht + b * fp.ht_stride : nullptr;
+  if (staged) {
+    for (int i = threadIdx.x; i < fp.tab_stride; i += blockDim.x) ctab[i] = tb[i];
+    if (fp.hterm)
+      for (int i = threadIdx.x; i < fp.ht_stride; i += blockDim.x) ctab[fp.tab_stride + i] = hb[i];
+    __syncthreads();
+    tb = ctab;
+    hb = fp.hterm ? ctab + fp.tab_stride : nullptr;
+  }
+  const int T = p.T, F = p.F, nu = fp.nu;
+  int npre = 1;
+  for (int t = 0; t + 1 < T; ++t) npre *= nu;
+  const int runs = (nu + kCombRun - 1) / kCombRun;
+  auto step_value = [&](int t, const int* hist) {
+    double g = 0.0;
     for (int gi = 0; gi < fp.G; ++gi) {
       const FactGroup& gr = fp.grp[gi];
       int64_t idx = hist[gr.f[0]];
@@ -663,16 +689,62 @@ __global__ void efe_fact_combine_kernel(const __grid_constant__ EfeParams p, con
       g += tb[gr.tab_off[t] + idx];
     }
     if (fp.hterm)
-      for (int f = 0; f < p.F; ++f) g += Ht[b * fp.ht_stride + fp.ht_off[f][t] + hist[f]];
+      for (int f = 0; f < F; ++f) g += hb[fp.ht_off[f][t] + hist[f]];
+    return g;
+  };
+  for (int item = threadIdx.x; item < npre * runs; item += blockDim.x) {
+    const int pre = item / runs, a0 = (item - pre * runs) * kCombRun;
+    // the prefix's actions, most significant (step 0) first
+    int act[kFactMaxT];
+    int rem = pre;
+    for (int t = T - 2; t >= 0; --t) {
+      act[t] = rem % nu;
+      rem /= nu;
+    }
+    int hist[kEfeMaxF];
+    for (int f = 0; f < F; ++f) hist[f] = 0;
+    double g = 0.0;
+    for (int t = 0; t + 1 < T; ++t) {
+      for (int f = 0; f < F; ++f) hist[f] = hist[f] * p.U[f] + (act[t] / fp.ustride[f]) % p.U[f];
+      g += step_value(t, hist);
+    }
+    // last step: the run's joint actions a0 .. a0 + kCombRun - 1 as per-factor digits
+    int dig[kEfeMaxF], base[kEfeMaxF];
+    for (int f = 0; f < F; ++f) {
+      dig[f] = (a0 / fp.ustride[f]) % p.U[f];
+      base[f] = hist[f] * p.U[f];
+    }
+    const int a1 = a0 + kCombRun < nu ? a0 + kCombRun : nu;
+    float* out = G + b * p.P + (int64_t)pre * nu;
+    for (int a = a0; a < a1; ++a) {
+      int h[kEfeMaxF];
+      for (int f = 0; f < F; ++f) h[f] = base[f] + dig[f];
+      out[a] = (float)(g + step_value(T - 1, h));
+      for (int f = F - 1; f >= 0; --f) {  // next joint action: the last factor's digit moves fastest
+        if (++dig[f] < p.U[f]) break;
+        dig[f] = 0;
+      }
+    }
   }
-  G[b * p.P + pol] = (float)g;
 }
+
 
 template <int SMAX, int TILE>
 int32_t launch_tail_s(dim3 grid, int smem, cudaStream_t stream, const EfeParams& p, const FactParams& fp,
                       const float* Qh, const float* V1, double* tab) {
-  B2_TRY(ensure_smem_attr((const void*)efe_fact_tail_kernel<SMAX, TILE>, smem, kEfeName));
-  efe_fact_tail_kernel<SMAX, TILE><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+  // every group's last factor exactly SMAX states: the last level runs unguarded
+  bool full = true;
+  for (int g = 0; g < fp.G; ++g) {
+    const FactGroup& gr = fp.grp[g];
+    full = full && gr.rank >= 2 && gr.S[gr.rank - 1] == SMAX;
+  }
+  if (full) {
+    B2_TRY(ensure_smem_attr((const void*)efe_fact_tail_kernel<SMAX, TILE, true>, smem, kEfeName));
+    efe_fact_tail_kernel<SMAX, TILE, true><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+  } else {
+    B2_TRY(ensure_smem_attr((const void*)efe_fact_tail_kernel<SMAX, TILE, false>, smem, kEfeName));
+    efe_fact_tail_kernel<SMAX, TILE, false><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+  }
   return check_launch("efe_ffi factored tail");
 }
 
@@ -694,6 +766,102 @@ void launch_l1(int nj, dim3 grid, cudaStream_t stream, const EfeParams& p, const
     case 3: efe_fact_l1_kernel<KC, 3><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
     case 4: efe_fact_l1_kernel<KC, 4><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
     default: efe_fact_l1_kernel<KC, 0><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
+  }
+}
+
+// Two-phase combine for models whose per-prefix and per-action offsets fit in
+// shared memory (CTA per agent): phase 1, one thread per prefix of the first
+// T-1 steps: its value (tables of steps 0..T-2) and, per group, the base of
+// its last-step table index; phase 2, one thread per policy: G = prefix value
+// + sum_g T_g,T-1[base_g(prefix) + off_g(last action)] (+ the last step's
+// history terms), where off_g(a) = sum_k u_{f_k}(a) mult_gk depends on the
+// last joint action alone.
+struct CombLayout {
+  int32_t npre, tab_w, ht_w;  // prefixes; staged table / history-term doubles
+  int32_t pv, base, off, hb, ua;  // double offset of prefix values; int offsets (in ints past the doubles)
+};
+
+__global__ void __launch_bounds__(256) efe_fact_combine2_kernel(const __grid_constant__ EfeParams p,
+                                                                const __grid_constant__ FactParams fp,
+                                                                const CombLayout L, const double* __restrict__ tab,
+                                                                const double* __restrict__ Ht, float* __restrict__ G) {
+  extern __shared__ double csm[];
+  const int64_t b = blockIdx.x;
+  const int T = p.T, F = p.F, nu = fp.nu, NG = fp.G;
+  double* tb = csm;
+  double* hb = csm + L.tab_w;
+  double* pv = csm + L.pv;
+  int* ib = reinterpret_cast<int*>(csm + L.pv + L.npre);
+  int* base = ib + L.base;  // [NG][npre]
+  int* off = ib + L.off;    // [NG][nu]
+  int* hbase = ib + L.hb;   // [F][npre] (history terms)
+  int* ua = ib + L.ua;      // [F][nu]
+  for (int i = threadIdx.x; i < L.tab_w; i += blockDim.x) tb[i] = tab[b * fp.tab_stride + i];
+  if (fp.hterm)
+    for (int i = threadIdx.x; i < L.ht_w; i += blockDim.x) hb[i] = Ht[b * fp.ht_stride + i];
+  // per last action: the factor digits and each group's index offset
+  for (int a = threadIdx.x; a < nu; a += blockDim.x) {
+    for (int gi = 0; gi < NG; ++gi) {
+      const FactGroup& gr = fp.grp[gi];
+      int o = 0;
+      for (int k = 0; k < gr.rank; ++k) {
+        int mult = 1;
+        for (int j = k + 1; j < gr.rank; ++j) mult *= gr.H[j][T - 1];
+        o += ((a / fp.ustride[gr.f[k]]) % p.U[gr.f[k]]) * mult;
+      }
+      off[gi * nu + a] = o;
+    }
+    if (fp.hterm)
+      for (int f = 0; f < F; ++f) ua[f * nu + a] = (a / fp.ustride[f]) % p.U[f];
+  }
+  __syncthreads();
+  // phase 1: prefixes
+  for (int pre = threadIdx.x; pre < L.npre; pre += blockDim.x) {
+    int act[kFactMaxT];
+    int rem = pre;
+    for (int t = T - 2; t >= 0; --t) {
+      act[t] = rem % nu;
+      rem /= nu;
+    }
+    int hist[kEfeMaxF];
+    for (int f = 0; f < F; ++f) hist[f] = 0;
+    double g = 0.0;
+    for (int t = 0; t + 1 < T; ++t) {
+      for (int f = 0; f < F; ++f) hist[f] = hist[f] * p.U[f] + (act[t] / fp.ustride[f]) % p.U[f];
+      for (int gi = 0; gi < NG; ++gi) {
+        const FactGroup& gr = fp.grp[gi];
+        int64_t idx = hist[gr.f[0]];
+        if (gr.rank > 1) idx = idx * gr.H[1][t] + hist[gr.f[1]];
+        if (gr.rank > 2) idx = idx * gr.H[2][t] + hist[gr.f[2]];
+        g += tb[gr.tab_off[t] + idx];
+      }
+      if (fp.hterm)
+        for (int f = 0; f < F; ++f) g += hb[fp.ht_off[f][t] + hist[f]];
+    }
+    pv[pre] = g;
+    for (int gi = 0; gi < NG; ++gi) {
+      const FactGroup& gr = fp.grp[gi];
+      int o = 0;
+      for (int k = 0; k < gr.rank; ++k) {
+        int mult = 1;
+        for (int j = k + 1; j < gr.rank; ++j) mult *= gr.H[j][T - 1];
+        o += hist[gr.f[k]] * p.U[gr.f[k]] * mult;
+      }
+      base[gi * L.npre + pre] = (int)gr.tab_off[T - 1] + o;
+    }
+    if (fp.hterm)
+      for (int f = 0; f < F; ++f) hbase[f * L.npre + pre] = (int)fp.ht_off[f][T - 1] + hist[f] * p.U[f];
+  }
+  __syncthreads();
+  // phase 2: one thread per policy, consecutive policies on consecutive threads
+  float* Gb = G + b * p.P;
+  for (int o = threadIdx.x; o < p.P; o += blockDim.x) {
+    const int pre = o / nu, a = o - pre * nu;
+    double g = pv[pre];
+    for (int gi = 0; gi < NG; ++gi) g += tb[base[gi * L.npre + pre] + off[gi * nu + a]];
+    if (fp.hterm)
+      for (int f = 0; f < F; ++f) g += hb[hbase[f * L.npre + pre] + ua[f * nu + a]];
+    Gb[o] = (float)g;
   }
 }
 
@@ -940,10 +1108,40 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
     rc = fp.h1_tile == 2 * kFactH1Tile ? launch_tail<2 * kFactH1Tile>(grid, smem, stream, p, fp, Qh, V1, tab)
                                        : launch_tail<kFactH1Tile>(grid, smem, stream, p, fp, Qh, V1, tab);
   }
-  if (rc == B2_OK) {
-    efe_fact_combine_kernel<<<dim3((unsigned)((p.P + 255) / 256), (unsigned)Bn), 256, 0, stream>>>(p, fp, tab, Ht,
-                                                                                                  G);
-    rc = check_launch("efe_ffi factored combine");
+  CombLayout cl{};
+  int64_t c2_bytes = 0;
+  {
+    int64_t npre = 1;
+    for (int t = 0; t + 1 < p.T; ++t) npre *= fp.nu;
+    const int64_t nhg = fp.G + (hterm ? p.F : 0);
+    cl.npre = (int32_t)(npre < (1 << 20) ? npre : (1 << 20));
+    cl.tab_w = (int32_t)fp.tab_stride;
+    cl.ht_w = hterm ? (int32_t)fp.ht_stride : 0;
+    cl.pv = cl.tab_w + cl.ht_w;
+    cl.base = 0;
+    cl.off = (int32_t)(fp.G * npre);
+    cl.hb = cl.off + (int32_t)(fp.G * fp.nu);
+    cl.ua = cl.hb + (hterm ? (int32_t)(p.F * npre) : 0);
+    const int64_t ints = nhg * (npre + fp.nu);
+    c2_bytes = (int64_t)(cl.pv + npre) * 8 + ints * 4;
+    if (npre >= (1 << 20) || c2_bytes > 96 * 1024) c2_bytes = 0;  // too large: the one-phase kernel
+  }
+  if (rc == B2_OK && c2_bytes > 0) {
+    rc = ensure_smem_attr((const void*)efe_fact_combine2_kernel, (int)c2_bytes, kEfeName);
+    if (rc == B2_OK) {
+      efe_fact_combine2_kernel<<<(unsigned)Bn, 256, (int)c2_bytes, stream>>>(p, fp, cl, tab, Ht, G);
+      rc = check_launch("efe_ffi factored combine");
+    }
+  } else if (rc == B2_OK) {
+    // the agent's tables in shared memory when they fit in 96 KB
+    const int64_t words = fp.tab_stride + (hterm ? fp.ht_stride : 0);
+    const int staged = words * 8 <= 96 * 1024 ? 1 : 0;
+    const int smem = staged ? (int)(words * 8) : 0;
+    rc = ensure_smem_attr((const void*)efe_fact_combine_kernel, smem, kEfeName);
+    if (rc == B2_OK) {
+      efe_fact_combine_kernel<<<(unsigned)Bn, 256, smem, stream>>>(p, fp, tab, Ht, G, staged);
+      rc = check_launch("efe_ffi factored combine");
+    }
   }
   cudaError_t fe = cudaFreeAsync(ws, stream);
   if (rc == B2_OK && fe != cudaSuccess) return cuda_fail(kEfeName, fe);
