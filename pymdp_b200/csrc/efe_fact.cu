@@ -212,8 +212,10 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
 // in shared memory), writes V1[h0][row][r] = sum_s0 q_{f0}^{h0}[s0] A and
 // accumulates the depth's linear row sum_row [sum_s0 q xlogx(A)] + C_t[o] V1
 // (information gain, utility).
+// KC <= 4: registers capped for eight resident CTAs per SM (the 256-agent
+// benchmark launch then fits in one wave)
 template <int KC, int NJ>
-__global__ void __launch_bounds__(128) efe_fact_l1_kernel(const __grid_constant__ EfeParams p,
+__global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const __grid_constant__ EfeParams p,
                                                           const __grid_constant__ FactParams fp,
                                                           const float* __restrict__ A, const float* __restrict__ C,
                                                           const float* __restrict__ Qh, float* __restrict__ V1,
