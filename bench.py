@@ -402,9 +402,13 @@ def efe_flops_per_agent(tree: bool = False) -> float:
     return 2.0 * cols * sum(o * K for o in O)
 
 
-# DRAM bytes per agent of the neg-EFE tensor-core kernel (policy-tree mode), from an ncu capture of 160 agents (the
-# W image is read from DRAM once per agent, so traffic scales with agents); None where no capture exists yet.
-EFE_TRAFFIC_PER_AGENT = {"tf32x3": (339.3e6 + 8.8e6) / 160}
+# DRAM bytes per agent of the neg-EFE launch, from ncu captures of 160 agents (A and the per-agent intermediates
+# are touched once per agent, so traffic scales with agents): the tensor-core kernel in policy-tree mode; the
+# factored launch's history, level-1, tail and combine kernels (dram__bytes_read.sum + dram__bytes_write.sum:
+# 3.39 + (136.48 + 29.74) + (54.72 + 0.39) + 5.68 MB; the level-1 intermediates partly spill from L2 and come back
+# in the tail).
+EFE_TRAFFIC_PER_AGENT = {"tf32x3": (339.3e6 + 8.8e6) / 160,
+                         "factored": (3.39e6 + 136.48e6 + 29.74e6 + 54.72e6 + 0.39e6 + 5.68e6) / 160}
 
 
 def efe_bytes_per_agent() -> float:

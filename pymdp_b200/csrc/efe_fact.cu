@@ -81,6 +81,7 @@ struct FactParams {
   int32_t h1_tile;                          // level-2 histories per tail CTA: 8 or 16
   int32_t hist_smem;                        // dynamic shared memory of the history kernel (bytes; 0: global path)
   int32_t bt_off[kEfeMaxF], bt_plane[kEfeMaxF];  // staged B_f^T: plane u at bt_off + u * bt_plane, [k][s]
+  int32_t bt_row[kEfeMaxF];                 // ... with row stride bt_row (odd)
   int32_t qi_sm, qh_sm, qh_words;           // staged qs_init and histories (float offsets); histories per agent
   int8_t mod_order[B2_MAX_MODALITIES];
   FactGroup grp[kFactMaxG];
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
       for (int pr = threadIdx.x; pr < S * S; pr += blockDim.x) {
         const int s = pr / S, k = pr - s * S;
         const float* sp = src + (int64_t)pr * U;
-        float* dp = dst + k * S + s;
+        float* dp = dst + k * fp.bt_row[f] + s;
         if (U == 4 && (reinterpret_cast<uintptr_t>(sp) & 15) == 0) {
           const float4 v = __ldg(reinterpret_cast<const float4*>(sp));
           dp[0] = v.x;
@@ -151,16 +152,17 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
           const int h = e / S, s = e - h * S;
           const int u = h % U;
           const float* q = t == 0 ? q0 + p.qs_off[f] : Qw + fp.qh_off[f][t - 1] + (h / U) * S;
+          const int br = fp.bt_row[f];
           const float* Bt = hsm + fp.bt_off[f] + u * fp.bt_plane[f] + s;
           float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
           int k = 0;
           for (; k + 4 <= S; k += 4) {
-            a0 = fmaf(Bt[k * S], q[k], a0);
-            a1 = fmaf(Bt[(k + 1) * S], q[k + 1], a1);
-            a2 = fmaf(Bt[(k + 2) * S], q[k + 2], a2);
-            a3 = fmaf(Bt[(k + 3) * S], q[k + 3], a3);
+            a0 = fmaf(Bt[k * br], q[k], a0);
+            a1 = fmaf(Bt[(k + 1) * br], q[k + 1], a1);
+            a2 = fmaf(Bt[(k + 2) * br], q[k + 2], a2);
+            a3 = fmaf(Bt[(k + 3) * br], q[k + 3], a3);
           }
-          for (; k < S; ++k) a0 = fmaf(Bt[k * S], q[k], a0);
+          for (; k < S; ++k) a0 = fmaf(Bt[k * br], q[k], a0);
           out[e] = (a0 + a1) + (a2 + a3);
         }
       } else {
@@ -798,9 +800,27 @@ __global__ void __launch_bounds__(256) efe_fact_combine2_kernel(const __grid_con
   int* off = ib + L.off;    // [NG][nu]
   int* hbase = ib + L.hb;   // [F][npre] (history terms)
   int* ua = ib + L.ua;      // [F][nu]
-  for (int i = threadIdx.x; i < L.tab_w; i += blockDim.x) tb[i] = tab[b * fp.tab_stride + i];
-  if (fp.hterm)
-    for (int i = threadIdx.x; i < L.ht_w; i += blockDim.x) hb[i] = Ht[b * fp.ht_stride + i];
+  // staging: 16-byte loads, eight in flight per thread (tab_stride and ht_stride are multiples of 32 doubles)
+  auto stage = [&](double* dst, const double* src, int n) {
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+    double2* d2 = reinterpret_cast<double2*>(dst);
+    const int n2 = n >> 1;
+    for (int i0 = threadIdx.x; i0 < n2; i0 += 8 * blockDim.x) {
+      double2 v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int i = i0 + k * blockDim.x;
+        if (i < n2) v[k] = s2[i];
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int i = i0 + k * blockDim.x;
+        if (i < n2) d2[i] = v[k];
+      }
+    }
+  };
+  stage(tb, tab + b * fp.tab_stride, L.tab_w);
+  if (fp.hterm) stage(hb, Ht + b * fp.ht_stride, L.ht_w);
   // per last action: the factor digits and each group's index offset
   for (int a = threadIdx.x; a < nu; a += blockDim.x) {
     for (int gi = 0; gi < NG; ++gi) {
@@ -901,7 +921,14 @@ bool fact_plan(const EfeParams& p, FactParams* fp, bool with_wA = false, bool wi
   // the history kernel's staging: B_f^T planes, qs_init, every history
   int64_t hw = 0;
   for (int f = 0; f < p.F; ++f) {
-    fp->bt_plane[f] = p.S[f] * p.S[f] + (p.S[f] < 32 ? p.S[f] : 0);
+    // rows of odd stride (the staging writes run down a column); planes of small
+    // factors shifted by S banks, so the half-warps of consecutive histories
+    // (consecutive actions, consecutive planes) read different banks
+    const int S = p.S[f];
+    fp->bt_row[f] = S | 1;
+    int plane = S * fp->bt_row[f];
+    if (S < 32) plane += ((S - plane) % 32 + 32) % 32;
+    fp->bt_plane[f] = plane;
     fp->bt_off[f] = (int32_t)hw;
     hw += (int64_t)p.U[f] * fp->bt_plane[f];
   }
