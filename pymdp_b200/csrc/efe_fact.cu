@@ -578,28 +578,49 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
     }
     __syncthreads();
     const float4* q1s4 = reinterpret_cast<const float4*>(q1s);
-    for (int e = tid; e < nrow * xs; e += kFactTailThreads) {
-      const int n = e / xs, s2 = e - n * xs;
-      float2 acc2[TILE / 2];  // histories (2i, 2i + 1)
+    // two outputs (n, s2) per thread at a time: twice the V1 loads in flight
+    constexpr int kStride = kFactTailThreads;
+    for (int e0 = tid; e0 < nrow * xs; e0 += 2 * kStride) {
+      float2 acc2[2][TILE / 2];  // [output][histories (2i, 2i + 1)]
 #pragma unroll
-      for (int h = 0; h < TILE / 2; ++h) acc2[h] = make_float2(0.f, 0.f);
-      if (s2 < SL) {
-        const float* vr = V1b + (int64_t)n * gr.R + s2;
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int h = 0; h < TILE / 2; ++h) acc2[u][h] = make_float2(0.f, 0.f);
+      const float* vr[2];
+      bool ok[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int e = e0 + u * kStride;
+        const int n = e / xs, s2 = e - n * xs;
+        ok[u] = e < nrow * xs && s2 < SL;
+        vr[u] = V1b + (int64_t)(ok[u] ? n : 0) * gr.R + (ok[u] ? s2 : 0);
+      }
 #pragma unroll 8
-        for (int s1 = 0; s1 < S1; ++s1) {
-          const float v = __ldg(vr + (int64_t)s1 * SL);
-          const float2 vv = make_float2(v, v);
+      for (int s1 = 0; s1 < S1; ++s1) {
+        float v[2];
 #pragma unroll
-          for (int h4 = 0; h4 < TILE / 4; ++h4) {
-            const float4 qa = q1s4[(TILE / 4) * s1 + h4];
-            acc2[2 * h4] = fma2(make_float2(qa.x, qa.y), vv, acc2[2 * h4]);
-            acc2[2 * h4 + 1] = fma2(make_float2(qa.z, qa.w), vv, acc2[2 * h4 + 1]);
+        for (int u = 0; u < 2; ++u) v[u] = ok[u] ? __ldg(vr[u] + (int64_t)s1 * SL) : 0.f;
+#pragma unroll
+        for (int h4 = 0; h4 < TILE / 4; ++h4) {
+          const float4 qa = q1s4[(TILE / 4) * s1 + h4];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const float2 vv = make_float2(v[u], v[u]);
+            acc2[u][2 * h4] = fma2(make_float2(qa.x, qa.y), vv, acc2[u][2 * h4]);
+            acc2[u][2 * h4 + 1] = fma2(make_float2(qa.z, qa.w), vv, acc2[u][2 * h4 + 1]);
           }
         }
       }
 #pragma unroll
-      for (int h = 0; h < TILE; ++h)
-        if (h < nblk) tsm[(h * nrow + n) * xs + s2] = h & 1 ? acc2[h >> 1].y : acc2[h >> 1].x;
+      for (int u = 0; u < 2; ++u) {
+        const int e = e0 + u * kStride;
+        if (e < nrow * xs) {
+          const int n = e / xs, s2 = e - n * xs;
+#pragma unroll
+          for (int h = 0; h < TILE; ++h)
+            if (h < nblk) tsm[(h * nrow + n) * xs + s2] = h & 1 ? acc2[u][h >> 1].y : acc2[u][h >> 1].x;
+        }
+      }
     }
   }
   __syncthreads();
