@@ -15,8 +15,10 @@
 //   q         = softmax(u - mean u), u = ln q + tau (ln A - ln q + past + future)
 //               (mirror_gradient_descent_step :157-168)
 // All of it in FP64 on chip: one CTA per agent; log-likelihoods of the whole
-// window and five [T][S_tot] planes in shared memory; B is read from global
-// memory (L1-resident across iterations).
+// window and five [T][S_tot] planes in shared memory. The agent's transition
+// sequence is staged there too when it fits (as FP64, already log-clipped for
+// VMP, with MMP's row sums for factor-local transitions), else read from
+// global memory; single-parent transitions take a direct S x S path.
 #include <string>
 
 #include "common.cuh"
@@ -48,6 +50,9 @@ struct SeqParams {
   int64_t B_off[kSeqMaxF];
   int64_t B_stride;
   int32_t smem_words;  // doubles of shared memory per agent
+  int32_t bstage;      // 1: B (and MMP row sums) staged in shared memory
+  int32_t b_sm, rs_sm; // their double offsets in the agent's shared memory
+  int32_t rs_off[kSeqMaxF];  // factor f's row sums: rs_sm + rs_off[f] + t * S_f + s
 };
 
 // joint of the marginals q[dep_0] x ... x q[dep_{r-1}] at flattened index k
@@ -104,6 +109,29 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
       }
     }
   for (int j = tid; j < St; j += nthr) lnp[j] = log(fmax((double)__ldg(prior + b * St + j), kMinD));
+  // the transition sequence: FP64 (log-clipped for VMP) in shared memory when it fits
+  const double* bsm = sm + p.b_sm;
+  double* rsm = sm + p.rs_sm;
+  if (p.bstage) {
+    for (int e = tid; e < (int)p.B_stride; e += nthr) {
+      const double bv = (double)__ldg(Bb + e);
+      sm[p.b_sm + e] = p.vmp ? log(fmax(bv, kMinD)) : bv;
+    }
+  }
+  __syncthreads();
+  if (p.bstage && !p.vmp) {
+    // MMP's normaliser of a single-parent transition: the row sum over the parent's states
+    for (int f = 0; f < p.F; ++f) {
+      if (p.brank[f] != 1) continue;
+      const int Sf = p.S[f], Kb = p.Kb[f];
+      for (int e = tid; e < (T - 1) * Sf; e += nthr) {
+        const double* row = bsm + p.B_off[f] + (int64_t)e * Kb;
+        double acc = 0.0;
+        for (int k = 0; k < Kb; ++k) acc += row[k];
+        rsm[p.rs_off[f] + e] = acc;
+      }
+    }
+  }
   for (int e = tid; e < T * St; e += nthr) {
     const int j = e % St;
     int f = 0;
@@ -125,13 +153,33 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
       if (t == 0) {
         fv = lnp[j];
       } else {
-        const float* Bs = Bb + p.B_off[f] + ((int64_t)(t - 1) * p.S[f] + s) * p.Kb[f];
+        const int64_t row = p.B_off[f] + ((int64_t)(t - 1) * p.S[f] + s) * p.Kb[f];
         const double* qp = q + (t - 1) * St;
         double acc = 0.0;
-        for (int k = 0; k < p.Kb[f]; ++k) {
-          const double w = joint_at(qp, p.qs_off, p.S, p.bdep[f], p.brank[f], k, -1);
-          const double bv = (double)__ldg(Bs + k);
-          acc += (p.vmp ? log(fmax(bv, kMinD)) : bv) * w;
+        if (p.bstage && p.brank[f] == 1) {
+          // single parent: M_{t-1}[s, :] . q_{t-1}[parent]
+          const double* Ms = bsm + row;
+          const double* qd = qp + p.qs_off[p.bdep[f][0]];
+          double a1 = 0.0;
+          int k = 0;
+          for (; k + 2 <= p.Kb[f]; k += 2) {
+            acc = fma(Ms[k], qd[k], acc);
+            a1 = fma(Ms[k + 1], qd[k + 1], a1);
+          }
+          if (k < p.Kb[f]) acc = fma(Ms[k], qd[k], acc);
+          acc += a1;
+        } else {
+          for (int k = 0; k < p.Kb[f]; ++k) {
+            const double w = joint_at(qp, p.qs_off, p.S, p.bdep[f], p.brank[f], k, -1);
+            double mv;
+            if (p.bstage) {
+              mv = bsm[row + k];
+            } else {
+              const double bv = (double)__ldg(Bb + row + k);
+              mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
+            }
+            acc += mv * w;
+          }
         }
         fv = p.vmp ? acc : log(fmax(acc, kMinD));
       }
@@ -151,16 +199,33 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
           // stride of f's axis inside B_i's parent index, and the number of other-parent combinations
           int stf = 1;
           for (int x = p.brank[i] - 1; x > pos; --x) stf *= p.S[p.bdep[i][x]];
-          const float* Bi = Bb + p.B_off[i] + (int64_t)t * Si * Kb;
+          const int64_t bi0 = p.B_off[i] + (int64_t)t * Si * Kb;
           double acc = 0.0;
+          if (p.bstage && p.brank[i] == 1) {
+            // single parent (f itself): M_t[si, s], MMP normalised by the row sum
+            const double* Mi = bsm + bi0 + s;
+            const double* rs = rsm + p.rs_off[i] + t * Si;
+            for (int si = 0; si < Si; ++si) {
+              const double mv = Mi[(int64_t)si * Kb];
+              acc += qn[p.qs_off[i] + si] * (p.vmp ? mv : mv / fmax(rs[si], kMinD));
+            }
+            pv += p.vmp ? acc : 0.5 * log(fmax(acc, kMinD));
+            continue;
+          }
+          const float* Bi = Bb + bi0;
           for (int si = 0; si < Si; ++si) {
             // bm[si][s] = sum over the other parents' states of M_i[si, k] prod q (k with digit_pos = s)
             double bm_s = 0.0, bm_sum = 0.0;
             for (int k = 0; k < Kb; ++k) {
               const int dig = (k / stf) % p.S[f];
               const double w = joint_at(qt, p.qs_off, p.S, p.bdep[i], p.brank[i], k, pos);
-              const double bv = (double)__ldg(Bi + (int64_t)si * Kb + k);
-              const double mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
+              double mv;
+              if (p.bstage) {
+                mv = bsm[bi0 + (int64_t)si * Kb + k];
+              } else {
+                const double bv = (double)__ldg(Bi + (int64_t)si * Kb + k);
+                mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
+              }
               if (dig == s) bm_s += mv * w;
               if (!p.vmp) bm_sum += mv * w;
             }
@@ -312,7 +377,17 @@ extern "C" int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, 
   if (words * 8 > 200 * 1024)
     return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": window of " + std::to_string(words * 8) +
                                         " bytes of FP64 state exceeds 200 KB of shared memory");
-  p.smem_words = (int32_t)words;
+  // stage B (and MMP's single-parent row sums) when the whole state stays under 200 KB
+  int64_t rs_words = 0;
+  for (int f = 0; f < F; ++f) {
+    p.rs_off[f] = (int32_t)rs_words;
+    if (p.brank[f] == 1) rs_words += (T - 1) * S[f];
+  }
+  const int64_t staged = words + boff + rs_words;
+  p.bstage = staged * 8 <= 200 * 1024 && boff < (1 << 30) ? 1 : 0;
+  p.b_sm = (int32_t)words;
+  p.rs_sm = (int32_t)(words + boff);
+  p.smem_words = (int32_t)(p.bstage ? staged : words);
   if (A_count != (A_batched ? Bn : 1) * aoff) return bad("A element_count mismatch");
   if (obs_count != Bn * T * (obs_distr ? ooff : M)) return bad("observation element_count mismatch");
   if (B_count != Bn * boff) return bad("B element_count mismatch");
@@ -320,7 +395,7 @@ extern "C" int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, 
   if (Bn == 0) return B2_OK;
   if (!A || (boff > 0 && !B_seq) || !prior || !qs_out) return bad("null buffer");
   if (Bn > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
-  const int bytes = (int)(words * 8);
+  const int bytes = (int)((int64_t)p.smem_words * 8);
   B2_TRY(ensure_smem_attr((const void*)seq_kernel, bytes, op));
   seq_kernel<<<(unsigned)Bn, 256, bytes, (cudaStream_t)stream>>>(p, A, obs_idx, obs_distr, B_seq, prior, qs_out);
   return check_launch(op);
