@@ -407,7 +407,7 @@ def efe_flops_per_agent(tree: bool = False) -> float:
 # factored launch's history, level-1, tail and combine kernels (dram__bytes_read.sum + dram__bytes_write.sum:
 # 3.39 + (136.48 + 29.74) + (54.72 + 0.39) + 5.68 MB; the level-1 intermediates partly spill from L2 and come back
 # in the tail).
-EFE_TRAFFIC_PER_AGENT = {"tf32x3": (339.3e6 + 8.8e6) / 160,
+EFE_TRAFFIC_PER_AGENT = {"tf32x3": (349.50e6 + 9.88e6) / 160,
                          "factored": (3.39e6 + 136.48e6 + 29.74e6 + 54.72e6 + 0.39e6 + 5.68e6) / 160}
 
 
