@@ -49,6 +49,7 @@ constexpr int kFactMaxG = 8;
 constexpr int kFactMaxS = 64;   // largest factor size on the factored path
 constexpr int kFactCombo = 8;   // (depth, history) combinations per level-1 pass over A
 constexpr int kFactTailThreads = 256;
+constexpr int kTailTpi = 2;  // threads per last-level work item (they split its observation rows)
 constexpr int kFactH1Tile = 8;  // level-2 histories per tail CTA (at least; 16 where shared memory allows)
 constexpr int kFactTailSmem = 96 * 1024;  // tail shared memory: level-2 blocks of one h1 tile
 
@@ -457,10 +458,10 @@ __device__ __forceinline__ float obs_term_f(bool ig, float d, bool w, float dw) 
 
 // Last level for HPT columns per thread: rows of X (shared memory, row stride
 // xs, a multiple of 4 floats read as float4, zero past S; [n_obs A rows]
-// [n_w wA rows][1 linear row]); observation rows o = half,
-// half + 2, ..., the linear row by half 0; the two halves of a column meet
-// by one shuffle (lanes 2i, 2i + 1). `act` false: the thread only joins the
-// shuffle.
+// [n_w wA rows][1 linear row]); observation rows o = part, part +
+// kTailTpi, ..., the linear row by part 0; the parts of a column meet by
+// shuffles within their kTailTpi consecutive lanes. `act` false: the thread
+// only joins the shuffles.
 template <int SMAX, bool FULL>
 __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, int n_obs, int n_w, bool ig,
                                            int S, const float2 (&qv)[TailShape<SMAX>::kHpt][SMAX / 2],
@@ -493,7 +494,7 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
   for (int c = 0; c < HPT; ++c) acc[c] = 0.f;
   if (act) {
 #pragma unroll 2
-    for (int o = half; o < n_obs; o += 2) {
+    for (int o = half; o < n_obs; o += kTailTpi) {
       float d[HPT], dw[HPT];
       dot(X + o * xs, d);
       if (n_w) dot(X + (n_obs + o) * xs, dw);
@@ -510,7 +511,8 @@ __device__ __forceinline__ void tail_final(const float* __restrict__ X, int xs, 
 #pragma unroll
   for (int c = 0; c < HPT; ++c) {
     out[c] += (double)acc[c];
-    out[c] += __shfl_xor_sync(0xffffffffu, out[c], 1);
+#pragma unroll
+    for (int x = 1; x < kTailTpi; x <<= 1) out[c] += __shfl_xor_sync(0xffffffffu, out[c], x);
   }
 }
 
@@ -629,8 +631,8 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
   // histories as float4: SL a multiple of 4 and the depth's block 16-byte aligned
   const bool q4 = (SL & 3) == 0 && (fp.qh_off[fl][t] & 3) == 0;
   const int items = nblk * groups;
-  for (int w0 = 0; w0 < items; w0 += kFactTailThreads / 2) {
-    const int w = w0 + (tid >> 1), half = tid & 1;
+  for (int w0 = 0; w0 < items; w0 += kFactTailThreads / kTailTpi) {
+    const int w = w0 + tid / kTailTpi, half = tid % kTailTpi;
     const bool act = w < items;  // uniform per lane pair; every lane still takes part in the shuffle
     const int hb = act ? w / groups : 0, hg = act ? w - hb * groups : 0;
     float2 qv[HPT][SMAX / 2];  // marginals of this thread's histories, zero past SL
