@@ -43,7 +43,32 @@ inline int32_t check_launch(const char* op, uint64_t n = 1) {
 // Opt a kernel into `bytes` of dynamic shared memory once per process/device.
 int32_t ensure_smem_attr(const void* kernel, int bytes, const char* op);
 
+// Programmatic dependent launch: the grid is launched with programmatic stream
+// serialization, so the GPU can schedule it while its predecessor on the
+// stream drains; a kernel launched this way calls grid_dependency_wait() before
+// it reads anything its predecessor wrote (a no-op under an ordinary launch).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...);
+}
+
 // ---------------------------------------------------------------- device
+// Waits until the grids this one depends on have completed and their writes
+// are visible (griddepcontrol.wait; returns at once without a programmatic
+// dependency).
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ float log_stable(float x) { return logf(fmaxf(x, kMinVal)); }
 
 // The same clip with the hardware base-2 logarithm (__logf: two instructions;

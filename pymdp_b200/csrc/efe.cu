@@ -353,6 +353,7 @@ __global__ void efe_inductive_kernel(const __grid_constant__ EfeParams p, const 
 __global__ void __launch_bounds__(256)
     policy_posterior_kernel(const float* __restrict__ G, const float* __restrict__ E, int E_batched,
                             const float* __restrict__ gamma, int gamma_batched, float* __restrict__ q_pi, int P) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   __shared__ float red[32];
   const int64_t b = blockIdx.x;
   const float gm = gamma[gamma_batched ? b : 0];
@@ -393,6 +394,7 @@ template <int EPT>
 __global__ void __launch_bounds__(256)
     policy_posterior_reg_kernel(const float* __restrict__ G, const float* __restrict__ E, int E_batched,
                                 const float* __restrict__ gamma, int gamma_batched, float* __restrict__ q_pi, int P) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   __shared__ float red[32];
   const int64_t b = blockIdx.x;
   const float gm = gamma[gamma_batched ? b : 0];
@@ -444,6 +446,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     select_action_kernel(const float* __restrict__ q_pi, const int32_t* __restrict__ pm, int32_t* __restrict__ action,
                          int P, int T, int F) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   __shared__ float sv[32];
   __shared__ int si[32];
   const int64_t b = blockIdx.x;
@@ -742,17 +745,18 @@ extern "C" int32_t b2_policy_posterior(void* stream, const float* neg_efe, const
   if (!neg_efe || !E || !gamma || !q_pi) return fail(B2_ERR_INVALID_ARGUMENT, "policy_posterior: null buffer");
   if (Bn > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, "policy_posterior: Bn too large");
   cudaStream_t st = (cudaStream_t)stream;
-  if (P <= 256 * 4)
-    policy_posterior_reg_kernel<4><<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi,
-                                                                 (int)P);
-  else if (P <= 256 * 16)
-    policy_posterior_reg_kernel<16><<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi,
-                                                                  (int)P);
-  else if (P <= 256 * 64)
-    policy_posterior_reg_kernel<64><<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi,
-                                                                  (int)P);
-  else
-    policy_posterior_kernel<<<(unsigned)Bn, 256, 0, st>>>(neg_efe, E, E_batched, gamma, gamma_batched, q_pi, (int)P);
+  const dim3 grid((unsigned)Bn), blk(256);
+  const int Pi = (int)P;
+  const cudaError_t e =
+      P <= 256 * 4    ? launch_pdl(policy_posterior_reg_kernel<4>, grid, blk, 0, st, neg_efe, E, E_batched, gamma,
+                                   gamma_batched, q_pi, Pi)
+      : P <= 256 * 16 ? launch_pdl(policy_posterior_reg_kernel<16>, grid, blk, 0, st, neg_efe, E, E_batched, gamma,
+                                   gamma_batched, q_pi, Pi)
+      : P <= 256 * 64 ? launch_pdl(policy_posterior_reg_kernel<64>, grid, blk, 0, st, neg_efe, E, E_batched, gamma,
+                                   gamma_batched, q_pi, Pi)
+                      : launch_pdl(policy_posterior_kernel, grid, blk, 0, st, neg_efe, E, E_batched, gamma,
+                                   gamma_batched, q_pi, Pi);
+  if (e != cudaSuccess) return cuda_fail("policy_posterior", e);
   return check_launch("policy_posterior");
 }
 
@@ -762,8 +766,9 @@ extern "C" int32_t b2_select_action(void* stream, const float* q_pi, const int32
     return fail(B2_ERR_INVALID_ARGUMENT, "select_action: invalid sizes");
   if (Bn == 0) return B2_OK;
   if (!q_pi || !policy_matrix || !action) return fail(B2_ERR_INVALID_ARGUMENT, "select_action: null buffer");
-  select_action_kernel<<<(unsigned)Bn, 256, 0, (cudaStream_t)stream>>>(q_pi, policy_matrix, action, (int)P,
-                                                                        (int)T, (int)F);
+  const cudaError_t e = launch_pdl(select_action_kernel, dim3((unsigned)Bn), dim3(256), 0, (cudaStream_t)stream, q_pi,
+                                   policy_matrix, action, (int)P, (int)T, (int)F);
+  if (e != cudaSuccess) return cuda_fail("select_action", e);
   return check_launch("select_action");
 }
 

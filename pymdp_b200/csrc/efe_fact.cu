@@ -107,6 +107,7 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
                                                             const float* __restrict__ B, float* __restrict__ Qh,
                                                             const float* __restrict__ wB,
                                                             const float* __restrict__ wI, double* __restrict__ Ht) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   extern __shared__ float hsm[];
   const int64_t b = blockIdx.x;
   float* Qb = Qh + b * fp.qh_stride;
@@ -223,6 +224,7 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
                                                           const float* __restrict__ A, const float* __restrict__ C,
                                                           const float* __restrict__ Qh, float* __restrict__ V1,
                                                           const float* __restrict__ wA) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   __shared__ __align__(16) float qsm[KC * kFactMaxS];  // [s][combination]
   const int64_t b = blockIdx.z;
   const int g = blockIdx.y;
@@ -522,6 +524,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
                                                                         const float* __restrict__ Qh,
                                                                         const float* __restrict__ V1,
                                                                         double* __restrict__ tab) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   constexpr int HPT = TailShape<SMAX>::kHpt;
   static_assert(TILE % 4 == 0, "level 2 reads the tile's marginals as float4");
   extern __shared__ float4 tsm4[];  // rank 3: [TILE][nrow][xs] level-2 blocks, then q1 tile [S1][TILE]
@@ -690,6 +693,7 @@ __global__ void __launch_bounds__(256) efe_fact_combine_kernel(const __grid_cons
                                                                const double* __restrict__ tab,
                                                                const double* __restrict__ Ht, float* __restrict__ G,
                                                                int staged) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   extern __shared__ double ctab[];  // staged: tables [tab_stride], then history terms [ht_stride]
   const int64_t b = blockIdx.x;
   const double* tb = tab + b * fp.tab_stride;
@@ -765,14 +769,17 @@ int32_t launch_tail_s(dim3 grid, int smem, cudaStream_t stream, const EfeParams&
     const FactGroup& gr = fp.grp[g];
     full = full && gr.rank >= 2 && gr.S[gr.rank - 1] == SMAX;
   }
+  cudaError_t e;
   if (full) {
     B2_TRY(ensure_smem_attr((const void*)efe_fact_tail_kernel<SMAX, TILE, true>, smem, kEfeName));
-    efe_fact_tail_kernel<SMAX, TILE, true><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+    e = launch_pdl(efe_fact_tail_kernel<SMAX, TILE, true>, grid, dim3(kFactTailThreads), smem, stream, p, fp, Qh, V1,
+                   tab);
   } else {
     B2_TRY(ensure_smem_attr((const void*)efe_fact_tail_kernel<SMAX, TILE, false>, smem, kEfeName));
-    efe_fact_tail_kernel<SMAX, TILE, false><<<grid, kFactTailThreads, smem, stream>>>(p, fp, Qh, V1, tab);
+    e = launch_pdl(efe_fact_tail_kernel<SMAX, TILE, false>, grid, dim3(kFactTailThreads), smem, stream, p, fp, Qh, V1,
+                   tab);
   }
-  return check_launch("efe_ffi factored tail");
+  return e != cudaSuccess ? cuda_fail(kEfeName, e) : check_launch("efe_ffi factored tail");
 }
 
 template <int TILE>
@@ -785,14 +792,15 @@ int32_t launch_tail(dim3 grid, int smem, cudaStream_t stream, const EfeParams& p
 }
 
 template <int KC>
-void launch_l1(int nj, dim3 grid, cudaStream_t stream, const EfeParams& p, const FactParams& fp, const float* A,
-               const float* C, const float* Qh, float* V1, const float* wA) {
+cudaError_t launch_l1(int nj, dim3 grid, cudaStream_t stream, const EfeParams& p, const FactParams& fp, const float* A,
+                      const float* C, const float* Qh, float* V1, const float* wA) {
+  const dim3 blk(128);
   switch (nj) {
-    case 1: efe_fact_l1_kernel<KC, 1><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
-    case 2: efe_fact_l1_kernel<KC, 2><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
-    case 3: efe_fact_l1_kernel<KC, 3><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
-    case 4: efe_fact_l1_kernel<KC, 4><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
-    default: efe_fact_l1_kernel<KC, 0><<<grid, 128, 0, stream>>>(p, fp, A, C, Qh, V1, wA); break;
+    case 1: return launch_pdl(efe_fact_l1_kernel<KC, 1>, grid, blk, 0, stream, p, fp, A, C, Qh, V1, wA);
+    case 2: return launch_pdl(efe_fact_l1_kernel<KC, 2>, grid, blk, 0, stream, p, fp, A, C, Qh, V1, wA);
+    case 3: return launch_pdl(efe_fact_l1_kernel<KC, 3>, grid, blk, 0, stream, p, fp, A, C, Qh, V1, wA);
+    case 4: return launch_pdl(efe_fact_l1_kernel<KC, 4>, grid, blk, 0, stream, p, fp, A, C, Qh, V1, wA);
+    default: return launch_pdl(efe_fact_l1_kernel<KC, 0>, grid, blk, 0, stream, p, fp, A, C, Qh, V1, wA);
   }
 }
 
@@ -812,6 +820,7 @@ __global__ void __launch_bounds__(256) efe_fact_combine2_kernel(const __grid_con
                                                                 const __grid_constant__ FactParams fp,
                                                                 const CombLayout L, const double* __restrict__ tab,
                                                                 const double* __restrict__ Ht, float* __restrict__ G) {
+  grid_dependency_wait();  // inputs come from the previous launch on the stream
   extern __shared__ double csm[];
   const int64_t b = blockIdx.x;
   const int T = p.T, F = p.F, nu = fp.nu, NG = fp.G;
@@ -1127,8 +1136,9 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
   float* V1 = reinterpret_cast<float*>(ws + tab_bytes + ht_bytes + qh_bytes);
   int32_t rc = ensure_smem_attr((const void*)efe_fact_hist_kernel, fp.hist_smem, kEfeName);
   if (rc == B2_OK) {
-    efe_fact_hist_kernel<<<(unsigned)Bn, 256, fp.hist_smem, stream>>>(p, fp, qs, B, Qh, wB, wI, Ht);
-    rc = check_launch("efe_ffi factored histories");
+    const cudaError_t e = launch_pdl(efe_fact_hist_kernel, dim3((unsigned)Bn), dim3(256), fp.hist_smem, stream, p, fp, qs,
+                                     B, Qh, wB, wI, Ht);
+    rc = e != cudaSuccess ? cuda_fail(kEfeName, e) : check_launch("efe_ffi factored histories");
   }
   if (rc == B2_OK) {
     dim3 grid((unsigned)((fp.max_R + 127) / 128), (unsigned)fp.G, (unsigned)Bn);
@@ -1144,15 +1154,11 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
     int nj = fp.grp[0].vec4 && fp.grp[0].S[0] <= 16 ? fp.grp[0].S[0] / 4 : 0;
     for (int g = 1; g < fp.G; ++g)
       if (!fp.grp[g].vec4 || fp.grp[g].S[0] != fp.grp[0].S[0]) nj = 0;
-    if (nc <= 1)
-      launch_l1<1>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
-    else if (nc <= 2)
-      launch_l1<2>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
-    else if (nc <= 4)
-      launch_l1<4>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
-    else
-      launch_l1<kFactCombo>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
-    rc = check_launch("efe_ffi factored level 1");
+    const cudaError_t e = nc <= 1   ? launch_l1<1>(nj, grid, stream, p, fp, A, C, Qh, V1, wA)
+                          : nc <= 2 ? launch_l1<2>(nj, grid, stream, p, fp, A, C, Qh, V1, wA)
+                          : nc <= 4 ? launch_l1<4>(nj, grid, stream, p, fp, A, C, Qh, V1, wA)
+                                    : launch_l1<kFactCombo>(nj, grid, stream, p, fp, A, C, Qh, V1, wA);
+    rc = e != cudaSuccess ? cuda_fail(kEfeName, e) : check_launch("efe_ffi factored level 1");
   }
   if (rc == B2_OK) {
     const dim3 grid((unsigned)fp.max_tiles, (unsigned)Bn);
@@ -1181,8 +1187,9 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
   if (rc == B2_OK && c2_bytes > 0) {
     rc = ensure_smem_attr((const void*)efe_fact_combine2_kernel, (int)c2_bytes, kEfeName);
     if (rc == B2_OK) {
-      efe_fact_combine2_kernel<<<(unsigned)Bn, 256, (int)c2_bytes, stream>>>(p, fp, cl, tab, Ht, G);
-      rc = check_launch("efe_ffi factored combine");
+      const cudaError_t e = launch_pdl(efe_fact_combine2_kernel, dim3((unsigned)Bn), dim3(256), (size_t)c2_bytes, stream,
+                                       p, fp, cl, tab, Ht, G);
+      rc = e != cudaSuccess ? cuda_fail(kEfeName, e) : check_launch("efe_ffi factored combine");
     }
   } else if (rc == B2_OK) {
     // the agent's tables in shared memory when they fit in 96 KB
@@ -1191,8 +1198,9 @@ int32_t launch_efe_fact(const EfeParams& p, int64_t Bn, const float* qs, const f
     const int smem = staged ? (int)(words * 8) : 0;
     rc = ensure_smem_attr((const void*)efe_fact_combine_kernel, smem, kEfeName);
     if (rc == B2_OK) {
-      efe_fact_combine_kernel<<<(unsigned)Bn, 256, smem, stream>>>(p, fp, tab, Ht, G, staged);
-      rc = check_launch("efe_ffi factored combine");
+      const cudaError_t e = launch_pdl(efe_fact_combine_kernel, dim3((unsigned)Bn), dim3(256), (size_t)smem, stream, p, fp,
+                                       tab, Ht, G, staged);
+      rc = e != cudaSuccess ? cuda_fail(kEfeName, e) : check_launch("efe_ffi factored combine");
     }
   }
   cudaError_t fe = cudaFreeAsync(ws, stream);
