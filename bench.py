@@ -1004,6 +1004,12 @@ def run_b200(args, rank, world, local_rank):
                                 f"tail, combine) + q_pi",
                       "bytes_per_launch": efe_bytes_per_agent() * n_agents, "ms_per_launch": efe_ms,
                       "executed_flops_per_launch": efe_factored_flops_per_agent() * n_agents,
+                      # the same launch against the FP32 SIMT peak measured in this run: the tail's
+                      # contractions and entropies make it compute-bound as much as HBM-bound
+                      "executed_tflops": efe_factored_flops_per_agent() * n_agents / (efe_ms * 1e-3) / 1e12,
+                      "fp32_simt_peak_tflops": peaks_run.get("fp32_simt_tflops"),
+                      "fp32_simt_frac": (efe_factored_flops_per_agent() * n_agents / (efe_ms * 1e-3) / 1e12
+                                         / peaks_run["fp32_simt_tflops"]) if "fp32_simt_tflops" in peaks_run else None,
                       "dense_equivalent_flops_per_launch": dense_flops,
                       "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"}
                      if factored else
