@@ -1179,6 +1179,245 @@ __global__ void __launch_bounds__(TEAM, TEAM >= 256 ? 2 : 4) fpi_r3_kernel(const
   }
 }
 
+// ----------------------------------------- rank <= 2, blocks in registers
+// The same models as the rank <= 2 path (every modality on at most two
+// factors of at most 16 states), with each rank-2 group's 16 x 16 FP64 block
+// held in registers across the sweeps: 16 lanes per block, lane i keeping row
+// i and column i (32 doubles), so both of the block's mat-vecs are 16 FMAs per
+// lane on broadcast q values and no block is re-read from shared memory.
+// A sweep: (M) every block lane writes its row message L q_b and column
+// message L^T q_a; barrier; (S) one lane per (factor, state) sums the messages
+// into its factor with the log prior and the 16-lane softmax; barrier.
+// APC agents per CTA, 32-lane aligned, so a warp never spans two agents.
+constexpr int kRRMaxBlocks = 16;
+constexpr int kRRMaxCon = 2 * kRRMaxBlocks;
+
+struct FpiR2Reg {
+  int32_t nb;     // rank-2 blocks per agent
+  int32_t lanes;  // threads per agent: 16 * max(nb, F) rounded up to 32
+  int32_t apc;    // agents per CTA
+  int32_t vec4;   // 16-byte loads of the observed rows (two sources at most per group)
+  int32_t stg_sm, lp_sm, q_sm, row_sm, agent_words;  // per agent: staging blocks | msg (reuses staging) | lp | q | rows
+  int8_t blk_g[kRRMaxBlocks];                       // block -> group
+  int8_t g_blk[kMaxM];                              // group -> block (-1: rank 1)
+  int8_t con_n[kMaxF];                              // messages into factor f: (block, dir) pairs,
+  int8_t con[kMaxF][kRRMaxCon];                     // 2 * block + dir (dir 0: rows -> dep 0, 1: columns -> dep 1)
+};
+
+bool build_r2reg(const FpiParams& p, FpiR2Reg* r) {
+  std::memset(r, 0, sizeof(*r));
+  for (int f = 0; f < p.F; ++f)
+    if (p.S[f] > 16) return false;
+  int nb = 0;
+  for (int g = 0; g < p.G; ++g) {
+    const FpiGroup& gr = p.grp[g];
+    if (gr.rank > 2) return false;
+    if (gr.rank == 1) {
+      r->g_blk[g] = -1;
+      continue;
+    }
+    if (nb >= kRRMaxBlocks) return false;
+    r->g_blk[g] = (int8_t)nb;
+    r->blk_g[nb] = (int8_t)g;
+    const int a = gr.dep[0], b = gr.dep[1];
+    r->con[a][r->con_n[a]++] = (int8_t)(2 * nb);
+    r->con[b][r->con_n[b]++] = (int8_t)(2 * nb + 1);
+    ++nb;
+  }
+  if (nb == 0) return false;
+  r->nb = nb;
+  const int need = 16 * (nb > p.F ? nb : p.F);
+  r->lanes = (need + 31) / 32 * 32;
+  r->apc = r->lanes <= 32 ? 8 : r->lanes <= 64 ? 4 : r->lanes <= 128 ? 2 : 1;
+  r->stg_sm = 0;                                  // [nb][16][17] staging; later [nb][2][16] messages
+  r->lp_sm = nb * 16 * 17;
+  r->q_sm = r->lp_sm + 16 * p.F;
+  r->row_sm = r->q_sm + 16 * p.F;
+  r->agent_words = (r->row_sm + p.M + 1) / 2 * 2;
+  return (int64_t)r->agent_words * 8 * r->apc <= 96 * 1024;
+}
+
+template <bool FUSED, int APC>
+__global__ void __launch_bounds__(256) fpi_r2reg_kernel(const __grid_constant__ FpiParams p,
+                                                        const __grid_constant__ FpiR2Reg r, const FpiIO io) {
+  extern __shared__ __align__(16) double rr_smem[];  // 16-byte aligned: q rows are read as double2
+  __shared__ uint32_t s_ok[APC];
+  __shared__ int8_t s_con[kMaxF][kRRMaxCon];
+  const int lanes = r.lanes;
+  const int slot = threadIdx.x / lanes, t = threadIdx.x - slot * lanes;
+  const int64_t b = (int64_t)blockIdx.x * APC + slot;
+  const bool live = b < io.batch;  // a missing agent's lanes still join every barrier and shuffle
+  double* sm = rr_smem + slot * r.agent_words;
+  double* stg = sm + r.stg_sm;
+  double* lp = sm + r.lp_sm;
+  double* qs = sm + r.q_sm;
+  int64_t* rowoff = reinterpret_cast<int64_t*>(sm + r.row_sm);
+
+  // ---- load phase: observation rows (one lane per modality of the agent's
+  // first warp, M <= 32; an out-of-range observation adds nothing, see
+  // fpi_kernel), log prior and the uniform first q (zero past S_f), zeroed blocks
+  if (t < 32) {
+    bool ok = false;
+    if (live && t < p.M) {
+      int64_t ro = b * io.src_stride + p.src[t].src_off;
+      ok = true;
+      if (FUSED) {
+        const int o = io.obs[b * p.M + t];
+        ok = o >= 0 && o < p.src[t].O;
+        ro += (int64_t)(ok ? o : 0) * p.src[t].K;
+      }
+      rowoff[t] = ro;
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, ok);
+    if (t == 0) s_ok[slot] = bal;
+  }
+  for (int i = threadIdx.x; i < kMaxF * kRRMaxCon; i += blockDim.x) {
+    const int f = i / kRRMaxCon, c = i - f * kRRMaxCon;
+    s_con[f][c] = r.con[f][c];
+  }
+  for (int i = t; i < 16 * p.F; i += lanes) {
+    const int f = i >> 4, s = i & 15;
+    double v = 0.0, q0 = 0.0;
+    if (s < p.S[f]) {
+      if (live) {
+        const float x = __ldg(io.prior + b * p.S_tot + p.lp_off[f] + s);
+        v = FUSED ? log_split(fmaxf(x, kMinVal)) : (double)x;
+      }
+      q0 = 1.0 / p.S[f];
+    }
+    lp[i] = v;
+    qs[i] = q0;
+  }
+  for (int i = t; i < r.nb * 16 * 17; i += lanes) stg[i] = 0.0;
+  __syncthreads();
+  const uint32_t obs_ok = s_ok[slot];
+  // log-likelihoods: rank-2 groups into their zero-padded blocks, rank-1 groups
+  // into the log prior (one group per rank-1 tuple, one thread per state: no race)
+  if (live) {
+    for (int g = 0; g < p.G; ++g) {
+      const FpiGroup& gr = p.grp[g];
+      const int blk = r.g_blk[g];
+      const int S1 = gr.rank == 2 ? p.S[gr.dep[1]] : 1;
+      for (int k0 = t; k0 < gr.K; k0 += 4 * lanes) {
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int si = gr.src_begin; si < gr.src_end; ++si) {
+          const int m = p.src_order[si];
+          if (!((obs_ok >> m) & 1u)) continue;
+          float a[4];
+#pragma unroll
+          for (int x = 0; x < 4; ++x) {
+            const int k = k0 + x * lanes;
+            a[x] = k < gr.K ? __ldg(io.src + rowoff[m] + k) : 1.f;
+          }
+#pragma unroll
+          for (int x = 0; x < 4; ++x) v[x] += FUSED ? log_split(fmaxf(a[x], kMinVal)) : (double)a[x];
+        }
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+          const int k = k0 + x * lanes;
+          if (k < gr.K) {
+            if (blk < 0) {
+              lp[16 * gr.dep[0] + k] += v[x];
+            } else {
+              const int i0 = k / S1, i1 = k - i0 * S1;
+              stg[(blk * 16 + i0) * 17 + i1] = v[x];
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // this lane's block row and column (lane t = 16 blk + i), in registers for every sweep
+  const int blk = t >> 4, ri = t & 15;
+  const bool has_blk = blk < r.nb;
+  double row[16], col[16];
+  int qa_off = 0, qb_off = 0;
+  if (has_blk) {
+    const FpiGroup& gr = p.grp[r.blk_g[blk]];
+    qa_off = 16 * gr.dep[0];
+    qb_off = 16 * gr.dep[1];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      row[j] = stg[(blk * 16 + ri) * 17 + j];
+      col[j] = stg[(blk * 16 + j) * 17 + ri];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) row[j] = col[j] = 0.0;
+  }
+  // this lane's (factor, state) for the softmax
+  const int f = t >> 4, s = t & 15;
+  const int Sf = f < p.F ? p.S[f] : 0;
+  const bool vs = s < Sf;
+  const int fcon = f < p.F ? r.con_n[f] : 0;
+  const int fout = f < p.F ? p.lp_off[f] + s : 0;
+  __syncthreads();  // the staging area now holds the messages [nb][2][16]
+  double* msg = stg;
+
+  // ---- sweeps (Jacobi: every factor uses the previous q)
+  for (int it = 0; it < p.num_iter; ++it) {
+    if (has_blk) {
+      // q rows start at even doubles of a 16-byte aligned buffer: 16-byte loads
+      const double2* qa = reinterpret_cast<const double2*>(qs + qa_off);
+      const double2* qb = reinterpret_cast<const double2*>(qs + qb_off);
+      double ra0 = 0.0, ra1 = 0.0, cb0 = 0.0, cb1 = 0.0;
+#pragma unroll
+      for (int j = 0; j < 16; j += 2) {
+        const double2 vb = qb[j >> 1], va = qa[j >> 1];
+        ra0 = fma(row[j], vb.x, ra0);
+        ra1 = fma(row[j + 1], vb.y, ra1);
+        cb0 = fma(col[j], va.x, cb0);
+        cb1 = fma(col[j + 1], va.y, cb1);
+      }
+      msg[blk * 32 + ri] = ra0 + ra1;       // into dep 0, state ri
+      msg[blk * 32 + 16 + ri] = cb0 + cb1;  // into dep 1, state ri
+    }
+    __syncthreads();
+    double x = 0.0;
+    if (vs) {
+      x = lp[16 * f + s];
+      for (int c = 0; c < fcon; ++c) x += msg[s_con[f][c] * 16 + s];
+    }
+    // 16-lane softmax: the maximum in FP32 (any shift near it cancels), the rest in FP64
+    float mf = vs ? (float)x : -INFINITY;
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) mf = fmaxf(mf, __shfl_xor_sync(0xffffffffu, mf, o));
+    const double e = vs ? exp(x - (double)mf) : 0.0;
+    double sum = e;
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    double inv = (double)__frcp_rn((float)sum);
+    inv = inv * fma(-sum, inv, 2.0);
+    if (it + 1 == p.num_iter) {
+      if (vs && live) io.q_out[b * p.S_tot + fout] = (float)(e * inv);
+    } else if (vs) {
+      qs[16 * f + s] = e * inv;
+    }
+    __syncthreads();
+  }
+}
+
+template <bool FUSED, int APC>
+int32_t launch_r2reg_t(const FpiParams& p, const FpiR2Reg& r, const FpiIO& io, cudaStream_t stream, const char* op) {
+  const int64_t grid = (io.batch + APC - 1) / APC;
+  if (grid > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
+  const int bytes = APC * r.agent_words * 8;
+  B2_TRY(ensure_smem_attr((const void*)fpi_r2reg_kernel<FUSED, APC>, bytes, op));
+  fpi_r2reg_kernel<FUSED, APC><<<(unsigned)grid, APC * r.lanes, bytes, stream>>>(p, r, io);
+  return check_launch(op);
+}
+
+template <bool FUSED>
+int32_t launch_r2reg(const FpiParams& p, const FpiR2Reg& r, const FpiIO& io, cudaStream_t stream, const char* op) {
+  switch (r.apc) {
+    case 8: return launch_r2reg_t<FUSED, 8>(p, r, io, stream, op);
+    case 4: return launch_r2reg_t<FUSED, 4>(p, r, io, stream, op);
+    case 2: return launch_r2reg_t<FUSED, 2>(p, r, io, stream, op);
+    default: return launch_r2reg_t<FUSED, 1>(p, r, io, stream, op);
+  }
+}
+
 // ------------------------------------------------------------ adjoint
 // Reverse pass of the fused-observation FPI for gradients of a loss on the
 // posteriors with respect to the observed A rows and the prior. The reference
@@ -1374,6 +1613,8 @@ int32_t launch_r3(const FpiParams& p, const FpiR3& r, const FpiIO& io, cudaStrea
 template <bool FUSED>
 int32_t launch(const FpiParams& p, const FpiIO& io, cudaStream_t stream, const char* op) {
   if (io.batch <= 0) return B2_OK;
+  FpiR2Reg rr;
+  if (build_r2reg(p, &rr)) return launch_r2reg<FUSED>(p, rr, io, stream, op);
   FpiR2 r2;
   if (build_r2(p, &r2)) {
     bool v4 = (reinterpret_cast<uintptr_t>(io.src) % 16 == 0) && io.src_stride % 4 == 0;
