@@ -445,6 +445,8 @@ FACT_CASES = [
     dict(S=[6, 4, 3], O=[4, 2], U=[5, 1, 2], T=1, A_deps=[[0, 1], [2, 1, 0]], B_deps=[[0], [1], [2]]),
     # a factor no modality observes
     dict(S=[4, 3, 5], O=[6], U=[2, 2, 3], T=2, A_deps=[[2, 0]], B_deps=[[0], [1], [2]]),
+    # 101 observation rows: the tail's level-2 tile falls back to 8 histories (16 would not fit shared memory)
+    dict(S=[16, 16, 16], O=[60, 41], U=[2, 2, 2], T=2, A_deps=[[0, 1, 2]] * 2, B_deps=[[0], [1], [2]]),
 ]
 
 

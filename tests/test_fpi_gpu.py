@@ -74,6 +74,8 @@ SHAPES = [
     ([32, 16, 8], [16, 16, 8, 8, 4], [[0, 1, 2]] * 5),
     ([64, 5, 3], [3, 4, 5], [[0, 1, 2], [2, 0], [1]]),
     ([7, 5, 3, 6], [3, 2, 4, 5], [[0, 1, 2], [1, 3], [3, 2, 0], [2]]),
+    # more X / Y entries than two per thread (64 x 40 = 2560 at 512 threads): the per-sweep addressing path
+    ([64, 32, 8], [3, 2], [[0, 1, 2], [1, 2]]),
 ]
 
 
