@@ -280,11 +280,18 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
     float lin[KC];
 #pragma unroll
     for (int i = 0; i < KC; ++i) lin[i] = 0.f;
+    // each combination's V1 column for this thread (row 0), advanced by R per row
+    float* vcol[KC];
+#pragma unroll
+    for (int i = 0; i < KC; ++i) vcol[i] = Vb + gr.v1_off[ct[i]] + (int64_t)ch[i] * nrow * gr.R + r;
     int row = 0;
     for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
       const EfeModality& md = p.mod[fp.mod_order[mi]];
       const float* Am = A + b * p.A_stride + md.A_off + base;
       const float* Cm = C + b * p.C_stride + md.C_off;
+      const float* crow[KC];  // each combination's C_t row of this modality
+#pragma unroll
+      for (int i = 0; i < KC; ++i) crow[i] = Cm + (int64_t)ct[i] * md.O;
       // NJ > 0: every group's level-1 axis is 4 NJ contiguous, 16-byte aligned
       // entries; the next row's loads are issued before this row's
       // arithmetic, two rows in flight per thread
@@ -365,8 +372,8 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
           if (i < nc) {
             const float vi = i & 1 ? v2[i >> 1].y : v2[i >> 1].x;
             const float wi = i & 1 ? w2[i >> 1].y : w2[i >> 1].x;
-            Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + row) * gr.R + r] = vi;
-            lin[i] += wi + (ut ? __ldg(Cm + (int64_t)ct[i] * md.O + o) * vi : 0.f);
+            vcol[i][(int64_t)row * gr.R] = vi;
+            lin[i] += wi + (ut ? __ldg(crow[i] + o) * vi : 0.f);
           }
         }
       }
@@ -389,13 +396,13 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
           }
 #pragma unroll
           for (int i = 0; i < KC; ++i)
-            if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + wrow) * gr.R + r] = v[i];
+            if (i < nc) vcol[i][(int64_t)wrow * gr.R] = v[i];
         }
       }
     }
 #pragma unroll
     for (int i = 0; i < KC; ++i)
-      if (i < nc) Vb[gr.v1_off[ct[i]] + ((int64_t)ch[i] * nrow + nrow - 1) * gr.R + r] = lin[i];
+      if (i < nc) vcol[i][(int64_t)(nrow - 1) * gr.R] = lin[i];
   }
 }
 
