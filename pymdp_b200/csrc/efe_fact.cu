@@ -150,12 +150,14 @@ __global__ void __launch_bounds__(256) efe_fact_hist_kernel(const __grid_constan
       const int H = ipow(U, t + 1);
       float* out = Qw + fp.qh_off[f][t];
       if (staged) {
+        const float* qprev = t == 0 ? q0 + p.qs_off[f] : Qw + fp.qh_off[f][t - 1];
+        const int br = fp.bt_row[f], plane = fp.bt_plane[f];
+        const float* Bf = hsm + fp.bt_off[f];
         for (int e = threadIdx.x; e < H * S; e += blockDim.x) {
           const int h = e / S, s = e - h * S;
           const int u = h % U;
-          const float* q = t == 0 ? q0 + p.qs_off[f] : Qw + fp.qh_off[f][t - 1] + (h / U) * S;
-          const int br = fp.bt_row[f];
-          const float* Bt = hsm + fp.bt_off[f] + u * fp.bt_plane[f] + s;
+          const float* q = t == 0 ? qprev : qprev + (h / U) * S;
+          const float* Bt = Bf + u * plane + s;
           float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
           int k = 0;
           for (; k + 4 <= S; k += 4) {
@@ -284,14 +286,17 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
     float* vcol[KC];
 #pragma unroll
     for (int i = 0; i < KC; ++i) vcol[i] = Vb + gr.v1_off[ct[i]] + (int64_t)ch[i] * nrow * gr.R + r;
+    const int64_t Rg = gr.R;  // parameter fields read once: a capped register file would re-read them per row
     int row = 0;
     for (int mi = gr.m_begin; mi < gr.m_end; ++mi) {
       const EfeModality& md = p.mod[fp.mod_order[mi]];
+      const int Om = md.O;
+      const int64_t Km = md.K;
       const float* Am = A + b * p.A_stride + md.A_off + base;
       const float* Cm = C + b * p.C_stride + md.C_off;
       const float* crow[KC];  // each combination's C_t row of this modality
 #pragma unroll
-      for (int i = 0; i < KC; ++i) crow[i] = Cm + (int64_t)ct[i] * md.O;
+      for (int i = 0; i < KC; ++i) crow[i] = Cm + (int64_t)ct[i] * Om;
       // NJ > 0: every group's level-1 axis is 4 NJ contiguous, 16-byte aligned
       // entries; the next row's loads are issued before this row's
       // arithmetic, two rows in flight per thread
@@ -303,13 +308,13 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
 #pragma unroll
         for (int j = 0; j < NJ1; ++j) nx[j] = __ldg(A4 + j);
       }
-      for (int o = 0; o < md.O; ++o, ++row) {
+      for (int o = 0; o < Om; ++o, ++row) {
         // combinations (2i, 2i + 1) in the halves of packed accumulators
         constexpr int KP = (KC + 1) / 2;
         float2 v2[KP], w2[KP];
 #pragma unroll
         for (int i = 0; i < KP; ++i) v2[i] = w2[i] = make_float2(0.f, 0.f);
-        const float* Ar = Am + (int64_t)o * md.K;
+        const float* Ar = Am + (int64_t)o * Km;
         auto take = [&](float a, int s) {
           const float xl = ig ? a * log_fast(a) : 0.f;
           const float2 aa = make_float2(a, a), xx = make_float2(xl, xl);
@@ -343,8 +348,8 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
           float4 cu[NJ1];
 #pragma unroll
           for (int j = 0; j < NJ1; ++j) cu[j] = nx[j];
-          if (o + 1 < md.O) {
-            const float4* A4 = reinterpret_cast<const float4*>(Ar + md.K);
+          if (o + 1 < Om) {
+            const float4* A4 = reinterpret_cast<const float4*>(Ar + Km);
 #pragma unroll
             for (int j = 0; j < NJ1; ++j) nx[j] = __ldg(A4 + j);
           }
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
           if (i < nc) {
             const float vi = i & 1 ? v2[i >> 1].y : v2[i >> 1].x;
             const float wi = i & 1 ? w2[i >> 1].y : w2[i >> 1].x;
-            vcol[i][(int64_t)row * gr.R] = vi;
+            vcol[i][(int64_t)row * Rg] = vi;
             lin[i] += wi + (ut ? __ldg(crow[i] + o) * vi : 0.f);
           }
         }
@@ -396,13 +401,13 @@ __global__ void __launch_bounds__(128, KC <= 4 ? 8 : 4) efe_fact_l1_kernel(const
           }
 #pragma unroll
           for (int i = 0; i < KC; ++i)
-            if (i < nc) vcol[i][(int64_t)wrow * gr.R] = v[i];
+            if (i < nc) vcol[i][(int64_t)wrow * Rg] = v[i];
         }
       }
     }
 #pragma unroll
     for (int i = 0; i < KC; ++i)
-      if (i < nc) vcol[i][(int64_t)(nrow - 1) * gr.R] = lin[i];
+      if (i < nc) vcol[i][(int64_t)(nrow - 1) * Rg] = lin[i];
   }
 }
 
