@@ -595,6 +595,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
     }
     __syncthreads();
     const float4* q1s4 = reinterpret_cast<const float4*>(q1s);
+    const int64_t R1 = gr.R;  // read once (the loop below runs near the register cap)
     // two outputs (n, s2) per thread at a time: twice the V1 loads in flight
     constexpr int kStride = kFactTailThreads;
     for (int e0 = tid; e0 < nrow * xs; e0 += 2 * kStride) {
@@ -610,7 +611,7 @@ __global__ void __launch_bounds__(kFactTailThreads) efe_fact_tail_kernel(const _
         const int e = e0 + u * kStride;
         const int n = e / xs, s2 = e - n * xs;
         ok[u] = e < nrow * xs && s2 < SL;
-        vr[u] = V1b + (int64_t)(ok[u] ? n : 0) * gr.R + (ok[u] ? s2 : 0);
+        vr[u] = V1b + (int64_t)(ok[u] ? n : 0) * R1 + (ok[u] ? s2 : 0);
       }
 #pragma unroll 8
       for (int s1 = 0; s1 < S1; ++s1) {
