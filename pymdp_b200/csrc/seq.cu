@@ -52,6 +52,8 @@ struct SeqParams {
   int32_t smem_words;  // doubles of shared memory per agent
   int32_t bstage;      // 1: B (and MMP row sums) staged in shared memory
   int32_t b_sm, rs_sm; // their double offsets in the agent's shared memory
+  int32_t kbp[kSeqMaxF];      // staged rows of factor f: odd stride Kb | 1 (conflict-free when lanes walk rows)
+  int64_t bsm_off[kSeqMaxF];  // factor f's staged block past b_sm: [(T - 1) S_f][kbp]
   int32_t rs_off[kSeqMaxF];  // factor f's row sums: rs_sm + rs_off[f] + t * S_f + s
 };
 
@@ -113,9 +115,14 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
   const double* bsm = sm + p.b_sm;
   double* rsm = sm + p.rs_sm;
   if (p.bstage) {
-    for (int e = tid; e < (int)p.B_stride; e += nthr) {
-      const double bv = (double)__ldg(Bb + e);
-      sm[p.b_sm + e] = p.vmp ? log(fmax(bv, kMinD)) : bv;
+    for (int f = 0; f < p.F; ++f) {
+      const int Kb = p.Kb[f], kbp = p.kbp[f];
+      const int n = (T - 1) * p.S[f] * Kb;
+      for (int e = tid; e < n; e += nthr) {
+        const int row = e / Kb, k = e - row * Kb;
+        const double bv = (double)__ldg(Bb + p.B_off[f] + e);
+        sm[p.b_sm + p.bsm_off[f] + (int64_t)row * kbp + k] = p.vmp ? log(fmax(bv, kMinD)) : bv;
+      }
     }
   }
   __syncthreads();
@@ -125,7 +132,7 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
       if (p.brank[f] != 1) continue;
       const int Sf = p.S[f], Kb = p.Kb[f];
       for (int e = tid; e < (T - 1) * Sf; e += nthr) {
-        const double* row = bsm + p.B_off[f] + (int64_t)e * Kb;
+        const double* row = bsm + p.bsm_off[f] + (int64_t)e * p.kbp[f];
         double acc = 0.0;
         for (int k = 0; k < Kb; ++k) acc += row[k];
         rsm[p.rs_off[f] + e] = acc;
@@ -154,11 +161,12 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
         fv = lnp[j];
       } else {
         const int64_t row = p.B_off[f] + ((int64_t)(t - 1) * p.S[f] + s) * p.Kb[f];
+        const int64_t srow = p.bsm_off[f] + ((int64_t)(t - 1) * p.S[f] + s) * p.kbp[f];  // staged copy
         const double* qp = q + (t - 1) * St;
         double acc = 0.0;
         if (p.bstage && p.brank[f] == 1) {
           // single parent: M_{t-1}[s, :] . q_{t-1}[parent]
-          const double* Ms = bsm + row;
+          const double* Ms = bsm + srow;
           const double* qd = qp + p.qs_off[p.bdep[f][0]];
           double a1 = 0.0;
           int k = 0;
@@ -173,7 +181,7 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
             const double w = joint_at(qp, p.qs_off, p.S, p.bdep[f], p.brank[f], k, -1);
             double mv;
             if (p.bstage) {
-              mv = bsm[row + k];
+              mv = bsm[srow + k];
             } else {
               const double bv = (double)__ldg(Bb + row + k);
               mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
@@ -203,10 +211,10 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
           double acc = 0.0;
           if (p.bstage && p.brank[i] == 1) {
             // single parent (f itself): M_t[si, s], MMP normalised by the row sum
-            const double* Mi = bsm + bi0 + s;
+            const double* Mi = bsm + p.bsm_off[i] + (int64_t)t * Si * p.kbp[i] + s;
             const double* rs = rsm + p.rs_off[i] + t * Si;
             for (int si = 0; si < Si; ++si) {
-              const double mv = Mi[(int64_t)si * Kb];
+              const double mv = Mi[(int64_t)si * p.kbp[i]];
               acc += qn[p.qs_off[i] + si] * (p.vmp ? mv : mv / fmax(rs[si], kMinD));
             }
             pv += p.vmp ? acc : 0.5 * log(fmax(acc, kMinD));
@@ -221,7 +229,7 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
               const double w = joint_at(qt, p.qs_off, p.S, p.bdep[i], p.brank[i], k, pos);
               double mv;
               if (p.bstage) {
-                mv = bsm[bi0 + (int64_t)si * Kb + k];
+                mv = bsm[p.bsm_off[i] + ((int64_t)t * Si + si) * p.kbp[i] + k];
               } else {
                 const double bv = (double)__ldg(Bi + (int64_t)si * Kb + k);
                 mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
@@ -378,15 +386,18 @@ extern "C" int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, 
     return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": window of " + std::to_string(words * 8) +
                                         " bytes of FP64 state exceeds 200 KB of shared memory");
   // stage B (and MMP's single-parent row sums) when the whole state stays under 200 KB
-  int64_t rs_words = 0;
+  int64_t rs_words = 0, bs_words = 0;
   for (int f = 0; f < F; ++f) {
     p.rs_off[f] = (int32_t)rs_words;
     if (p.brank[f] == 1) rs_words += (T - 1) * S[f];
+    p.kbp[f] = p.Kb[f] | 1;
+    p.bsm_off[f] = bs_words;
+    bs_words += (T - 1) * S[f] * p.kbp[f];
   }
-  const int64_t staged = words + boff + rs_words;
+  const int64_t staged = words + bs_words + rs_words;
   p.bstage = staged * 8 <= 200 * 1024 && boff < (1 << 30) ? 1 : 0;
   p.b_sm = (int32_t)words;
-  p.rs_sm = (int32_t)(words + boff);
+  p.rs_sm = (int32_t)(words + bs_words);
   p.smem_words = (int32_t)(p.bstage ? staged : words);
   if (A_count != (A_batched ? Bn : 1) * aoff) return bad("A element_count mismatch");
   if (obs_count != Bn * T * (obs_distr ? ooff : M)) return bad("observation element_count mismatch");
