@@ -254,9 +254,35 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
         for (int x = 0; x < p.rank[m]; ++x)
           if (p.dep[m][x] == f) pos = x;
         if (pos < 0) continue;
+        const double* L = ll + t * ll_step + p.ll_off[m];
+        if (p.rank[m] == 1) {
+          lv += L[s];
+          continue;
+        }
+        if (p.rank[m] == 2) {
+          // one other parent o: a row (f first) or a column (f second) of L_m against q_t[o]
+          const int o = p.dep[m][1 - pos], n = p.S[o];
+          const double* qo = qt + p.qs_off[o];
+          if (pos == 0) {
+            // lanes walk rows of length n: each starts at its own column so they spread over the banks
+            const double* Lr = L + s * n;
+            int c = s % n;
+            double acc = 0.0;
+            for (int x = 0; x < n; ++x) {
+              acc = fma(Lr[c], qo[c], acc);
+              c = c + 1 == n ? 0 : c + 1;
+            }
+            lv += acc;
+          } else {
+            const int Sf = p.S[f];
+            double acc = 0.0;
+            for (int x = 0; x < n; ++x) acc = fma(L[x * Sf + s], qo[x], acc);
+            lv += acc;
+          }
+          continue;
+        }
         int stf = 1;
         for (int x = p.rank[m] - 1; x > pos; --x) stf *= p.S[p.dep[m][x]];
-        const double* L = ll + t * ll_step + p.ll_off[m];
         const int Km = p.K[m], outer = Km / (stf * p.S[f]);
         for (int a = 0; a < outer; ++a)
           for (int c = 0; c < stf; ++c) {
@@ -286,10 +312,14 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
 #pragma unroll
       for (int x = 16; x > 0; x >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, x));
       double z = 0.0;
-      for (int s = lane; s < n; s += 32) z += exp(lnq[o + s] - mean - mx);
+      for (int s = lane; s < n; s += 32) {
+        const double ev = exp(lnq[o + s] - mean - mx);
+        lnq[o + s] = ev;  // kept for the normalisation below (lnq is rebuilt from q next iteration)
+        z += ev;
+      }
 #pragma unroll
       for (int x = 16; x > 0; x >>= 1) z += __shfl_xor_sync(0xffffffffu, z, x);
-      for (int s = lane; s < n; s += 32) q[o + s] = exp(lnq[o + s] - mean - mx) / z;
+      for (int s = lane; s < n; s += 32) q[o + s] = lnq[o + s] / z;
     }
     __syncthreads();
   }
