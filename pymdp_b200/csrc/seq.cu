@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
   }
   __syncthreads();
   if (p.bstage && !p.vmp) {
-    // MMP's normaliser of a single-parent transition: the row sum over the parent's states
+    // MMP's normaliser of a single-parent transition: the reciprocal of the row sum over the parent's states
     for (int f = 0; f < p.F; ++f) {
       if (p.brank[f] != 1) continue;
       const int Sf = p.S[f], Kb = p.Kb[f];
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
         const double* row = bsm + p.bsm_off[f] + (int64_t)e * p.kbp[f];
         double acc = 0.0;
         for (int k = 0; k < Kb; ++k) acc += row[k];
-        rsm[p.rs_off[f] + e] = acc;
+        rsm[p.rs_off[f] + e] = 1.0 / fmax(acc, kMinD);
       }
     }
   }
@@ -144,11 +144,11 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
     int f = 0;
     while (f + 1 < p.F && j >= p.qs_off[f + 1]) ++f;
     q[e] = 1.0 / p.S[f];
+    lnq[e] = log(q[e]);  // afterwards the softmax below writes log q directly
   }
   __syncthreads();
 
   for (int it = 0; it < p.num_iter; ++it) {
-    for (int e = tid; e < T * St; e += nthr) lnq[e] = log(fmax(q[e], kMinD));
     // messages and marginal log-likelihoods from the previous iterate
     for (int e = tid; e < T * St; e += nthr) {
       const int t = e / St, j = e - t * St;
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
             const double* rs = rsm + p.rs_off[i] + t * Si;
             for (int si = 0; si < Si; ++si) {
               const double mv = Mi[(int64_t)si * p.kbp[i]];
-              acc += qn[p.qs_off[i] + si] * (p.vmp ? mv : mv / fmax(rs[si], kMinD));
+              acc += qn[p.qs_off[i] + si] * (p.vmp ? mv : mv * rs[si]);
             }
             pv += p.vmp ? acc : 0.5 * log(fmax(acc, kMinD));
             continue;
@@ -314,12 +314,17 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
       double z = 0.0;
       for (int s = lane; s < n; s += 32) {
         const double ev = exp(lnq[o + s] - mean - mx);
-        lnq[o + s] = ev;  // kept for the normalisation below (lnq is rebuilt from q next iteration)
+        fut[o + s] = ev;  // the messages of (t, f) are spent: keep the exponentials there
         z += ev;
       }
 #pragma unroll
       for (int x = 16; x > 0; x >>= 1) z += __shfl_xor_sync(0xffffffffu, z, x);
-      for (int s = lane; s < n; s += 32) q[o + s] = lnq[o + s] / z;
+      // q = e / z, and log(max(q, eps)) for the next iteration as (u - mean - max) - log z, clipped at log eps
+      const double rz = 1.0 / z, lz = log(z), lmin = log(kMinD);
+      for (int s = lane; s < n; s += 32) {
+        q[o + s] = fut[o + s] * rz;
+        lnq[o + s] = fmax(lnq[o + s] - mean - mx - lz, lmin);
+      }
     }
     __syncthreads();
   }
