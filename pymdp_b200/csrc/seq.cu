@@ -16,10 +16,13 @@
 //               (mirror_gradient_descent_step :157-168)
 // All of it in FP64 on chip: one CTA per agent; log-likelihoods of the whole
 // window and five [T][S_tot] planes in shared memory. The agent's transition
-// sequence is staged there too when it fits (as FP64, already log-clipped for
-// VMP, with MMP's row sums for factor-local transitions), else read from
-// global memory; single-parent transitions take a direct S x S path.
+// sequence is staged there too when it fits (VMP: log-clipped FP64; MMP: the
+// FP32 entries themselves, with reciprocal row sums for factor-local
+// transitions), else read from global memory; single-parent transitions take
+// a direct S x S path.
+#include <algorithm>
 #include <string>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -71,7 +74,9 @@ __device__ __forceinline__ double joint_at(const double* __restrict__ q, const i
   return w;
 }
 
-__global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqParams p, const float* __restrict__ A,
+// VMP stages log B in FP64; MMP stages B itself, whose FP32 entries a float holds exactly (half the shared memory)
+template <bool VMP>
+__global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ SeqParams p, const float* __restrict__ A,
                                                   const int32_t* __restrict__ obs_idx,
                                                   const float* __restrict__ obs_distr, const float* __restrict__ B,
                                                   const float* __restrict__ prior, float* __restrict__ qs_out) {
@@ -112,7 +117,8 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
     }
   for (int j = tid; j < St; j += nthr) lnp[j] = log(fmax((double)__ldg(prior + b * St + j), kMinD));
   // the transition sequence: FP64 (log-clipped for VMP) in shared memory when it fits
-  const double* bsm = sm + p.b_sm;
+  using BT = typename std::conditional<VMP, double, float>::type;
+  const BT* bsm = reinterpret_cast<const BT*>(sm + p.b_sm);
   double* rsm = sm + p.rs_sm;
   if (p.bstage) {
     for (int f = 0; f < p.F; ++f) {
@@ -121,20 +127,21 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
       for (int e = tid; e < n; e += nthr) {
         const int row = e / Kb, k = e - row * Kb;
         const double bv = (double)__ldg(Bb + p.B_off[f] + e);
-        sm[p.b_sm + p.bsm_off[f] + (int64_t)row * kbp + k] = p.vmp ? log(fmax(bv, kMinD)) : bv;
+        reinterpret_cast<BT*>(sm + p.b_sm)[p.bsm_off[f] + (int64_t)row * kbp + k] =
+            VMP ? (BT)log(fmax(bv, kMinD)) : (BT)bv;
       }
     }
   }
   __syncthreads();
-  if (p.bstage && !p.vmp) {
+  if (p.bstage && !VMP) {
     // MMP's normaliser of a single-parent transition: the reciprocal of the row sum over the parent's states
     for (int f = 0; f < p.F; ++f) {
       if (p.brank[f] != 1) continue;
       const int Sf = p.S[f], Kb = p.Kb[f];
       for (int e = tid; e < (T - 1) * Sf; e += nthr) {
-        const double* row = bsm + p.bsm_off[f] + (int64_t)e * p.kbp[f];
+        const BT* row = bsm + p.bsm_off[f] + (int64_t)e * p.kbp[f];
         double acc = 0.0;
-        for (int k = 0; k < Kb; ++k) acc += row[k];
+        for (int k = 0; k < Kb; ++k) acc += (double)row[k];
         rsm[p.rs_off[f] + e] = 1.0 / fmax(acc, kMinD);
       }
     }
@@ -166,32 +173,32 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
         double acc = 0.0;
         if (p.bstage && p.brank[f] == 1) {
           // single parent: M_{t-1}[s, :] . q_{t-1}[parent]
-          const double* Ms = bsm + srow;
+          const BT* Ms = bsm + srow;
           const double* qd = qp + p.qs_off[p.bdep[f][0]];
           double a1 = 0.0;
           int k = 0;
           for (; k + 2 <= p.Kb[f]; k += 2) {
-            acc = fma(Ms[k], qd[k], acc);
-            a1 = fma(Ms[k + 1], qd[k + 1], a1);
+            acc = fma((double)Ms[k], qd[k], acc);
+            a1 = fma((double)Ms[k + 1], qd[k + 1], a1);
           }
-          if (k < p.Kb[f]) acc = fma(Ms[k], qd[k], acc);
+          if (k < p.Kb[f]) acc = fma((double)Ms[k], qd[k], acc);
           acc += a1;
         } else {
           for (int k = 0; k < p.Kb[f]; ++k) {
             const double w = joint_at(qp, p.qs_off, p.S, p.bdep[f], p.brank[f], k, -1);
             double mv;
             if (p.bstage) {
-              mv = bsm[srow + k];
+              mv = (double)bsm[srow + k];
             } else {
               const double bv = (double)__ldg(Bb + row + k);
-              mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
+              mv = VMP ? log(fmax(bv, kMinD)) : bv;
             }
             acc += mv * w;
           }
         }
-        fv = p.vmp ? acc : log(fmax(acc, kMinD));
+        fv = VMP ? acc : log(fmax(acc, kMinD));
       }
-      if (!p.vmp && t < T - 1) fv *= 0.5;
+      if (!VMP && t < T - 1) fv *= 0.5;
       fut[e] = fv;
       // past message: transitions out of step t into every factor i whose B depends on f
       double pv = 0.0;
@@ -211,13 +218,13 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
           double acc = 0.0;
           if (p.bstage && p.brank[i] == 1) {
             // single parent (f itself): M_t[si, s], MMP normalised by the row sum
-            const double* Mi = bsm + p.bsm_off[i] + (int64_t)t * Si * p.kbp[i] + s;
+            const BT* Mi = bsm + p.bsm_off[i] + (int64_t)t * Si * p.kbp[i] + s;
             const double* rs = rsm + p.rs_off[i] + t * Si;
             for (int si = 0; si < Si; ++si) {
-              const double mv = Mi[(int64_t)si * p.kbp[i]];
-              acc += qn[p.qs_off[i] + si] * (p.vmp ? mv : mv * rs[si]);
+              const double mv = (double)Mi[(int64_t)si * p.kbp[i]];
+              acc += qn[p.qs_off[i] + si] * (VMP ? mv : mv * rs[si]);
             }
-            pv += p.vmp ? acc : 0.5 * log(fmax(acc, kMinD));
+            pv += VMP ? acc : 0.5 * log(fmax(acc, kMinD));
             continue;
           }
           const float* Bi = Bb + bi0;
@@ -229,20 +236,20 @@ __global__ void __launch_bounds__(256) seq_kernel(const __grid_constant__ SeqPar
               const double w = joint_at(qt, p.qs_off, p.S, p.bdep[i], p.brank[i], k, pos);
               double mv;
               if (p.bstage) {
-                mv = bsm[p.bsm_off[i] + ((int64_t)t * Si + si) * p.kbp[i] + k];
+                mv = (double)bsm[p.bsm_off[i] + ((int64_t)t * Si + si) * p.kbp[i] + k];
               } else {
                 const double bv = (double)__ldg(Bi + (int64_t)si * Kb + k);
-                mv = p.vmp ? log(fmax(bv, kMinD)) : bv;
+                mv = VMP ? log(fmax(bv, kMinD)) : bv;
               }
               if (dig == s) bm_s += mv * w;
-              if (!p.vmp) bm_sum += mv * w;
+              if (!VMP) bm_sum += mv * w;
             }
-            if (p.vmp)
+            if (VMP)
               acc += qn[p.qs_off[i] + si] * bm_s;
             else
               acc += qn[p.qs_off[i] + si] * (bm_s / fmax(bm_sum, kMinD));
           }
-          pv += p.vmp ? acc : 0.5 * log(fmax(acc, kMinD));
+          pv += VMP ? acc : 0.5 * log(fmax(acc, kMinD));
         }
       }
       past[e] = pv;
@@ -421,14 +428,15 @@ extern "C" int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, 
     return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": window of " + std::to_string(words * 8) +
                                         " bytes of FP64 state exceeds 200 KB of shared memory");
   // stage B (and MMP's single-parent row sums) when the whole state stays under 200 KB
-  int64_t rs_words = 0, bs_words = 0;
+  int64_t rs_words = 0, bs_elems = 0;
   for (int f = 0; f < F; ++f) {
     p.rs_off[f] = (int32_t)rs_words;
     if (p.brank[f] == 1) rs_words += (T - 1) * S[f];
     p.kbp[f] = p.Kb[f] | 1;
-    p.bsm_off[f] = bs_words;
-    bs_words += (T - 1) * S[f] * p.kbp[f];
+    p.bsm_off[f] = bs_elems;
+    bs_elems += (T - 1) * S[f] * p.kbp[f];
   }
+  const int64_t bs_words = vmp ? bs_elems : (bs_elems + 1) / 2;  // MMP stages floats
   const int64_t staged = words + bs_words + rs_words;
   p.bstage = staged * 8 <= 200 * 1024 && boff < (1 << 30) ? 1 : 0;
   p.b_sm = (int32_t)words;
@@ -442,7 +450,10 @@ extern "C" int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, 
   if (!A || (boff > 0 && !B_seq) || !prior || !qs_out) return bad("null buffer");
   if (Bn > 0x7fffffff) return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": batch too large");
   const int bytes = (int)((int64_t)p.smem_words * 8);
-  B2_TRY(ensure_smem_attr((const void*)seq_kernel, bytes, op));
-  seq_kernel<<<(unsigned)Bn, 256, bytes, (cudaStream_t)stream>>>(p, A, obs_idx, obs_distr, B_seq, prior, qs_out);
+  const auto kernel = vmp ? seq_kernel<true> : seq_kernel<false>;
+  B2_TRY(ensure_smem_attr((const void*)kernel, bytes, op));
+  // one thread per (step, state) up to 256: idle warps would only hold registers that other agents could use
+  const int nthr = (int)std::min<int64_t>(256, (T * St + 31) / 32 * 32);
+  kernel<<<(unsigned)Bn, nthr, bytes, (cudaStream_t)stream>>>(p, A, obs_idx, obs_distr, B_seq, prior, qs_out);
   return check_launch(op);
 }
