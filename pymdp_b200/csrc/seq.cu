@@ -76,13 +76,17 @@ __device__ __forceinline__ double joint_at(const double* __restrict__ q, const i
 
 // VMP stages log B in FP64; MMP stages B itself, whose FP32 entries a float holds exactly (half the shared memory)
 template <bool VMP>
-__global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ SeqParams p, const float* __restrict__ A,
+__global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ SeqParams p, const float* __restrict__ A,
                                                   const int32_t* __restrict__ obs_idx,
                                                   const float* __restrict__ obs_distr, const float* __restrict__ B,
                                                   const float* __restrict__ prior, float* __restrict__ qs_out) {
   extern __shared__ double sm[];
+  __shared__ SeqParams ps;  // fields indexed per lane read from here, not from the constant bank
   const int64_t b = blockIdx.x;
   const int T = p.T, St = p.S_tot, nthr = blockDim.x, tid = threadIdx.x;
+  static_assert(sizeof(SeqParams) % 4 == 0, "SeqParams copies in words");
+  for (int w = tid; w < (int)(sizeof(SeqParams) / 4); w += nthr)
+    reinterpret_cast<int32_t*>(&ps)[w] = reinterpret_cast<const int32_t*>(&p)[w];
   const int ll_step = p.ll_off[p.M];
   double* ll = sm;                      // [T][ll_step]
   double* q = ll + (int64_t)T * ll_step;  // [T][St]
@@ -155,37 +159,39 @@ __global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ Seq
   }
   __syncthreads();
 
+  const double lmin = log(kMinD);
   for (int it = 0; it < p.num_iter; ++it) {
-    // messages and marginal log-likelihoods from the previous iterate
+    // messages and marginal log-likelihoods from the previous iterate; factor-indexed fields come from
+    // the shared copy of the parameters (lanes of a warp sit in different factors)
     for (int e = tid; e < T * St; e += nthr) {
       const int t = e / St, j = e - t * St;
       int f = 0;
-      while (f + 1 < p.F && j >= p.qs_off[f + 1]) ++f;
-      const int s = j - p.qs_off[f];
+      while (f + 1 < p.F && j >= ps.qs_off[f + 1]) ++f;
+      const int s = j - ps.qs_off[f];
       // future message
       double fv;
       if (t == 0) {
         fv = lnp[j];
       } else {
-        const int64_t row = p.B_off[f] + ((int64_t)(t - 1) * p.S[f] + s) * p.Kb[f];
-        const int64_t srow = p.bsm_off[f] + ((int64_t)(t - 1) * p.S[f] + s) * p.kbp[f];  // staged copy
+        const int64_t row = ps.B_off[f] + ((int64_t)(t - 1) * ps.S[f] + s) * ps.Kb[f];
+        const int64_t srow = ps.bsm_off[f] + ((int64_t)(t - 1) * ps.S[f] + s) * ps.kbp[f];  // staged copy
         const double* qp = q + (t - 1) * St;
         double acc = 0.0;
-        if (p.bstage && p.brank[f] == 1) {
+        if (p.bstage && ps.brank[f] == 1) {
           // single parent: M_{t-1}[s, :] . q_{t-1}[parent]
           const BT* Ms = bsm + srow;
-          const double* qd = qp + p.qs_off[p.bdep[f][0]];
+          const double* qd = qp + ps.qs_off[ps.bdep[f][0]];
           double a1 = 0.0;
           int k = 0;
-          for (; k + 2 <= p.Kb[f]; k += 2) {
+          for (; k + 2 <= ps.Kb[f]; k += 2) {
             acc = fma((double)Ms[k], qd[k], acc);
             a1 = fma((double)Ms[k + 1], qd[k + 1], a1);
           }
-          if (k < p.Kb[f]) acc = fma((double)Ms[k], qd[k], acc);
+          if (k < ps.Kb[f]) acc = fma((double)Ms[k], qd[k], acc);
           acc += a1;
         } else {
-          for (int k = 0; k < p.Kb[f]; ++k) {
-            const double w = joint_at(qp, p.qs_off, p.S, p.bdep[f], p.brank[f], k, -1);
+          for (int k = 0; k < ps.Kb[f]; ++k) {
+            const double w = joint_at(qp, ps.qs_off, ps.S, ps.bdep[f], ps.brank[f], k, -1);
             double mv;
             if (p.bstage) {
               mv = (double)bsm[srow + k];
@@ -199,7 +205,6 @@ __global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ Seq
         fv = VMP ? acc : log(fmax(acc, kMinD));
       }
       if (!VMP && t < T - 1) fv *= 0.5;
-      fut[e] = fv;
       // past message: transitions out of step t into every factor i whose B depends on f
       double pv = 0.0;
       if (t < T - 1) {
@@ -207,22 +212,22 @@ __global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ Seq
         const double* qn = q + (t + 1) * St;
         for (int i = 0; i < p.F; ++i) {
           int pos = -1;
-          for (int x = 0; x < p.brank[i]; ++x)
-            if (p.bdep[i][x] == f) pos = x;
+          for (int x = 0; x < ps.brank[i]; ++x)
+            if (ps.bdep[i][x] == f) pos = x;
           if (pos < 0) continue;
-          const int Si = p.S[i], Kb = p.Kb[i];
+          const int Si = ps.S[i], Kb = ps.Kb[i];
           // stride of f's axis inside B_i's parent index, and the number of other-parent combinations
           int stf = 1;
-          for (int x = p.brank[i] - 1; x > pos; --x) stf *= p.S[p.bdep[i][x]];
-          const int64_t bi0 = p.B_off[i] + (int64_t)t * Si * Kb;
+          for (int x = ps.brank[i] - 1; x > pos; --x) stf *= ps.S[ps.bdep[i][x]];
+          const int64_t bi0 = ps.B_off[i] + (int64_t)t * Si * Kb;
           double acc = 0.0;
-          if (p.bstage && p.brank[i] == 1) {
+          if (p.bstage && ps.brank[i] == 1) {
             // single parent (f itself): M_t[si, s], MMP normalised by the row sum
-            const BT* Mi = bsm + p.bsm_off[i] + (int64_t)t * Si * p.kbp[i] + s;
-            const double* rs = rsm + p.rs_off[i] + t * Si;
+            const BT* Mi = bsm + ps.bsm_off[i] + (int64_t)t * Si * ps.kbp[i] + s;
+            const double* rs = rsm + ps.rs_off[i] + t * Si;
             for (int si = 0; si < Si; ++si) {
-              const double mv = (double)Mi[(int64_t)si * p.kbp[i]];
-              acc += qn[p.qs_off[i] + si] * (VMP ? mv : mv * rs[si]);
+              const double mv = (double)Mi[(int64_t)si * ps.kbp[i]];
+              acc += qn[ps.qs_off[i] + si] * (VMP ? mv : mv * rs[si]);
             }
             pv += VMP ? acc : 0.5 * log(fmax(acc, kMinD));
             continue;
@@ -232,11 +237,11 @@ __global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ Seq
             // bm[si][s] = sum over the other parents' states of M_i[si, k] prod q (k with digit_pos = s)
             double bm_s = 0.0, bm_sum = 0.0;
             for (int k = 0; k < Kb; ++k) {
-              const int dig = (k / stf) % p.S[f];
-              const double w = joint_at(qt, p.qs_off, p.S, p.bdep[i], p.brank[i], k, pos);
+              const int dig = (k / stf) % ps.S[f];
+              const double w = joint_at(qt, ps.qs_off, ps.S, ps.bdep[i], ps.brank[i], k, pos);
               double mv;
               if (p.bstage) {
-                mv = (double)bsm[p.bsm_off[i] + ((int64_t)t * Si + si) * p.kbp[i] + k];
+                mv = (double)bsm[ps.bsm_off[i] + ((int64_t)t * Si + si) * ps.kbp[i] + k];
               } else {
                 const double bv = (double)__ldg(Bi + (int64_t)si * Kb + k);
                 mv = VMP ? log(fmax(bv, kMinD)) : bv;
@@ -245,31 +250,30 @@ __global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ Seq
               if (!VMP) bm_sum += mv * w;
             }
             if (VMP)
-              acc += qn[p.qs_off[i] + si] * bm_s;
+              acc += qn[ps.qs_off[i] + si] * bm_s;
             else
-              acc += qn[p.qs_off[i] + si] * (bm_s / fmax(bm_sum, kMinD));
+              acc += qn[ps.qs_off[i] + si] * (bm_s / fmax(bm_sum, kMinD));
           }
           pv += VMP ? acc : 0.5 * log(fmax(acc, kMinD));
         }
       }
-      past[e] = pv;
       // marginal log-likelihood of factor f's state s at step t
       double lv = 0.0;
       const double* qt = q + t * St;
       for (int m = 0; m < p.M; ++m) {
         int pos = -1;
-        for (int x = 0; x < p.rank[m]; ++x)
-          if (p.dep[m][x] == f) pos = x;
+        for (int x = 0; x < ps.rank[m]; ++x)
+          if (ps.dep[m][x] == f) pos = x;
         if (pos < 0) continue;
-        const double* L = ll + t * ll_step + p.ll_off[m];
-        if (p.rank[m] == 1) {
+        const double* L = ll + t * ll_step + ps.ll_off[m];
+        if (ps.rank[m] == 1) {
           lv += L[s];
           continue;
         }
-        if (p.rank[m] == 2) {
+        if (ps.rank[m] == 2) {
           // one other parent o: a row (f first) or a column (f second) of L_m against q_t[o]
-          const int o = p.dep[m][1 - pos], n = p.S[o];
-          const double* qo = qt + p.qs_off[o];
+          const int o = ps.dep[m][1 - pos], n = ps.S[o];
+          const double* qo = qt + ps.qs_off[o];
           if (pos == 0) {
             // lanes walk rows of length n: each starts at its own column so they spread over the banks
             const double* Lr = L + s * n;
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ Seq
             }
             lv += acc;
           } else {
-            const int Sf = p.S[f];
+            const int Sf = ps.S[f];
             double acc = 0.0;
             for (int x = 0; x < n; ++x) acc = fma(L[x * Sf + s], qo[x], acc);
             lv += acc;
@@ -289,49 +293,45 @@ __global__ void __launch_bounds__(256, 5) seq_kernel(const __grid_constant__ Seq
           continue;
         }
         int stf = 1;
-        for (int x = p.rank[m] - 1; x > pos; --x) stf *= p.S[p.dep[m][x]];
-        const int Km = p.K[m], outer = Km / (stf * p.S[f]);
+        for (int x = ps.rank[m] - 1; x > pos; --x) stf *= ps.S[ps.dep[m][x]];
+        const int Km = ps.K[m], outer = Km / (stf * ps.S[f]);
         for (int a = 0; a < outer; ++a)
           for (int c = 0; c < stf; ++c) {
-            const int k = (a * p.S[f] + s) * stf + c;
-            lv += L[k] * joint_at(qt, p.qs_off, p.S, p.dep[m], p.rank[m], k, pos);
+            const int k = (a * ps.S[f] + s) * stf + c;
+            lv += L[k] * joint_at(qt, ps.qs_off, ps.S, ps.dep[m], ps.rank[m], k, pos);
           }
       }
-      la[e] = lv;
+      // mirror-descent step (pymdp/algos.py:157-168): u = ln q + tau (ll - ln q + past + future)
+      fut[e] = lnq[e] + p.tau * (lv - lnq[e] + pv + fv);
     }
     __syncthreads();
-    // mirror-descent step and softmax, one warp per (t, f)
-    const int warp = tid >> 5, lane = tid & 31, nw = nthr >> 5;
-    for (int tf = warp; tf < T * p.F; tf += nw) {
-      const int t = tf / p.F, f = tf - t * p.F;
-      const int o = t * St + p.qs_off[f], n = p.S[f];
+    // softmax of every (t, f) segment, one thread per entry: each reads its segment's mean and max back
+    // from shared memory, then the segment's exponentials for the normaliser
+    for (int e = tid; e < T * St; e += nthr) {
+      const int t = e / St, j = e - t * St;
+      int f = 0;
+      while (f + 1 < p.F && j >= ps.qs_off[f + 1]) ++f;
+      const int o = t * St + ps.qs_off[f], n = ps.S[f];
       double sum = 0.0;
-      for (int s = lane; s < n; s += 32) {
-        const double u = lnq[o + s] + p.tau * (la[o + s] - lnq[o + s] + past[o + s] + fut[o + s]);
-        lnq[o + s] = u;  // this warp alone owns (t, f): reuse the plane
-        sum += u;
-      }
-#pragma unroll
-      for (int x = 16; x > 0; x >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, x);
+      for (int x = 0; x < n; ++x) sum += fut[o + x];
       const double mean = sum / n;
       double mx = -INFINITY;
-      for (int s = lane; s < n; s += 32) mx = fmax(mx, lnq[o + s] - mean);
-#pragma unroll
-      for (int x = 16; x > 0; x >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, x));
+      for (int x = 0; x < n; ++x) mx = fmax(mx, fut[o + x] - mean);
+      const double d = fut[e] - mean - mx;
+      past[e] = d;
+      la[e] = exp(d);
+    }
+    __syncthreads();
+    // q = e / z, and log(max(q, eps)) for the next iteration as d - log z, clipped at log eps
+    for (int e = tid; e < T * St; e += nthr) {
+      const int t = e / St, j = e - t * St;
+      int f = 0;
+      while (f + 1 < p.F && j >= ps.qs_off[f + 1]) ++f;
+      const int o = t * St + ps.qs_off[f], n = ps.S[f];
       double z = 0.0;
-      for (int s = lane; s < n; s += 32) {
-        const double ev = exp(lnq[o + s] - mean - mx);
-        fut[o + s] = ev;  // the messages of (t, f) are spent: keep the exponentials there
-        z += ev;
-      }
-#pragma unroll
-      for (int x = 16; x > 0; x >>= 1) z += __shfl_xor_sync(0xffffffffu, z, x);
-      // q = e / z, and log(max(q, eps)) for the next iteration as (u - mean - max) - log z, clipped at log eps
-      const double rz = 1.0 / z, lz = log(z), lmin = log(kMinD);
-      for (int s = lane; s < n; s += 32) {
-        q[o + s] = fut[o + s] * rz;
-        lnq[o + s] = fmax(lnq[o + s] - mean - mx - lz, lmin);
-      }
+      for (int x = 0; x < n; ++x) z += la[o + x];
+      q[e] = la[e] / z;
+      lnq[e] = fmax(past[e] - log(z), lmin);
     }
     __syncthreads();
   }
