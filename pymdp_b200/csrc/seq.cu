@@ -95,6 +95,9 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
   double* past = fut + T * St;
   double* la = past + T * St;
   double* lnp = la + T * St;  // [St]
+  // entry x of a pass over the window, factor-major (f, t, s), so that a warp's lanes share one factor:
+  // f << 26 | t << 13 | s (t and s < 8192 since 5 T S_tot doubles fit in shared memory, F <= 16)
+  int32_t* emap = reinterpret_cast<int32_t*>(lnp + St);
   const float* Ab = A + b * p.A_stride;
   const float* Bb = B + b * p.B_stride;
 
@@ -150,6 +153,12 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
       }
     }
   }
+  for (int x = tid; x < T * St; x += nthr) {
+    int f = 0;
+    while (f + 1 < p.F && x >= T * p.qs_off[f + 1]) ++f;
+    const int local = x - T * p.qs_off[f], t = local / p.S[f];
+    emap[x] = f << 26 | t << 13 | (local - t * p.S[f]);
+  }
   for (int e = tid; e < T * St; e += nthr) {
     const int j = e % St;
     int f = 0;
@@ -162,12 +171,11 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
   const double lmin = log(kMinD);
   for (int it = 0; it < p.num_iter; ++it) {
     // messages and marginal log-likelihoods from the previous iterate; factor-indexed fields come from
-    // the shared copy of the parameters (lanes of a warp sit in different factors)
-    for (int e = tid; e < T * St; e += nthr) {
-      const int t = e / St, j = e - t * St;
-      int f = 0;
-      while (f + 1 < p.F && j >= ps.qs_off[f + 1]) ++f;
-      const int s = j - ps.qs_off[f];
+    // the shared copy of the parameters (a warp's lanes can straddle two factors)
+    for (int ei = tid; ei < T * St; ei += nthr) {
+      const int32_t em = emap[ei];
+      const int f = em >> 26, t = (em >> 13) & 8191, j = ps.qs_off[f] + (em & 8191), e = t * St + j;
+      const int s = em & 8191;
       // future message
       double fv;
       if (t == 0) {
@@ -307,10 +315,9 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
     __syncthreads();
     // softmax of every (t, f) segment, one thread per entry: each reads its segment's mean and max back
     // from shared memory, then the segment's exponentials for the normaliser
-    for (int e = tid; e < T * St; e += nthr) {
-      const int t = e / St, j = e - t * St;
-      int f = 0;
-      while (f + 1 < p.F && j >= ps.qs_off[f + 1]) ++f;
+    for (int ei = tid; ei < T * St; ei += nthr) {
+      const int32_t em = emap[ei];
+      const int f = em >> 26, t = (em >> 13) & 8191, j = ps.qs_off[f] + (em & 8191), e = t * St + j;
       const int o = t * St + ps.qs_off[f], n = ps.S[f];
       double sum = 0.0;
       for (int x = 0; x < n; ++x) sum += fut[o + x];
@@ -323,10 +330,9 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
     }
     __syncthreads();
     // q = e / z, and log(max(q, eps)) for the next iteration as d - log z, clipped at log eps
-    for (int e = tid; e < T * St; e += nthr) {
-      const int t = e / St, j = e - t * St;
-      int f = 0;
-      while (f + 1 < p.F && j >= ps.qs_off[f + 1]) ++f;
+    for (int ei = tid; ei < T * St; ei += nthr) {
+      const int32_t em = emap[ei];
+      const int f = em >> 26, t = (em >> 13) & 8191, j = ps.qs_off[f] + (em & 8191), e = t * St + j;
       const int o = t * St + ps.qs_off[f], n = ps.S[f];
       double z = 0.0;
       for (int x = 0; x < n; ++x) z += la[o + x];
@@ -423,7 +429,7 @@ extern "C" int32_t b2_sequence_infer(void* stream, int32_t vmp, const float* A, 
     boff += (T - 1) * S[f] * K;
   }
   p.B_stride = boff;
-  const int64_t words = T * ll + 5 * T * St + St;
+  const int64_t words = T * ll + 5 * T * St + St + (T * St + 1) / 2;  // + the int32 entry map
   if (words * 8 > 200 * 1024)
     return fail(B2_ERR_UNSUPPORTED, std::string(op) + ": window of " + std::to_string(words * 8) +
                                         " bytes of FP64 state exceeds 200 KB of shared memory");
