@@ -60,6 +60,13 @@ struct SeqParams {
   int32_t rs_off[kSeqMaxF];  // factor f's row sums: rs_sm + rs_off[f] + t * S_f + s
 };
 
+// 4-byte asynchronous copy global -> shared (no register round trip); completed by cp_async_wait_all
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // joint of the marginals q[dep_0] x ... x q[dep_{r-1}] at flattened index k
 // (row-major), skipping position `skip` (-1: none).
 __device__ __forceinline__ double joint_at(const double* __restrict__ q, const int32_t* qs_off, const int32_t* S,
@@ -101,45 +108,104 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
   const float* Ab = A + b * p.A_stride;
   const float* Bb = B + b * p.B_stride;
 
+  __syncthreads();  // ps
+  // Every global read of the prologue is issued before any is waited on: cp.async for the observed rows
+  // of A (index observations) and for MMP's transitions, plain loads for the rest.
+  const int nll = T * ll_step;
+  // raw A entries of the observed rows, 4 bytes each, in the upper half of the ll plane shifted by 8 bytes
+  // (the last 8 run into q, written only after they are read): converting batch by batch in place, the
+  // doubles of a batch land on raw entries of that batch or earlier ones only
+  float* raw = reinterpret_cast<float*>(ll) + nll + 2;
+  if (!p.distr) {
+    for (int e = tid; e < nll; e += nthr) {
+      const int t = e / ll_step, r = e - t * ll_step;
+      int m = 0;
+      while (m + 1 < p.M && r >= ps.ll_off[m + 1]) ++m;
+      const int o = __ldg(obs_idx + (b * T + t) * p.M + m), Om = ps.O[m];
+      // an index outside [0, O) selects no row: jnp clamps it (A_m[o_m]), as here
+      const int oc = o < 0 ? (o + Om < 0 ? 0 : o + Om) : (o >= Om ? Om - 1 : o);
+      cp_async4(raw + e, Ab + ps.A_off[m] + (int64_t)oc * ps.K[m] + (r - ps.ll_off[m]));
+    }
+  }
+  // the transition sequence in shared memory when it fits: VMP's log-clipped in FP64, MMP's entries as they are
+  using BT = typename std::conditional<VMP, double, float>::type;
+  const BT* bsm = reinterpret_cast<const BT*>(sm + p.b_sm);
+  double* rsm = sm + p.rs_sm;
+  if (p.bstage && !VMP) {
+    for (int f = 0; f < p.F; ++f) {
+      const int Kb = p.Kb[f], kbp = p.kbp[f];
+      const int n = (T - 1) * p.S[f] * Kb;
+      const float* Bf = Bb + p.B_off[f];
+      BT* dst = reinterpret_cast<BT*>(sm + p.b_sm) + p.bsm_off[f];
+      for (int e = tid; e < n; e += nthr) {
+        const int row = e / Kb;
+        cp_async4(dst + (int64_t)row * kbp + (e - row * Kb), Bf + e);
+      }
+    }
+  }
   // log-likelihoods of every step (compute_log_likelihood_single_modality, pymdp/maths.py:214-238)
-  for (int t = 0; t < T; ++t)
-    for (int m = 0; m < p.M; ++m) {
-      const float* Am = Ab + p.A_off[m];
-      for (int k = tid; k < p.K[m]; k += nthr) {
-        double v = 0.0;
-        if (p.distr) {
-          const float* o = obs_distr + (b * T + t) * p.O_off[p.M] + p.O_off[m];
+  if (p.distr) {
+    for (int t = 0; t < T; ++t)
+      for (int m = 0; m < p.M; ++m) {
+        const float* Am = Ab + p.A_off[m];
+        const float* o = obs_distr + (b * T + t) * p.O_off[p.M] + p.O_off[m];
+        for (int k = tid; k < p.K[m]; k += nthr) {
+          double v = 0.0;
           for (int x = 0; x < p.O[m]; ++x) {
             const double ov = (double)o[x];
             if (ov != 0.0) v += ov * log(fmax((double)__ldg(Am + (int64_t)x * p.K[m] + k), kMinD));
           }
-        } else {
-          const int o = obs_idx[(b * T + t) * p.M + m];
-          // an index outside [0, O) selects no row: jnp clamps it (A_m[o_m]), as here
-          const int oc = o < 0 ? (o + p.O[m] < 0 ? 0 : o + p.O[m]) : (o >= p.O[m] ? p.O[m] - 1 : o);
-          v = log(fmax((double)__ldg(Am + (int64_t)oc * p.K[m] + k), kMinD));
+          ll[t * ll_step + p.ll_off[m] + k] = v;
         }
-        ll[t * ll_step + p.ll_off[m] + k] = v;
       }
-    }
+  }
   for (int j = tid; j < St; j += nthr) lnp[j] = log(fmax((double)__ldg(prior + b * St + j), kMinD));
-  // the transition sequence: FP64 (log-clipped for VMP) in shared memory when it fits
-  using BT = typename std::conditional<VMP, double, float>::type;
-  const BT* bsm = reinterpret_cast<const BT*>(sm + p.b_sm);
-  double* rsm = sm + p.rs_sm;
-  if (p.bstage) {
+  if (p.bstage && VMP) {
     for (int f = 0; f < p.F; ++f) {
       const int Kb = p.Kb[f], kbp = p.kbp[f];
       const int n = (T - 1) * p.S[f] * Kb;
-      for (int e = tid; e < n; e += nthr) {
-        const int row = e / Kb, k = e - row * Kb;
-        const double bv = (double)__ldg(Bb + p.B_off[f] + e);
-        reinterpret_cast<BT*>(sm + p.b_sm)[p.bsm_off[f] + (int64_t)row * kbp + k] =
-            VMP ? (BT)log(fmax(bv, kMinD)) : (BT)bv;
+      const float* Bf = Bb + p.B_off[f];
+      BT* dst = reinterpret_cast<BT*>(sm + p.b_sm) + p.bsm_off[f];
+      for (int e0 = tid; e0 < n; e0 += 4 * nthr) {
+        float bv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) bv[u] = e0 + u * nthr < n ? __ldg(Bf + e0 + u * nthr) : 0.0f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = e0 + u * nthr;
+          if (e < n) {
+            const int row = e / Kb, k = e - row * Kb;
+            dst[(int64_t)row * kbp + k] = (BT)log(fmax((double)bv[u], kMinD));
+          }
+        }
       }
     }
   }
+  for (int x = tid; x < T * St; x += nthr) {
+    int f = 0;
+    while (f + 1 < p.F && x >= T * p.qs_off[f + 1]) ++f;
+    const int local = x - T * p.qs_off[f], t = local / p.S[f];
+    emap[x] = f << 26 | t << 13 | (local - t * p.S[f]);
+  }
+  cp_async_wait_all();
   __syncthreads();
+  if (!p.distr) {
+    // in place, four entries per thread per batch: the whole batch read before any of it is written
+    for (int base = 0; base < nll; base += 4 * nthr) {
+      float av[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = base + u * nthr + tid;
+        av[u] = e < nll ? raw[e] : 1.0f;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = base + u * nthr + tid;
+        if (e < nll) ll[e] = log(fmax((double)av[u], kMinD));
+      }
+    }
+  }
   if (p.bstage && !VMP) {
     // MMP's normaliser of a single-parent transition: the reciprocal of the row sum over the parent's states
     for (int f = 0; f < p.F; ++f) {
@@ -153,12 +219,6 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
       }
     }
   }
-  for (int x = tid; x < T * St; x += nthr) {
-    int f = 0;
-    while (f + 1 < p.F && x >= T * p.qs_off[f + 1]) ++f;
-    const int local = x - T * p.qs_off[f], t = local / p.S[f];
-    emap[x] = f << 26 | t << 13 | (local - t * p.S[f]);
-  }
   for (int e = tid; e < T * St; e += nthr) {
     const int j = e % St;
     int f = 0;
@@ -167,7 +227,6 @@ __global__ void __launch_bounds__(256, 4) seq_kernel(const __grid_constant__ Seq
     lnq[e] = log(q[e]);  // afterwards the softmax below writes log q directly
   }
   __syncthreads();
-
   const double lmin = log(kMinD);
   for (int it = 0; it < p.num_iter; ++it) {
     // messages and marginal log-likelihoods from the previous iterate; factor-indexed fields come from

@@ -76,3 +76,28 @@ def test_batched_sequence_inference_matches_oracle(case, kind, distr):
                                distr_obs=distr)
         for f in range(len(S)):
             np.testing.assert_allclose(qs[f][b].cpu().numpy(), ref[f], rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("kind", ["mmp", "vmp"])
+def test_prepared_plan_reruns_equal_the_list_call(kind):
+    """seq.prepare packs the inputs once; every run() of the plan gives the
+    list-taking call's posteriors bitwise (the same kernel on the same
+    values)."""
+    from pymdp_b200 import seq
+    rng = np.random.default_rng(29)
+    S, O, T, batch = [4, 3], [5, 2], 5, 7
+    A_deps, B_deps = [[0, 1], [1]], [[0], [1, 0]]
+    A = [cuda(np.stack([_cols(rng, (O[m],) + tuple(S[d] for d in A_deps[m])) for _ in range(batch)]))
+         for m in range(len(O))]
+    B = [cuda(np.stack([np.moveaxis(_cols(rng, (S[f], T - 1) + tuple(S[d] for d in B_deps[f]), 0.5), 1, 0)
+                        for _ in range(batch)])) for f in range(len(S))]
+    prior = [cuda(np.stack([_cols(rng, (s,), 1.0) for _ in range(batch)])) for s in S]
+    obs = [cuda(rng.integers(0, O[m], size=(batch, T)), torch.int32) for m in range(len(O))]
+    fn = seq.run_mmp if kind == "mmp" else seq.run_vmp
+    want = fn(A, B, obs, prior, A_deps, B_deps, num_iter=6, tau=0.5, distr_obs=False)
+    plan = seq.prepare(kind == "vmp", A, B, obs, prior, A_deps, B_deps, num_iter=6, tau=0.5, distr_obs=False)
+    for _ in range(3):
+        got = plan.run()
+        torch.cuda.synchronize()
+        for f in range(len(S)):
+            assert torch.equal(got[f], want[f])
