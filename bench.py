@@ -917,24 +917,28 @@ def run_b200(args, rank, world, local_rank):
     launches = args.steps * per_step_launches
     ms = sum(a.elapsed_time(b) for a, b in evs)
     efe_ms = sum(a.elapsed_time(b) for a, b in efe_ev) / len(efe_ev)
-    # e2e through the public API (Agent.capture_step -> GraphedAgentStep.step)
-    # with host buffers: pinned observations and prior in, the action out
-    estep = agent.capture_step(warmup=1)
+    # e2e through the public API (Agent.capture_pipeline -> PipelinedAgentStep.step) with host buffers: every
+    # step copies pinned observations and prior in and its action out, on copy streams beside the compute of
+    # the neighbouring steps; the timed region starts before the first input copy and ends after the last
+    # action has landed in host memory
+    pipe = agent.capture_pipeline(warmup=1)
     obs_h = torch.as_tensor(obs).pin_memory()
     prior_h = torch.cat([torch.as_tensor(d).reshape(n_agents, -1) for d in D], dim=1).pin_memory()
     act_h = torch.empty((n_agents, len(S)), dtype=torch.int32).pin_memory()
 
     def e2e_step():
-        _, _, _, act = estep.step(obs_h, prior_h)
-        act_h.copy_(act, non_blocking=True)
+        pipe.step(obs_h, prior_h, act_h)
 
     for _ in range(args.warmup):
         e2e_step()
+    pipe.drain()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
+    pipe.begin(ev0)
     for _ in range(args.steps):
         e2e_step()
+    pipe.drain()
     ev1.record(stream)
     barrier()
     e2e_ms = ev0.elapsed_time(ev1)
@@ -1008,7 +1012,10 @@ def run_b200(args, rank, world, local_rank):
                    "efe_algorithm": args.efe, "precision": "fp32 (factored)" if factored else agent.precision, "l2": "flushed (256 MiB write) between timed steps",
                    "parallelism": f"agents sharded over {world} GPU(s), no collective"},
         "e2e": {"value": total_agents * args.steps / (e2e_ms * 1e-3), "unit": "agent-steps/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "form": "Agent.capture_pipeline: each step's copies on copy streams beside the neighbouring steps' "
+                        "compute (two buffer sets); the region ends after the last action reached host memory",
+                "l2": "not flushed between steps: the model's A (218 MB at 256 agents) exceeds the 126 MB L2"},
         "gpu_launches": int(launches),
         "step_form": {"timed": "CUDA graph replay (belief update | policies + action)",
                       "kernels_per_step": per_step_launches, "eager_ms_per_step": eager_ms,

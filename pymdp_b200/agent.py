@@ -271,6 +271,13 @@ class Agent:
         (two with ``split``: the belief update, then policies and action)."""
         return GraphedAgentStep(self, warmup, split)
 
+    def capture_pipeline(self, warmup: int = 2) -> "PipelinedAgentStep":
+        """The graphed agent step over two buffer sets that successive steps
+        alternate between (``PipelinedAgentStep``): a step's host inputs are
+        copied in, and its action copied out, on copy streams while the GPU
+        computes the neighbouring steps."""
+        return PipelinedAgentStep(self, warmup)
+
     def update_empirical_prior(self, action, qs: Sequence[torch.Tensor]):
         """``pymdp/agent.py:825-851`` for ``inference_algo="fpi"``: the prior of
         the next ``infer_states``, ``compute_expected_state`` of the latest
@@ -458,8 +465,14 @@ class GraphedAgentStep:
         arrays; ``empirical_prior``: a list of F ``(batch, S_f)`` arrays or
         one flat ``(batch, sum S)`` tensor. Omitted inputs keep the buffers'
         contents."""
-        # tensors (host or device) are copied straight into the buffers, on the
-        # current stream; a pinned host tensor makes that an asynchronous copy
+        self.load(observations, empirical_prior)
+        for g in self.graphs:
+            g.replay()
+        return self.qs, self.q_pi, self.G, self.action
+
+    def load(self, observations=None, empirical_prior=None):
+        """Copy new inputs into the static buffers on the current stream
+        (asynchronous from pinned host memory); omitted inputs are kept."""
         if observations is not None:
             if isinstance(observations, (list, tuple)):
                 obs = torch.stack([torch.as_tensor(x).reshape(-1) for x in observations], dim=-1)
@@ -474,6 +487,75 @@ class GraphedAgentStep:
                                                        non_blocking=True)
             else:
                 self.prior.copy_(torch.as_tensor(empirical_prior).reshape(self.prior.shape), non_blocking=True)
-        for g in self.graphs:
+
+
+class PipelinedAgentStep:
+    """Successive agent steps from host buffers with the copies off the
+    compute stream: two ``GraphedAgentStep`` buffer sets, used by steps k and
+    k + 1 in turn. Step k copies its observations and prior from host memory
+    into set k % 2 on an input stream, which waits only until step k - 2 has
+    finished with that set. It then replays the set's graphs on the current
+    stream once the copy has landed, and copies the action back on an output
+    stream. So the input copy of step k + 1 and the output copy of step k run
+    while the GPU computes. Every step still makes both copies. ``step``
+    returns the set's static outputs, which step k + 2 overwrites.
+    Deterministic action selection only (as ``GraphedAgentStep``). Host
+    inputs are read by an asynchronous copy: they must not change until the
+    step's outputs are ready.
+
+    ``begin(event)`` makes the copy streams wait for ``event`` (recorded on
+    the compute stream, e.g. the start of a timed region), and ``drain()``
+    makes the current stream wait for every copy issued so far, so that an
+    event recorded after it covers them."""
+
+    def __init__(self, agent: Agent, warmup: int = 2):
+        dev = agent.device
+        self.sets = [GraphedAgentStep(agent, warmup) for _ in range(2)]
+        self.in_stream, self.out_stream = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        self._in_ready = [torch.cuda.Event() for _ in range(2)]  # inputs of the set's current step landed
+        self._done = [torch.cuda.Event() for _ in range(2)]      # the set's step computed: inputs free, outputs ready
+        self._out_done = [torch.cuda.Event() for _ in range(2)]  # the set's action copied out: action buffer free
+        self._k = 0
+
+    def begin(self, event: torch.cuda.Event) -> None:
+        self.in_stream.wait_event(event)
+        self.out_stream.wait_event(event)
+
+    def step(self, observations, empirical_prior, action_out: torch.Tensor | None = None):
+        """One step from host (pinned) or device inputs: ``observations``
+        ``(batch, M)``, ``empirical_prior`` flat ``(batch, sum S)`` or a list
+        of F ``(batch, S_f)`` arrays. With ``action_out`` (a pinned
+        ``(batch, F)`` int32 host tensor) the action is copied into it.
+        Returns ``(qs, q_pi, G, action)`` of this step's buffer set."""
+        i = self._k & 1
+        s = self.sets[i]
+        comp = torch.cuda.current_stream(s.obs.device)
+        parts = list(empirical_prior) if isinstance(empirical_prior, (list, tuple)) else [empirical_prior]
+        parts += list(observations) if isinstance(observations, (list, tuple)) else [observations]
+        dev_parts = [x for x in parts if isinstance(x, torch.Tensor) and x.is_cuda]
+        if dev_parts:
+            self.in_stream.wait_stream(comp)  # device inputs may still be in the making on the compute stream
+            for x in dev_parts:
+                x.record_stream(self.in_stream)  # and their memory stays theirs until the copy has read it
+        with torch.cuda.stream(self.in_stream):
+            self.in_stream.wait_event(self._done[i])  # step k - 2 has read this set's inputs
+            s.load(observations, empirical_prior)
+            self._in_ready[i].record(self.in_stream)
+        comp.wait_event(self._in_ready[i])
+        comp.wait_event(self._out_done[i])  # step k - 2's action has left this set's buffer
+        for g in s.graphs:
             g.replay()
-        return self.qs, self.q_pi, self.G, self.action
+        self._done[i].record(comp)
+        if action_out is not None:
+            with torch.cuda.stream(self.out_stream):
+                self.out_stream.wait_event(self._done[i])
+                action_out.copy_(s.action, non_blocking=True)
+                self._out_done[i].record(self.out_stream)
+        self._k += 1
+        return s.qs, s.q_pi, s.G, s.action
+
+    def drain(self) -> None:
+        comp = torch.cuda.current_stream(self.sets[0].obs.device)
+        comp.wait_stream(self.in_stream)
+        comp.wait_stream(self.out_stream)
+

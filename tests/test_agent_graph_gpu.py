@@ -67,3 +67,50 @@ def test_graphed_step_rejects_stochastic_selection():
     agent = Agent(A, B, C=C, D=D, batch_size=2, action_selection="stochastic")
     with pytest.raises(ValueError, match="deterministic"):
         agent.capture_step()
+
+
+@pytest.mark.parametrize("algo,precision", [("factored", "fp32"), ("dense", "tf32x3")])
+def test_pipelined_steps_equal_eager(algo, precision):
+    """Agent.capture_pipeline alternates two buffer sets with the copies on
+    side streams: every step's qs, q_pi, G and action (also the action copied
+    into pinned host memory) equal the eager step on the same inputs,
+    bitwise, while step k + 1's inputs are copied in during step k."""
+    rng = np.random.default_rng(11)
+    S, O, U, batch = [6, 4, 3], [5, 7, 3], [3, 2, 1], 12
+    A, B, C, D, F = model(rng, S, O, U, batch)
+    agent = Agent(A, B, C=C, D=D, policy_len=2, gamma=16.0, batch_size=batch, num_iter=16, precision=precision,
+                  efe_algorithm=algo)
+    pipe = agent.capture_pipeline(warmup=2)
+    steps = 5
+    obs = [rng.integers(0, np.array(O), size=(batch, len(O))).astype(np.int32) for _ in range(steps)]
+    prior = [[rng.dirichlet(np.ones(s), size=batch).astype(np.float32) for s in S] for _ in range(steps)]
+    want = []
+    for k in range(steps):
+        qs_e = agent.infer_states(torch.as_tensor(obs[k], device="cuda"),
+                                  [torch.as_tensor(p, device="cuda") for p in prior[k]])
+        q_pi_e, G_e = agent.infer_policies(qs_e)
+        want.append(([q.clone() for q in qs_e], q_pi_e.clone(), G_e.clone(), agent.sample_action(q_pi_e).clone()))
+    torch.cuda.synchronize()
+    obs_h = [torch.as_tensor(o).pin_memory() for o in obs]
+    prior_h = [torch.as_tensor(np.concatenate(p, 1)).pin_memory() for p in prior]
+    act_h = [torch.empty((batch, F), dtype=torch.int32).pin_memory() for _ in range(steps)]
+    got = []
+    for k in range(steps):
+        if k == 3:  # device inputs, made on the compute stream just before the step
+            o_in, p_in = obs_h[k].cuda(), prior_h[k].cuda()
+        else:
+            o_in, p_in = obs_h[k], prior_h[k]
+        qs_g, q_pi_g, G_g, act_g = pipe.step(o_in, p_in, act_h[k])
+        # a step's outputs live until step k + 2 overwrites them: copy them out on the compute stream
+        got.append(([q.clone() for q in qs_g], q_pi_g.clone(), G_g.clone(), act_g.clone()))
+    pipe.drain()
+    torch.cuda.synchronize()
+    for k in range(steps):
+        qs_e, q_pi_e, G_e, act_e = want[k]
+        qs_g, q_pi_g, G_g, act_g = got[k]
+        for f in range(F):
+            assert torch.equal(qs_g[f], qs_e[f].reshape(qs_g[f].shape)), f"step {k} factor {f}"
+        assert torch.equal(G_g, G_e), f"step {k}"
+        assert torch.equal(q_pi_g, q_pi_e), f"step {k}"
+        assert torch.equal(act_g, act_e), f"step {k}"
+        assert torch.equal(act_h[k], act_e.cpu()), f"step {k}"
