@@ -52,6 +52,10 @@ def _cols(rng, shape, alpha=0.7):
     dict(S=[3, 2, 4], O=[3, 4, 2], A_deps=[[2, 0], [1], [0, 1, 2]], B_deps=[[0, 2], [1], [2]], T=3, num_iter=4,
          tau=1.0),
     dict(S=[5], O=[3], A_deps=[[0]], B_deps=[[0]], T=1, num_iter=3, tau=0.25),
+    # transition sequences too large to stage in shared memory (read from global memory): single-parent and
+    # multi-parent
+    dict(S=[100], O=[6], A_deps=[[0]], B_deps=[[0]], T=8, num_iter=3, tau=0.5),
+    dict(S=[40, 30], O=[7, 5], A_deps=[[0, 1], [1]], B_deps=[[0, 1], [1]], T=5, num_iter=3, tau=0.5),
 ])
 def test_batched_sequence_inference_matches_oracle(case, kind, distr):
     from pymdp_b200 import seq
