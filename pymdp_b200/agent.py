@@ -527,6 +527,9 @@ class PipelinedAgentStep:
         of F ``(batch, S_f)`` arrays. With ``action_out`` (a pinned
         ``(batch, F)`` int32 host tensor) the action is copied into it.
         Returns ``(qs, q_pi, G, action)`` of this step's buffer set."""
+        if observations is None or empirical_prior is None:
+            # the buffer set was last filled two steps back: there is no previous input to keep
+            raise ValueError("PipelinedAgentStep.step needs both observations and empirical_prior")
         i = self._k & 1
         s = self.sets[i]
         comp = torch.cuda.current_stream(s.obs.device)
