@@ -205,3 +205,15 @@ def test_sample_action_validation():
     assert rc == _lib.B2_ERR_UNSUPPORTED
     rc = lib.b2_sample_action(None, 0x1000, 0x1000, None, 0x1000, 4, 6, 1, 2, 1, 0, 0x1000, 0, 0)
     assert rc == _lib.B2_ERR_INVALID_ARGUMENT
+
+
+def test_pipelined_step_needs_both_inputs():
+    """PipelinedAgentStep alternates two buffer sets: a set's buffers hold the
+    inputs of two steps back, so an omitted input is an error, raised before
+    any device work."""
+    from pymdp_b200.agent import PipelinedAgentStep
+    pipe = PipelinedAgentStep.__new__(PipelinedAgentStep)  # no device: the check comes first
+    with pytest.raises(ValueError, match="both"):
+        pipe.step(None, np.zeros((1, 3), np.float32))
+    with pytest.raises(ValueError, match="both"):
+        pipe.step(np.zeros((1, 2), np.int32), None)
