@@ -16,8 +16,9 @@ infer_policies (neg-EFE of all policies + q_pi) -> sample_action
   policies + action; ``Agent.capture_step``); L2 is flushed (a 256 MiB
   write) between timed steps, outside the per-step event pairs.
 * ``e2e``: the same step through the public API
-  (``Agent.capture_step().step``) with host buffers: pinned observations +
-  priors copied in, actions copied out, inside the timed region.
+  (``Agent.capture_pipeline().step``) with host buffers: every step copies
+  pinned observations + priors in and its actions out, on copy streams
+  beside the neighbouring steps' compute, all inside the timed region.
 * ``roofline``: the dominant launch (the factored neg-EFE + q_pi), its
   algorithmic HBM bytes per agent over its event-timed duration inside the
   timed steps (tensor-pipe FLOPs for ``--efe dense``).
