@@ -217,3 +217,56 @@ def test_pipelined_step_needs_both_inputs():
         pipe.step(None, np.zeros((1, 3), np.float32))
     with pytest.raises(ValueError, match="both"):
         pipe.step(np.zeros((1, 2), np.int32), None)
+
+
+def _seq(S=(3,), O=(2,), A_deps=((0,),), B_deps=((0,),), T=4, Bn=0, num_iter=4, counts=None, index_obs=True):
+    """b2_sequence_infer with host-side arguments only: every case here is
+    decided by the validation before any device work (Bn = 0 or an error)."""
+    lib = _lib.load()
+    i64 = _lib.i64
+    size = lambda d: S[d] if 0 <= d < len(S) else 1  # noqa: E731 (out-of-range deps are the library's to reject)
+    K = [int(np.prod([size(d) for d in deps])) for deps in A_deps]
+    Kb = [int(np.prod([size(d) for d in deps])) for deps in B_deps]
+    c = dict(A=sum(o * k for o, k in zip(O, K)), obs=Bn * T * len(O),
+             B=Bn * sum((T - 1) * s * kb for s, kb in zip(S, Kb)), prior=Bn * sum(S), qs=Bn * T * sum(S))
+    c.update(counts or {})
+    adf = [d for deps in A_deps for d in deps]
+    ado = list(np.cumsum([0] + [len(d) for d in A_deps]))
+    bdf = [d for deps in B_deps for d in deps]
+    bdo = list(np.cumsum([0] + [len(d) for d in B_deps]))
+    dummy = (ctypes.c_int32 * 1)()  # an observation pointer is required; Bn = 0 never reads it
+    obs_idx = ctypes.addressof(dummy) if index_obs else None
+    obs_distr = None if index_obs else ctypes.cast(dummy, ctypes.POINTER(ctypes.c_float))
+    return lib.b2_sequence_infer(None, 0, None, c["A"], 0, i64(list(O)), len(O), obs_idx, obs_distr, c["obs"], None,
+                                 c["B"], None, c["prior"], None, c["qs"], Bn, T, len(S), i64(list(S)), i64(adf),
+                                 len(adf), i64(ado), i64(bdf), len(bdf), i64(bdo), num_iter, 0.5)
+
+
+def test_sequence_empty_batch_is_a_noop():
+    assert _seq() == _lib.B2_OK, _lib.last_error()
+    assert _seq(S=(4, 3), O=(5, 2), A_deps=((0, 1), (1,)), B_deps=((0,), (1, 0)), T=6) == _lib.B2_OK
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(T=0), "invalid T"),
+    (dict(num_iter=-1), "invalid T, num_iter or Bn"),
+    (dict(A_deps=((0, 0),), S=(3,)), "duplicate factor in A_dependencies"),
+    (dict(A_deps=((1,),)), "A dependency out of range"),
+    (dict(B_deps=((2,),)), "B dependency out of range"),
+    (dict(counts={"A": 5}), "A element_count mismatch"),
+    (dict(Bn=2, counts={"obs": 7}), "observation element_count mismatch"),
+    (dict(Bn=2, counts={"B": 1}), "B element_count mismatch"),
+    (dict(Bn=2, counts={"qs": 3}), "prior / qs element_count mismatch"),
+])
+def test_sequence_validation_errors(kw, msg):
+    rc = _seq(**kw)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT, (rc, _lib.last_error())
+    assert msg in _lib.last_error()
+    assert _lib.last_error().startswith("run_mmp:")
+
+
+def test_sequence_window_beyond_shared_memory_is_unsupported():
+    # 8 steps of a 1000-state factor: the FP64 window state alone is about 424 KB
+    rc = _seq(S=(1000,), O=(2,), T=8)
+    assert rc == _lib.B2_ERR_UNSUPPORTED, (rc, _lib.last_error())
+    assert "exceeds 200 KB" in _lib.last_error()
