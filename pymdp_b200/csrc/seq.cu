@@ -19,7 +19,10 @@
 // sequence is staged there too when it fits (VMP: log-clipped FP64; MMP: the
 // FP32 entries themselves, with reciprocal row sums for factor-local
 // transitions), else read from global memory; single-parent transitions take
-// a direct S x S path.
+// a direct S x S path. An iteration is three passes over the window, one
+// thread per (factor, step, state) in factor-major order so that a warp's
+// lanes share a factor: the messages folded into u; each (step, factor)
+// segment's mean, maximum and exponentials; the normaliser, q and log q.
 #include <algorithm>
 #include <string>
 #include <type_traits>
