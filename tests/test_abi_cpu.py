@@ -270,3 +270,69 @@ def test_sequence_window_beyond_shared_memory_is_unsupported():
     rc = _seq(S=(1000,), O=(2,), T=8)
     assert rc == _lib.B2_ERR_UNSUPPORTED, (rc, _lib.last_error())
     assert "exceeds 200 KB" in _lib.last_error()
+
+
+def _expected_state(S=(3, 2), U=(2, 1), B_deps=((0,), (1, 0)), Bn=0, qs_offsets=None, B_offsets=None, counts=None):
+    """b2_expected_state with host-side arguments only (Bn = 0 or an error:
+    nothing reaches the device)."""
+    lib = _lib.load()
+    i64 = _lib.i64
+    K = [int(np.prod([S[d] if 0 <= d < len(S) else 1 for d in deps])) for deps in B_deps]
+    qo = qs_offsets if qs_offsets is not None else list(np.cumsum([0] + list(S)))
+    bo = B_offsets if B_offsets is not None else list(np.cumsum([0] + [s * k * u for s, k, u in zip(S, K, U)]))
+    c = dict(qs=Bn * sum(S), B=Bn * int(bo[-1]), action=Bn * len(S))
+    c.update(counts or {})
+    bdf = [d for deps in B_deps for d in deps]
+    bdo = list(np.cumsum([0] + [len(d) for d in B_deps]))
+    return lib.b2_expected_state(None, None, c["qs"], None, c["B"], None, c["action"], None, Bn, len(S),
+                                 i64(list(S)), i64(list(U)), i64(qo), i64(bo), i64(bdf), len(bdf), i64(bdo))
+
+
+def test_expected_state_empty_batch_is_a_noop():
+    assert _expected_state() == _lib.B2_OK, _lib.last_error()
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(S=(3, 0)), "S and U must lie in [1, 4096]"),
+    (dict(U=(2, 0)), "S and U must lie in [1, 4096]"),
+    (dict(qs_offsets=[0, 3, 4]), "qs_offsets inconsistent with S"),
+    (dict(B_offsets=[0, 18, 31]), "B_offsets inconsistent"),
+    (dict(B_deps=((0,), (2,))), "B dependency out of range"),
+    (dict(Bn=2, counts={"action": 3}), "element counts do not match Bn"),
+    (dict(Bn=-1), "negative Bn"),
+])
+def test_expected_state_validation_errors(kw, msg):
+    rc = _expected_state(**kw)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT, (rc, _lib.last_error())
+    assert msg in _lib.last_error()
+    assert _lib.last_error().startswith("expected_state:")
+
+
+def _multiaction(U=(3, 2), n_unique=6, marginal=1, Bn=0, P=6, T=1, ptrs=False):
+    lib = _lib.load()
+    dummy = (ctypes.c_float * 1)()
+    q = ctypes.cast(dummy, ctypes.POINTER(ctypes.c_float)) if ptrs else None
+    addr = ctypes.addressof(dummy) if ptrs else None
+    return lib.b2_multiaction_probabilities(None, q, addr, addr, n_unique, marginal, Bn, P, T, len(U),
+                                            _lib.i64(list(U)), q)
+
+
+def test_multiaction_empty_batch_is_a_noop():
+    assert _multiaction() == _lib.B2_OK, _lib.last_error()
+    assert _multiaction(marginal=0, n_unique=4) == _lib.B2_OK, _lib.last_error()
+
+
+@pytest.mark.parametrize("kw,rc,msg", [
+    (dict(P=0), "invalid", "invalid sizes"),
+    (dict(n_unique=0), "invalid", "invalid sizes"),
+    (dict(U=(3, 0)), "invalid", "U must be positive"),
+    (dict(n_unique=5), "invalid", "marginal mode writes prod(U) probabilities"),
+    (dict(Bn=1), "invalid", "null buffer"),
+    # marginal mode keeps one FP64 sum per control in shared memory: 7000 controls are 56 KB
+    (dict(U=(7000,), n_unique=7000, Bn=1, ptrs=True), "unsupported", "too many controls"),
+])
+def test_multiaction_validation_errors(kw, rc, msg):
+    want = _lib.B2_ERR_INVALID_ARGUMENT if rc == "invalid" else _lib.B2_ERR_UNSUPPORTED
+    got = _multiaction(**kw)
+    assert got == want, (got, _lib.last_error())
+    assert msg in _lib.last_error()
