@@ -336,3 +336,66 @@ def test_multiaction_validation_errors(kw, rc, msg):
     got = _multiaction(**kw)
     assert got == want, (got, _lib.last_error())
     assert msg in _lib.last_error()
+
+
+@pytest.mark.parametrize("Bn,P,rc,msg", [
+    (0, 8, "ok", ""),
+    (-1, 8, "invalid", "invalid Bn or P"),
+    (2, 0, "invalid", "invalid Bn or P"),
+    (2, 8, "invalid", "null buffer"),
+])
+def test_policy_posterior_validation(Bn, P, rc, msg):
+    got = _lib.load().b2_policy_posterior(None, None, None, 0, None, 0, None, Bn, P)
+    want = _lib.B2_OK if rc == "ok" else _lib.B2_ERR_INVALID_ARGUMENT
+    assert got == want, (got, _lib.last_error())
+    if msg:
+        assert _lib.last_error() == "policy_posterior: " + msg
+
+
+@pytest.mark.parametrize("Bn,P,T,F,rc,msg", [
+    (0, 8, 2, 2, "ok", ""),
+    (2, 8, 0, 2, "invalid", "invalid sizes"),
+    (2, 8, 2, 0, "invalid", "invalid sizes"),
+    (-1, 8, 2, 2, "invalid", "invalid sizes"),
+    (2, 8, 2, 2, "invalid", "null buffer"),
+])
+def test_select_action_validation(Bn, P, T, F, rc, msg):
+    got = _lib.load().b2_select_action(None, None, None, None, Bn, P, T, F)
+    want = _lib.B2_OK if rc == "ok" else _lib.B2_ERR_INVALID_ARGUMENT
+    assert got == want, (got, _lib.last_error())
+    if msg:
+        assert _lib.last_error() == "select_action: " + msg
+
+
+def _fpi_obs(S=(3, 2), O=(4, 5), deps=((0, 1), (1,)), A_offsets=None, batch=0, stride=0, num_iter=16, O_len=None):
+    """b2_fpi_obs (the fused observation form) with host-side arguments only."""
+    lib = _lib.load()
+    i64 = _lib.i64
+    K = [int(np.prod([S[d] if 0 <= d < len(S) else 1 for d in dd])) for dd in deps]
+    ao = A_offsets if A_offsets is not None else list(np.cumsum([0] + [o * k for o, k in zip(O, K)]))
+    df = [d for dd in deps for d in dd]
+    do = list(np.cumsum([0] + [len(dd) for dd in deps]))
+    return lib.b2_fpi_obs(None, None, stride, i64(ao), len(ao), i64(list(O)), len(O) if O_len is None else O_len,
+                          None, None, None, batch, i64(list(S)), len(S), i64(df), len(df), i64(do), len(do), num_iter)
+
+
+def test_fpi_obs_empty_batch_is_a_noop():
+    assert _fpi_obs() == _lib.B2_OK, _lib.last_error()
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(O_len=1), "O / A_offsets sizes inconsistent with M = 2"),
+    (dict(O=(4, 0)), "must be positive"),
+    (dict(A_offsets=[0, 24, 33]), "A_offsets inconsistent with O/deps for modality 1"),
+    (dict(A_offsets=[1, 25, 35]), "A_offsets must start at zero"),
+    (dict(batch=-1), "negative batch"),
+    (dict(stride=10), "A_agent_stride smaller than one agent's A"),
+    (dict(batch=2), "null buffer"),
+    (dict(num_iter=0), "num_iter = 0, must be positive"),
+    (dict(deps=((0, 0), (1,))), "duplicate factor"),
+])
+def test_fpi_obs_validation_errors(kw, msg):
+    rc = _fpi_obs(**kw)
+    assert rc == _lib.B2_ERR_INVALID_ARGUMENT, (rc, _lib.last_error())
+    assert msg in _lib.last_error(), _lib.last_error()
+    assert _lib.last_error().startswith("fpi_obs:")
