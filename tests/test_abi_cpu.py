@@ -399,3 +399,27 @@ def test_fpi_obs_validation_errors(kw, msg):
     assert rc == _lib.B2_ERR_INVALID_ARGUMENT, (rc, _lib.last_error())
     assert msg in _lib.last_error(), _lib.last_error()
     assert _lib.last_error().startswith("fpi_obs:")
+
+
+def _fpi_obs_bwd(batch=0, num_iter=16, O=(4, 5)):
+    """b2_fpi_obs_bwd (the FPI adjoint) with host-side arguments only."""
+    lib = _lib.load()
+    i64 = _lib.i64
+    S, deps = (3, 2), ((0, 1), (1,))
+    K = [6, 2]
+    ao = list(np.cumsum([0] + [o * k for o, k in zip(O, K)]))
+    return lib.b2_fpi_obs_bwd(None, None, 0, i64(ao), len(ao), i64(list(O)), len(O), None, None, None, None, None,
+                              batch, i64(list(S)), len(S), i64([0, 1, 1]), 3, i64([0, 2, 3]), 3, num_iter)
+
+
+def test_fpi_obs_bwd_validation():
+    assert _fpi_obs_bwd() == _lib.B2_OK, _lib.last_error()
+    assert _fpi_obs_bwd(batch=-1) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert _lib.last_error() == "fpi_obs bwd: negative batch"
+    assert _fpi_obs_bwd(batch=3) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert _lib.last_error() == "fpi_obs bwd: null buffer"
+    assert _fpi_obs_bwd(O=(4, 0)) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "must be positive" in _lib.last_error()
+    # the reverse pass keeps every sweep's posterior on chip: 20000 sweeps do not fit
+    assert _fpi_obs_bwd(num_iter=20000) == _lib.B2_ERR_UNSUPPORTED, _lib.last_error()
+    assert "exceeds shared memory" in _lib.last_error()
