@@ -12,9 +12,9 @@ infer_policies (neg-EFE of all policies + q_pi) -> sample_action
 (deterministic). Synthetic seeded inputs with those shapes/distributions.
 
 * ``value``: device time (CUDA events, max over ranks) with every input
-  resident in HBM, the step replayed as CUDA graphs (belief update, then
-  policies + action; ``Agent.capture_step``); L2 is flushed (a 256 MiB
-  write) between timed steps, outside the per-step event pairs.
+  resident in HBM, the whole step replayed as one CUDA graph
+  (``Agent.capture_step``); L2 is flushed (a 256 MiB write) between timed
+  steps, outside the per-step event pairs.
 * ``e2e``: the same step through the public API
   (``Agent.capture_pipeline().step``) with host buffers: every step copies
   pinned observations + priors in and its actions out, on copy streams
@@ -880,39 +880,52 @@ def run_b200(args, rank, world, local_rank):
     barrier()
     per_step_launches = (_lib.launch_count() - n0) // args.steps
     eager_ms = ev0.elapsed_time(ev1) / args.steps
-    # the timed step: the agent step captured as CUDA graphs (belief update |
-    # policies + action) and replayed, inputs resident; events between the two
-    # graphs time the neg-EFE launch for the roofline
+    # the timed step: the whole agent step captured as one CUDA graph and replayed, inputs resident (its launches
+    # chained by programmatic dependent launch throughout). The same step as two graphs (belief update | policies
+    # + action), replayed after the timed steps with an event between them, times the neg-EFE launch for the
+    # roofline.
+    gfull = agent.capture_step(warmup=args.warmup)
     gstep = agent.capture_step(warmup=args.warmup, split=True)
-    gstep.obs.copy_(obs_d)
-    gstep.prior.copy_(torch.cat([p.reshape(n_agents, -1) for p in prior_d], dim=1))
+    flat_prior = torch.cat([p.reshape(n_agents, -1) for p in prior_d], dim=1)
+    for g in (gfull, gstep):
+        g.obs.copy_(obs_d)
+        g.prior.copy_(flat_prior)
+    (g_full,) = gfull.graphs
     g_states, g_policies = gstep.graphs
     for _ in range(args.warmup):
+        gfull.step()
         gstep.step()
     barrier()
-    graph_same = int((gstep.action.cpu().numpy() == chk[3]).all(axis=1).sum())
+    graph_same = int((gfull.action.cpu().numpy() == chk[3]).all(axis=1).sum())
+    split_same = int((gstep.action.cpu().numpy() == chk[3]).all(axis=1).sum())
     evs, efe_ev = [], []
     with ClockSampler(local_rank) as clocks:
         # nvidia-smi answers every 0.2 s or so, far longer than the timed steps take: identical untimed
-        # steps (flush + both graphs) run until the sampler holds three readings under this load (2 s at
+        # steps (flush + the step's graph) run until the sampler holds three readings under this load (2 s at
         # most), and the timed steps follow with no gap
         t_end = time.time() + 2.0
         while len(clocks.rows) < 3 and time.time() < t_end:
             for _ in range(20):
                 flush.zero_()
-                g_states.replay()
-                g_policies.replay()
+                g_full.replay()
             torch.cuda.synchronize()
         barrier()
         for _ in range(args.steps):
             flush.zero_()
-            e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
             e0.record(stream)
+            g_full.replay()
+            e1.record(stream)
+            evs.append((e0, e1))
+        barrier()
+        # the neg-EFE launch alone, for the roofline: same flush, belief update untimed
+        for _ in range(args.steps):
+            flush.zero_()
             g_states.replay()
+            em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(2))
             em.record(stream)
             g_policies.replay()
             e1.record(stream)
-            evs.append((e0, e1))
             efe_ev.append((em, e1))
         barrier()
     launches = args.steps * per_step_launches
@@ -1018,9 +1031,11 @@ def run_b200(args, rank, world, local_rank):
                         "compute (two buffer sets); the region ends after the last action reached host memory",
                 "l2": "not flushed between steps: the model's A (218 MB at 256 agents) exceeds the 126 MB L2"},
         "gpu_launches": int(launches),
-        "step_form": {"timed": "CUDA graph replay (belief update | policies + action)",
+        "step_form": {"timed": "CUDA graph replay (the whole step as one graph; the neg-EFE launch timed on the "
+                               "two-graph form, belief update | policies + action)",
                       "kernels_per_step": per_step_launches, "eager_ms_per_step": eager_ms,
-                      "graph_actions_equal_eager": graph_same, "e2e_actions_equal_eager": e2e_same},
+                      "graph_actions_equal_eager": graph_same, "split_graph_actions_equal_eager": split_same,
+                      "e2e_actions_equal_eager": e2e_same},
         "fused_over_plain": fused_over_plain,
         "plain": plain_res,
         "config1": c1_res,
