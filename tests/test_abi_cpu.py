@@ -423,3 +423,38 @@ def test_fpi_obs_bwd_validation():
     # the reverse pass keeps every sweep's posterior on chip: 20000 sweeps do not fit
     assert _fpi_obs_bwd(num_iter=20000) == _lib.B2_ERR_UNSUPPORTED, _lib.last_error()
     assert "exceeds shared memory" in _lib.last_error()
+
+
+def _trans_joint(Bn=0, T=3, S=(3, 2), U=(2, 1), B_deps=((0,), (1, 0)), counts=None, B_offsets=None):
+    """b2_update_state_transition_from_joint with host-side arguments only."""
+    lib = _lib.load()
+    i64 = _lib.i64
+    K = [int(np.prod([S[d] if 0 <= d < len(S) else 1 for d in deps])) for deps in B_deps]
+    bo = B_offsets if B_offsets is not None else list(np.cumsum([0] + [s * k * u for s, k, u in zip(S, K, U)]))
+    c = dict(B=Bn * int(bo[-1]), joint=Bn * sum((T - 1) * s * k for s, k in zip(S, K)), actions=Bn * (T - 1) * len(S))
+    c.update(counts or {})
+    bdf = [d for deps in B_deps for d in deps]
+    bdo = list(np.cumsum([0] + [len(d) for d in B_deps]))
+    qo = list(np.cumsum([0] + list(S)))
+    return lib.b2_update_state_transition_from_joint(None, None, None, c["B"], None, c["joint"], None, c["actions"],
+                                                     None, 0, None, Bn, T, len(S), i64(list(S)), i64(list(U)),
+                                                     i64(qo), i64(bo), i64(bdf), len(bdf), i64(bdo), -1)
+
+
+def test_transition_from_joint_validation():
+    op = "update_state_transition_from_joint: "
+    assert _trans_joint() == _lib.B2_OK, _lib.last_error()
+    assert _trans_joint(Bn=2, T=1) == _lib.B2_OK, _lib.last_error()  # one step: no transition to learn
+    cases = [
+        (dict(T=0), "invalid sizes"),
+        (dict(U=(2, 0)), "num_controls must be positive"),
+        (dict(B_offsets=[0, 18, 31]), "B_offsets inconsistent with S, U and dependencies"),
+        (dict(Bn=2, counts={"B": 1}), "B_count mismatch"),
+        (dict(Bn=2, counts={"joint": 1}), "joint_count mismatch"),
+        (dict(Bn=2, counts={"actions": 1}), "actions_count mismatch"),
+        (dict(Bn=2), "null buffer"),
+    ]
+    for kw, msg in cases:
+        rc = _trans_joint(**kw)
+        assert rc == _lib.B2_ERR_INVALID_ARGUMENT, (kw, rc, _lib.last_error())
+        assert _lib.last_error().startswith(op + msg), (kw, _lib.last_error())
