@@ -458,3 +458,32 @@ def test_transition_from_joint_validation():
         rc = _trans_joint(**kw)
         assert rc == _lib.B2_ERR_INVALID_ARGUMENT, (kw, rc, _lib.last_error())
         assert _lib.last_error().startswith(op + msg), (kw, _lib.last_error())
+
+
+def _efe_bwd_call(lay, Bn=0, P=3, flags=3, counts=None):
+    """b2_neg_efe_bwd (the neg-EFE adjoint) with host-side arguments only."""
+    lib = _lib.load()
+    c = lay._c
+    cnt = dict(pm=P * lay.T * lay.F, qs=Bn * lay.qs_offsets[-1], A=Bn * lay.A_offsets[-1],
+               B=Bn * lay.B_offsets[-1], C=Bn * lay.C_offsets[-1], dG=Bn * P)
+    cnt.update(counts or {})
+    return lib.b2_neg_efe_bwd(None, None, cnt["pm"], 0, None, cnt["qs"], None, cnt["A"], None, cnt["B"], None,
+                              cnt["C"], None, cnt["dG"], None, None, None, None, Bn, P, lay.T, lay.F, lay.M,
+                              c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[9], len(lay.A_dep_flat), c[10], c[11],
+                              len(lay.B_dep_flat), c[12], flags)
+
+
+def test_neg_efe_bwd_validation():
+    lay = _efe_layout_args()
+    op = "efe_ffi bwd: "
+    assert _efe_bwd_call(lay) == _lib.B2_OK, _lib.last_error()
+    assert _efe_bwd_call(lay, Bn=-1) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert _lib.last_error() == op + "negative Bn"
+    # the adjoint covers the utility and state-information-gain terms only
+    for flag in (_lib.FLAG_USE_PARAM_INFO_GAIN, _lib.FLAG_USE_INDUCTIVE):
+        assert _efe_bwd_call(lay, flags=3 | flag) == _lib.B2_ERR_UNSUPPORTED
+        assert _lib.last_error() == op + "only the utility and state-information-gain terms"
+    assert _efe_bwd_call(lay, Bn=2, counts={"dG": 5}) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert _lib.last_error() == op + "d_neg_efe element_count = 5, expected 6"
+    assert _efe_bwd_call(lay, Bn=2) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert _lib.last_error() == op + "null buffer"
