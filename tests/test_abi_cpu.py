@@ -487,3 +487,30 @@ def test_neg_efe_bwd_validation():
     assert _lib.last_error() == op + "d_neg_efe element_count = 5, expected 6"
     assert _efe_bwd_call(lay, Bn=2) == _lib.B2_ERR_INVALID_ARGUMENT
     assert _lib.last_error() == op + "null buffer"
+
+
+def test_neg_efe_cached_needs_its_cache_and_shares_the_validation():
+    """b2_neg_efe_cached is b2_neg_efe plus a caller-owned operand cache: a
+    missing cache is an error; the rest of the validation and the empty-batch
+    no-op are b2_neg_efe's."""
+    lib = _lib.load()
+    lay = _efe_layout_args()
+    c = lay._c
+    P = 3
+    cache = (ctypes.c_uint8 * 256)()
+    valid = ctypes.c_int32(0)
+
+    def call(Bn, A_count, cache_ptr, valid_ptr):
+        return lib.b2_neg_efe_cached(None, 1, P * lay.T * lay.F, 0, 1, Bn * lay.qs_offsets[-1], 1, A_count, 1,
+                                     Bn * lay.B_offsets[-1], 1, Bn * lay.C_offsets[-1], 1, Bn * lay.I_offsets[-1], 1,
+                                     0, 1, 0, 1, 1, 1, Bn * P, Bn, P, lay.T, lay.F, lay.M, c[0], c[1], c[2], c[3],
+                                     c[4], c[5], c[6], c[7], c[8], c[9], len(lay.A_dep_flat), c[10], c[11],
+                                     len(lay.B_dep_flat), c[12], 3, cache_ptr, 256, valid_ptr)
+
+    assert call(0, 0, None, ctypes.byref(valid)) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "null pack cache" in _lib.last_error()
+    assert call(0, 0, cache, None) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert call(0, 0, cache, ctypes.byref(valid)) == _lib.B2_OK, _lib.last_error()
+    assert valid.value == 0  # nothing packed for an empty batch
+    assert call(0, 5, cache, ctypes.byref(valid)) == _lib.B2_ERR_INVALID_ARGUMENT
+    assert "A element_count = 5, expected 0" in _lib.last_error()
