@@ -36,6 +36,12 @@ CASES = {
     "seq_mmp_index": ("mmp", [4, 3, 2], [5, 2], [[0, 2], [1]], [[0], [1], [2, 0]], 4, 6, 0.5, False),
     "seq_vmp": ("vmp", [3, 2], [4, 3], [[0, 1], [1]], [[0], [1, 0]], 5, 8, 0.25, True),
     "seq_vmp_index": ("vmp", [4, 3, 2], [5, 2], [[0, 2], [1]], [[0], [1], [2, 0]], 4, 6, 0.5, False),
+    # the benchmark's window: 8 steps, S = [16, 8], both modalities on both factors, factor-local transitions
+    "seq_mmp_bench": ("mmp", [16, 8], [16, 8], [[0, 1], [0, 1]], [[0], [1]], 8, 16, 0.25, False),
+    "seq_vmp_bench": ("vmp", [16, 8], [16, 8], [[0, 1], [0, 1]], [[0], [1]], 8, 16, 0.25, False),
+    # a modality on three factors, and a single-step window (no transition at all)
+    "seq_mmp_rank3": ("mmp", [3, 4, 2], [5, 3], [[2, 0, 1], [1]], [[0, 1], [1], [2]], 4, 6, 0.5, True),
+    "seq_vmp_t1": ("vmp", [5, 3], [4, 6], [[0], [0, 1]], [[0], [1]], 1, 5, 1.0, False),
 }
 
 
@@ -62,15 +68,18 @@ def make_case(ref, cfg, seed):
     return out
 
 
-def main(ref_root):
+def main(ref_root, names=None):
+    """Write every case, or only ``names`` (each case keeps its seed, 500 + its position in CASES)."""
     sys.path.insert(0, HERE)
     import refshim
 
     ref = refshim.load_reference(ref_root, modules=("utils", "maths", "algos"))
     for i, (name, cfg) in enumerate(CASES.items()):
+        if names and name not in names:
+            continue
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **make_case(ref, cfg, 500 + i))
         print("wrote", name)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2:] or None)

@@ -26,7 +26,8 @@ def cuda(x, dtype=torch.float32):
     return torch.as_tensor(np.asarray(x), device="cuda").to(dtype)
 
 
-@pytest.mark.parametrize("name", ["seq_mmp", "seq_mmp_index", "seq_vmp", "seq_vmp_index"])
+@pytest.mark.parametrize("name", ["seq_mmp", "seq_mmp_index", "seq_vmp", "seq_vmp_index", "seq_mmp_bench",
+                                  "seq_vmp_bench", "seq_mmp_rank3", "seq_vmp_t1"])
 def test_sequence_inference_matches_reference(name):
     from pymdp_b200 import seq
     d = load_golden(name)

@@ -17,7 +17,8 @@ def _deps(d, key):
     return out
 
 
-@pytest.mark.parametrize("name", ["seq_mmp", "seq_mmp_index", "seq_vmp", "seq_vmp_index"])
+@pytest.mark.parametrize("name", ["seq_mmp", "seq_mmp_index", "seq_vmp", "seq_vmp_index", "seq_mmp_bench",
+                                  "seq_vmp_bench", "seq_mmp_rank3", "seq_vmp_t1"])
 def test_oracle_matches_reference_fixture(name):
     d = load_golden(name)
     qs = mmp.run_sequence(str(d["kind"]), unpack(d, "A"), unpack(d, "B"), unpack(d, "obs"), unpack(d, "prior"),
